@@ -1,0 +1,150 @@
+"""ctypes mirror of the reference ABI structs (include/fire_cuda.h).
+
+Field order, types and defaults follow src/fire_cuda.h:5-100 of native-firesim,
+so a FireSettings built here has the byte layout the reference's callers pass.
+"""
+from __future__ import annotations
+
+import ctypes
+
+# Field ids shared by every copy/compare entry point (FIRE_FIELD_* in include/fire_ext.h).
+FIELDS = {
+    "heat": 0, "fuel": 1, "oxygen": 2, "soot": 3, "char": 4, "ash": 5, "pyrolysis": 6,
+    "progress": 7, "turbulence_energy": 8, "soot_optics": 9, "pressure": 10, "divergence": 11,
+    "u": 12, "v": 13, "w": 14, "scene_light": 15, "scene_shadow": 16, "hdr": 17, "bgra": 18,
+    "divergence_after": 19,
+}
+SCALAR_FIELDS = ["heat", "fuel", "oxygen", "soot", "char", "ash", "pyrolysis", "progress",
+                 "turbulence_energy", "soot_optics"]
+
+# Stage ids (FIRE_STAGE_* in include/fire_ext.h), in step order.
+STAGES = {
+    "advect_velocity": 0, "advect_react": 1, "force": 2, "velocity_boundary": 3, "divergence": 4,
+    "pressure_sor": 5, "subtract": 6, "wall_boundary": 7, "light_build": 8, "light_propagate": 9,
+    "render": 10, "embers": 11, "tonemap": 12, "overlay": 13, "metrics": 14, "reset": 15,
+}
+
+
+class FireCudaDiagnostics(ctypes.Structure):
+    _fields_ = [
+        ("driverVersion", ctypes.c_int), ("runtimeVersion", ctypes.c_int), ("deviceCount", ctypes.c_int),
+        ("activeDevice", ctypes.c_int), ("computeMajor", ctypes.c_int), ("computeMinor", ctypes.c_int),
+        ("totalGlobalMem", ctypes.c_uint64), ("deviceName", ctypes.c_char * 128),
+    ]
+
+    def __init__(self):
+        super().__init__()
+        self.activeDevice = -1
+
+
+_METRIC_INTS = ["frameIndex", "gridX", "gridY", "gridZ", "pressureIterations", "invalidCells"]
+_METRIC_FLOATS = [
+    "timeSeconds", "gpuSolveMs", "gpuRenderMs", "gpuVelocityMs", "gpuReactionMs", "gpuProjectionMs",
+    "gpuLightingMs", "gpuRaymarchMs", "gpuPackMs", "heatSum", "fuelSum", "oxygenSum", "sootSum", "charSum",
+    "ashSum", "pyrolysisSum", "progressSum", "turbulenceEnergySum", "sootOpticalDepthSum", "maxHeat",
+    "maxFuel", "maxSoot", "maxPyrolysis", "maxProgress", "maxTurbulenceEnergy", "flameHeightMeters",
+    "meanOpticalDepth", "meanSceneLight", "meanSceneShadow", "flameMassProxy", "smokeMassProxy",
+    "flameSmokeOverlapProxy", "meanVolumetricShadow", "meanRoomIrradiance", "heatReleaseProxy",
+    "divergenceBeforeL2", "divergenceBeforeMax", "divergenceAfterL2", "divergenceAfterMax",
+    "divergenceReduction",
+]
+
+
+class FireCudaFrameMetrics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in _METRIC_INTS] + [(n, ctypes.c_float) for n in _METRIC_FLOATS]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class FireSettings(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("dt", ctypes.c_float),
+        ("mouseX", ctypes.c_float), ("mouseY", ctypes.c_float), ("leftDown", ctypes.c_int),
+        ("rightDown", ctypes.c_int), ("reset", ctypes.c_int), ("showGizmos", ctypes.c_int),
+        ("activeGizmo", ctypes.c_int), ("sceneId", ctypes.c_int), ("wind", ctypes.c_float),
+        ("turbulence", ctypes.c_float), ("detail", ctypes.c_float), ("smoke", ctypes.c_float),
+        ("intensity", ctypes.c_float), ("cameraYaw", ctypes.c_float), ("cameraPitch", ctypes.c_float),
+        ("cameraDistance", ctypes.c_float), ("cinematicMode", ctypes.c_int), ("raymarchSteps", ctypes.c_int),
+        ("emberCount", ctypes.c_int), ("renderDebugMode", ctypes.c_int), ("exposure", ctypes.c_float),
+        ("reflectionGain", ctypes.c_float), ("smokeDarkness", ctypes.c_float),
+        ("emitterCenterX", ctypes.c_float), ("emitterCenterZ", ctypes.c_float),
+        ("emitterHeightNorm", ctypes.c_float), ("emitterHeightBandNorm", ctypes.c_float),
+        ("emitterRadius", ctypes.c_float), ("burnerCenterCount", ctypes.c_int),
+        ("burnerCenterX", ctypes.c_float * 4), ("burnerCenterY", ctypes.c_float * 4),
+        ("burnerCenterZ", ctypes.c_float * 4),
+    ]
+
+    # src/fire_cuda.h:64-100 defaults.
+    _DEFAULTS = dict(
+        width=1280, height=720, dt=1.0 / 60.0, mouseX=0.5, mouseY=0.12, leftDown=0, rightDown=0, reset=0,
+        showGizmos=1, activeGizmo=1, sceneId=0, wind=0.0, turbulence=0.72, detail=0.88, smoke=0.92,
+        intensity=1.0, cameraYaw=0.0, cameraPitch=0.18, cameraDistance=3.35, cinematicMode=0,
+        raymarchSteps=56, emberCount=96, renderDebugMode=0, exposure=1.0, reflectionGain=1.0,
+        smokeDarkness=1.0, emitterCenterX=0.0, emitterCenterZ=0.0, emitterHeightNorm=0.0,
+        emitterHeightBandNorm=0.06, emitterRadius=0.48, burnerCenterCount=0,
+    )
+
+    def __init__(self, **kw):
+        super().__init__()
+        for k, v in {**self._DEFAULTS, **kw}.items():
+            if k.startswith("burnerCenter") and k != "burnerCenterCount":
+                arr = getattr(self, k)
+                for i, x in enumerate(v):
+                    arr[i] = x
+            else:
+                setattr(self, k, v)
+
+    def as_dict(self) -> dict:
+        out = {}
+        for n, _ in self._fields_:
+            v = getattr(self, n)
+            out[n] = list(v) if n.startswith("burnerCenter") and n != "burnerCenterCount" else v
+        return out
+
+
+def f32(x: float) -> float:
+    """Round a Python float to the nearest binary32 value."""
+    return ctypes.c_float(x).value
+
+
+# Canonical host constants, src/main.cpp:33-43, applied by applyCanonicalFireSettings (src/main.cpp:2758-2770).
+CANONICAL = dict(cinematicMode=1, raymarchSteps=104, emberCount=176, exposure=0.84, reflectionGain=0.54,
+                 smokeDarkness=1.26, intensity=1.42, smoke=0.96, turbulence=1.34, renderDebugMode=0)
+
+
+def validation_settings(frame: int, scene: int = 0, width: int = 960, height: int = 540,
+                        pool_fire: bool = False) -> FireSettings:
+    """FireSettings of frame `frame` of the reference's validation harness.
+
+    Restates src/main.cpp:4284-4311 (runValidation): deterministic mouse/wind
+    motion, canonical constants, then the validation floors for turbulence,
+    smoke and intensity and the fixed validation camera.  Scene emitter
+    parameters are the built-in defaults of SceneEmitterParams
+    (src/main.cpp:173, used when no scene contract is loaded).
+    """
+    import numpy as np
+    f = np.float32
+    s = FireSettings(width=width, height=height, dt=1.0 / 60.0)
+    if pool_fire:
+        s.mouseX, s.mouseY = 0.50, 0.12
+    else:
+        s.mouseX = float(f(0.50) + f(0.07) * np.sin(f(frame) * f(0.071)))
+        s.mouseY = float(f(0.12) + f(0.035) * np.sin(f(frame) * f(0.053)))
+    s.leftDown = 0
+    s.rightDown = 0
+    s.showGizmos = 0
+    s.activeGizmo = 1
+    s.sceneId = scene
+    s.reset = 1 if frame == 0 else 0
+    s.wind = 0.0 if pool_fire else float(f(0.10) + f(0.05) * np.sin(f(frame) * f(0.037)))
+    s.detail = 0.98
+    for k, v in CANONICAL.items():
+        setattr(s, k, v)
+    s.turbulence = max(s.turbulence, f32(1.08))
+    s.smoke = max(s.smoke, f32(1.02))
+    s.intensity = max(s.intensity, f32(1.18))
+    s.cameraYaw = 0.18
+    s.cameraPitch = 0.08
+    s.cameraDistance = 2.62
+    return s
