@@ -1,0 +1,395 @@
+"""Benchmark of the firesim-b200 frame pipeline (one JSON line on rank 0).
+
+Workload: the reference's per-frame pipeline (native-firesim's physics, its
+ten transported scalars on a MAC grid) on a 128x128x128 grid in FP32, with the
+128^3 configuration's solver and render cadence: 60 red-black SOR iterations
+at omega 1.8, and one 512x512 HDR raymarch every 10 steps (128 primary samples
+requested; the reference ABI clamps them to 120).  Settings are the
+reference's validation-harness frames (scene 0, canonical constants), the
+scene is reset on the first warm-up step, and the fire develops during the
+timed steps.  A "step" is one call of the reference ABI: fireCudaStepD3D11,
+or fireCudaStepAndRenderD3D11 on every 10th step (render into a device HDR
+buffer).
+
+value  : voxel-steps/s over all ranks, device-timed with CUDA events on the
+         scene's own stream, inputs resident in HBM (the per-step state,
+         ~270 MB at 128^3, exceeds the 126 MB L2).
+e2e    : the same metric through the host path: fireCudaStepD3D11 and, every
+         10th step, fireCudaStepAndRender with a host BGRA8 buffer (the frame
+         is copied to the host inside the timed region), wall-clock timed.
+N > 1  : replicas only -- every rank steps its own scene on its own GPU; the
+         ranks meet only at the barriers and the max-reduction of the timings.
+
+--impl reference times the CPU restatement of the reference's step
+(OpenMP, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_package():
+    if "firesim_b200" in sys.modules:
+        return sys.modules["firesim_b200"]
+    pkg_dir = ROOT / "native-firesim_b200"
+    spec = importlib.util.spec_from_file_location("firesim_b200", pkg_dir / "__init__.py",
+                                                  submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["firesim_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self._thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._thread = threading.Thread(target=self._read, daemon=True)
+            self._thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if os.environ.get("FIRESIM_BENCH_BACKEND", "nccl") == "nccl" else "gloo",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def workload_settings(abi, frame: int, args) -> object:
+    s = abi.validation_settings(frame, scene=0, width=args.frame, height=args.frame)
+    s.raymarchSteps = args.samples
+    s.reset = 1 if frame == 0 else 0
+    return s
+
+
+# Algorithmic bytes per cell of each timed stage (FP32 layout of this library):
+# scalars 40 B/cell packed, three face grids ~12 B/cell, p/div 4 B each.
+STAGE_BYTES_PER_CELL = {
+    "advect_velocity": 24.0,          # read 3 faces + write 3 faces (velocity gathers hit L1/L2)
+    "advect_react": 40.0 * 2 + 12.0,  # read + write the 10 scalars, read the 3 faces
+    "force_project": 16.0 + 12.0 * 2 + 16.0 + 8.0,  # read heat/soot/k/progress, read+write faces, force scratch w+r, div+p
+    "pressure_sor": 6.0,              # per half-sweep: 12 B/cell per iteration (read p, write p, read div)
+    "subtract_walls": 4.0 + 24.0,     # read p, read+write faces
+    "light": 0.0,                     # quarter-resolution grid, small
+}
+
+
+def stage_timings(pkg, sim, args, settings, iters: int = 3) -> dict:
+    """Average device time of each stage range, from CUDA events on the scene stream."""
+    import torch
+    ext = torch.cuda.ExternalStream(sim.stream())
+    ranges = {
+        "advect_velocity": ("advect_velocity", "advect_velocity"),
+        "advect_react": ("advect_react", "advect_react"),
+        "force_project": ("force", "divergence"),
+        "pressure_sor": ("pressure_sor", "pressure_sor"),
+        "subtract_walls": ("subtract", "wall_boundary"),
+        "light": ("light_build", "light_propagate"),
+        "render": ("render", "render"),
+        "embers": ("embers", "embers"),
+    }
+    t_sim, t_render, _ = sim.times()
+    out = {}
+    for name, (a, b) in ranges.items():
+        ms = []
+        for _ in range(iters):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            sim.stages(a, b, settings, t_render if name in ("render", "embers") else t_sim)
+            e1.record(ext)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        out[name] = min(ms)
+    return out
+
+
+def cpu_baseline(pkg, args, n_sim_steps: int = 2) -> dict:
+    """The CPU restatement (OpenMP, all host threads) on a bounded sample of the workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as om  # noqa: PLC0415
+    abi = pkg.abi
+    o = om.OracleFire(abi, args.frame, args.frame, args.grid, args.grid, args.grid)
+    o.set_pressure_solver(args.sor_iters, args.omega)
+    threads = os.cpu_count() or 1
+    om.OracleFire.set_threads(threads)
+    o.step(workload_settings(abi, 0, args), mode=2)  # reset + first step (warm-up)
+    t0 = time.perf_counter()
+    for f in range(1, 1 + n_sim_steps):
+        o.step(workload_settings(abi, f, args), mode=2)
+    t_sim = (time.perf_counter() - t0) / n_sim_steps
+    t1 = time.perf_counter()
+    o.step(workload_settings(abi, 1 + n_sim_steps, args), mode=3)
+    t_render = time.perf_counter() - t1
+    per_step = t_sim + t_render / args.render_every
+    cells = args.grid ** 3
+    return {"value": cells / per_step, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n_sim_steps} simulation steps of the {args.grid}^3 workload after a reset step, plus one "
+                      f"{args.frame}^2 render amortised over {args.render_every} steps",
+            "seconds_per_step": per_step}
+
+
+def run_reference(args, world: int, rank: int) -> None:
+    if rank != 0:
+        return
+    pkg = load_package()
+    steps = min(args.steps, args.reference_steps)
+    cb = cpu_baseline(pkg, args, n_sim_steps=steps)
+    line = {
+        "impl": "reference", "metric": "voxel-steps/s", "value": cb["value"], "unit": "voxel-steps/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": cb["seconds_per_step"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_block(args),
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args) -> dict:
+    return {"workload": f"reference frame pipeline (native-firesim physics, 10 scalars, MAC velocity), FP32, "
+                        f"{args.grid}^3 grid, SOR {args.sor_iters} iterations omega {args.omega}, "
+                        f"{args.frame}x{args.frame} HDR raymarch every {args.render_every} steps "
+                        f"({args.samples} samples requested, clamped to 120)",
+            "grid": [args.grid] * 3, "frame": [args.frame, args.frame], "sor_iterations": args.sor_iters,
+            "omega": args.omega, "render_every": args.render_every, "settings": "validation harness frames, scene 0",
+            "l2": "per-step state (~270 MB at 128^3) exceeds the 126 MB L2; no flush", "parallelism": "replicas"}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--frame", type=int, default=512)
+    ap.add_argument("--sor-iters", type=int, default=60)
+    ap.add_argument("--omega", type=float, default=1.8)
+    ap.add_argument("--render-every", type=int, default=10)
+    ap.add_argument("--samples", type=int, default=128)
+    ap.add_argument("--reference-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        dist_barrier(world)
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    abi = pkg.abi
+    lib = pkg.load_library()
+    if not lib.fireCudaSelectDevice(local):
+        raise RuntimeError(pkg.firesim.last_error())
+    sim = pkg.FireSim(args.frame, args.frame, args.grid, args.grid, args.grid)
+    sim.set_pressure_solver(args.sor_iters, args.omega)
+    hdr = torch.zeros((args.frame, args.frame, 4), dtype=torch.float32, device="cuda")
+    sim.register_hdr_slot(0, hdr.data_ptr(), args.frame * 16, 0)
+    sim.set_hdr_slot(0)
+    ext = torch.cuda.ExternalStream(sim.stream())
+    frame = 0
+
+    def one_step(host_bgra=None):
+        nonlocal frame
+        s = workload_settings(abi, frame, args)
+        render = (frame % args.render_every) == args.render_every - 1
+        if host_bgra is not None and render:
+            ok = lib.fireCudaStepAndRender(host_bgra.ctypes.data, s)
+            if not ok:
+                raise RuntimeError(pkg.firesim.last_error())
+        elif render:
+            sim.step_and_render_hdr(s)
+        else:
+            sim.step(s)
+        frame += 1
+
+    for _ in range(args.warmup):
+        one_step()
+    sim.synchronize()
+
+    # Device-timed region.
+    sampler = ClockSampler(local)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = sim.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(args.steps):
+        one_step()
+    e1.record(ext)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clocks = sampler.stop()
+    launches = sim.launch_count() - launches0
+    device_s = dist_max(e0.elapsed_time(e1) / 1e3, world)
+    cells = args.grid ** 3
+    value = cells * args.steps * world / device_s
+
+    # End-to-end through the host path.
+    e2e = None
+    if not args.no_e2e:
+        host = np.zeros((args.frame, args.frame), dtype=np.uint32)
+        dist_barrier(world)
+        sim.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            one_step(host_bgra=host)
+        sim.synchronize()
+        wall = dist_max(time.perf_counter() - t0, world)
+        renders = sum(1 for f in range(frame - args.steps, frame) if f % args.render_every == args.render_every - 1)
+        e2e = {"value": cells * args.steps * world / wall, "unit": "voxel-steps/s",
+               "h2d_bytes_per_step": int(ctypes_sizeof_settings(abi)),
+               "d2h_bytes_per_step": int(renders * args.frame * args.frame * 4 / args.steps),
+               "ms_per_step": wall * 1e3 / args.steps}
+
+    # Per-stage device times and the roofline of the dominant kernel.
+    s = workload_settings(abi, frame, args)
+    st = stage_timings(pkg, sim, args, s)
+    per_step_ms = {k: (v / args.render_every if k in ("render", "embers") else v) for k, v in st.items()}
+    dominant = max(per_step_ms, key=per_step_ms.get)
+    peaks, peak_src = measured_peaks()
+    roofline = roofline_block(dominant, st, args, cells, peaks, peak_src)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(pkg, args)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": device_s * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural fuel bed + validation-harness settings)",
+            "config": config_block(args), "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "roofline": roofline, "stage_ms": per_step_ms, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_sizeof_settings(abi) -> int:
+    import ctypes
+    return ctypes.sizeof(abi.FireSettings)
+
+
+def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str) -> dict:
+    """achieved = algorithmic bytes of one launch / that launch's average device time."""
+    if dominant == "pressure_sor":
+        launches = 2 * args.sor_iters
+        per_launch_ms = st["pressure_sor"] / launches
+        bytes_per_launch = STAGE_BYTES_PER_CELL["pressure_sor"] * cells
+    elif dominant in STAGE_BYTES_PER_CELL and STAGE_BYTES_PER_CELL[dominant] > 0:
+        per_launch_ms = st[dominant]
+        bytes_per_launch = STAGE_BYTES_PER_CELL[dominant] * cells
+    else:
+        # render: compulsory bytes = one read of the fields the rays touch + 16 B/pixel; report against HBM too.
+        per_launch_ms = st[dominant]
+        bytes_per_launch = 40.0 * cells + 16.0 * args.frame * args.frame
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    return {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+            "bytes_per_launch": bytes_per_launch, "launch_ms": per_launch_ms}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

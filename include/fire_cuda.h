@@ -20,6 +20,13 @@
 
 #include <stdint.h>
 
+/* Exported symbols of libfiresim_b200.so (built with hidden default visibility). */
+#if defined(__GNUC__)
+#define FIRE_API __attribute__((visibility("default")))
+#else
+#define FIRE_API
+#endif
+
 #ifdef __cplusplus
 #define FIRE_DEFAULT(v) = v
 #define FIRE_DEFAULT_ARRAY = {}
@@ -140,33 +147,33 @@ typedef struct FireSettings {
 /* src/fire_cuda.h:102 -- grid derived from the request exactly as the reference
  * does (src/fire_cuda.cu:2916-2922); fireCudaInitializeGrid in fire_ext.h takes
  * explicit dimensions. */
-bool fireCudaInitialize(int frameWidth, int frameHeight, int gridWidth, int gridHeight);
+FIRE_API bool fireCudaInitialize(int frameWidth, int frameHeight, int gridWidth, int gridHeight);
 /* src/fire_cuda.h:103 -- one step + render; writes W*H BGRA8 pixels to host memory, synchronous. */
-bool fireCudaStepAndRender(uint32_t* bgraPixels, FIRE_SETTINGS_ARG settings);
+FIRE_API bool fireCudaStepAndRender(uint32_t* bgraPixels, FIRE_SETTINGS_ARG settings);
 /* src/fire_cuda.h:104 -- as above plus FireCudaFrameMetrics (FP64 sums, divergence norms, pass timings). */
-bool fireCudaStepAndRenderMeasured(uint32_t* bgraPixels, FIRE_SETTINGS_ARG settings, FireCudaFrameMetrics* metrics);
+FIRE_API bool fireCudaStepAndRenderMeasured(uint32_t* bgraPixels, FIRE_SETTINGS_ARG settings, FireCudaFrameMetrics* metrics);
 /* src/fire_cuda.h:105 -- headless: returns false ("D3D11 unavailable on headless build"). */
-bool fireCudaSelectDeviceForD3D11(void* d3d11Device);
+FIRE_API bool fireCudaSelectDeviceForD3D11(void* d3d11Device);
 /* src/fire_cuda.h:106-107 -- headless: returns false; use fireCudaRegisterHdrBufferSlot. */
-bool fireCudaRegisterD3D11Texture(void* d3d11Texture);
-bool fireCudaRegisterD3D11TextureSlot(int slot, void* d3d11Texture);
+FIRE_API bool fireCudaRegisterD3D11Texture(void* d3d11Texture);
+FIRE_API bool fireCudaRegisterD3D11TextureSlot(int slot, void* d3d11Texture);
 /* src/fire_cuda.h:108 -- selects which registered HDR buffer slot the *D3D11 paths write. */
-bool fireCudaSetD3D11TextureSlot(int slot);
+FIRE_API bool fireCudaSetD3D11TextureSlot(int slot);
 /* src/fire_cuda.h:109 -- step only (no render), asynchronous until fireCudaSynchronize. */
-bool fireCudaStepD3D11(FIRE_SETTINGS_ARG settings);
+FIRE_API bool fireCudaStepD3D11(FIRE_SETTINGS_ARG settings);
 /* src/fire_cuda.h:110-111 -- step + render into the active HDR buffer slot (float4 per pixel). */
-bool fireCudaStepAndRenderD3D11(FIRE_SETTINGS_ARG settings);
-bool fireCudaStepAndRenderD3D11Measured(FIRE_SETTINGS_ARG settings, FireCudaFrameMetrics* metrics);
+FIRE_API bool fireCudaStepAndRenderD3D11(FIRE_SETTINGS_ARG settings);
+FIRE_API bool fireCudaStepAndRenderD3D11Measured(FIRE_SETTINGS_ARG settings, FireCudaFrameMetrics* metrics);
 /* src/fire_cuda.h:112 -- render only (advances render time, not simulation time). */
-bool fireCudaRenderD3D11(FIRE_SETTINGS_ARG settings);
+FIRE_API bool fireCudaRenderD3D11(FIRE_SETTINGS_ARG settings);
 /* src/fire_cuda.h:113 -- forgets every registered HDR buffer slot. */
-void fireCudaUnregisterD3D11Texture(void);
+FIRE_API void fireCudaUnregisterD3D11Texture(void);
 /* src/fire_cuda.h:114-118 */
-bool fireCudaSynchronize(void);
-bool fireCudaReset(void);
-bool fireCudaGetDiagnostics(FireCudaDiagnostics* diagnostics);
-void fireCudaShutdown(void);
-const char* fireCudaLastError(void);
+FIRE_API bool fireCudaSynchronize(void);
+FIRE_API bool fireCudaReset(void);
+FIRE_API bool fireCudaGetDiagnostics(FireCudaDiagnostics* diagnostics);
+FIRE_API void fireCudaShutdown(void);
+FIRE_API const char* fireCudaLastError(void);
 
 #ifdef __cplusplus
 }

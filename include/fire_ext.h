@@ -1,0 +1,123 @@
+/*
+ * fire_ext.h -- extensions of the fire_cuda.h ABI (C linkage, plain pointers and sizes).
+ *
+ * None of these entry points exists in native-firesim; they cover what its
+ * ABI cannot express on a headless Linux box (see each comment).  They act on
+ * the same singleton scene as fire_cuda.h ("scene 0"), except the fireScene*
+ * family, which manages independent scenes by handle.  Every function returns
+ * false (or NULL) on error and sets fireCudaLastError().
+ */
+#pragma once
+
+#include <stddef.h>
+
+#include "fire_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Field ids for fireCudaGetField / fireCudaSetField.  Scalars and the pressure
+ * and divergence fields hold nx*ny*nz floats (x fastest); the MAC faces hold
+ * (nx+1)*ny*nz, nx*(ny+1)*nz and nx*ny*(nz+1) floats; SCENE_LIGHT holds four
+ * floats per light cell (radiance RGB, extinction); HDR four floats per pixel;
+ * BGRA one uint32 per pixel. */
+enum FireFieldId {
+    FIRE_FIELD_HEAT = 0,
+    FIRE_FIELD_FUEL = 1,
+    FIRE_FIELD_OXYGEN = 2,
+    FIRE_FIELD_SOOT = 3,
+    FIRE_FIELD_CHAR = 4,
+    FIRE_FIELD_ASH = 5,
+    FIRE_FIELD_PYROLYSIS = 6,
+    FIRE_FIELD_PROGRESS = 7,
+    FIRE_FIELD_TURBULENCE_ENERGY = 8,
+    FIRE_FIELD_SOOT_OPTICS = 9,
+    FIRE_FIELD_PRESSURE = 10,
+    FIRE_FIELD_DIVERGENCE = 11,
+    FIRE_FIELD_U = 12,
+    FIRE_FIELD_V = 13,
+    FIRE_FIELD_W = 14,
+    FIRE_FIELD_SCENE_LIGHT = 15,
+    FIRE_FIELD_SCENE_SHADOW = 16,
+    FIRE_FIELD_HDR = 17,
+    FIRE_FIELD_BGRA = 18,
+    FIRE_FIELD_DIVERGENCE_AFTER = 19
+};
+
+/* The passes of one frame, in order (the launch sequence of
+ * stepAndRenderInternal, src/fire_cuda.cu:3196-3471). */
+enum FireStageId {
+    FIRE_STAGE_ADVECT_VELOCITY = 0,
+    FIRE_STAGE_ADVECT_REACT = 1,
+    FIRE_STAGE_FORCE = 2,
+    FIRE_STAGE_VELOCITY_BOUNDARY = 3,
+    FIRE_STAGE_DIVERGENCE = 4,
+    FIRE_STAGE_PRESSURE_SOR = 5,
+    FIRE_STAGE_SUBTRACT = 6,
+    FIRE_STAGE_WALL_BOUNDARY = 7,
+    FIRE_STAGE_LIGHT_BUILD = 8,
+    FIRE_STAGE_LIGHT_PROPAGATE = 9,
+    FIRE_STAGE_RENDER = 10,
+    FIRE_STAGE_EMBERS = 11,
+    FIRE_STAGE_TONEMAP = 12,
+    FIRE_STAGE_OVERLAY = 13,
+    FIRE_STAGE_METRICS = 14,
+    FIRE_STAGE_RESET = 15
+};
+
+enum FireHdrFormat {
+    FIRE_HDR_RGBA32F = 0, /* float4 per pixel */
+    FIRE_HDR_RGBA16F = 1  /* half4 per pixel, negatives clamped to 0 (as packFp16SurfaceKernel) */
+};
+
+/* Grid-explicit initialisation: fireCudaInitialize derives the grid from a
+ * window request and clamps it to nx>=72 (src/fire_cuda.cu:2916-2922), so it
+ * cannot express 64^3, 128^3 or 256^3.  The light grid follows the reference's
+ * rule (ceil(n/4) clamped to [18,48] x [20,56] x [16,36]). */
+FIRE_API bool fireCudaInitializeGrid(int frameWidth, int frameHeight, int nx, int ny, int nz);
+
+/* Headless stand-in for fireCudaSelectDeviceForD3D11: picks the CUDA device by
+ * ordinal for the next initialisation. */
+FIRE_API bool fireCudaSelectDevice(int device);
+
+/* Registers a caller-owned device buffer (frameWidth x frameHeight pixels,
+ * pitchBytes per row, FireHdrFormat) as HDR output slot 0..3: the headless form
+ * of fireCudaRegisterD3D11TextureSlot.  The *D3D11 entry points write the
+ * active slot (fireCudaSetD3D11TextureSlot). */
+FIRE_API bool fireCudaRegisterHdrBufferSlot(int slot, void* devicePtr, size_t pitchBytes, int format);
+
+/* Pressure-solver policy: SOR iterations and over-relaxation factor
+ * (the reference hard-codes 40 and 1.52, src/fire_cuda.cu:104-105). */
+FIRE_API bool fireCudaSetPressureSolver(int iterations, float omega);
+
+/* nx, ny, nz, lightNx, lightNy, lightNz, frameWidth, frameHeight. */
+FIRE_API bool fireCudaGetGridInfo(int* dims8);
+
+/* Copies one field between host memory and the scene (bytes must match). */
+FIRE_API bool fireCudaGetField(int field, void* host, size_t bytes);
+FIRE_API bool fireCudaSetField(int field, const void* host, size_t bytes);
+
+/* Runs stages [first, last] on the current fields at an explicit simulation
+ * time, with the settings clamped as in a step (src/fire_cuda.cu:3135-3179).
+ * The clocks are not advanced. */
+FIRE_API bool fireCudaRunStages(int first, int last, const FireSettings* settings, float time);
+
+/* Simulation clock, render clock and frame index of the singleton scene. */
+FIRE_API bool fireCudaGetTimes(float* simTime, float* renderTime, int* frameIndex);
+FIRE_API bool fireCudaSetTimes(float simTime, float renderTime, int frameIndex);
+
+/* The CUDA stream (cudaStream_t) the singleton scene launches on, so callers can
+ * order their own work or record events against it. */
+FIRE_API bool fireCudaGetStream(void** stream);
+
+/* Kernels launched by the singleton scene since initialisation (kernels inside
+ * captured graphs are counted one by one). */
+FIRE_API bool fireCudaGetLaunchCount(unsigned long long* count);
+
+/* Name of the build and its compute capability target, for diagnostics. */
+FIRE_API const char* fireCudaBuildInfo(void);
+
+#ifdef __cplusplus
+}
+#endif

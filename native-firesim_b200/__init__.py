@@ -9,5 +9,6 @@ tests, benchmarks and Python callers; it performs no computation itself.
 from __future__ import annotations
 
 from . import abi  # noqa: F401
+from .firesim import FireSim, FireSimError, load_library  # noqa: F401
 
-__all__ = ["abi"]
+__all__ = ["abi", "FireSim", "FireSimError", "load_library"]

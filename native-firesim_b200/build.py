@@ -1,0 +1,84 @@
+"""Build recipe for native-firesim_b200/libfiresim_b200.so (sm_100a).
+
+Compiles every csrc/*.cu with nvcc for compute_100a/sm_100a (-O3 -lineinfo),
+in parallel, and links them into one shared library next to this file.
+nvcc cross-compiles without a GPU, so this runs on a CPU-only host.
+
+Usage: python native-firesim_b200/build.py [--force] [--ptxas-verbose]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+OBJ = HERE / "_build"
+LIB = HERE / "libfiresim_b200.so"
+INCLUDE = HERE.parent / "include"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr"]
+
+
+def _nvcc() -> str:
+    return os.environ.get("NVCC", "nvcc")
+
+
+def sources() -> list[Path]:
+    return sorted(CSRC.glob("*.cu"))
+
+
+def headers() -> list[Path]:
+    return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _compile(src: Path, force: bool, verbose_ptxas: bool) -> tuple[Path, str]:
+    obj = OBJ / (src.stem + ".o")
+    newest_dep = max([src.stat().st_mtime] + [h.stat().st_mtime for h in headers()])
+    if not force and obj.exists() and obj.stat().st_mtime >= newest_dep and not verbose_ptxas:
+        return obj, ""
+    cmd = [_nvcc(), *ARCH, *CUFLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+    if verbose_ptxas:
+        cmd[1:1] = ["-Xptxas", "-v"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{res.stdout}\n{res.stderr}")
+    return obj, res.stderr
+
+
+def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True) -> Path:
+    OBJ.mkdir(parents=True, exist_ok=True)
+    srcs = sources()
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        results = list(ex.map(lambda s: _compile(s, force, verbose_ptxas), srcs))
+    if verbose_ptxas:
+        for _, log in results:
+            print(log)
+    objs = [o for o, _ in results]
+    if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+        os.replace(tmp, LIB)
+        if not quiet:
+            print(f"linked {LIB}")
+    return LIB
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas-verbose", action="store_true")
+    args = ap.parse_args()
+    print(build(force=args.force, verbose_ptxas=args.ptxas_verbose, quiet=False))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

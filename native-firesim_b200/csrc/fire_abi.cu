@@ -1,0 +1,259 @@
+// fire_abi.cu -- the C ABI of include/fire_cuda.h and include/fire_ext.h.
+//
+// The reference keeps one global scene (src/fire_cuda.cu:116-195) behind
+// seventeen entry points that return bool and leave a message for
+// fireCudaLastError() in the form "label: cudaGetErrorString" (:197-207).
+// This file keeps that contract over one firesim::Scene.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/fire_ext.h"
+#include "fire_scene.h"
+
+namespace {
+
+std::unique_ptr<firesim::Scene> g_scene;
+int g_device = 0;
+char g_lastError[512] = "No CUDA error.";
+
+bool fail(const std::string& msg) {
+    std::snprintf(g_lastError, sizeof(g_lastError), "%s", msg.c_str());
+    return false;
+}
+
+bool requireScene() {
+    if (!g_scene) {
+        return fail("CUDA renderer is not initialized.");
+    }
+    return true;
+}
+
+bool initialize(int frameW, int frameH, int nx, int ny, int nz) {
+    fireCudaShutdown();
+    std::strcpy(g_lastError, "No CUDA error.");
+    auto scene = std::make_unique<firesim::Scene>();
+    std::string err;
+    if (!scene->init(g_device, frameW, frameH, nx, ny, nz, err)) {
+        return fail(err);
+    }
+    if (!scene->reset(err)) {
+        return fail(err);
+    }
+    g_scene = std::move(scene);
+    return true;
+}
+
+bool frame(uint32_t* bgra, const FireSettings* s, FireCudaFrameMetrics* metrics, bool toHdr, bool advance, bool render) {
+    if (!requireScene()) return false;
+    if (s == nullptr) return fail("Settings pointer was null.");
+    std::string err;
+    if (!g_scene->frame(bgra, *s, metrics, toHdr, advance, render, err)) return fail(err);
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// src/fire_cuda.cu:2912-3004 -- grid derived from the window request.
+bool fireCudaInitialize(int frameWidth, int frameHeight, int gridWidth, int gridHeight) {
+    const bool highQualityRequest = gridWidth >= 320 || gridHeight >= 220;
+    auto clampI = [](int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); };
+    const int nx = clampI(gridWidth / 2, 72, highQualityRequest ? 176 : 104);
+    const int ny = clampI(gridHeight - 32, 80, highQualityRequest ? 208 : 112);
+    const int nz = clampI(gridWidth / 3, 48, highQualityRequest ? 132 : 72);
+    return initialize(frameWidth, frameHeight, nx, ny, nz);
+}
+
+bool fireCudaInitializeGrid(int frameWidth, int frameHeight, int nx, int ny, int nz) {
+    return initialize(frameWidth, frameHeight, nx, ny, nz);
+}
+
+bool fireCudaStepAndRender(uint32_t* bgraPixels, const FireSettings& settings) {
+    return frame(bgraPixels, &settings, nullptr, false, true, true);
+}
+
+bool fireCudaStepAndRenderMeasured(uint32_t* bgraPixels, const FireSettings& settings, FireCudaFrameMetrics* metrics) {
+    if (metrics == nullptr) return fail("Metrics output pointer was null.");
+    return frame(bgraPixels, &settings, metrics, false, true, true);
+}
+
+bool fireCudaSelectDeviceForD3D11(void* d3d11Device) {
+    (void)d3d11Device;
+    return fail("D3D11 unavailable on headless build; use fireCudaSelectDevice.");
+}
+
+bool fireCudaSelectDevice(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return fail("fireCudaSelectDevice: no such CUDA device.");
+    }
+    g_device = device;
+    const cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return true;
+}
+
+bool fireCudaRegisterD3D11Texture(void* d3d11Texture) {
+    (void)d3d11Texture;
+    return fail("D3D11 unavailable on headless build; use fireCudaRegisterHdrBufferSlot.");
+}
+
+bool fireCudaRegisterD3D11TextureSlot(int slot, void* d3d11Texture) {
+    (void)slot;
+    (void)d3d11Texture;
+    return fail("D3D11 unavailable on headless build; use fireCudaRegisterHdrBufferSlot.");
+}
+
+bool fireCudaRegisterHdrBufferSlot(int slot, void* devicePtr, size_t pitchBytes, int format) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->registerHdrSlot(slot, devicePtr, pitchBytes, format, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaSetD3D11TextureSlot(int slot) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->setActiveSlot(slot, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaStepD3D11(const FireSettings& settings) { return frame(nullptr, &settings, nullptr, false, true, false); }
+
+bool fireCudaStepAndRenderD3D11(const FireSettings& settings) { return frame(nullptr, &settings, nullptr, true, true, true); }
+
+bool fireCudaStepAndRenderD3D11Measured(const FireSettings& settings, FireCudaFrameMetrics* metrics) {
+    if (metrics == nullptr) return fail("Metrics output pointer was null.");
+    return frame(nullptr, &settings, metrics, true, true, true);
+}
+
+bool fireCudaRenderD3D11(const FireSettings& settings) { return frame(nullptr, &settings, nullptr, true, false, true); }
+
+void fireCudaUnregisterD3D11Texture(void) {
+    if (g_scene) g_scene->clearSlots();
+}
+
+bool fireCudaSynchronize(void) {
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(std::string("cudaDeviceSynchronize: ") + cudaGetErrorString(e));
+    return true;
+}
+
+bool fireCudaReset(void) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->reset(err)) return fail(err);
+    return true;
+}
+
+// src/fire_cuda.cu:3066-3104
+bool fireCudaGetDiagnostics(FireCudaDiagnostics* diagnostics) {
+    if (diagnostics == nullptr) return fail("Diagnostics output pointer was null.");
+    FireCudaDiagnostics out{};
+    cudaError_t e = cudaDriverGetVersion(&out.driverVersion);
+    if (e != cudaSuccess) return fail(std::string("cudaDriverGetVersion: ") + cudaGetErrorString(e));
+    e = cudaRuntimeGetVersion(&out.runtimeVersion);
+    if (e != cudaSuccess) return fail(std::string("cudaRuntimeGetVersion: ") + cudaGetErrorString(e));
+    e = cudaGetDeviceCount(&out.deviceCount);
+    if (e != cudaSuccess) return fail(std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    if (out.deviceCount <= 0) return fail("No CUDA-capable device was found.");
+    int device = 0;
+    e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    cudaDeviceProp props{};
+    e = cudaGetDeviceProperties(&props, device);
+    if (e != cudaSuccess) return fail(std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e));
+    out.activeDevice = device;
+    out.computeMajor = props.major;
+    out.computeMinor = props.minor;
+    out.totalGlobalMem = static_cast<uint64_t>(props.totalGlobalMem);
+    std::snprintf(out.deviceName, sizeof(out.deviceName), "%s", props.name);
+    *diagnostics = out;
+    return true;
+}
+
+void fireCudaShutdown(void) { g_scene.reset(); }
+
+const char* fireCudaLastError(void) { return g_lastError; }
+
+bool fireCudaSetPressureSolver(int iterations, float omega) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->setPressureSolver(iterations, omega, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaGetGridInfo(int* dims8) {
+    if (!requireScene()) return false;
+    if (dims8 == nullptr) return fail("dims pointer was null.");
+    const firesim::Scene& s = *g_scene;
+    const int d[8] = {s.nx, s.ny, s.nz, s.lnx, s.lny, s.lnz, s.frameW, s.frameH};
+    std::memcpy(dims8, d, sizeof(d));
+    return true;
+}
+
+bool fireCudaGetField(int field, void* host, size_t bytes) {
+    if (!requireScene()) return false;
+    if (host == nullptr) return fail("field host pointer was null.");
+    std::string err;
+    if (!g_scene->getField(field, host, bytes, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaSetField(int field, const void* host, size_t bytes) {
+    if (!requireScene()) return false;
+    if (host == nullptr) return fail("field host pointer was null.");
+    std::string err;
+    if (!g_scene->setField(field, host, bytes, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaRunStages(int first, int last, const FireSettings* settings, float time) {
+    if (!requireScene()) return false;
+    if (settings == nullptr) return fail("Settings pointer was null.");
+    std::string err;
+    const firesim::FrameParams p = g_scene->paramsFrom(*settings, time);
+    if (!g_scene->runStages(first, last, p, err) || !g_scene->synchronize(err)) return fail(err);
+    return true;
+}
+
+bool fireCudaGetTimes(float* simTime, float* renderTime, int* frameIndex) {
+    if (!requireScene()) return false;
+    if (simTime) *simTime = g_scene->simTime;
+    if (renderTime) *renderTime = g_scene->renderTime;
+    if (frameIndex) *frameIndex = g_scene->frameIndex;
+    return true;
+}
+
+bool fireCudaSetTimes(float simTime, float renderTime, int frameIndex) {
+    if (!requireScene()) return false;
+    g_scene->simTime = simTime;
+    g_scene->renderTime = renderTime;
+    g_scene->frameIndex = frameIndex;
+    return true;
+}
+
+bool fireCudaGetStream(void** stream) {
+    if (!requireScene()) return false;
+    if (stream == nullptr) return fail("stream pointer was null.");
+    *stream = static_cast<void*>(g_scene->stream);
+    return true;
+}
+
+bool fireCudaGetLaunchCount(unsigned long long* count) {
+    if (!requireScene()) return false;
+    if (count == nullptr) return fail("count pointer was null.");
+    *count = g_scene->launchCount();
+    return true;
+}
+
+const char* fireCudaBuildInfo(void) { return "firesim-b200 sm_100a"; }
+
+}  // extern "C"

@@ -1,0 +1,708 @@
+// fire_scene.cu -- allocation, launch sequencing and clocks of one scene.
+#include "fire_scene.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace firesim {
+
+namespace {
+
+enum Stage {
+    kAdvectVelocity = 0, kAdvectReact, kForce, kVelocityBoundary, kDivergence, kPressureSor, kSubtract, kWallBoundary,
+    kLightBuild, kLightPropagate, kRender, kEmbers, kTonemap, kOverlay, kMetrics, kReset,
+};
+
+enum Event { kStart = 0, kAfterVelocity, kAfterReaction, kAfterProjection, kAfterSolve, kAfterLighting, kAfterRaymarch, kAfterPack, kAfterRender };
+
+int clampI(int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); }
+float clampF(float v, float lo, float hi) { return std::max(lo, std::min(hi, v)); }
+
+// Threads along x for a row of n cells (rows are launched one CTA row each).
+int rowThreads(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : 128); }
+
+dim3 cellGrid(int bx, int n, int ny, int nz) { return dim3((n + bx - 1) / bx, ny, nz); }
+
+}  // namespace
+
+bool MaterialKey::operator==(const MaterialKey& o) const {
+    return sceneId == o.sceneId && emitterRadius == o.emitterRadius && emitterCenterX == o.emitterCenterX &&
+           emitterCenterZ == o.emitterCenterZ && burnerCenterCount == o.burnerCenterCount && burnerX0 == o.burnerX0 &&
+           burnerZ0 == o.burnerZ0;
+}
+
+Scene::~Scene() { release(); }
+
+bool Scene::check(const char* label, cudaError_t e, std::string& err) {
+    if (e != cudaSuccess) {
+        err = std::string(label) + ": " + cudaGetErrorString(e);
+        return false;
+    }
+    return true;
+}
+
+bool Scene::alloc(void** p, size_t bytes, const char* label, std::string& err) {
+    if (!check(label, cudaMalloc(p, bytes), err)) {
+        *p = nullptr;
+        return false;
+    }
+    deviceBytes_ += bytes;
+    return true;
+}
+
+void Scene::release() {
+    if (device >= 0 && (stream != nullptr || sa_[0] != nullptr)) {
+        cudaSetDevice(device);
+    }
+    if (stream != nullptr) {
+        cudaStreamSynchronize(stream);
+    }
+    if (sorExec_ != nullptr) {
+        cudaGraphExecDestroy(sorExec_);
+        sorExec_ = nullptr;
+    }
+    void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
+                    vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
+                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_};
+    for (void* b : bufs) {
+        if (b != nullptr) cudaFree(b);
+    }
+    if (metricHost_ != nullptr) cudaFreeHost(metricHost_);
+    for (cudaEvent_t& e : events_) {
+        if (e != nullptr) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    if (stream != nullptr) cudaStreamDestroy(stream);
+    stream = nullptr;
+    std::memset(sa_, 0, sizeof(sa_));
+    std::memset(sb_, 0, sizeof(sb_));
+    std::memset(sc_, 0, sizeof(sc_));
+    std::memset(vel_, 0, sizeof(vel_));
+    pressure_ = divergence_ = divergenceAfter_ = material_ = breathing_ = shadow_ = nullptr;
+    contrib_ = light_ = lightNext_ = hdr_ = nullptr;
+    bgra_ = nullptr;
+    embers_ = nullptr;
+    partials_ = metricDevice_ = metricHost_ = nullptr;
+    deviceBytes_ = 0;
+}
+
+bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err) {
+    if (x < 2 || y < 2 || z < 2 || fw < 1 || fh < 1) {
+        err = "invalid grid or frame dimensions";
+        return false;
+    }
+    const long long cells = static_cast<long long>(x) * y * z;
+    if (cells > (1LL << 30) || static_cast<long long>(fw) * fh > (1LL << 28) || y > 65535 || z > 65535 || fh > 65535 * 8) {
+        err = "grid or frame too large for the 32-bit index layout";
+        return false;
+    }
+    device = dev;
+    nx = x;
+    ny = y;
+    nz = z;
+    frameW = fw;
+    frameH = fh;
+    // Light grid, src/fire_cuda.cu:2920-2922.
+    lnx = clampI((nx + 3) / 4, 18, 48);
+    lny = clampI((ny + 3) / 4, 20, 56);
+    lnz = clampI((nz + 3) / 4, 16, 36);
+    cells_ = static_cast<size_t>(cells);
+    nu_ = static_cast<size_t>(nx + 1) * ny * nz;
+    nv_ = static_cast<size_t>(nx) * (ny + 1) * nz;
+    nw_ = static_cast<size_t>(nx) * ny * (nz + 1);
+    lightCells_ = static_cast<size_t>(lnx) * lny * lnz;
+    pixels_ = static_cast<size_t>(fw) * fh;
+    if (!check("cudaSetDevice", cudaSetDevice(device), err)) return false;
+    if (!check("cudaStreamCreate", cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), err)) return false;
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i) {
+        ok = alloc(reinterpret_cast<void**>(&sa_[i]), cells_ * sizeof(float4), "cudaMalloc scalars a", err) &&
+             alloc(reinterpret_cast<void**>(&sb_[i]), cells_ * sizeof(float4), "cudaMalloc scalars b", err) &&
+             alloc(reinterpret_cast<void**>(&sc_[i]), cells_ * sizeof(float2), "cudaMalloc scalars c", err) &&
+             alloc(reinterpret_cast<void**>(&vel_[0][i]), nu_ * sizeof(float), "cudaMalloc u", err) &&
+             alloc(reinterpret_cast<void**>(&vel_[1][i]), nv_ * sizeof(float), "cudaMalloc v", err) &&
+             alloc(reinterpret_cast<void**>(&vel_[2][i]), nw_ * sizeof(float), "cudaMalloc w", err);
+    }
+    ok = ok && alloc(reinterpret_cast<void**>(&pressure_), cells_ * sizeof(float), "cudaMalloc pressure", err) &&
+         alloc(reinterpret_cast<void**>(&divergence_), cells_ * sizeof(float), "cudaMalloc divergence", err) &&
+         alloc(reinterpret_cast<void**>(&divergenceAfter_), cells_ * sizeof(float), "cudaMalloc divergence after", err) &&
+         alloc(reinterpret_cast<void**>(&contrib_), cells_ * sizeof(float4), "cudaMalloc force scratch", err) &&
+         alloc(reinterpret_cast<void**>(&material_), static_cast<size_t>(nx) * nz * sizeof(float), "cudaMalloc material", err) &&
+         alloc(reinterpret_cast<void**>(&breathing_), static_cast<size_t>(nx) * nz * sizeof(float), "cudaMalloc breathing", err) &&
+         alloc(reinterpret_cast<void**>(&light_), lightCells_ * sizeof(float4), "cudaMalloc scene light", err) &&
+         alloc(reinterpret_cast<void**>(&lightNext_), lightCells_ * sizeof(float4), "cudaMalloc scene light next", err) &&
+         alloc(reinterpret_cast<void**>(&shadow_), lightCells_ * sizeof(float), "cudaMalloc scene shadow", err) &&
+         alloc(reinterpret_cast<void**>(&hdr_), pixels_ * sizeof(float4), "cudaMalloc hdr frame", err) &&
+         alloc(reinterpret_cast<void**>(&bgra_), pixels_ * sizeof(uint32_t), "cudaMalloc frame", err) &&
+         alloc(reinterpret_cast<void**>(&embers_), kMaxEmberCount * sizeof(EmberSplat), "cudaMalloc embers", err) &&
+         alloc(reinterpret_cast<void**>(&partials_), kMetricBlocks * sizeof(MetricPartial), "cudaMalloc metric partials", err) &&
+         alloc(reinterpret_cast<void**>(&metricDevice_), sizeof(MetricPartial), "cudaMalloc metrics", err) &&
+         check("cudaMallocHost metrics", cudaMallocHost(reinterpret_cast<void**>(&metricHost_), sizeof(MetricPartial)), err);
+    for (int i = 0; i < 9 && ok; ++i) {
+        ok = check("cudaEventCreate", cudaEventCreate(&events_[i]), err);
+    }
+    ok = ok && check("clear hdr", cudaMemsetAsync(hdr_, 0, pixels_ * sizeof(float4), stream), err) &&
+         check("clear frame", cudaMemsetAsync(bgra_, 0, pixels_ * sizeof(uint32_t), stream), err);
+    if (!ok) {
+        release();
+        return false;
+    }
+    return true;
+}
+
+ScalarFieldsIn Scene::scalarsIn() const { return {sa_[cur_], sb_[cur_], sc_[cur_]}; }
+ScalarFields Scene::scalarsOut() const { return {sa_[1 - cur_], sb_[1 - cur_], sc_[1 - cur_]}; }
+Velocity Scene::velocity() const { return {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]}; }
+
+FrameParams Scene::paramsFrom(const FireSettings& s, float time) const {
+    FrameParams p{};
+    p.nx = nx; p.ny = ny; p.nz = nz; p.frameW = frameW; p.frameH = frameH; p.lnx = lnx; p.lny = lny; p.lnz = lnz;
+    p.dt = clampF(s.dt, 0.001f, 1.0f / 30.0f);
+    p.time = time;
+    p.mouseX = clampF(s.mouseX, 0.0f, 1.0f);
+    p.mouseY = clampF(s.mouseY, 0.0f, 1.0f);
+    p.leftDown = s.leftDown;
+    p.rightDown = s.rightDown;
+    p.showGizmos = s.showGizmos;
+    p.activeGizmo = s.activeGizmo;
+    p.sceneId = clampI(s.sceneId, 0, kSceneCount - 1);
+    p.wind = clampF(s.wind, -1.0f, 1.0f);
+    p.turbulence = clampF(s.turbulence, 0.05f, 1.8f);
+    p.detail = clampF(s.detail, 0.1f, 1.5f);
+    p.smokeGain = clampF(s.smoke, 0.0f, 1.6f);
+    p.intensity = clampF(s.intensity, 0.2f, 2.4f);
+    const float yaw = s.cameraYaw;
+    const float pitch = clampF(s.cameraPitch, -0.75f, 0.75f);
+    const float distance = clampF(s.cameraDistance, 1.5f, 6.0f);
+    p.cinematicMode = s.cinematicMode != 0 ? 1 : 0;
+    p.raymarchSteps = clampI(s.raymarchSteps, 24, kMaxRaymarchSteps);
+    p.emberCount = clampI(s.emberCount, 0, kMaxEmberCount);
+    p.renderDebugMode = clampI(s.renderDebugMode, 0, 6);
+    p.exposure = clampF(s.exposure, 0.45f, 2.40f);
+    p.reflectionGain = clampF(s.reflectionGain, 0.0f, 2.2f);
+    p.smokeDarkness = clampF(s.smokeDarkness, 0.35f, 2.4f);
+    p.emitterCenterX = clampF(s.emitterCenterX, -1.05f, 1.05f);
+    p.emitterCenterZ = clampF(s.emitterCenterZ, -0.82f, 0.82f);
+    p.emitterHeightNorm = clampF(s.emitterHeightNorm, 0.0f, 0.96f);
+    p.emitterHeightBandNorm = clampF(s.emitterHeightBandNorm, 0.006f, 0.20f);
+    p.emitterRadius = clampF(s.emitterRadius, 0.035f, 0.80f);
+    p.burnerCenterCount = clampI(s.burnerCenterCount, 0, 4);
+    for (int i = 0; i < 4; ++i) {
+        p.burnerCenterX[i] = clampF(s.burnerCenterX[i], -1.05f, 1.05f);
+        p.burnerCenterY[i] = clampF(s.burnerCenterY[i], 0.0f, 2.03f);
+        p.burnerCenterZ[i] = clampF(s.burnerCenterZ[i], -0.82f, 0.82f);
+    }
+    if (p.sceneId == 2 && p.burnerCenterCount > 0) {
+        p.emitterHeightNorm = clampF((p.burnerCenterY[0] - 0.02f) / 2.03f, 0.0f, 0.96f);
+    }
+    // Camera basis, evaluated on the host as the reference does (src/fire_cuda.cu:315-329).
+    const float3 target = make_float3(0.0f, 0.72f, 0.0f);
+    const float cp = std::cos(pitch);
+    p.eye = make_float3(std::sin(yaw) * distance * cp, target.y + std::sin(pitch) * distance, std::cos(yaw) * distance * cp);
+    p.forward = normalize3(sub3(target, p.eye));
+    p.right = normalize3(cross3(p.forward, make_float3(0.0f, 1.0f, 0.0f)));
+    p.up = normalize3(cross3(p.right, p.forward));
+    p.tanHalfFov = 0.50f;
+    p.aspect = static_cast<float>(frameW) / static_cast<float>(frameH);
+    return p;
+}
+
+FrameParams Scene::defaultParams(float time) const {
+    FireSettings s{};
+    s.dt = 1.0f / 60.0f;
+    s.mouseX = 0.5f;
+    s.mouseY = 0.12f;
+    s.sceneId = 0;
+    s.turbulence = 0.72f;
+    s.detail = 0.88f;
+    s.smoke = 0.92f;
+    s.intensity = 1.0f;
+    s.cameraPitch = 0.18f;
+    s.cameraDistance = 3.35f;
+    s.cinematicMode = 1;
+    s.raymarchSteps = 56;
+    s.emberCount = 96;
+    s.showGizmos = 0;
+    s.activeGizmo = 0;
+    return paramsFrom(s, time);
+}
+
+bool Scene::ensureMaterial(const FrameParams& p, std::string& err) {
+    MaterialKey key;
+    key.sceneId = p.sceneId;
+    key.emitterRadius = p.emitterRadius;
+    key.emitterCenterX = p.emitterCenterX;
+    key.emitterCenterZ = p.emitterCenterZ;
+    key.burnerCenterCount = p.burnerCenterCount;
+    key.burnerX0 = p.burnerCenterX[0];
+    key.burnerZ0 = p.burnerCenterZ[0];
+    const int withMaterial = key == materialKey_ ? 0 : 1;
+    const int bx = rowThreads(nx);
+    fuelBedTables<<<dim3((nx + bx - 1) / bx, nz), bx, 0, stream>>>(material_, breathing_, p, withMaterial);
+    launches_ += 1;
+    if (!check("fuel bed tables launch", cudaGetLastError(), err)) return false;
+    materialKey_ = key;
+    return true;
+}
+
+bool Scene::setPressureSolver(int iterations, float omega, std::string& err) {
+    if (iterations < 0 || iterations > 100000 || !(omega > 0.0f && omega < 2.0f)) {
+        err = "pressure solver: iterations must be in [0, 100000] and omega in (0, 2)";
+        return false;
+    }
+    pressureIterations = iterations;
+    pressureOmega = omega;
+    return true;
+}
+
+// src/fire_cuda.cu:3280-3284 -- 2N half sweeps, captured once per (N, omega)
+// into a CUDA graph so a step pays one graph launch instead of 2N launches.
+bool Scene::runSor(const FrameParams& p, std::string& err) {
+    (void)p;
+    if (pressureIterations == 0) return true;
+    if (sorExec_ == nullptr || sorIterations_ != pressureIterations || sorOmega_ != pressureOmega) {
+        if (sorExec_ != nullptr) {
+            cudaGraphExecDestroy(sorExec_);
+            sorExec_ = nullptr;
+        }
+        const Grid g{nx, ny, nz};
+        const int half = (nx + 1) / 2;
+        const int bx = rowThreads(half);
+        const dim3 grid = cellGrid(bx, half, ny, nz);
+        cudaGraph_t graph = nullptr;
+        if (!check("SOR capture begin", cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), err)) return false;
+        for (int i = 0; i < pressureIterations; ++i) {
+            sorHalfSweep<<<grid, bx, 0, stream>>>(pressure_, divergence_, g, 0, pressureOmega);
+            sorHalfSweep<<<grid, bx, 0, stream>>>(pressure_, divergence_, g, 1, pressureOmega);
+        }
+        const cudaError_t launchErr = cudaGetLastError();
+        const cudaError_t endErr = cudaStreamEndCapture(stream, &graph);
+        if (!check("SOR capture launch", launchErr, err) || !check("SOR capture end", endErr, err)) {
+            if (graph) cudaGraphDestroy(graph);
+            return false;
+        }
+        const cudaError_t instErr = cudaGraphInstantiate(&sorExec_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (!check("SOR graph instantiate", instErr, err)) return false;
+        sorIterations_ = pressureIterations;
+        sorOmega_ = pressureOmega;
+    }
+    launches_ += 2ull * static_cast<unsigned long long>(pressureIterations);
+    return check("SOR graph launch", cudaGraphLaunch(sorExec_, stream), err);
+}
+
+bool Scene::runMetrics(const FrameParams& p, std::string& err) {
+    const int bx = rowThreads(nx);
+    divergenceOf<<<cellGrid(bx, nx, ny, nz), bx, 0, stream>>>(divergenceAfter_, nullptr, velocity(), p);
+    metricsPartials<<<kMetricBlocks, kMetricThreads, kMetricThreads * sizeof(MetricPartial), stream>>>(
+        partials_, scalarsIn(), light_, shadow_, divergence_, divergenceAfter_, p);
+    metricsFinal<<<1, kMetricThreads, kMetricThreads * sizeof(MetricPartial), stream>>>(metricDevice_, partials_, kMetricBlocks);
+    launches_ += 3;
+    if (!check("metrics launch", cudaGetLastError(), err)) return false;
+    return check("metrics readback", cudaMemcpyAsync(metricHost_, metricDevice_, sizeof(MetricPartial), cudaMemcpyDeviceToHost, stream), err);
+}
+
+bool Scene::runStages(int first, int last, const FrameParams& p, std::string& err) {
+    if (first < 0 || last > kReset || first > last) {
+        err = "stage range out of order";
+        return false;
+    }
+    const Grid g{nx, ny, nz};
+    const int bx = rowThreads(nx);
+    const int bxFace = rowThreads(nx + 1);
+    const dim3 cells = cellGrid(bx, nx, ny, nz);
+    const dim3 faces = cellGrid(bxFace, nx + 1, ny + 1, nz + 1);
+    const dim3 frameBlock(16, 8);
+    const dim3 frameGrid((frameW + 15) / 16, (frameH + 7) / 8);
+    int s = first;
+    while (s <= last) {
+        switch (s) {
+            case kAdvectVelocity:
+                advectVelocity<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), p); ++launches_;
+                vcur_ = 1 - vcur_;
+                s = kAdvectReact;
+                break;
+            case kAdvectReact:
+                if (!ensureMaterial(p, err)) return false;
+                advectReact<<<cells, bx, 0, stream>>>(scalarsOut(), scalarsIn(), velocity(), material_, breathing_, p); ++launches_;
+                cur_ = 1 - cur_;
+                s = kForce;
+                break;
+            case kForce:
+                forceContributions<<<cells, bx, 0, stream>>>(contrib_, scalarsIn(), velocity(), p); ++launches_;
+                if (last >= kDivergence) {
+                    forceProjectSetup<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], divergence_,
+                                                               pressure_, contrib_, velocity(), p); ++launches_;
+                    vcur_ = 1 - vcur_;
+                    s = kPressureSor;
+                } else {
+                    forceApply<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], contrib_, velocity(), p); ++launches_;
+                    vcur_ = 1 - vcur_;
+                    s = kVelocityBoundary;
+                }
+                break;
+            case kVelocityBoundary:
+                velocityBoundary<<<faces, bxFace, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], p, 1); ++launches_;
+                s = kDivergence;
+                break;
+            case kDivergence:
+                divergenceOf<<<cells, bx, 0, stream>>>(divergence_, pressure_, velocity(), p); ++launches_;
+                s = kPressureSor;
+                break;
+            case kPressureSor:
+                if (!runSor(p, err)) return false;
+                s = kSubtract;
+                break;
+            case kSubtract:
+                subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 1, last >= kWallBoundary ? 1 : 0); ++launches_;
+                s = last >= kWallBoundary ? kLightBuild : kWallBoundary;
+                break;
+            case kWallBoundary:
+                subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 0, 1); ++launches_;
+                s = kLightBuild;
+                break;
+            case kLightBuild: {
+                const int lbx = rowThreads(lnx);
+                lightBuild<<<dim3((lnx + lbx - 1) / lbx, lny, lnz), lbx, 0, stream>>>(light_, shadow_, scalarsIn(), p); ++launches_;
+                s = kLightPropagate;
+                break;
+            }
+            case kLightPropagate: {
+                const int lbx = rowThreads(lnx);
+                const dim3 lg((lnx + lbx - 1) / lbx, lny, lnz);
+                lightPropagate<<<lg, lbx, 0, stream>>>(lightNext_, light_, shadow_, p, 0.48f, 0.92f); ++launches_;
+                lightPropagate<<<lg, lbx, 0, stream>>>(light_, lightNext_, shadow_, p, 0.34f, 0.96f); ++launches_;
+                s = kRender;
+                break;
+            }
+            case kRender:
+                raymarch<<<frameGrid, frameBlock, 0, stream>>>(hdr_, scalarsIn(), velocity(), light_, shadow_, p); ++launches_;
+                s = kEmbers;
+                break;
+            case kEmbers:
+                if (p.emberCount > 0 && p.renderDebugMode == 0) {
+                    emberSetup<<<1, 256, 0, stream>>>(embers_, scalarsIn(), velocity(), p); ++launches_;
+                    emberGather<<<dim3((frameW + 15) / 16, (frameH + 15) / 16), dim3(16, 16), 0, stream>>>(hdr_, embers_, p); ++launches_;
+                }
+                s = kTonemap;
+                break;
+            case kTonemap:
+                tonemapOverlay<<<dim3((frameW + 15) / 16, (frameH + 15) / 16), dim3(16, 16), 0, stream>>>(bgra_, hdr_, p, 1,
+                                                                                                      last >= kOverlay ? 1 : 0); ++launches_;
+                s = last >= kOverlay ? kMetrics : kOverlay;
+                break;
+            case kOverlay:
+                tonemapOverlay<<<dim3((frameW + 15) / 16, (frameH + 15) / 16), dim3(16, 16), 0, stream>>>(bgra_, hdr_, p, 0, 1); ++launches_;
+                s = kMetrics;
+                break;
+            case kMetrics:
+                if (!runMetrics(p, err)) return false;
+                s = kReset;
+                break;
+            case kReset: {
+                // src/fire_cuda.cu:3006-3048: procedural scalars, zero faces, zero light.
+                if (!ensureMaterial(p, err)) return false;
+                resetCells<<<cells, bx, 0, stream>>>(scalarsOut(), pressure_, divergence_, divergenceAfter_, material_, breathing_, p); ++launches_;
+                cur_ = 1 - cur_;
+                bool ok = true;
+                for (int c = 0; c < 3 && ok; ++c) {
+                    const size_t n = c == 0 ? nu_ : (c == 1 ? nv_ : nw_);
+                    ok = check("reset velocity", cudaMemsetAsync(vel_[c][0], 0, n * sizeof(float), stream), err) &&
+                         check("reset velocity", cudaMemsetAsync(vel_[c][1], 0, n * sizeof(float), stream), err);
+                }
+                ok = ok && check("reset scene light", cudaMemsetAsync(light_, 0, lightCells_ * sizeof(float4), stream), err) &&
+                     check("reset scene light next", cudaMemsetAsync(lightNext_, 0, lightCells_ * sizeof(float4), stream), err) &&
+                     check("reset scene shadow", cudaMemsetAsync(shadow_, 0, lightCells_ * sizeof(float), stream), err);
+                if (!ok) return false;
+                s = kReset + 1;
+                break;
+            }
+            default:
+                err = "unknown stage";
+                return false;
+        }
+        if (!check("stage launch", cudaGetLastError(), err)) return false;
+    }
+    return true;
+}
+
+bool Scene::reset(std::string& err) {
+    const FrameParams p = defaultParams(simTime);
+    if (!runStages(kReset, kReset, p, err)) return false;
+    simTime = 0.0f;
+    renderTime = 0.0f;
+    frameIndex = 0;
+    return check("reset kernels sync", cudaStreamSynchronize(stream), err);
+}
+
+bool Scene::frame(uint32_t* hostBgra, const FireSettings& s, FireCudaFrameMetrics* metrics, bool toHdrSlot, bool advance, bool render,
+                  std::string& err) {
+    if (render && !toHdrSlot && hostBgra == nullptr) {
+        err = "Output pixel pointer was null.";
+        return false;
+    }
+    if (render && toHdrSlot && slots_[activeSlot_].ptr == nullptr) {
+        err = "HDR output buffer slot is not registered.";
+        return false;
+    }
+    if (!render && !advance) {
+        err = "Step-only path requires simulation advancement.";
+        return false;
+    }
+    const bool collect = metrics != nullptr;
+    if (collect && !advance) {
+        err = "Render-only measured path is not supported.";
+        return false;
+    }
+    const float stepDt = std::max(0.001f, std::min(s.dt, 1.0f / 30.0f));
+    renderTime += stepDt;
+    if (advance) simTime += stepDt;
+    FrameParams p = paramsFrom(s, advance ? simTime : renderTime);
+    if (s.reset != 0) {
+        // The reset zeroes the clocks, but the frame keeps the parameter block
+        // built before it (src/fire_cuda.cu:3181, :3053-3055).
+        if (!runStages(kReset, kReset, p, err)) return false;
+        simTime = 0.0f;
+        renderTime = 0.0f;
+        frameIndex = 0;
+    }
+    auto rec = [&](int e) { return !collect || check("cudaEventRecord", cudaEventRecord(events_[e], stream), err); };
+    if (!rec(kStart)) return false;
+    if (advance) {
+        // Event points of the reference (src/fire_cuda.cu:3188-3321).  The
+        // forcing is fused with the divergence, so it is timed in the
+        // projection interval rather than the reaction interval.
+        if (!runStages(kAdvectVelocity, kAdvectVelocity, p, err) || !rec(kAfterVelocity)) return false;
+        if (!runStages(kAdvectReact, kAdvectReact, p, err) || !rec(kAfterReaction)) return false;
+        if (!runStages(kForce, kWallBoundary, p, err) || !rec(kAfterProjection) || !rec(kAfterSolve)) return false;
+        if (!runStages(kLightBuild, kLightPropagate, p, err) || !rec(kAfterLighting)) return false;
+    }
+    if (!render) {
+        return true;
+    }
+    p.time = renderTime;
+    if (!runStages(kRender, kEmbers, p, err) || !rec(kAfterRaymarch)) return false;
+    if (toHdrSlot) {
+        const HdrSlot& slot = slots_[activeSlot_];
+        packHdr<<<dim3((frameW + 15) / 16, (frameH + 15) / 16), dim3(16, 16), 0, stream>>>(slot.ptr, slot.pitchBytes, slot.format, hdr_, p); ++launches_;
+        if (!check("HDR pack launch", cudaGetLastError(), err)) return false;
+    } else if (!runStages(kTonemap, kOverlay, p, err)) {
+        return false;
+    }
+    if (!rec(kAfterPack) || !rec(kAfterRender)) return false;
+    if (!toHdrSlot) {
+        if (!check("cudaMemcpy frame", cudaMemcpyAsync(hostBgra, bgra_, pixels_ * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), err) ||
+            !check("frame sync", cudaStreamSynchronize(stream), err)) {
+            return false;
+        }
+    }
+    if (collect) {
+        if (!runStages(kMetrics, kMetrics, p, err) || !check("metrics sync", cudaStreamSynchronize(stream), err) || !fillMetrics(metrics, err)) {
+            return false;
+        }
+    }
+    ++frameIndex;
+    return true;
+}
+
+// src/fire_cuda.cu:3476-3545 -- event intervals and the accumulator into FireCudaFrameMetrics.
+bool Scene::fillMetrics(FireCudaFrameMetrics* out, std::string& err) {
+    float solveMs = 0, renderMs = 0, velocityMs = 0, reactionMs = 0, projectionMs = 0, lightingMs = 0, raymarchMs = 0, packMs = 0;
+    if (!check("cudaEventElapsedTime solve", cudaEventElapsedTime(&solveMs, events_[kStart], events_[kAfterSolve]), err) ||
+        !check("cudaEventElapsedTime render", cudaEventElapsedTime(&renderMs, events_[kAfterSolve], events_[kAfterRender]), err) ||
+        !check("cudaEventElapsedTime velocity", cudaEventElapsedTime(&velocityMs, events_[kStart], events_[kAfterVelocity]), err) ||
+        !check("cudaEventElapsedTime reaction", cudaEventElapsedTime(&reactionMs, events_[kAfterVelocity], events_[kAfterReaction]), err) ||
+        !check("cudaEventElapsedTime projection", cudaEventElapsedTime(&projectionMs, events_[kAfterReaction], events_[kAfterProjection]), err) ||
+        !check("cudaEventElapsedTime lighting", cudaEventElapsedTime(&lightingMs, events_[kAfterProjection], events_[kAfterLighting]), err) ||
+        !check("cudaEventElapsedTime raymarch", cudaEventElapsedTime(&raymarchMs, events_[kAfterLighting], events_[kAfterRaymarch]), err) ||
+        !check("cudaEventElapsedTime pack", cudaEventElapsedTime(&packMs, events_[kAfterRaymarch], events_[kAfterPack]), err)) {
+        return false;
+    }
+    const MetricPartial& m = *metricHost_;
+    const double cellCount = static_cast<double>(cells_);
+    auto bits = [](int b) {
+        float f;
+        std::memcpy(&f, &b, 4);
+        return f;
+    };
+    const float divBeforeL2 = static_cast<float>(std::sqrt(m.sums[19] / std::max(1.0, cellCount)));
+    const float divAfterL2 = static_cast<float>(std::sqrt(m.sums[20] / std::max(1.0, cellCount)));
+    FireCudaFrameMetrics o{};
+    o.frameIndex = frameIndex;
+    o.gridX = nx;
+    o.gridY = ny;
+    o.gridZ = nz;
+    o.pressureIterations = pressureIterations;
+    o.invalidCells = m.invalidCells;
+    o.timeSeconds = simTime;
+    o.gpuSolveMs = solveMs;
+    o.gpuRenderMs = renderMs;
+    o.gpuVelocityMs = velocityMs;
+    o.gpuReactionMs = reactionMs;
+    o.gpuProjectionMs = projectionMs;
+    o.gpuLightingMs = lightingMs;
+    o.gpuRaymarchMs = raymarchMs;
+    o.gpuPackMs = packMs;
+    o.heatSum = static_cast<float>(m.sums[0]);
+    o.fuelSum = static_cast<float>(m.sums[1]);
+    o.oxygenSum = static_cast<float>(m.sums[2]);
+    o.sootSum = static_cast<float>(m.sums[3]);
+    o.charSum = static_cast<float>(m.sums[4]);
+    o.ashSum = static_cast<float>(m.sums[5]);
+    o.pyrolysisSum = static_cast<float>(m.sums[6]);
+    o.progressSum = static_cast<float>(m.sums[7]);
+    o.turbulenceEnergySum = static_cast<float>(m.sums[8]);
+    o.sootOpticalDepthSum = static_cast<float>(m.sums[9]);
+    o.maxHeat = bits(m.maxBits[0]);
+    o.maxFuel = bits(m.maxBits[1]);
+    o.maxSoot = bits(m.maxBits[2]);
+    o.maxPyrolysis = bits(m.maxBits[3]);
+    o.maxProgress = bits(m.maxBits[4]);
+    o.maxTurbulenceEnergy = bits(m.maxBits[5]);
+    o.flameHeightMeters = bits(m.maxBits[6]);
+    o.meanOpticalDepth = static_cast<float>(m.sums[17] / std::max(1.0, cellCount));
+    o.meanSceneLight = static_cast<float>(m.sums[10] / std::max(1.0, cellCount));
+    o.meanSceneShadow = static_cast<float>(m.sums[11] / std::max(1.0, cellCount));
+    o.flameMassProxy = static_cast<float>(m.sums[12]);
+    o.smokeMassProxy = static_cast<float>(m.sums[13]);
+    o.flameSmokeOverlapProxy = static_cast<float>(m.sums[14]);
+    o.meanVolumetricShadow = static_cast<float>(m.sums[15] / std::max(1.0, cellCount));
+    o.meanRoomIrradiance = static_cast<float>(m.sums[16] / std::max(1.0, cellCount));
+    o.heatReleaseProxy = static_cast<float>(m.sums[18]);
+    o.divergenceBeforeL2 = divBeforeL2;
+    o.divergenceBeforeMax = bits(m.maxBits[7]);
+    o.divergenceAfterL2 = divAfterL2;
+    o.divergenceAfterMax = bits(m.maxBits[8]);
+    o.divergenceReduction = divBeforeL2 > 0.000001f ? 1.0f - divAfterL2 / divBeforeL2 : 0.0f;
+    *out = o;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Field access (tests, checkpoints): one field at a time, converting between
+// the packed records and the reference's one-array-per-field layout.
+namespace {
+
+struct FieldView {
+    void* base;
+    size_t count;    // elements of `stride` floats
+    int stride;      // floats per element in device memory
+    int component;   // float offset inside the element
+    int width;       // floats per element in the host layout
+};
+
+}  // namespace
+
+static bool fieldView(int field, float4* sa, float4* sb, float2* sc, float* const vel[3], float* pressure, float* divergence,
+                      float* divergenceAfter, float4* light, float* shadow, float4* hdr, uint32_t* bgra, size_t cells, size_t nu,
+                      size_t nv, size_t nw, size_t lightCells, size_t pixels, FieldView& v) {
+    switch (field) {
+        case 0: case 1: case 2: case 3: v = {sa, cells, 4, field, 1}; return true;
+        case 4: case 5: case 6: case 7: v = {sb, cells, 4, field - 4, 1}; return true;
+        case 8: case 9: v = {sc, cells, 2, field - 8, 1}; return true;
+        case 10: v = {pressure, cells, 1, 0, 1}; return true;
+        case 11: v = {divergence, cells, 1, 0, 1}; return true;
+        case 12: v = {vel[0], nu, 1, 0, 1}; return true;
+        case 13: v = {vel[1], nv, 1, 0, 1}; return true;
+        case 14: v = {vel[2], nw, 1, 0, 1}; return true;
+        case 15: v = {light, lightCells, 4, 0, 4}; return true;
+        case 16: v = {shadow, lightCells, 1, 0, 1}; return true;
+        case 17: v = {hdr, pixels, 4, 0, 4}; return true;
+        case 18: v = {bgra, pixels, 1, 0, 1}; return true;
+        case 19: v = {divergenceAfter, cells, 1, 0, 1}; return true;
+        default: return false;
+    }
+}
+
+bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
+    float* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
+    FieldView v;
+    if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_, bgra_,
+                   cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
+        err = "unknown field id";
+        return false;
+    }
+    if (bytes != v.count * v.width * 4) {
+        err = "field size mismatch";
+        return false;
+    }
+    if (!check("field sync", cudaStreamSynchronize(stream), err)) return false;
+    if (v.width == v.stride) {
+        return check("cudaMemcpy field", cudaMemcpy(host, v.base, bytes, cudaMemcpyDeviceToHost), err);
+    }
+    std::vector<float> staging(v.count * v.stride);
+    if (!check("cudaMemcpy field", cudaMemcpy(staging.data(), v.base, staging.size() * 4, cudaMemcpyDeviceToHost), err)) return false;
+    float* out = static_cast<float*>(host);
+    for (size_t i = 0; i < v.count; ++i) out[i] = staging[i * v.stride + v.component];
+    return true;
+}
+
+bool Scene::setField(int field, const void* host, size_t bytes, std::string& err) {
+    float* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
+    FieldView v;
+    if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_, bgra_,
+                   cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
+        err = "unknown field id";
+        return false;
+    }
+    if (bytes != v.count * v.width * 4) {
+        err = "field size mismatch";
+        return false;
+    }
+    if (!check("field sync", cudaStreamSynchronize(stream), err)) return false;
+    if (v.width == v.stride) {
+        return check("cudaMemcpy field", cudaMemcpy(v.base, host, bytes, cudaMemcpyHostToDevice), err);
+    }
+    std::vector<float> staging(v.count * v.stride);
+    if (!check("cudaMemcpy field", cudaMemcpy(staging.data(), v.base, staging.size() * 4, cudaMemcpyDeviceToHost), err)) return false;
+    const float* in = static_cast<const float*>(host);
+    for (size_t i = 0; i < v.count; ++i) staging[i * v.stride + v.component] = in[i];
+    return check("cudaMemcpy field", cudaMemcpy(v.base, staging.data(), staging.size() * 4, cudaMemcpyHostToDevice), err);
+}
+
+bool Scene::registerHdrSlot(int slot, void* ptr, size_t pitch, int format, std::string& err) {
+    if (slot < 0 || slot >= 4) {
+        err = "HDR buffer slot is outside the supported slot range.";
+        return false;
+    }
+    if (ptr == nullptr) {
+        err = "HDR buffer pointer was null.";
+        return false;
+    }
+    const size_t rowBytes = static_cast<size_t>(frameW) * (format == 1 ? 8 : 16);
+    if ((format != 0 && format != 1) || pitch < rowBytes || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0 || (pitch & 15) != 0) {
+        err = "HDR buffer: format must be 0 or 1, pitch >= width*pixel bytes, pointer and pitch 16-byte aligned";
+        return false;
+    }
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess || attr.type != cudaMemoryTypeDevice || attr.device != device) {
+        cudaGetLastError();
+        err = "HDR buffer must be device memory of the scene's GPU";
+        return false;
+    }
+    slots_[slot] = HdrSlot{ptr, pitch, format};
+    return true;
+}
+
+bool Scene::setActiveSlot(int slot, std::string& err) {
+    if (slot < 0 || slot >= 4 || slots_[slot].ptr == nullptr) {
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "HDR buffer slot %d is not registered.", slot);
+        err = buf;
+        return false;
+    }
+    activeSlot_ = slot;
+    return true;
+}
+
+void Scene::clearSlots() {
+    for (HdrSlot& s : slots_) s = HdrSlot{};
+    activeSlot_ = 0;
+}
+
+bool Scene::synchronize(std::string& err) { return check("cudaStreamSynchronize", cudaStreamSynchronize(stream), err); }
+
+}  // namespace firesim

@@ -1,0 +1,116 @@
+// fire_scene.h -- host-side owner of one fire scene on one GPU.
+//
+// A Scene holds every device buffer of the frame pipeline, its own CUDA
+// stream, the captured SOR graph and the clocks, and runs any contiguous range
+// of the frame's stages with the fusions of the B200 kernels.  The C ABI
+// (fire_abi.cu) is a thin layer over it: the reference's singleton is one
+// Scene.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/fire_cuda.h"
+#include "fire_kernels.h"
+
+namespace firesim {
+
+struct HdrSlot {
+    void* ptr = nullptr;
+    size_t pitchBytes = 0;
+    int format = 0;
+};
+
+// Inputs of the per-scene fuel-bed material table (fuelBedMaterial depends on nothing else).
+struct MaterialKey {
+    int sceneId = -1;
+    float emitterRadius = 0.0f, emitterCenterX = 0.0f, emitterCenterZ = 0.0f;
+    int burnerCenterCount = 0;
+    float burnerX0 = 0.0f, burnerZ0 = 0.0f;
+    bool operator==(const MaterialKey& o) const;
+};
+
+class Scene {
+public:
+    Scene() = default;
+    ~Scene();
+    Scene(const Scene&) = delete;
+    Scene& operator=(const Scene&) = delete;
+
+    bool init(int device, int frameW, int frameH, int nx, int ny, int nz, std::string& err);
+
+    // The reference's settings clamps (src/fire_cuda.cu:3135-3179) and the
+    // host-computed camera basis (:2696-2704).
+    FrameParams paramsFrom(const FireSettings& s, float time) const;
+    // makeParams() defaults of the reference (src/fire_cuda.cu:2655-2694), used by fireCudaReset.
+    FrameParams defaultParams(float time) const;
+
+    bool runStages(int first, int last, const FrameParams& p, std::string& err);
+    // One frame with the reference's time bookkeeping (src/fire_cuda.cu:3106-3549).
+    bool frame(uint32_t* hostBgra, const FireSettings& s, FireCudaFrameMetrics* metrics, bool toHdrSlot, bool advance, bool render,
+               std::string& err);
+    bool reset(std::string& err);
+
+    bool getField(int field, void* host, size_t bytes, std::string& err);
+    bool setField(int field, const void* host, size_t bytes, std::string& err);
+    bool registerHdrSlot(int slot, void* ptr, size_t pitch, int format, std::string& err);
+    bool setActiveSlot(int slot, std::string& err);
+    void clearSlots();
+    bool setPressureSolver(int iterations, float omega, std::string& err);
+    bool synchronize(std::string& err);
+    size_t deviceBytes() const { return deviceBytes_; }
+    unsigned long long launchCount() const { return launches_; }
+
+    int nx = 0, ny = 0, nz = 0, lnx = 0, lny = 0, lnz = 0, frameW = 0, frameH = 0, device = 0;
+    float simTime = 0.0f, renderTime = 0.0f;
+    int frameIndex = 0;
+    int pressureIterations = kDefaultPressureIterations;
+    float pressureOmega = kDefaultPressureOmega;
+    cudaStream_t stream = nullptr;
+
+private:
+    bool check(const char* label, cudaError_t e, std::string& err);
+    bool alloc(void** p, size_t bytes, const char* label, std::string& err);
+    void release();
+    ScalarFieldsIn scalarsIn() const;
+    ScalarFields scalarsOut() const;
+    Velocity velocity() const;
+    bool ensureMaterial(const FrameParams& p, std::string& err);
+    bool runSor(const FrameParams& p, std::string& err);
+    bool runMetrics(const FrameParams& p, std::string& err);
+    bool fillMetrics(FireCudaFrameMetrics* out, std::string& err);
+
+    unsigned long long launches_ = 0;
+    size_t cells_ = 0, nu_ = 0, nv_ = 0, nw_ = 0, lightCells_ = 0, pixels_ = 0, deviceBytes_ = 0;
+    float4* sa_[2] = {};
+    float4* sb_[2] = {};
+    float2* sc_[2] = {};
+    int cur_ = 0;
+    float* vel_[3][2] = {};
+    int vcur_ = 0;
+    float* pressure_ = nullptr;
+    float* divergence_ = nullptr;
+    float* divergenceAfter_ = nullptr;
+    float4* contrib_ = nullptr;
+    float* material_ = nullptr;
+    float* breathing_ = nullptr;
+    MaterialKey materialKey_;
+    float4* light_ = nullptr;
+    float4* lightNext_ = nullptr;
+    float* shadow_ = nullptr;
+    float4* hdr_ = nullptr;
+    uint32_t* bgra_ = nullptr;
+    EmberSplat* embers_ = nullptr;
+    MetricPartial* partials_ = nullptr;
+    MetricPartial* metricDevice_ = nullptr;
+    MetricPartial* metricHost_ = nullptr;
+    HdrSlot slots_[4];
+    int activeSlot_ = 0;
+    cudaEvent_t events_[9] = {};
+    cudaGraphExec_t sorExec_ = nullptr;
+    int sorIterations_ = -1;
+    float sorOmega_ = 0.0f;
+};
+
+}  // namespace firesim

@@ -1,0 +1,595 @@
+// fire_sim.cu -- simulation kernels of one frame (sm_100a).
+//
+// Stage map against native-firesim's src/fire_cuda.cu:
+//   resetScalarsKernel            :805-848   -> resetCells (+ fuel-bed tables)
+//   advectU/V/WKernel             :880-932   -> advectVelocity (all three face grids, one launch)
+//   advectReactKernel             :934-1126  -> advectReact (packed records, tabled fuel bed)
+//   forceVelocityKernel           :1128-1183 -> forceContributions + face gathers (no atomics)
+//   velocityBoundaryKernel        :1261-1291 -> velocityBoundary / fused into forceProject
+//   divergenceKernel              :1185-1199 -> divergence / fused into forceProject
+//   sorPressureParityKernel       :1201-1227 -> sorHalfSweep
+//   subtractPressureKernel        :1229-1245 -> subtractWall (fused with the wall zeroing)
+//   velocityWallBoundaryKernel    :1293-1317
+#include "fire_kernels.h"
+
+namespace firesim {
+
+namespace {
+
+__device__ __forceinline__ int uAt(const Grid& g, int x, int y, int z) { return (z * g.ny + y) * (g.nx + 1) + x; }
+__device__ __forceinline__ int vAt(const Grid& g, int x, int y, int z) { return (z * (g.ny + 1) + y) * g.nx + x; }
+__device__ __forceinline__ int wAt(const Grid& g, int x, int y, int z) { return (z * g.ny + y) * g.nx + x; }
+__device__ __forceinline__ int sAt(const Grid& g, int x, int y, int z) { return (z * g.ny + y) * g.nx + x; }
+__device__ __forceinline__ int sClamped(const Grid& g, int x, int y, int z) {
+    x = min(max(x, 0), g.nx - 1);
+    y = min(max(y, 0), g.ny - 1);
+    z = min(max(z, 0), g.nz - 1);
+    return (z * g.ny + y) * g.nx + x;
+}
+
+__device__ __forceinline__ float worldXOf(int x, int nx) { return (cellCoord(x, nx) - 0.50f) * 2.10f; }
+__device__ __forceinline__ float worldZOf(int z, int nz) { return (cellCoord(z, nz) - 0.50f) * 1.64f; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Fuel-bed tables: material(x, z) per scene, breathing(x, z, time) per frame.
+__global__ void __launch_bounds__(256) fuelBedTables(float* __restrict__ material, float* __restrict__ breathing,
+                                                     FrameParams p, int withMaterial) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y;
+    if (x >= p.nx || z >= p.nz) {
+        return;
+    }
+    const float wx = worldXOf(x, p.nx);
+    const float wz = worldZOf(z, p.nz);
+    if (withMaterial) {
+        material[z * p.nx + x] = fuelBedMaterial(wx, wz, p);
+    }
+    breathing[z * p.nx + x] = emberBreathing(wx, wz, p.time);
+}
+
+// src/fire_cuda.cu:805-848 -- procedural initial state of every cell.
+__global__ void __launch_bounds__(256) resetCells(ScalarFields out, float* __restrict__ pressure, float* __restrict__ divergence,
+                                                  float* __restrict__ divergenceAfter, const float* __restrict__ material,
+                                                  const float* __restrict__ breathing, FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) {
+        return;
+    }
+    const Grid g{p.nx, p.ny, p.nz};
+    const int idx = sAt(g, x, y, z);
+    const float v = cellCoord(y, p.ny);
+    const float worldX = worldXOf(x, p.nx);
+    const float worldZ = worldZOf(z, p.nz);
+    const float mat = __ldg(material + z * p.nx + x);
+    const float chunkNoise = fbm(worldX * 18.0f + worldZ * 2.0f, worldZ * 22.0f - worldX * 5.0f);
+    const float bed = fuelBedSourceFrom(mat, __ldg(breathing + z * p.nx + x), v, p);
+    const int sc = p.sceneId;
+    const float charScale = sc == 2 ? 0.004f : (sc == 1 ? 1.18f : 1.0f);
+    const float sootScale = sc == 2 ? 0.004f : (sc == 1 ? 0.92f : 1.0f);
+    const float heat = bed * (sc == 2 ? 1.34f : (sc == 1 ? 0.78f + chunkNoise * 0.26f : 0.86f + chunkNoise * 0.24f));
+    const float fuel = bed * (sc == 2 ? 1.42f : (sc == 1 ? 1.05f + chunkNoise * 0.30f : 1.08f + chunkNoise * 0.26f));
+    const float soot = bed * (sc == 2 ? 0.00065f : 0.018f) * sootScale;
+    const float charMass = mat * (0.92f + chunkNoise * 0.72f) * charScale;
+    const float ash = mat * (0.018f + smoothstepf(0.56f, 0.86f, chunkNoise) * 0.055f) * (sc == 2 ? 0.10f : 1.0f);
+    const float pyrolysis = bed * (sc == 2 ? 0.018f : (sc == 1 ? 0.060f + chunkNoise * 0.034f : 0.058f + chunkNoise * 0.028f));
+    const float progress = bed * (sc == 2 ? 0.11f : (sc == 1 ? 0.24f : 0.21f));
+    const float turbulence = bed * (sc == 2 ? 0.012f : (sc == 1 ? 0.082f : 0.065f));
+    const float sootOptics = bed * (sc == 2 ? 0.00050f : 0.018f) * sootScale;
+    out.a[idx] = make_float4(heat, fuel, 1.0f, soot);
+    out.b[idx] = make_float4(charMass, ash, pyrolysis, progress);
+    out.c[idx] = make_float2(turbulence, sootOptics);
+    pressure[idx] = 0.0f;
+    divergence[idx] = 0.0f;
+    divergenceAfter[idx] = 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// src/fire_cuda.cu:880-932 -- self-advection of the three face grids.  One
+// thread owns the u, v and w faces that share its (x, y, z) index.
+__global__ void __launch_bounds__(256) advectVelocity(float* __restrict__ uOut, float* __restrict__ vOut, float* __restrict__ wOut,
+                                                      Velocity vel, FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    const Grid g{p.nx, p.ny, p.nz};
+    const float back = p.dt;
+    if (x <= p.nx && y < p.ny && z < p.nz) {
+        float r = 0.0f;
+        if (x != 0 && x != p.nx) {
+            const float fu = static_cast<float>(x) / static_cast<float>(p.nx);
+            const float fv = cellCoord(y, p.ny);
+            const float fw = cellCoord(z, p.nz);
+            const float3 c = sampleVelocity(vel, g, fu, fv, fw);
+            r = sampleU(vel.u, g, fu - c.x * back * kAdvectionScale, fv - c.y * back * kAdvectionScale,
+                        fw - c.z * back * kAdvectionScale) * 0.995f;
+        }
+        uOut[uAt(g, x, y, z)] = r;
+    }
+    if (x < p.nx && y <= p.ny && z < p.nz) {
+        float r = 0.0f;
+        if (y != 0) {
+            const float fu = cellCoord(x, p.nx);
+            const float fv = static_cast<float>(y) / static_cast<float>(p.ny);
+            const float fw = cellCoord(z, p.nz);
+            const float3 c = sampleVelocity(vel, g, fu, fv, fw);
+            r = sampleV(vel.v, g, fu - c.x * back * kAdvectionScale, fv - c.y * back * kAdvectionScale,
+                        fw - c.z * back * kAdvectionScale) * 0.996f;
+        }
+        vOut[vAt(g, x, y, z)] = r;
+    }
+    if (x < p.nx && y < p.ny && z <= p.nz) {
+        float r = 0.0f;
+        if (z != 0 && z != p.nz) {
+            const float fu = cellCoord(x, p.nx);
+            const float fv = cellCoord(y, p.ny);
+            const float fw = static_cast<float>(z) / static_cast<float>(p.nz);
+            const float3 c = sampleVelocity(vel, g, fu, fv, fw);
+            r = sampleW(vel.w, g, fu - c.x * back * kAdvectionScale, fv - c.y * back * kAdvectionScale,
+                        fw - c.z * back * kAdvectionScale) * 0.995f;
+        }
+        wOut[wAt(g, x, y, z)] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MacCormack gathers of the packed records (src/fire_cuda.cu:666-732): the
+// first-order sample and the clamp bounds share the eight corners.
+namespace {
+
+struct PackedSample {
+    float4 a, b;
+    float2 c;
+};
+
+struct PackedBounded {
+    PackedSample value, lo, hi;
+};
+
+__device__ __forceinline__ float4 min4(float4 a, float4 b) {
+    return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
+}
+__device__ __forceinline__ float4 max4(float4 a, float4 b) {
+    return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+}
+__device__ __forceinline__ float2 min2(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+__device__ __forceinline__ float2 max2(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+
+template <class V>
+__device__ __forceinline__ void gatherBounded(const V* __restrict__ f, const Corners& c, int sx, int sy, V& value, V& lo, V& hi);
+
+template <>
+__device__ __forceinline__ void gatherBounded<float4>(const float4* __restrict__ f, const Corners& c, int sx, int sy, float4& value,
+                                                      float4& lo, float4& hi) {
+    const float4 c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
+    const float4 c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
+    const float4 c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
+    const float4 c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
+    const float4 c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
+    const float4 c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
+    const float4 c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
+    const float4 c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
+    value = lerp4(lerp4(lerp4(c000, c100, c.tx), lerp4(c010, c110, c.tx), c.ty),
+                  lerp4(lerp4(c001, c101, c.tx), lerp4(c011, c111, c.tx), c.ty), c.tz);
+    lo = min4(min4(min4(c000, c100), min4(c010, c110)), min4(min4(c001, c101), min4(c011, c111)));
+    hi = max4(max4(max4(c000, c100), max4(c010, c110)), max4(max4(c001, c101), max4(c011, c111)));
+}
+
+template <>
+__device__ __forceinline__ void gatherBounded<float2>(const float2* __restrict__ f, const Corners& c, int sx, int sy, float2& value,
+                                                      float2& lo, float2& hi) {
+    const float2 c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
+    const float2 c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
+    const float2 c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
+    const float2 c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
+    const float2 c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
+    const float2 c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
+    const float2 c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
+    const float2 c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
+    value = lerp2v(lerp2v(lerp2v(c000, c100, c.tx), lerp2v(c010, c110, c.tx), c.ty),
+                   lerp2v(lerp2v(c001, c101, c.tx), lerp2v(c011, c111, c.tx), c.ty), c.tz);
+    lo = min2(min2(min2(c000, c100), min2(c010, c110)), min2(min2(c001, c101), min2(c011, c111)));
+    hi = max2(max2(max2(c000, c100), max2(c010, c110)), max2(max2(c001, c101), max2(c011, c111)));
+}
+
+__device__ __forceinline__ float macCormack(float firstOrder, float lo, float hi, float current, float roundTrip, float blend) {
+    const float corrected = fminf(hi, fmaxf(lo, firstOrder + 0.5f * (current - roundTrip)));
+    return lerpf(firstOrder, corrected, saturate(blend));
+}
+
+}  // namespace
+
+// src/fire_cuda.cu:934-1126 -- advection of the ten scalars plus the reaction network.
+__global__ void __launch_bounds__(128) advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel,
+                                                   const float* __restrict__ material, const float* __restrict__ breathing,
+                                                   FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) {
+        return;
+    }
+    const Grid g{p.nx, p.ny, p.nz};
+    const float u = cellCoord(x, p.nx);
+    const float v = cellCoord(y, p.ny);
+    const float w = cellCoord(z, p.nz);
+    const int idx = sAt(g, x, y, z);
+    const Cell10 cur = loadCell(in, idx);
+    const float currentActivity = cur.heat + cur.fuel * 0.18f + cur.soot * 0.24f + cur.pyrolysis * 0.20f + cur.progress * 0.14f +
+                                  cur.sootOptics * 0.08f + cur.turbulenceEnergy * 0.06f;
+    const float sourceDx = u - p.mouseX;
+    const float sourceDy = v - p.mouseY;
+    const float sourceDz = w - 0.5f;
+    const bool outsideInteractiveSource =
+        p.leftDown == 0 || (sourceDx * sourceDx + sourceDy * sourceDy + sourceDz * sourceDz) > 0.090f;
+    if (v > 0.18f && currentActivity < 0.00035f && cur.charMass < 0.00010f && cur.ash < 0.00010f && outsideInteractiveSource &&
+        p.rightDown == 0) {
+        // Cold-air early out (src/fire_cuda.cu:984-1001).
+        out.a[idx] = make_float4(0.0f, 0.0f, fminf(1.0f, cur.oxygen + (1.0f - cur.oxygen) * p.dt * 0.08f), 0.0f);
+        out.b[idx] = make_float4(cur.charMass, cur.ash, 0.0f, 0.0f);
+        out.c[idx] = make_float2(cur.turbulenceEnergy * fmaxf(0.0f, 1.0f - p.dt * 0.54f), 0.0f);
+        return;
+    }
+    const float3 velHere = sampleVelocity(vel, g, u, v, w);
+    const float prevU = u - velHere.x * p.dt * kAdvectionScale;
+    const float prevV = v - velHere.y * p.dt * kAdvectionScale;
+    const float prevW = w - velHere.z * p.dt * kAdvectionScale;
+    const float3 prevVel = sampleVelocity(vel, g, prevU, prevV, prevW);
+
+    // First-order samples with their clamp bounds, and the forward round trip.
+    const Corners cp = scalarCorners(g, prevU, prevV, prevW);
+    PackedBounded f1;
+    gatherBounded(in.a, cp, g.nx, g.ny, f1.value.a, f1.lo.a, f1.hi.a);
+    gatherBounded(in.b, cp, g.nx, g.ny, f1.value.b, f1.lo.b, f1.hi.b);
+    gatherBounded(in.c, cp, g.nx, g.ny, f1.value.c, f1.lo.c, f1.hi.c);
+    const float fwdU = prevU + prevVel.x * p.dt * kAdvectionScale;
+    const float fwdV = prevV + prevVel.y * p.dt * kAdvectionScale;
+    const float fwdW = prevW + prevVel.z * p.dt * kAdvectionScale;
+    const Corners cf = scalarCorners(g, fwdU, fwdV, fwdW);
+    const float4 rtA = gatherVec(in.a, cf, g.nx, g.ny);
+    const float4 rtB = gatherVec(in.b, cf, g.nx, g.ny);
+    const float2 rtC = gatherVec(in.c, cf, g.nx, g.ny);
+
+    const float antiDiffusion = saturate(0.30f + p.detail * 0.34f);
+    float heat = macCormack(f1.value.a.x, f1.lo.a.x, f1.hi.a.x, cur.heat, rtA.x, antiDiffusion);
+    float fuel = macCormack(f1.value.a.y, f1.lo.a.y, f1.hi.a.y, cur.fuel, rtA.y, antiDiffusion * 0.92f);
+    float oxygen = macCormack(f1.value.a.z, f1.lo.a.z, f1.hi.a.z, cur.oxygen, rtA.z, antiDiffusion * 0.70f);
+    float soot = macCormack(f1.value.a.w, f1.lo.a.w, f1.hi.a.w, cur.soot, rtA.w, antiDiffusion);
+    float charMass = cur.charMass;
+    float ash = cur.ash;
+    float pyrolysisRate = macCormack(f1.value.b.z, f1.lo.b.z, f1.hi.b.z, cur.pyrolysis, rtB.z, antiDiffusion * 0.72f) * 0.55f;
+    float progress = macCormack(f1.value.b.w, f1.lo.b.w, f1.hi.b.w, cur.progress, rtB.w, antiDiffusion * 0.82f);
+    float turbulenceEnergy = macCormack(f1.value.c.x, f1.lo.c.x, f1.hi.c.x, cur.turbulenceEnergy, rtC.x, antiDiffusion * 0.52f);
+    float sootOptics = macCormack(f1.value.c.y, f1.lo.c.y, f1.hi.c.y, cur.sootOptics, rtC.y, antiDiffusion * 0.72f);
+
+    const int sc = p.sceneId;
+    const float worldX = (u - 0.50f) * 2.10f;
+    const float worldZ = (w - 0.50f) * 1.64f;
+    const float mat = __ldg(material + z * p.nx + x);
+    const float sourceNoise = 0.70f + 0.48f * fbm(worldX * 13.0f + worldZ * 3.0f + p.time * 0.38f, v * 31.0f + worldZ * 11.0f);
+    const float exposedChar = saturate(charMass / fmaxf(0.055f, charMass + ash * 1.75f));
+    const float charEdges = smoothstepf(0.06f, 0.78f, mat) * smoothstepf(0.92f, 0.02f, ash);
+    const float gasFeed = sc == 2 ? 1.18f : exposedChar * charEdges;
+    const float scenePyrolysisGain = sc == 2 ? 0.42f : (sc == 1 ? 1.34f : 1.0f);
+    const float sceneFuelGain = sc == 2 ? 0.46f : (sc == 1 ? 1.18f : 1.0f);
+    const float sceneHeatGain = sc == 2 ? 1.18f : (sc == 1 ? 1.08f : 1.0f);
+    const float sceneSootGain = sc == 2 ? 0.18f : (sc == 1 ? 1.22f : 1.0f);
+    const float bed = fuelBedSourceFrom(mat, __ldg(breathing + z * p.nx + x), v, p) * sourceNoise * gasFeed * p.intensity;
+    const float ambientK = 293.0f;
+    float tempK = ambientK + heat * 335.0f;
+    const float radiativeFeedback = smoothstepf(430.0f, 980.0f, tempK);
+    const float solidOxygen = saturate(oxygen * 1.28f - soot * 0.030f);
+    const float heatFlux = saturate((tempK - 405.0f) / 900.0f) + bed * 0.34f + sootOptics * 0.024f;
+    const float charRelease = fminf(charMass, charMass * heatFlux * solidOxygen * (0.14f + radiativeFeedback * 1.38f) * p.dt);
+    pyrolysisRate += (bed * (0.34f + radiativeFeedback * 1.05f) * p.dt + charRelease * (2.45f + sourceNoise * 0.72f)) * scenePyrolysisGain;
+    charMass += mat * p.dt * (sc == 2 ? 0.00005f : (sc == 1 ? 0.050f : 0.026f));
+    charMass -= charRelease * 0.92f;
+    ash += charRelease * (sc == 2 ? 0.025f : 0.16f + 0.22f * saturate(1.0f - oxygen));
+
+    heat += (bed * (sc == 2 ? 10.40f : 6.20f) * p.dt * (1.0f + radiativeFeedback * 1.12f) + charRelease * 3.35f) * sceneHeatGain;
+    fuel += pyrolysisRate * (sc == 2 ? 1.34f : 3.70f) * sceneFuelGain;
+    soot += pyrolysisRate * (0.090f + ash * 0.032f + saturate(1.0f - oxygen) * 0.13f) * p.smokeGain *
+            (sc == 2 ? 0.010f : (sc == 1 ? 0.92f : 1.0f)) * sceneSootGain;
+
+    if (p.leftDown != 0) {
+        const float mx = p.mouseX;
+        const float my = p.mouseY;
+        const float source = expf(-((u - mx) * (u - mx)) / 0.0180f - ((w - 0.5f) * (w - 0.5f)) / 0.0550f - ((v - my) * (v - my)) / 0.0020f);
+        heat += source * p.dt * 2.8f;
+        fuel += source * p.dt * 1.4f;
+        pyrolysisRate += source * p.dt * 0.45f;
+        progress += source * p.dt * 0.75f;
+        turbulenceEnergy += source * p.dt * 0.28f;
+        oxygen = fmaxf(oxygen, 0.72f + source * 0.20f);
+    }
+    if (p.rightDown != 0) {
+        const float source =
+            expf(-((u - p.mouseX) * (u - p.mouseX) + (w - 0.5f) * (w - 0.5f)) / 0.0100f - (v - p.mouseY) * (v - p.mouseY) / 0.0100f);
+        soot += source * p.dt * 8.0f;
+        heat *= 1.0f - source * p.dt * 1.2f;
+        fuel *= 1.0f - source * p.dt * 0.7f;
+    }
+
+    tempK = ambientK + heat * 335.0f;
+    const float thermalActivation = smoothstepf(575.0f, 1220.0f, tempK);
+    const float arrhenius = expf(-3800.0f / fmaxf(640.0f, tempK));
+    const float oxygenLimited = fminf(fuel, oxygen * 1.42f);
+    const float burnMass = fminf(oxygenLimited, oxygenLimited * thermalActivation * arrhenius * (118.0f + p.intensity * 34.0f) * p.dt);
+    const float incomplete = saturate(1.0f - oxygen * 1.30f + fuel * 0.065f + soot * 0.015f);
+    const float heatRelease = burnMass * 7.0f;
+    const float sootYield = burnMass * (0.035f + incomplete * 0.34f) * p.smokeGain * (sc == 2 ? 0.006f : (sc == 1 ? 0.96f : 1.0f));
+    const float sootOxidation = soot * oxygen * smoothstepf(760.0f, 1540.0f, tempK) * p.dt * 0.82f;
+    const float frontProduction = burnMass * (9.8f + turbulenceEnergy * 3.4f) + pyrolysisRate * 0.70f + charRelease * 2.10f;
+    const float boundaryAir = smoothstepf(0.70f, 0.96f, v) + smoothstepf(0.11f, 0.03f, u) + smoothstepf(0.89f, 0.97f, u) +
+                              smoothstepf(0.11f, 0.03f, w) + smoothstepf(0.89f, 0.97f, w);
+    const float upperEntrainment = smoothstepf(0.52f, 0.98f, v);
+
+    heat += heatRelease;
+    fuel -= burnMass * 1.20f;
+    oxygen -= burnMass * 0.98f;
+    soot += sootYield;
+    soot -= sootOxidation;
+    progress += frontProduction;
+    progress *= expf(-p.dt * (0.72f + v * 0.45f + oxygen * 0.16f + saturate(boundaryAir) * 1.05f + upperEntrainment * 0.26f));
+
+    oxygen = lerpf(oxygen, 1.0f, saturate(boundaryAir) * p.dt * 1.7f);
+    oxygen += (1.0f - oxygen) * p.dt * 0.08f;
+
+    tempK = ambientK + heat * 335.0f;
+    const float radiationBase = fmaxf(0.0f, (tempK - ambientK) / 1560.0f);
+    const float radiationSq = radiationBase * radiationBase;
+    const float radiationLoss = radiationSq * radiationSq;
+    heat -= radiationLoss * p.dt * (0.88f + soot * 0.085f + sootOptics * 0.018f);
+    heat *= expf(-p.dt * (0.31f + v * 0.64f + soot * 0.022f + saturate(boundaryAir) * 0.26f + upperEntrainment * 0.18f));
+    fuel *= expf(-p.dt * (0.58f + heat * 0.20f + v * 0.92f + saturate(boundaryAir) * 0.18f));
+    soot *= expf(-p.dt * (0.060f + v * 0.092f + oxygen * 0.028f + saturate(boundaryAir) * 0.96f + upperEntrainment * 0.22f));
+    pyrolysisRate *= expf(-p.dt * (1.55f + v * 0.58f + saturate(boundaryAir) * 0.18f));
+
+    const float uL = __ldg(vel.u + uAt(g, x, y, z));
+    const float uR = __ldg(vel.u + uAt(g, x + 1, y, z));
+    const float vD = __ldg(vel.v + vAt(g, x, y, z));
+    const float vU = __ldg(vel.v + vAt(g, x, y + 1, z));
+    const float wB = __ldg(vel.w + wAt(g, x, y, z));
+    const float wF = __ldg(vel.w + wAt(g, x, y, z + 1));
+    const float shear = fabsf(uR - uL) + fabsf(vU - vD) + fabsf(wF - wB);
+    const float flameActivity = saturate(progress * 0.64f + burnMass * 5.2f + heat * 0.065f);
+    turbulenceEnergy += p.dt * (shear * (0.72f + progress * 0.06f) + flameActivity * p.turbulence * 0.62f + frontProduction * 0.085f + soot * 0.018f);
+    turbulenceEnergy *= expf(-p.dt * (0.54f + v * 0.24f + saturate(boundaryAir) * 0.42f + upperEntrainment * 0.16f));
+    const float particleGrowth =
+        saturate(incomplete * 0.36f + ash * 0.13f + soot * 0.055f + smoothstepf(0.65f, 1.55f, tempK / 1000.0f) * 0.18f);
+    sootOptics = soot * (1.04f + 0.28f * sqrtf(fmaxf(0.0f, heat)) + 0.24f * ash + 0.46f * particleGrowth);
+    sootOptics = lerpf(sootOptics, sootOptics * 0.48f, saturate(sootOxidation * 0.92f));
+
+    out.a[idx] = make_float4(fminf(8.8f, fmaxf(0.0f, heat)), fminf(5.5f, fmaxf(0.0f, fuel)), fminf(1.0f, fmaxf(0.0f, oxygen)),
+                             fminf(7.4f, fmaxf(0.0f, soot)));
+    out.b[idx] = make_float4(fminf(2.8f, fmaxf(0.0f, charMass)), fminf(1.9f, fmaxf(0.0f, ash)), fminf(3.6f, fmaxf(0.0f, pyrolysisRate)),
+                             fminf(3.4f, fmaxf(0.0f, progress)));
+    out.c[idx] = make_float2(fminf(4.2f, fmaxf(0.0f, turbulenceEnergy)), fminf(10.0f, fmaxf(0.0f, sootOptics)));
+}
+
+// ---------------------------------------------------------------------------
+// src/fire_cuda.cu:1128-1183 -- per-cell forcing.  Every face is read before
+// any force is added; the per-cell increments go to `contrib` and the faces
+// gather them (lower cell first), which makes the result deterministic.
+__global__ void __launch_bounds__(128) forceContributions(float4* __restrict__ contrib, ScalarFieldsIn s, Velocity vel, FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) {
+        return;
+    }
+    const Grid g{p.nx, p.ny, p.nz};
+    const int idx = sAt(g, x, y, z);
+    const float4 here = __ldg(s.a + idx);
+    const float h = here.x;
+    const float sv = here.w;
+    const float k = __ldg(&s.c[idx].x);
+    const float c = __ldg(&s.b[idx].w);
+    const float u = cellCoord(x, p.nx);
+    const float v = cellCoord(y, p.ny);
+    const float w = cellCoord(z, p.nz);
+    auto heatAt = [&](int xx, int yy, int zz) { return __ldg(&s.a[sClamped(g, xx, yy, zz)].x); };
+    const float gradX = heatAt(x + 1, y, z) - heatAt(x - 1, y, z);
+    const float gradY = heatAt(x, y + 1, z) - heatAt(x, y - 1, z);
+    const float gradZ = heatAt(x, y, z + 1) - heatAt(x, y, z - 1);
+    const float uL = __ldg(vel.u + uAt(g, x, y, z));
+    const float uR = __ldg(vel.u + uAt(g, x + 1, y, z));
+    const float vD = __ldg(vel.v + vAt(g, x, y, z));
+    const float vU = __ldg(vel.v + vAt(g, x, y + 1, z));
+    const float wB = __ldg(vel.w + wAt(g, x, y, z));
+    const float wF = __ldg(vel.w + wAt(g, x, y, z + 1));
+    const float curlX = (wF - wB) - (vU - vD);
+    const float curlY = (uR - uL) - (wF - wB);
+    const float curlZ = (vU - vD) - (uR - uL);
+    const float curlMagnitude = fabsf(curlX) + fabsf(curlY) + fabsf(curlZ);
+    const float curlNoiseA = fbm(u * 9.0f + w * 3.7f + p.time * 0.22f, v * 13.0f - p.time * 0.31f) - 0.5f;
+    const float curlNoiseB = fbm(w * 10.0f - p.time * 0.19f, u * 8.0f + v * 5.5f + p.time * 0.27f) - 0.5f;
+    const float thermalActivity = smoothstepf(0.04f, 4.20f, h + sv * 0.28f);
+    const float upperDrag = smoothstepf(0.26f, 0.94f, v);
+    const float lesGain = sqrtf(fmaxf(0.0f, k)) * (0.30f + c * 0.54f);
+    const int sc = p.sceneId;
+    const float sceneCurlScale = sc == 2 ? 0.38f : (sc == 1 ? 1.18f : 1.0f);
+    const float sceneBuoyancyScale = sc == 2 ? 0.42f : (sc == 1 ? 1.06f : 1.0f);
+    const float curlGain = p.turbulence * sceneCurlScale * (0.18f + thermalActivity * 0.82f + lesGain * 1.12f);
+    const float vortexGain = p.turbulence * sceneCurlScale * thermalActivity * saturate(curlMagnitude * 0.46f) * 0.68f;
+    const float buoyancyFade = sc == 2 ? smoothstepf(0.24f, 0.035f, v) : smoothstepf(0.96f, 0.08f, v);
+    const float verticalVelocity = 0.5f * (vD + vU);
+    const float verticalDamping = verticalVelocity * (0.10f + upperDrag * 0.72f + sv * 0.020f);
+    const float buoyancy =
+        h * sceneBuoyancyScale * (1.62f + p.turbulence * 0.34f + c * 0.16f) * buoyancyFade - sv * 0.095f - gradY * 0.18f - verticalDamping;
+    const float dv = p.dt * (buoyancy + curlY * vortexGain * 0.22f);
+    const float du = p.dt * (p.wind * (0.34f + v * 0.96f) + (-gradZ * 1.36f + curlNoiseA * (0.20f + upperDrag * 0.16f) + curlX * vortexGain) * curlGain);
+    const float dw = p.dt * ((gradX * 1.36f + curlNoiseB * (0.20f + upperDrag * 0.16f) + curlZ * vortexGain) * curlGain);
+    contrib[idx] = make_float4(du, dv, dw, 0.0f);
+}
+
+namespace {
+
+// Velocity of one face after the force gather and, optionally, the boundary
+// clamp of src/fire_cuda.cu:1261-1291.
+__device__ __forceinline__ float forcedU(const float* __restrict__ u, const float4* __restrict__ contrib, const Grid& g, int x, int y,
+                                         int z, bool clampWalls) {
+    float val = __ldg(u + uAt(g, x, y, z));
+    if (x > 0) val += __ldg(&contrib[sAt(g, x - 1, y, z)].x);
+    if (x < g.nx) val += __ldg(&contrib[sAt(g, x, y, z)].x);
+    if (clampWalls) val = (x == 0 || x == g.nx) ? 0.0f : fminf(4.0f, fmaxf(-4.0f, val));
+    return val;
+}
+__device__ __forceinline__ float forcedV(const float* __restrict__ v, const float4* __restrict__ contrib, const Grid& g, int x, int y,
+                                         int z, bool clampWalls) {
+    float val = __ldg(v + vAt(g, x, y, z));
+    if (y > 0) val += __ldg(&contrib[sAt(g, x, y - 1, z)].y);
+    if (clampWalls) val = y == 0 ? 0.0f : fminf(6.4f, fmaxf(-0.9f, val));
+    return val;
+}
+__device__ __forceinline__ float forcedW(const float* __restrict__ w, const float4* __restrict__ contrib, const Grid& g, int x, int y,
+                                         int z, bool clampWalls) {
+    float val = __ldg(w + wAt(g, x, y, z));
+    if (z > 0) val += __ldg(&contrib[sAt(g, x, y, z - 1)].z);
+    if (z < g.nz) val += __ldg(&contrib[sAt(g, x, y, z)].z);
+    if (clampWalls) val = (z == 0 || z == g.nz) ? 0.0f : fminf(4.0f, fmaxf(-4.0f, val));
+    return val;
+}
+
+}  // namespace
+
+// The force gather alone (stage "force"): every face adds its cells' increments.
+__global__ void __launch_bounds__(256) forceApply(float* __restrict__ uOut, float* __restrict__ vOut, float* __restrict__ wOut,
+                                                  const float4* __restrict__ contrib, Velocity vel, FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    const Grid g{p.nx, p.ny, p.nz};
+    if (x <= p.nx && y < p.ny && z < p.nz) uOut[uAt(g, x, y, z)] = forcedU(vel.u, contrib, g, x, y, z, false);
+    if (x < p.nx && y <= p.ny && z < p.nz) vOut[vAt(g, x, y, z)] = forcedV(vel.v, contrib, g, x, y, z, false);
+    if (x < p.nx && y < p.ny && z <= p.nz) wOut[wAt(g, x, y, z)] = forcedW(vel.w, contrib, g, x, y, z, false);
+}
+
+// Fused force gather + boundary clamp + divergence (+ pressure reset): one cell
+// per thread computes its six faces, writes the faces it owns (lower faces, and
+// the upper ones on the last layer) and div = -(sum of differences).
+__global__ void __launch_bounds__(256) forceProjectSetup(float* __restrict__ uOut, float* __restrict__ vOut, float* __restrict__ wOut,
+                                                         float* __restrict__ divergence, float* __restrict__ pressure,
+                                                         const float4* __restrict__ contrib, Velocity vel, FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) {
+        return;
+    }
+    const Grid g{p.nx, p.ny, p.nz};
+    const float uL = forcedU(vel.u, contrib, g, x, y, z, true);
+    const float uR = forcedU(vel.u, contrib, g, x + 1, y, z, true);
+    const float vD = forcedV(vel.v, contrib, g, x, y, z, true);
+    const float vU = forcedV(vel.v, contrib, g, x, y + 1, z, true);
+    const float wB = forcedW(vel.w, contrib, g, x, y, z, true);
+    const float wF = forcedW(vel.w, contrib, g, x, y, z + 1, true);
+    uOut[uAt(g, x, y, z)] = uL;
+    vOut[vAt(g, x, y, z)] = vD;
+    wOut[wAt(g, x, y, z)] = wB;
+    if (x == p.nx - 1) uOut[uAt(g, x + 1, y, z)] = uR;
+    if (y == p.ny - 1) vOut[vAt(g, x, y + 1, z)] = vU;
+    if (z == p.nz - 1) wOut[wAt(g, x, y, z + 1)] = wF;
+    const float div = uR - uL + vU - vD + wF - wB;
+    const int idx = sAt(g, x, y, z);
+    divergence[idx] = -div;
+    pressure[idx] = 0.0f;
+}
+
+// src/fire_cuda.cu:1261-1317 -- wall zeroing, with (clampValues) or without the value clamps.
+__global__ void __launch_bounds__(256) velocityBoundary(float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                                                        FrameParams p, int clampValues) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    const Grid g{p.nx, p.ny, p.nz};
+    if (x <= p.nx && y < p.ny && z < p.nz) {
+        float& f = u[uAt(g, x, y, z)];
+        if (x == 0 || x == p.nx) f = 0.0f;
+        else if (clampValues) f = fminf(4.0f, fmaxf(-4.0f, f));
+    }
+    if (x < p.nx && y <= p.ny && z < p.nz) {
+        float& f = v[vAt(g, x, y, z)];
+        if (y == 0) f = 0.0f;
+        else if (clampValues) f = fminf(6.4f, fmaxf(-0.9f, f));
+    }
+    if (x < p.nx && y < p.ny && z <= p.nz) {
+        float& f = w[wAt(g, x, y, z)];
+        if (z == 0 || z == p.nz) f = 0.0f;
+        else if (clampValues) f = fminf(4.0f, fmaxf(-4.0f, f));
+    }
+}
+
+// src/fire_cuda.cu:1185-1199 / :1247-1259.
+__global__ void __launch_bounds__(256) divergenceOf(float* __restrict__ divergence, float* __restrict__ pressureOrNull, Velocity vel,
+                                                    FrameParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) {
+        return;
+    }
+    const Grid g{p.nx, p.ny, p.nz};
+    const float div = __ldg(vel.u + uAt(g, x + 1, y, z)) - __ldg(vel.u + uAt(g, x, y, z)) + __ldg(vel.v + vAt(g, x, y + 1, z)) -
+                      __ldg(vel.v + vAt(g, x, y, z)) + __ldg(vel.w + wAt(g, x, y, z + 1)) - __ldg(vel.w + wAt(g, x, y, z));
+    const int idx = sAt(g, x, y, z);
+    divergence[idx] = -div;
+    if (pressureOrNull != nullptr) pressureOrNull[idx] = 0.0f;
+}
+
+// src/fire_cuda.cu:1201-1227 -- one colour of in-place red-black SOR.  Thread
+// (i, y, z) owns cell x = 2i + ((parity ^ y ^ z) & 1); walls are Neumann
+// through the clamped neighbour index.
+__global__ void __launch_bounds__(256) sorHalfSweep(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g, int parity,
+                                                    float omega) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    const int x = 2 * i + ((parity ^ y ^ z) & 1);
+    if (x >= g.nx) {
+        return;
+    }
+    const int idx = sAt(g, x, y, z);
+    const int row = idx - x;
+    const float pL = pressure[row + max(x - 1, 0)];
+    const float pR = pressure[row + min(x + 1, g.nx - 1)];
+    const float pD = pressure[sAt(g, x, max(y - 1, 0), z)];
+    const float pU = pressure[sAt(g, x, min(y + 1, g.ny - 1), z)];
+    const float pB = pressure[sAt(g, x, y, max(z - 1, 0))];
+    const float pF = pressure[sAt(g, x, y, min(z + 1, g.nz - 1))];
+    const float self = pressure[idx];
+    const float projected = (__ldg(divergence + idx) + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
+    pressure[idx] = self + omega * (projected - self);
+}
+
+// src/fire_cuda.cu:1229-1245 + :1293-1317 -- u -= grad p on interior faces,
+// then the wall faces are zeroed (doSubtract / doWalls select either half).
+__global__ void __launch_bounds__(256) subtractWall(float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                                                    const float* __restrict__ pressure, FrameParams p, int doSubtract, int doWalls) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) {
+        return;
+    }
+    const Grid g{p.nx, p.ny, p.nz};
+    const int idx = sAt(g, x, y, z);
+    if (doSubtract) {
+        const float pc = __ldg(pressure + idx);
+        if (x > 0) u[uAt(g, x, y, z)] -= pc - __ldg(pressure + idx - 1);
+        if (y > 0) v[vAt(g, x, y, z)] -= pc - __ldg(pressure + idx - g.nx);
+        if (z > 0) w[wAt(g, x, y, z)] -= pc - __ldg(pressure + idx - g.nx * g.ny);
+    }
+    if (doWalls) {
+        if (x == 0) u[uAt(g, 0, y, z)] = 0.0f;
+        if (x == p.nx - 1) u[uAt(g, p.nx, y, z)] = 0.0f;
+        if (y == 0) v[vAt(g, x, 0, z)] = 0.0f;
+        if (z == 0) w[wAt(g, x, y, 0)] = 0.0f;
+        if (z == p.nz - 1) w[wAt(g, x, y, p.nz)] = 0.0f;
+    }
+}
+
+}  // namespace firesim

@@ -1,0 +1,199 @@
+"""ctypes binding over libfiresim_b200.so, the sm_100a frame pipeline.
+
+`FireSim` drives the library's singleton scene through the same entry points
+a native-firesim caller uses (fireCudaInitialize, fireCudaStepAndRender,
+fireCudaStepAndRenderMeasured, the *D3D11 family with a device HDR buffer, ...)
+plus the extensions of include/fire_ext.h.  Every call raises FireSimError
+with fireCudaLastError() when the library returns false.  There is no CPU
+fallback: without the built library or without a CUDA device, construction
+fails.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libfiresim_b200.so"
+
+
+class FireSimError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Loads the in-tree library (build it with native-firesim_b200/build.py)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise FireSimError(f"{LIB_PATH} is missing: run `python native-firesim_b200/build.py` first")
+    L = ctypes.CDLL(str(LIB_PATH))
+    S = ctypes.POINTER(abi.FireSettings)
+    M = ctypes.POINTER(abi.FireCudaFrameMetrics)
+    b = ctypes.c_bool
+    sig = {
+        "fireCudaInitialize": (b, [ctypes.c_int] * 4),
+        "fireCudaInitializeGrid": (b, [ctypes.c_int] * 5),
+        "fireCudaStepAndRender": (b, [ctypes.c_void_p, S]),
+        "fireCudaStepAndRenderMeasured": (b, [ctypes.c_void_p, S, M]),
+        "fireCudaSelectDeviceForD3D11": (b, [ctypes.c_void_p]),
+        "fireCudaRegisterD3D11Texture": (b, [ctypes.c_void_p]),
+        "fireCudaRegisterD3D11TextureSlot": (b, [ctypes.c_int, ctypes.c_void_p]),
+        "fireCudaSetD3D11TextureSlot": (b, [ctypes.c_int]),
+        "fireCudaStepD3D11": (b, [S]),
+        "fireCudaStepAndRenderD3D11": (b, [S]),
+        "fireCudaStepAndRenderD3D11Measured": (b, [S, M]),
+        "fireCudaRenderD3D11": (b, [S]),
+        "fireCudaUnregisterD3D11Texture": (None, []),
+        "fireCudaSynchronize": (b, []),
+        "fireCudaReset": (b, []),
+        "fireCudaGetDiagnostics": (b, [ctypes.POINTER(abi.FireCudaDiagnostics)]),
+        "fireCudaShutdown": (None, []),
+        "fireCudaLastError": (ctypes.c_char_p, []),
+        "fireCudaSelectDevice": (b, [ctypes.c_int]),
+        "fireCudaRegisterHdrBufferSlot": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
+        "fireCudaSetPressureSolver": (b, [ctypes.c_int, ctypes.c_float]),
+        "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
+        "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
+        "fireCudaSetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
+        "fireCudaRunStages": (b, [ctypes.c_int, ctypes.c_int, S, ctypes.c_float]),
+        "fireCudaGetTimes": (b, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]),
+        "fireCudaSetTimes": (b, [ctypes.c_float, ctypes.c_float, ctypes.c_int]),
+        "fireCudaGetStream": (b, [ctypes.POINTER(ctypes.c_void_p)]),
+        "fireCudaGetLaunchCount": (b, [ctypes.POINTER(ctypes.c_ulonglong)]),
+        "fireCudaBuildInfo": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def last_error() -> str:
+    return load_library().fireCudaLastError().decode()
+
+
+class FireSim:
+    """The library's singleton scene on one GPU."""
+
+    def __init__(self, frame_w: int, frame_h: int, nx: int | None = None, ny: int | None = None,
+                 nz: int | None = None, grid_request: tuple[int, int] | None = None):
+        self.lib = load_library()
+        if grid_request is not None:
+            ok = self.lib.fireCudaInitialize(frame_w, frame_h, grid_request[0], grid_request[1])
+        else:
+            ok = self.lib.fireCudaInitializeGrid(frame_w, frame_h, nx, ny, nz)
+        self._check(ok, "initialize")
+        dims = (ctypes.c_int * 8)()
+        self._check(self.lib.fireCudaGetGridInfo(dims), "grid info")
+        self.nx, self.ny, self.nz, lx, ly, lz, self.frame_w, self.frame_h = list(dims)
+        self.light_dims = (lx, ly, lz)
+
+    def _check(self, ok, what):
+        if not ok:
+            raise FireSimError(f"{what}: {last_error()}")
+
+    def close(self):
+        self.lib.fireCudaShutdown()
+
+    # --- the reference's entry points -------------------------------------
+    def step_and_render(self, settings, metrics: bool = False):
+        """fireCudaStepAndRender(Measured): returns (bgra HxW uint32, metrics or None)."""
+        bgra = np.zeros((self.frame_h, self.frame_w), dtype=np.uint32)
+        if metrics:
+            m = abi.FireCudaFrameMetrics()
+            self._check(self.lib.fireCudaStepAndRenderMeasured(bgra.ctypes.data, ctypes.byref(settings), ctypes.byref(m)),
+                        "fireCudaStepAndRenderMeasured")
+            return bgra, m
+        self._check(self.lib.fireCudaStepAndRender(bgra.ctypes.data, ctypes.byref(settings)), "fireCudaStepAndRender")
+        return bgra, None
+
+    def step(self, settings):
+        self._check(self.lib.fireCudaStepD3D11(ctypes.byref(settings)), "fireCudaStepD3D11")
+
+    def step_and_render_hdr(self, settings, metrics: bool = False):
+        if metrics:
+            m = abi.FireCudaFrameMetrics()
+            self._check(self.lib.fireCudaStepAndRenderD3D11Measured(ctypes.byref(settings), ctypes.byref(m)),
+                        "fireCudaStepAndRenderD3D11Measured")
+            return m
+        self._check(self.lib.fireCudaStepAndRenderD3D11(ctypes.byref(settings)), "fireCudaStepAndRenderD3D11")
+        return None
+
+    def render_hdr(self, settings):
+        self._check(self.lib.fireCudaRenderD3D11(ctypes.byref(settings)), "fireCudaRenderD3D11")
+
+    def register_hdr_slot(self, slot: int, device_ptr: int, pitch_bytes: int, fmt: int = 0):
+        self._check(self.lib.fireCudaRegisterHdrBufferSlot(slot, ctypes.c_void_p(device_ptr), pitch_bytes, fmt),
+                    "fireCudaRegisterHdrBufferSlot")
+
+    def set_hdr_slot(self, slot: int):
+        self._check(self.lib.fireCudaSetD3D11TextureSlot(slot), "fireCudaSetD3D11TextureSlot")
+
+    def synchronize(self):
+        self._check(self.lib.fireCudaSynchronize(), "fireCudaSynchronize")
+
+    def reset(self):
+        self._check(self.lib.fireCudaReset(), "fireCudaReset")
+
+    def diagnostics(self) -> abi.FireCudaDiagnostics:
+        d = abi.FireCudaDiagnostics()
+        self._check(self.lib.fireCudaGetDiagnostics(ctypes.byref(d)), "fireCudaGetDiagnostics")
+        return d
+
+    # --- extensions ---------------------------------------------------------
+    def set_pressure_solver(self, iterations: int, omega: float):
+        self._check(self.lib.fireCudaSetPressureSolver(iterations, omega), "fireCudaSetPressureSolver")
+
+    def shape_of(self, name: str):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        lx, ly, lz = self.light_dims
+        return {
+            "u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx),
+            "scene_light": (lz, ly, lx, 4), "scene_shadow": (lz, ly, lx),
+            "hdr": (self.frame_h, self.frame_w, 4), "bgra": (self.frame_h, self.frame_w),
+        }.get(name, (nz, ny, nx))
+
+    def get(self, name: str) -> np.ndarray:
+        dtype = np.uint32 if name == "bgra" else np.float32
+        out = np.empty(self.shape_of(name), dtype=dtype)
+        self._check(self.lib.fireCudaGetField(abi.FIELDS[name], out.ctypes.data, out.nbytes), f"get {name}")
+        return out
+
+    def set(self, name: str, arr: np.ndarray) -> None:
+        dtype = np.uint32 if name == "bgra" else np.float32
+        a = np.ascontiguousarray(arr, dtype=dtype).reshape(self.shape_of(name))
+        self._check(self.lib.fireCudaSetField(abi.FIELDS[name], a.ctypes.data, a.nbytes), f"set {name}")
+
+    def stages(self, first: str, last: str, settings, time: float) -> None:
+        s = abi.STAGES
+        self._check(self.lib.fireCudaRunStages(s[first], s[last], ctypes.byref(settings), time), f"stages {first}..{last}")
+
+    def times(self):
+        t, r, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+        self._check(self.lib.fireCudaGetTimes(ctypes.byref(t), ctypes.byref(r), ctypes.byref(f)), "times")
+        return t.value, r.value, f.value
+
+    def stream(self) -> int:
+        """cudaStream_t of the scene, as an integer handle."""
+        ptr = ctypes.c_void_p()
+        self._check(self.lib.fireCudaGetStream(ctypes.byref(ptr)), "fireCudaGetStream")
+        return int(ptr.value or 0)
+
+    def launch_count(self) -> int:
+        n = ctypes.c_ulonglong()
+        self._check(self.lib.fireCudaGetLaunchCount(ctypes.byref(n)), "fireCudaGetLaunchCount")
+        return int(n.value)
+
+    def set_times(self, sim_time: float, render_time: float, frame_index: int) -> None:
+        self._check(self.lib.fireCudaSetTimes(sim_time, render_time, frame_index), "set times")

@@ -431,6 +431,21 @@ void ref_light_dims(int* dims) {
 
 const char* ref_last_error() { return g_lastError; }
 
+// Host-side parameter block of a frame (camera basis and clamped settings), for
+// comparing host arithmetic; needs no GPU.
+void ref_frame_params(const FireSettings* settings, float time, int frameW, int frameH, float* out16) {
+    const int w = g_frameW, h = g_frameH;
+    g_frameW = frameW;
+    g_frameH = frameH;
+    const SimParams p = refh::paramsFrom(*settings, time);
+    g_frameW = w;
+    g_frameH = h;
+    const float v[16] = {p.cameraEye.x, p.cameraEye.y, p.cameraEye.z, p.cameraForward.x, p.cameraForward.y, p.cameraForward.z,
+                         p.cameraRight.x, p.cameraRight.y, p.cameraRight.z, p.cameraUp.x, p.cameraUp.y, p.cameraUp.z,
+                         p.cameraTanHalfFov, p.cameraAspect, p.time, p.dt};
+    for (int i = 0; i < 16; ++i) out16[i] = v[i];
+}
+
 void ref_shutdown() { fireCudaShutdown(); }
 
 }  // extern "C"

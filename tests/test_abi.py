@@ -1,0 +1,84 @@
+"""The C ABI of libfiresim_b200.so without a GPU: symbols, struct layouts, error paths.
+
+No test here launches device work; the calls exercised return before any CUDA
+call, exactly as the reference's entry points do when uninitialised.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from conftest import ROOT
+
+HEADERS = [ROOT / "include" / "fire_cuda.h", ROOT / "include" / "fire_ext.h"]
+
+
+def declared_symbols() -> set[str]:
+    names = set()
+    for h in HEADERS:
+        names |= set(re.findall(r"^FIRE_API [^(]*?\b(fire\w+)\(", h.read_text(), flags=re.M))
+    return names
+
+
+def test_headers_declare_the_reference_abi():
+    names = declared_symbols()
+    reference = {
+        "fireCudaInitialize", "fireCudaStepAndRender", "fireCudaStepAndRenderMeasured", "fireCudaSelectDeviceForD3D11",
+        "fireCudaRegisterD3D11Texture", "fireCudaRegisterD3D11TextureSlot", "fireCudaSetD3D11TextureSlot",
+        "fireCudaStepD3D11", "fireCudaStepAndRenderD3D11", "fireCudaStepAndRenderD3D11Measured", "fireCudaRenderD3D11",
+        "fireCudaUnregisterD3D11Texture", "fireCudaSynchronize", "fireCudaReset", "fireCudaGetDiagnostics",
+        "fireCudaShutdown", "fireCudaLastError",
+    }
+    assert reference <= names, reference - names
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg.load_library()
+    for name in sorted(declared_symbols()):
+        assert hasattr(lib, name), name
+
+
+def test_struct_layouts(abi):
+    # Byte sizes of the reference structs (src/fire_cuda.h:5-100) on LP64.
+    assert ctypes.sizeof(abi.FireCudaDiagnostics) == 6 * 4 + 8 + 128
+    assert ctypes.sizeof(abi.FireCudaFrameMetrics) == 6 * 4 + 40 * 4
+    assert ctypes.sizeof(abi.FireSettings) == 32 * 4 + 3 * 16
+    assert abi.FireSettings().showGizmos == 1 and abi.FireSettings().raymarchSteps == 56
+
+
+def test_uninitialised_calls_fail_with_reference_messages(pkg, abi):
+    lib = pkg.load_library()
+    lib.fireCudaShutdown()
+    s = abi.FireSettings()
+    buf = (ctypes.c_uint32 * 4)()
+    assert not lib.fireCudaStepAndRender(buf, ctypes.byref(s))
+    assert pkg.firesim.last_error() == "CUDA renderer is not initialized."
+    assert not lib.fireCudaStepAndRenderMeasured(buf, ctypes.byref(s), None)
+    assert pkg.firesim.last_error() == "Metrics output pointer was null."
+    assert not lib.fireCudaReset()
+    assert not lib.fireCudaRunStages(0, 0, ctypes.byref(s), 0.0)
+    assert not lib.fireCudaGetDiagnostics(None)
+    assert pkg.firesim.last_error() == "Diagnostics output pointer was null."
+
+
+def test_d3d11_entry_points_report_headless(pkg):
+    lib = pkg.load_library()
+    assert not lib.fireCudaSelectDeviceForD3D11(ctypes.c_void_p(1))
+    assert "D3D11 unavailable on headless build" in pkg.firesim.last_error()
+    assert not lib.fireCudaRegisterD3D11Texture(ctypes.c_void_p(1))
+    assert not lib.fireCudaRegisterD3D11TextureSlot(0, ctypes.c_void_p(1))
+    assert "fireCudaRegisterHdrBufferSlot" in pkg.firesim.last_error()
+
+
+def test_library_has_no_oracle_dependency():
+    """The product neither links nor names the oracle."""
+    import subprocess
+    lib = ROOT / "native-firesim_b200" / "libfiresim_b200.so"
+    needed = subprocess.run(["readelf", "-d", str(lib)], capture_output=True, text=True).stdout
+    assert "oracle" not in needed and "fire_ref" not in needed
+    for src in (ROOT / "native-firesim_b200").rglob("*"):
+        if src.suffix in (".cu", ".cuh", ".h", ".py", ".cpp"):
+            assert "oracle" not in src.read_text().lower(), src
