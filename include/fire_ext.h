@@ -115,6 +115,33 @@ FIRE_API bool fireCudaGetStream(void** stream);
  * captured graphs are counted one by one). */
 FIRE_API bool fireCudaGetLaunchCount(unsigned long long* count);
 
+/* The force pass (stages FORCE..DIVERGENCE: force increments, their face
+ * gather with the boundary clamps, divergence, pressure reset) on buffers the
+ * caller owns, without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot let a library allocate --
+ * engines that own all device memory through their own arena, frames being
+ * captured into a CUDA graph (cudaMalloc cannot be captured), plugins whose
+ * host forbids allocations after start-up.
+ *
+ * Inputs: the cell records in this library's packed layout (recordsA: float4
+ * heat, fuel, oxygen, soot; recordsB: float4 char, ash, pyrolysis, progress;
+ * recordsC: float2 turbulenceEnergy, sootOptics; nx*ny*nz each, x fastest) and
+ * the MAC faces u, v, w.  Outputs: uOut, vOut, wOut, divergence (nx*ny*nz) and
+ * pressure (set to 0).  All device pointers; work is queued on `stream`
+ * (0 = legacy default stream) and the call returns without synchronising.
+ *
+ * Limit: at most 1,048,576 cells (nx*ny*nz); larger grids are rejected.  The
+ * per-cell increments live in one fixed 16 MiB array that every GPU loading
+ * the library holds until exit.  The first call on each device resolves that
+ * array's device address, so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race.  Each call overwrites the first nx*ny*nz entries before
+ * reading them, so nothing has to be cleared between calls. */
+FIRE_API bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float time, int nx, int ny, int nz,
+                                          const void* recordsA, const void* recordsB, const void* recordsC,
+                                          const float* u, const float* v, const float* w, float* uOut, float* vOut,
+                                          float* wOut, float* divergence, float* pressure, void* stream);
+
 /* Name of the build and its compute capability target, for diagnostics. */
 FIRE_API const char* fireCudaBuildInfo(void);
 

@@ -257,3 +257,9 @@ bool fireCudaGetLaunchCount(unsigned long long* count) {
 const char* fireCudaBuildInfo(void) { return "firesim-b200 sm_100a"; }
 
 }  // extern "C"
+
+namespace firesim {
+// Lets entry points defined in other translation units report through
+// fireCudaLastError().
+void setLastErrorMessage(const char* msg) { fail(msg); }
+}  // namespace firesim

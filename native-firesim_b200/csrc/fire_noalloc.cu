@@ -1,0 +1,102 @@
+// fire_noalloc.cu -- the force pass for callers that cannot allocate device memory.
+//
+// The regular force pass (Scene::runStages, stages FORCE..DIVERGENCE) keeps its
+// per-cell force increments in a buffer the scene allocated with cudaMalloc.
+// Some callers cannot let a library allocate: an engine that owns every byte
+// of device memory through its own arena, a caller capturing its frame into a
+// CUDA graph (cudaMalloc is not capturable), or a plugin whose host forbids
+// third-party allocations after start-up.  fireCudaForceProjectNoAlloc runs
+// the same two kernels (forceContributions, forceProjectSetup) on buffers the
+// caller owns, and keeps the increments in the fixed array below instead.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+
+#include "../../include/fire_ext.h"
+#include "fire_scene.h"
+
+namespace {
+
+// Per-cell force increments (du, dv, dw, unused) for at most kNoAllocMaxCells
+// cells: 16 MiB, held by every GPU that loads the library until the process exits.
+constexpr int kNoAllocMaxCells = 1 << 20;
+static __device__ __align__(256) float4 g_forceScratch[kNoAllocMaxCells];
+
+// Device address of g_forceScratch per device ordinal.  In host code the
+// symbol is only a host-side stand-in, so the address is resolved with
+// cudaGetSymbolAddress on each device, once, while that device is current.
+constexpr int kMaxDevices = 64;
+float4* g_scratchAddress[kMaxDevices] = {};
+
+}  // namespace
+
+namespace firesim {
+void setLastErrorMessage(const char* msg);
+}  // namespace firesim
+
+namespace {
+
+bool fail(const std::string& msg) {
+    firesim::setLastErrorMessage(msg.c_str());
+    return false;
+}
+
+}  // namespace
+
+extern "C" bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float time, int nx, int ny, int nz,
+                                            const void* recordsA, const void* recordsB, const void* recordsC,
+                                            const float* u, const float* v, const float* w, float* uOut, float* vOut,
+                                            float* wOut, float* divergence, float* pressure, void* stream) {
+    if (settings == nullptr || recordsA == nullptr || recordsB == nullptr || recordsC == nullptr || u == nullptr ||
+        v == nullptr || w == nullptr || uOut == nullptr || vOut == nullptr || wOut == nullptr || divergence == nullptr ||
+        pressure == nullptr) {
+        return fail("fireCudaForceProjectNoAlloc: a pointer argument was null.");
+    }
+    if (nx < 2 || ny < 2 || nz < 2) {
+        return fail("fireCudaForceProjectNoAlloc: grid dimensions must be at least 2.");
+    }
+    const long long cells = static_cast<long long>(nx) * ny * nz;
+    if (cells > kNoAllocMaxCells) {
+        char buf[200];
+        std::snprintf(buf, sizeof(buf),
+                      "fireCudaForceProjectNoAlloc: grid of %lld cells exceeds the %d-cell scratch of this entry point.",
+                      cells, kNoAllocMaxCells);
+        return fail(buf);
+    }
+    if ((reinterpret_cast<uintptr_t>(recordsA) & 15) != 0 || (reinterpret_cast<uintptr_t>(recordsB) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(recordsC) & 7) != 0) {
+        return fail("fireCudaForceProjectNoAlloc: records A/B must be 16-byte aligned and records C 8-byte aligned.");
+    }
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= kMaxDevices) return fail("fireCudaForceProjectNoAlloc: device ordinal out of range.");
+    if (g_scratchAddress[device] == nullptr) {
+        void* addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_forceScratch);
+        if (e != cudaSuccess) return fail(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_scratchAddress[device] = static_cast<float4*>(addr);
+    }
+    float4* scratch = g_scratchAddress[device];
+
+    // The settings clamps of a step; Scene allocates nothing until init().
+    firesim::Scene dims;
+    dims.nx = nx;
+    dims.ny = ny;
+    dims.nz = nz;
+    dims.frameW = 1;
+    dims.frameH = 1;
+    const firesim::FrameParams p = dims.paramsFrom(*settings, time);
+    const firesim::ScalarFieldsIn in{static_cast<const float4*>(recordsA), static_cast<const float4*>(recordsB),
+                                     static_cast<const float2*>(recordsC)};
+    const firesim::Velocity vel{u, v, w};
+    const int bx = nx <= 32 ? 32 : (nx <= 64 ? 64 : 128);
+    const dim3 grid((nx + bx - 1) / bx, ny, nz);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    firesim::forceContributions<<<grid, bx, 0, s>>>(scratch, in, vel, p);
+    firesim::forceProjectSetup<<<grid, bx, 0, s>>>(uOut, vOut, wOut, divergence, pressure, scratch, vel, p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(std::string("force pass launch: ") + cudaGetErrorString(e));
+    return true;
+}
