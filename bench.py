@@ -238,7 +238,8 @@ def config_block(args) -> dict:
                         f"{args.frame}x{args.frame} HDR raymarch every {args.render_every} steps "
                         f"({args.samples} samples requested, clamped to 120)",
             "grid": [args.grid] * 3, "frame": [args.frame, args.frame], "sor_iterations": args.sor_iters,
-            "omega": args.omega, "render_every": args.render_every, "settings": "validation harness frames, scene 0",
+            "omega": args.omega, "sor_path": args.sor_path, "render_every": args.render_every,
+            "settings": "validation harness frames, scene 0",
             "l2": "per-step state (~270 MB at 128^3) exceeds the 126 MB L2; no flush", "parallelism": "replicas"}
 
 
@@ -257,6 +258,8 @@ def main() -> int:
     ap.add_argument("--reference-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sor-path", default="auto", choices=["auto", "graph", "resident"],
+                    help="pressure SOR: per-launch half sweeps in a CUDA graph, one cooperative resident launch, or auto")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -275,6 +278,7 @@ def main() -> int:
         raise RuntimeError(pkg.firesim.last_error())
     sim = pkg.FireSim(args.frame, args.frame, args.grid, args.grid, args.grid)
     sim.set_pressure_solver(args.sor_iters, args.omega)
+    sim.set_pressure_path({"auto": 0, "graph": 1, "resident": 2}[args.sor_path])
     hdr = torch.zeros((args.frame, args.frame, 4), dtype=torch.float32, device="cuda")
     sim.register_hdr_slot(0, hdr.data_ptr(), args.frame * 16, 0)
     sim.set_hdr_slot(0)

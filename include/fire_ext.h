@@ -91,6 +91,13 @@ FIRE_API bool fireCudaRegisterHdrBufferSlot(int slot, void* devicePtr, size_t pi
  * (the reference hard-codes 40 and 1.52, src/fire_cuda.cu:104-105). */
 FIRE_API bool fireCudaSetPressureSolver(int iterations, float omega);
 
+/* Execution path of the SOR solve (identical results): 0 = automatic (one
+ * cooperative launch that keeps p and div in shared memory when every brick of
+ * the grid can be co-resident, else one launch per half sweep), 1 = one launch
+ * per half sweep, 2 = shared-memory-resident only (fails if the grid does not
+ * fit). */
+FIRE_API bool fireCudaSetPressurePath(int path);
+
 /* nx, ny, nz, lightNx, lightNy, lightNz, frameWidth, frameHeight. */
 FIRE_API bool fireCudaGetGridInfo(int* dims8);
 

@@ -190,6 +190,13 @@ bool fireCudaSetPressureSolver(int iterations, float omega) {
     return true;
 }
 
+bool fireCudaSetPressurePath(int path) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->setPressurePath(path, err)) return fail(err);
+    return true;
+}
+
 bool fireCudaGetGridInfo(int* dims8) {
     if (!requireScene()) return false;
     if (dims8 == nullptr) return fail("dims pointer was null.");

@@ -23,6 +23,14 @@ struct MetricPartial {
     int invalidCells;
 };
 constexpr int kMetricBlocks = 296;
+
+// Brick decomposition of the shared-memory-resident SOR (sorResident).
+struct ResidentBrick {
+    int bx, by, bz;     // brick extent, all even
+    int kx;             // bx / 2: cells of one colour per brick row
+    int ex, ey, ez;     // colour-plane extents with the one-cell halo: kx + 2, by + 2, bz + 2
+    int nbx, nby, nbz;  // bricks per axis
+};
 constexpr int kMetricThreads = 128;
 
 // fire_sim.cu
@@ -38,6 +46,8 @@ __global__ void forceProjectSetup(float* uOut, float* vOut, float* wOut, float* 
 __global__ void velocityBoundary(float* u, float* v, float* w, FrameParams p, int clampValues);
 __global__ void divergenceOf(float* divergence, float* pressureOrNull, Velocity vel, FrameParams p);
 __global__ void sorHalfSweep(float* pressure, const float* divergence, Grid g, int parity, float omega);
+template <int BX, int BY, int BZ>
+__global__ void sorResident(float* pressure, const float* divergence, Grid g, ResidentBrick r, int iterations, float omega);
 __global__ void subtractWall(float* u, float* v, float* w, const float* pressure, FrameParams p, int doSubtract, int doWalls);
 
 // fire_light.cu

@@ -258,11 +258,85 @@ bool Scene::setPressureSolver(int iterations, float omega, std::string& err) {
     return true;
 }
 
-// src/fire_cuda.cu:3280-3284 -- 2N half sweeps, captured once per (N, omega)
-// into a CUDA graph so a step pays one graph launch instead of 2N launches.
+bool Scene::setPressurePath(int path, std::string& err) {
+    if (path < 0 || path > 2) {
+        err = "pressure path must be 0 (automatic), 1 (per-launch) or 2 (resident)";
+        return false;
+    }
+    pressurePath_ = path;
+    return true;
+}
+
+// Brick plan of the shared-memory-resident SOR: 32x16x16 bricks (256 threads,
+// 78 KB of shared memory, two CTAs per SM), or 16^3 bricks (128 threads, 42 KB)
+// when the larger ones do not fit co-resident; one CTA per brick.
+bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
+    int coop = 0, sms = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const int shapes[2][3] = {{32, 16, 16}, {16, 16, 16}};
+    for (const auto& sh : shapes) {
+        r.bx = sh[0];
+        r.by = sh[1];
+        r.bz = sh[2];
+        r.kx = r.bx / 2;
+        r.ex = r.kx + 2;
+        r.ey = r.by + 2;
+        r.ez = r.bz + 2;
+        r.nbx = (nx + r.bx - 1) / r.bx;
+        r.nby = (ny + r.by - 1) / r.by;
+        r.nbz = (nz + r.bz - 1) / r.bz;
+        threads = r.kx * r.by;
+        smemBytes = (2ull * r.ez * r.ey * r.ex + 2ull * r.bz * r.by * r.kx) * sizeof(float);
+        const void* fn = r.bx == 32 ? reinterpret_cast<const void*>(sorResident<32, 16, 16>)
+                                    : reinterpret_cast<const void*>(sorResident<16, 16, 16>);
+        int perSm = 0;
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemBytes)) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, threads, smemBytes) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        const long long bricks = static_cast<long long>(r.nbx) * r.nby * r.nbz;
+        if (bricks <= static_cast<long long>(perSm) * sms) {
+            return true;
+        }
+    }
+    return false;
+}
+
+// src/fire_cuda.cu:3280-3284 -- 2N half sweeps.  When the grid fits, one
+// cooperative launch keeps p and div in shared memory for all of them
+// (sorResident); otherwise the 2N launches are captured once per (N, omega)
+// into a CUDA graph so a step pays one graph launch.
 bool Scene::runSor(const FrameParams& p, std::string& err) {
     (void)p;
     if (pressureIterations == 0) return true;
+    if (pressurePath_ != 1) {
+        ResidentBrick r;
+        size_t smem = 0;
+        int threads = 0;
+        if (residentPlan(r, smem, threads)) {
+            Grid g{nx, ny, nz};
+            int iterations = pressureIterations;
+            float omega = pressureOmega;
+            void* args[] = {&pressure_, &divergence_, &g, &r, &iterations, &omega};
+            const unsigned bricks = static_cast<unsigned>(r.nbx * r.nby * r.nbz);
+            void* fn = r.bx == 32 ? reinterpret_cast<void*>(sorResident<32, 16, 16>) : reinterpret_cast<void*>(sorResident<16, 16, 16>);
+            if (!check("SOR cooperative launch", cudaLaunchCooperativeKernel(fn, dim3(bricks), dim3(threads), args, smem, stream), err)) {
+                return false;
+            }
+            ++launches_;
+            lastPressurePath_ = 2;
+            return true;
+        }
+        if (pressurePath_ == 2) {
+            err = "resident SOR: the grid does not fit co-resident on this device";
+            return false;
+        }
+    }
     if (sorExec_ == nullptr || sorIterations_ != pressureIterations || sorOmega_ != pressureOmega) {
         if (sorExec_ != nullptr) {
             cudaGraphExecDestroy(sorExec_);
@@ -291,6 +365,7 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
         sorOmega_ = pressureOmega;
     }
     launches_ += 2ull * static_cast<unsigned long long>(pressureIterations);
+    lastPressurePath_ = 1;
     return check("SOR graph launch", cudaGraphLaunch(sorExec_, stream), err);
 }
 

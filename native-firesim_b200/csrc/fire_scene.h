@@ -58,6 +58,9 @@ public:
     bool setActiveSlot(int slot, std::string& err);
     void clearSlots();
     bool setPressureSolver(int iterations, float omega, std::string& err);
+    // 0 = automatic (shared-memory-resident when the grid fits co-resident), 1 = one launch per half sweep, 2 = resident only.
+    bool setPressurePath(int path, std::string& err);
+    int lastPressurePath() const { return lastPressurePath_; }
     bool synchronize(std::string& err);
     size_t deviceBytes() const { return deviceBytes_; }
     unsigned long long launchCount() const { return launches_; }
@@ -108,6 +111,9 @@ private:
     HdrSlot slots_[4];
     int activeSlot_ = 0;
     cudaEvent_t events_[9] = {};
+    bool residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads);
+    int pressurePath_ = 0;
+    int lastPressurePath_ = 0;
     cudaGraphExec_t sorExec_ = nullptr;
     int sorIterations_ = -1;
     float sorOmega_ = 0.0f;

@@ -10,6 +10,8 @@
 //   sorPressureParityKernel       :1201-1227 -> sorHalfSweep
 //   subtractPressureKernel        :1229-1245 -> subtractWall (fused with the wall zeroing)
 //   velocityWallBoundaryKernel    :1293-1317
+#include <cooperative_groups.h>
+
 #include "fire_kernels.h"
 
 namespace firesim {
@@ -591,5 +593,196 @@ __global__ void __launch_bounds__(256) subtractWall(float* __restrict__ u, float
         if (z == p.nz - 1) w[wAt(g, x, y, p.nz)] = 0.0f;
     }
 }
+
+}  // namespace firesim
+
+namespace firesim {
+
+// ---------------------------------------------------------------------------
+// Shared-memory-resident red-black SOR: all 2N half sweeps in one cooperative
+// launch.  Each CTA owns one brick of BX*BY*BZ cells (all even, so a brick's
+// colour pattern equals the global one) and keeps its p and div in shared
+// memory, split by colour: for colour c, row (y, z) holds the cells
+// x = 2k + ((c + y + z) & 1), k = 0..BX/2-1, so a cell's x/y/z-neighbour reads
+// of the other colour are unit-stride.  Thread t owns the column
+// (k = t % KX, y = t / KX) of both colours and walks z.  A half sweep writes
+// its updated face cells straight to global p; after the grid barrier every
+// CTA reads the updated cells of its six neighbours' faces into its one-cell
+// halo, all of a thread's halo loads in flight at once.  Walls are Neumann
+// through the clamped neighbour (the cell itself), as in
+// sorPressureParityKernel.  Per-cell arithmetic is identical to sorHalfSweep,
+// so the result is bit-identical to the per-launch path.
+namespace cg = cooperative_groups;
+
+namespace {
+
+// Halo cells of one colour: both x faces (BY*BZ/2 each), both y faces
+// (KX*BZ each), both z faces (KX*BY each).
+template <int BX, int BY, int BZ>
+struct ResidentShape {
+    static constexpr int KX = BX / 2;
+    static constexpr int EX = KX + 2, EY = BY + 2, EZ = BZ + 2;
+    static constexpr int PLANE = EZ * EY * EX;
+    static constexpr int THREADS = KX * BY;
+    static constexpr int HX = BY * BZ;
+    static constexpr int HY = 2 * KX * BZ;
+    static constexpr int HZ = 2 * KX * BY;
+    static constexpr int HALO = HX + HY + HZ;
+    static constexpr int PER_THREAD = (HALO + THREADS - 1) / THREADS;
+    __device__ static int pidx(int c, int z, int y, int k) { return c * PLANE + ((z + 1) * EY + (y + 1)) * EX + (k + 1); }
+    __device__ static int didx(int c, int z, int y, int k) { return ((c * BZ + z) * BY + y) * KX + k; }
+};
+
+// Global and shared index of halo cell i of colour c, or gi = -1 when the
+// cell lies outside the grid (a wall: the update uses the cell itself).
+template <int BX, int BY, int BZ>
+__device__ __forceinline__ void residentHaloCell(int i, int c, int ox, int oy, int oz, const Grid& g, int& gi, int& si) {
+    using S = ResidentShape<BX, BY, BZ>;
+    int lx, ly, lz, k;
+    if (i < S::HX) {
+        const int side = i / (S::HX / 2);
+        const int r = i % (S::HX / 2);
+        lz = r / (BY / 2);
+        lx = side ? BX : -1;
+        ly = 2 * (r % (BY / 2)) + ((c + lx + lz) & 1);
+        k = side ? S::KX : -1;
+    } else if (i < S::HX + S::HY) {
+        const int j = i - S::HX;
+        const int side = j / (S::KX * BZ);
+        const int r = j % (S::KX * BZ);
+        k = r % S::KX;
+        lz = r / S::KX;
+        ly = side ? BY : -1;
+        lx = 2 * k + ((c + ly + lz) & 1);
+    } else {
+        const int j = i - S::HX - S::HY;
+        const int side = j / (S::KX * BY);
+        const int r = j % (S::KX * BY);
+        k = r % S::KX;
+        ly = r / S::KX;
+        lz = side ? BZ : -1;
+        lx = 2 * k + ((c + ly + lz) & 1);
+    }
+    const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+    si = S::pidx(c, lz, ly, k);
+    gi = (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) ? (gz * g.ny + gy) * g.nx + gx : -1;
+}
+
+}  // namespace
+
+template <int BX, int BY, int BZ>
+__global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g,
+                                                            ResidentBrick r, int iterations, float omega) {
+    using S = ResidentShape<BX, BY, BZ>;
+    constexpr int KX = S::KX;
+    extern __shared__ float smem[];
+    float* planes = smem;                // [2][EZ][EY][EX]
+    float* divs = smem + 2 * S::PLANE;   // [2][BZ][BY][KX]
+    cg::grid_group grid = cg::this_grid();
+    const int brick = blockIdx.x;
+    const int ox = (brick % r.nbx) * BX;
+    const int oy = ((brick / r.nbx) % r.nby) * BY;
+    const int oz = (brick / (r.nbx * r.nby)) * BZ;
+    const int k = threadIdx.x % KX;
+    const int y = threadIdx.x / KX;
+    const int gy = oy + y;
+
+    // This thread's halo cells of each colour, fixed for the whole solve.
+    int haloG[2][S::PER_THREAD], haloS[2][S::PER_THREAD];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+        for (int j = 0; j < S::PER_THREAD; ++j) {
+            const int i = threadIdx.x + j * S::THREADS;
+            haloG[c][j] = -1;
+            haloS[c][j] = 0;
+            if (i < S::HALO) {
+                residentHaloCell<BX, BY, BZ>(i, c, ox, oy, oz, g, haloG[c][j], haloS[c][j]);
+            }
+        }
+    }
+    auto loadHalo = [&](int c) {
+        float v[S::PER_THREAD];
+#pragma unroll
+        for (int j = 0; j < S::PER_THREAD; ++j) {
+            v[j] = haloG[c][j] >= 0 ? __ldcg(pressure + haloG[c][j]) : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < S::PER_THREAD; ++j) {
+            if (haloG[c][j] >= 0) planes[haloS[c][j]] = v[j];
+        }
+    };
+
+    // Load both colours of the brick column, then the halo.
+#pragma unroll 4
+    for (int z = 0; z < BZ; ++z) {
+        const int gz = oz + z;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int gx = ox + 2 * k + ((c + y + z) & 1);
+            if (gx < g.nx && gy < g.ny && gz < g.nz) {
+                const int gi = (gz * g.ny + gy) * g.nx + gx;
+                planes[S::pidx(c, z, y, k)] = __ldcg(pressure + gi);
+                divs[S::didx(c, z, y, k)] = __ldg(divergence + gi);
+            }
+        }
+    }
+    loadHalo(0);
+    loadHalo(1);
+    __syncthreads();
+
+    const bool yFace = y == 0 || y == BY - 1;
+    const bool yIn = gy < g.ny;
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int o = 1 - c;
+            const bool last = it == iterations - 1 && c == 1;
+#pragma unroll
+            for (int z = 0; z < BZ; ++z) {
+                const int s = (c + y + z) & 1;
+                const int x = 2 * k + s;
+                const int gx = ox + x, gz = oz + z;
+                if (gx < g.nx && yIn && gz < g.nz) {
+                    const float self = planes[S::pidx(c, z, y, k)];
+                    const float pL = gx == 0 ? self : planes[S::pidx(o, z, y, k + s - 1)];
+                    const float pR = gx == g.nx - 1 ? self : planes[S::pidx(o, z, y, k + s)];
+                    const float pD = gy == 0 ? self : planes[S::pidx(o, z, y - 1, k)];
+                    const float pU = gy == g.ny - 1 ? self : planes[S::pidx(o, z, y + 1, k)];
+                    const float pB = gz == 0 ? self : planes[S::pidx(o, z - 1, y, k)];
+                    const float pF = gz == g.nz - 1 ? self : planes[S::pidx(o, z + 1, y, k)];
+                    const float d = divs[S::didx(c, z, y, k)];
+                    const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
+                    const float next = self + omega * (projected - self);
+                    planes[S::pidx(c, z, y, k)] = next;
+                    if (!last && (yFace || z == 0 || z == BZ - 1 || x == 0 || x == BX - 1)) {
+                        __stcg(pressure + (gz * g.ny + gy) * g.nx + gx, next);
+                    }
+                }
+            }
+            if (last) {
+                break;
+            }
+            grid.sync();
+            loadHalo(c);
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int z = 0; z < BZ; ++z) {
+        const int gz = oz + z;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int gx = ox + 2 * k + ((c + y + z) & 1);
+            if (gx < g.nx && gy < g.ny && gz < g.nz) {
+                pressure[(gz * g.ny + gy) * g.nx + gx] = planes[S::pidx(c, z, y, k)];
+            }
+        }
+    }
+}
+
+template __global__ void sorResident<32, 16, 16>(float*, const float*, Grid, ResidentBrick, int, float);
+template __global__ void sorResident<16, 16, 16>(float*, const float*, Grid, ResidentBrick, int, float);
 
 }  // namespace firesim

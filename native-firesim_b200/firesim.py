@@ -61,6 +61,7 @@ def load_library() -> ctypes.CDLL:
         "fireCudaSelectDevice": (b, [ctypes.c_int]),
         "fireCudaRegisterHdrBufferSlot": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
         "fireCudaSetPressureSolver": (b, [ctypes.c_int, ctypes.c_float]),
+        "fireCudaSetPressurePath": (b, [ctypes.c_int]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
         "fireCudaSetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -154,6 +155,10 @@ class FireSim:
     # --- extensions ---------------------------------------------------------
     def set_pressure_solver(self, iterations: int, omega: float):
         self._check(self.lib.fireCudaSetPressureSolver(iterations, omega), "fireCudaSetPressureSolver")
+
+    def set_pressure_path(self, path: int):
+        """0 automatic, 1 one launch per half sweep, 2 shared-memory-resident."""
+        self._check(self.lib.fireCudaSetPressurePath(path), "fireCudaSetPressurePath")
 
     def shape_of(self, name: str):
         nx, ny, nz = self.nx, self.ny, self.nz
