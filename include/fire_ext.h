@@ -98,6 +98,19 @@ FIRE_API bool fireCudaSetPressureSolver(int iterations, float omega);
  * fit). */
 FIRE_API bool fireCudaSetPressurePath(int path);
 
+/* Path the latest SOR solve took: 0 = none yet (or no grid), 1 = one launch
+ * per half sweep, 2 = shared-memory-resident. */
+FIRE_API int fireCudaGetPressurePathUsed(void);
+
+/* Failure detection of the shared-memory-resident SOR (no counterpart in the
+ * reference, whose solve is one launch per half sweep).  Each brick waits only
+ * for its face neighbours; every wait gives up after waitUs microseconds
+ * (default 1 s), records the brick and lets the whole solve return, and the
+ * next fireCudaSynchronize (or synchronous step) fails with "timed out".
+ * silentBrick >= 0 injects the fault from the host: that brick never
+ * announces its half sweeps.  Pass (-1, 1000000) to restore the defaults. */
+FIRE_API bool fireCudaSetResidentSorFault(int silentBrick, long long waitUs);
+
 /* nx, ny, nz, lightNx, lightNy, lightNz, frameWidth, frameHeight. */
 FIRE_API bool fireCudaGetGridInfo(int* dims8);
 

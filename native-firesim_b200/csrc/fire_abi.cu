@@ -143,6 +143,8 @@ void fireCudaUnregisterD3D11Texture(void) {
 bool fireCudaSynchronize(void) {
     const cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return fail(std::string("cudaDeviceSynchronize: ") + cudaGetErrorString(e));
+    std::string err;
+    if (g_scene && !g_scene->checkSolverStatus(err)) return fail(err);
     return true;
 }
 
@@ -194,6 +196,15 @@ bool fireCudaSetPressurePath(int path) {
     if (!requireScene()) return false;
     std::string err;
     if (!g_scene->setPressurePath(path, err)) return fail(err);
+    return true;
+}
+
+int fireCudaGetPressurePathUsed(void) { return g_scene ? g_scene->lastPressurePath() : 0; }
+
+bool fireCudaSetResidentSorFault(int silentBrick, long long waitUs) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->setResidentFault(silentBrick, waitUs, err)) return fail(err);
     return true;
 }
 

@@ -27,10 +27,26 @@ constexpr int kMetricBlocks = 296;
 // Brick decomposition of the shared-memory-resident SOR (sorResident).
 struct ResidentBrick {
     int bx, by, bz;     // brick extent, all even
-    int kx;             // bx / 2: cells of one colour per brick row
-    int ex, ey, ez;     // colour-plane extents with the one-cell halo: kx + 2, by + 2, bz + 2
     int nbx, nby, nbz;  // bricks per axis
 };
+// Neighbour-to-neighbour synchronisation of the resident SOR.  Brick b
+// announces that its face cells of half sweep h are in global memory by
+// storing epoch + h + 1 into flags[b * kResidentFlagStride]; its six
+// neighbours wait for that value before reading them.  Every wait gives up
+// after waitNs nanoseconds (or kResidentMaxPolls polls), records epoch + 1 in
+// *status so the other bricks stop waiting too, writes brick + 1 into the
+// host-mapped *hostStatus and returns.  silentBrick >= 0 is a host-side fault
+// injection: that brick never announces, so its neighbours' waits run out.
+struct ResidentSync {
+    unsigned* flags;
+    unsigned* status;
+    unsigned* hostStatus;
+    unsigned epoch;
+    int silentBrick;
+    unsigned long long waitNs;
+};
+constexpr int kResidentFlagStride = 32;  // one 128-byte line per brick
+constexpr unsigned kResidentMaxPolls = 1u << 24;
 constexpr int kMetricThreads = 128;
 
 // fire_sim.cu
@@ -46,8 +62,11 @@ __global__ void forceProjectSetup(float* uOut, float* vOut, float* wOut, float* 
 __global__ void velocityBoundary(float* u, float* v, float* w, FrameParams p, int clampValues);
 __global__ void divergenceOf(float* divergence, float* pressureOrNull, Velocity vel, FrameParams p);
 __global__ void sorHalfSweep(float* pressure, const float* divergence, Grid g, int parity, float omega);
-template <int BX, int BY, int BZ>
-__global__ void sorResident(float* pressure, const float* divergence, Grid g, ResidentBrick r, int iterations, float omega);
+// The sorResident<BX, 16, 16> instantiation for brick width bx (32 or 16),
+// for cudaFuncSetAttribute / cudaLaunchCooperativeKernel.
+const void* sorResidentKernel(int bx);
+// Dynamic shared memory of that instantiation (padded colour planes + div).
+size_t sorResidentSharedBytes(int bx);
 __global__ void subtractWall(float* u, float* v, float* w, const float* pressure, FrameParams p, int doSubtract, int doWalls);
 
 // fire_light.cu

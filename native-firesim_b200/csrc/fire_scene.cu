@@ -66,11 +66,14 @@ void Scene::release() {
     }
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
-                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_};
+                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorSync_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
     if (metricHost_ != nullptr) cudaFreeHost(metricHost_);
+    if (sorHostStatus_ != nullptr) cudaFreeHost(sorHostStatus_);
+    sorSync_ = nullptr;
+    sorHostStatus_ = nullptr;
     for (cudaEvent_t& e : events_) {
         if (e != nullptr) cudaEventDestroy(e);
         e = nullptr;
@@ -141,6 +144,12 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
          alloc(reinterpret_cast<void**>(&partials_), kMetricBlocks * sizeof(MetricPartial), "cudaMalloc metric partials", err) &&
          alloc(reinterpret_cast<void**>(&metricDevice_), sizeof(MetricPartial), "cudaMalloc metrics", err) &&
          check("cudaMallocHost metrics", cudaMallocHost(reinterpret_cast<void**>(&metricHost_), sizeof(MetricPartial)), err);
+    // Flag lines for the largest brick plan (16^3 bricks) plus the status line.
+    sorFlagLines_ = 1 + static_cast<size_t>((nx + 15) / 16) * ((ny + 15) / 16) * ((nz + 15) / 16);
+    ok = ok && alloc(reinterpret_cast<void**>(&sorSync_), sorFlagLines_ * kResidentFlagStride * sizeof(unsigned), "cudaMalloc SOR flags", err) &&
+         check("clear SOR flags", cudaMemsetAsync(sorSync_, 0, sorFlagLines_ * kResidentFlagStride * sizeof(unsigned), stream), err) &&
+         check("cudaHostAlloc SOR status", cudaHostAlloc(reinterpret_cast<void**>(&sorHostStatus_), sizeof(unsigned), cudaHostAllocMapped), err);
+    if (ok) *sorHostStatus_ = 0;
     for (int i = 0; i < 9 && ok; ++i) {
         ok = check("cudaEventCreate", cudaEventCreate(&events_[i]), err);
     }
@@ -268,7 +277,7 @@ bool Scene::setPressurePath(int path, std::string& err) {
 }
 
 // Brick plan of the shared-memory-resident SOR: 32x16x16 bricks (256 threads,
-// 78 KB of shared memory, two CTAs per SM), or 16^3 bricks (128 threads, 42 KB)
+// 93 KB of shared memory, two CTAs per SM), or 16^3 bricks (128 threads, 67 KB)
 // when the larger ones do not fit co-resident; one CTA per brick.
 bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
     int coop = 0, sms = 0;
@@ -282,17 +291,12 @@ bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
         r.bx = sh[0];
         r.by = sh[1];
         r.bz = sh[2];
-        r.kx = r.bx / 2;
-        r.ex = r.kx + 2;
-        r.ey = r.by + 2;
-        r.ez = r.bz + 2;
         r.nbx = (nx + r.bx - 1) / r.bx;
         r.nby = (ny + r.by - 1) / r.by;
         r.nbz = (nz + r.bz - 1) / r.bz;
-        threads = r.kx * r.by;
-        smemBytes = (2ull * r.ez * r.ey * r.ex + 2ull * r.bz * r.by * r.kx) * sizeof(float);
-        const void* fn = r.bx == 32 ? reinterpret_cast<const void*>(sorResident<32, 16, 16>)
-                                    : reinterpret_cast<const void*>(sorResident<16, 16, 16>);
+        threads = (r.bx / 2) * r.by;
+        smemBytes = sorResidentSharedBytes(r.bx);
+        const void* fn = sorResidentKernel(r.bx);
         int perSm = 0;
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemBytes)) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, threads, smemBytes) != cudaSuccess) {
@@ -322,9 +326,11 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
             Grid g{nx, ny, nz};
             int iterations = pressureIterations;
             float omega = pressureOmega;
-            void* args[] = {&pressure_, &divergence_, &g, &r, &iterations, &omega};
+            ResidentSync sync{sorSync_ + kResidentFlagStride, sorSync_, sorHostStatus_, sorEpoch_, sorSilentBrick_, sorWaitNs_};
+            sorEpoch_ += 2u * static_cast<unsigned>(iterations);
+            void* args[] = {&pressure_, &divergence_, &g, &r, &sync, &iterations, &omega};
             const unsigned bricks = static_cast<unsigned>(r.nbx * r.nby * r.nbz);
-            void* fn = r.bx == 32 ? reinterpret_cast<void*>(sorResident<32, 16, 16>) : reinterpret_cast<void*>(sorResident<16, 16, 16>);
+            void* fn = const_cast<void*>(sorResidentKernel(r.bx));
             if (!check("SOR cooperative launch", cudaLaunchCooperativeKernel(fn, dim3(bricks), dim3(threads), args, smem, stream), err)) {
                 return false;
             }
@@ -570,12 +576,13 @@ bool Scene::frame(uint32_t* hostBgra, const FireSettings& s, FireCudaFrameMetric
     if (!rec(kAfterPack) || !rec(kAfterRender)) return false;
     if (!toHdrSlot) {
         if (!check("cudaMemcpy frame", cudaMemcpyAsync(hostBgra, bgra_, pixels_ * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), err) ||
-            !check("frame sync", cudaStreamSynchronize(stream), err)) {
+            !check("frame sync", cudaStreamSynchronize(stream), err) || !checkSolverStatus(err)) {
             return false;
         }
     }
     if (collect) {
-        if (!runStages(kMetrics, kMetrics, p, err) || !check("metrics sync", cudaStreamSynchronize(stream), err) || !fillMetrics(metrics, err)) {
+        if (!runStages(kMetrics, kMetrics, p, err) || !check("metrics sync", cudaStreamSynchronize(stream), err) || !checkSolverStatus(err) ||
+            !fillMetrics(metrics, err)) {
             return false;
         }
     }
@@ -778,6 +785,29 @@ void Scene::clearSlots() {
     activeSlot_ = 0;
 }
 
-bool Scene::synchronize(std::string& err) { return check("cudaStreamSynchronize", cudaStreamSynchronize(stream), err); }
+bool Scene::synchronize(std::string& err) {
+    return check("cudaStreamSynchronize", cudaStreamSynchronize(stream), err) && checkSolverStatus(err);
+}
+
+// A resident SOR wait that ran out leaves brick + 1 in the host-mapped status
+// word; the pressure of that solve is incomplete.  Read after a stream sync.
+bool Scene::checkSolverStatus(std::string& err) {
+    if (sorHostStatus_ == nullptr) return true;
+    const unsigned st = *reinterpret_cast<volatile unsigned*>(sorHostStatus_);
+    if (st == 0) return true;
+    *sorHostStatus_ = 0;
+    err = "resident SOR: brick " + std::to_string(st - 1) + " timed out waiting for a neighbour's half sweep";
+    return false;
+}
+
+bool Scene::setResidentFault(int silentBrick, long long waitUs, std::string& err) {
+    if (waitUs <= 0 || waitUs > 10000000) {
+        err = "resident SOR wait limit must be in (0, 10 s]";
+        return false;
+    }
+    sorSilentBrick_ = silentBrick < 0 ? -1 : silentBrick;
+    sorWaitNs_ = static_cast<unsigned long long>(waitUs) * 1000ull;
+    return true;
+}
 
 }  // namespace firesim

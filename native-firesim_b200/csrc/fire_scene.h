@@ -61,7 +61,12 @@ public:
     // 0 = automatic (shared-memory-resident when the grid fits co-resident), 1 = one launch per half sweep, 2 = resident only.
     bool setPressurePath(int path, std::string& err);
     int lastPressurePath() const { return lastPressurePath_; }
+    // Fault injection for the resident SOR's bounded waits: brick `silentBrick`
+    // (-1 = none) never announces its half sweeps; each wait gives up after waitUs.
+    bool setResidentFault(int silentBrick, long long waitUs, std::string& err);
     bool synchronize(std::string& err);
+    // After a host sync: fails once with "timed out" if a resident SOR wait ran out since the last check.
+    bool checkSolverStatus(std::string& err);
     size_t deviceBytes() const { return deviceBytes_; }
     unsigned long long launchCount() const { return launches_; }
 
@@ -115,6 +120,12 @@ private:
     int pressurePath_ = 0;
     int lastPressurePath_ = 0;
     cudaGraphExec_t sorExec_ = nullptr;
+    unsigned* sorSync_ = nullptr;        // device: [0] status, then one flag line per brick
+    unsigned* sorHostStatus_ = nullptr;  // host-mapped: brick + 1 of a wait that ran out
+    size_t sorFlagLines_ = 0;
+    unsigned sorEpoch_ = 0;
+    int sorSilentBrick_ = -1;
+    unsigned long long sorWaitNs_ = 1000000000ull;
     int sorIterations_ = -1;
     float sorOmega_ = 0.0f;
 };

@@ -10,8 +10,6 @@
 //   sorPressureParityKernel       :1201-1227 -> sorHalfSweep
 //   subtractPressureKernel        :1229-1245 -> subtractWall (fused with the wall zeroing)
 //   velocityWallBoundaryKernel    :1293-1317
-#include <cooperative_groups.h>
-
 #include "fire_kernels.h"
 
 namespace firesim {
@@ -606,31 +604,79 @@ namespace firesim {
 // x = 2k + ((c + y + z) & 1), k = 0..BX/2-1, so a cell's x/y/z-neighbour reads
 // of the other colour are unit-stride.  Thread t owns the column
 // (k = t % KX, y = t / KX) of both colours and walks z.  A half sweep writes
-// its updated face cells straight to global p; after the grid barrier every
-// CTA reads the updated cells of its six neighbours' faces into its one-cell
-// halo, all of a thread's halo loads in flight at once.  Walls are Neumann
-// through the clamped neighbour (the cell itself), as in
+// its updated face cells straight to global p and announces them through the
+// brick's flag (ResidentSync); each brick then waits for its six neighbours'
+// flags only -- no grid-wide barrier -- and reads their updated face cells
+// into its one-cell halo, all of a thread's halo loads in flight at once.
+// The cooperative launch guarantees that all bricks are resident, so every
+// wait is for a running CTA; each wait is still bounded in time.  Walls are
+// Neumann through the clamped neighbour (the cell itself), as in
 // sorPressureParityKernel.  Per-cell arithmetic is identical to sorHalfSweep,
 // so the result is bit-identical to the per-launch path.
-namespace cg = cooperative_groups;
-
 namespace {
+
+__device__ __forceinline__ unsigned loadVolatile(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
+__device__ __forceinline__ void storeVolatile(unsigned* p, unsigned v) { *reinterpret_cast<volatile unsigned*>(p) = v; }
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait until *flag has reached target (wrap-safe).  False when the
+// wait ran out or another brick's wait already did.
+__device__ bool residentWait(const unsigned* flag, unsigned target, const ResidentSync& sync, int brick) {
+    const unsigned failTag = sync.epoch + 1u;
+    unsigned long long start = 0;
+    for (unsigned n = 0; n < kResidentMaxPolls; ++n) {
+        if (static_cast<int>(loadVolatile(flag) - target) >= 0) {
+            return true;
+        }
+        if ((n & 15u) == 15u) {
+            if (loadVolatile(sync.status) == failTag) {
+                return false;
+            }
+            const unsigned long long now = globalTimerNs();
+            if (start == 0) {
+                start = now;
+            } else if (now - start > sync.waitNs) {
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    storeVolatile(sync.status, failTag);
+    storeVolatile(sync.hostStatus, static_cast<unsigned>(brick) + 1u);
+    __threadfence_system();
+    return false;
+}
 
 // Halo cells of one colour: both x faces (BY*BZ/2 each), both y faces
 // (KX*BZ each), both z faces (KX*BY each).
 template <int BX, int BY, int BZ>
 struct ResidentShape {
     static constexpr int KX = BX / 2;
-    static constexpr int EX = KX + 2, EY = BY + 2, EZ = BZ + 2;
+    // A warp covers KX cells of each of RPW rows y0, y0 + 2, ...: rows of the
+    // same parity, so all of its lanes read at the same x shift.  The row
+    // pitch EX is padded until 2 * EX == KX (mod 32), which puts those rows
+    // in disjoint bank windows: every shared access of the update is
+    // conflict-free.
+    static constexpr int RPW = 32 / KX;
+    static constexpr int EX = ((KX + 2) + ((KX / 2 - (KX + 2) % 16) % 16 + 16) % 16);
+    static constexpr int EY = BY + 2, EZ = BZ + 2;
     static constexpr int PLANE = EZ * EY * EX;
     static constexpr int THREADS = KX * BY;
+    static constexpr size_t SHARED_BYTES = (2ull * PLANE + 2ull * BZ * THREADS) * sizeof(float);
+    static_assert((2 * EX) % 32 == KX % 32 && EX >= KX + 2, "row pitch");
+    static_assert(BY % (2 * RPW) == 0 && THREADS % 32 == 0, "warp-to-row mapping");
     static constexpr int HX = BY * BZ;
     static constexpr int HY = 2 * KX * BZ;
     static constexpr int HZ = 2 * KX * BY;
     static constexpr int HALO = HX + HY + HZ;
     static constexpr int PER_THREAD = (HALO + THREADS - 1) / THREADS;
     __device__ static int pidx(int c, int z, int y, int k) { return c * PLANE + ((z + 1) * EY + (y + 1)) * EX + (k + 1); }
-    __device__ static int didx(int c, int z, int y, int k) { return ((c * BZ + z) * BY + y) * KX + k; }
+    // div of the thread's own cells, laid out by thread: [colour][z][thread].
+    __device__ static int didx(int c, int z, int t) { return (c * BZ + z) * THREADS + t; }
 };
 
 // Global and shared index of halo cell i of colour c, or gi = -1 when the
@@ -672,19 +718,29 @@ __device__ __forceinline__ void residentHaloCell(int i, int c, int ox, int oy, i
 
 template <int BX, int BY, int BZ>
 __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g,
-                                                            ResidentBrick r, int iterations, float omega) {
+                                                               ResidentBrick r, ResidentSync sync, int iterations, float omega) {
     using S = ResidentShape<BX, BY, BZ>;
     constexpr int KX = S::KX;
     extern __shared__ float smem[];
     float* planes = smem;                // [2][EZ][EY][EX]
     float* divs = smem + 2 * S::PLANE;   // [2][BZ][BY][KX]
-    cg::grid_group grid = cg::this_grid();
     const int brick = blockIdx.x;
-    const int ox = (brick % r.nbx) * BX;
-    const int oy = ((brick / r.nbx) % r.nby) * BY;
-    const int oz = (brick / (r.nbx * r.nby)) * BZ;
-    const int k = threadIdx.x % KX;
-    const int y = threadIdx.x / KX;
+    const int bi = brick % r.nbx, bj = (brick / r.nbx) % r.nby, bk = brick / (r.nbx * r.nby);
+    const int ox = bi * BX;
+    const int oy = bj * BY;
+    const int oz = bk * BZ;
+    // Threads 0..5 each watch one face neighbour (-x, +x, -y, +y, -z, +z).
+    int watched = -1;
+    if (threadIdx.x < 6) {
+        const int axis = threadIdx.x >> 1, step = (threadIdx.x & 1) ? 1 : -1;
+        const int ni = bi + (axis == 0 ? step : 0), nj = bj + (axis == 1 ? step : 0), nk = bk + (axis == 2 ? step : 0);
+        if (ni >= 0 && ni < r.nbx && nj >= 0 && nj < r.nby && nk >= 0 && nk < r.nbz) {
+            watched = (nk * r.nby + nj) * r.nbx + ni;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k = lane % KX;
+    const int y = (warp >> 1) * 2 * S::RPW + (warp & 1) + 2 * (lane / KX);
     const int gy = oy + y;
 
     // This thread's halo cells of each colour, fixed for the whole solve.
@@ -723,7 +779,7 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             if (gx < g.nx && gy < g.ny && gz < g.nz) {
                 const int gi = (gz * g.ny + gy) * g.nx + gx;
                 planes[S::pidx(c, z, y, k)] = __ldcg(pressure + gi);
-                divs[S::didx(c, z, y, k)] = __ldg(divergence + gi);
+                divs[S::didx(c, z, threadIdx.x)] = __ldg(divergence + gi);
             }
         }
     }
@@ -751,7 +807,7 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                     const float pU = gy == g.ny - 1 ? self : planes[S::pidx(o, z, y + 1, k)];
                     const float pB = gz == 0 ? self : planes[S::pidx(o, z - 1, y, k)];
                     const float pF = gz == g.nz - 1 ? self : planes[S::pidx(o, z + 1, y, k)];
-                    const float d = divs[S::didx(c, z, y, k)];
+                    const float d = divs[S::didx(c, z, threadIdx.x)];
                     const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
                     const float next = self + omega * (projected - self);
                     planes[S::pidx(c, z, y, k)] = next;
@@ -763,7 +819,20 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             if (last) {
                 break;
             }
-            grid.sync();
+            const unsigned target = sync.epoch + static_cast<unsigned>(2 * it + c + 1);
+            __syncthreads();
+            if (threadIdx.x == 0 && brick != sync.silentBrick) {
+                __threadfence();
+                storeVolatile(sync.flags + brick * kResidentFlagStride, target);
+            }
+            bool failed = false;
+            if (watched >= 0) {
+                failed = !residentWait(sync.flags + watched * kResidentFlagStride, target, sync, brick);
+                __threadfence();
+            }
+            if (__syncthreads_or(failed)) {
+                return;
+            }
             loadHalo(c);
             __syncthreads();
         }
@@ -782,7 +851,12 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
     }
 }
 
-template __global__ void sorResident<32, 16, 16>(float*, const float*, Grid, ResidentBrick, int, float);
-template __global__ void sorResident<16, 16, 16>(float*, const float*, Grid, ResidentBrick, int, float);
+const void* sorResidentKernel(int bx) {
+    return bx == 32 ? reinterpret_cast<const void*>(sorResident<32, 16, 16>) : reinterpret_cast<const void*>(sorResident<16, 16, 16>);
+}
+
+size_t sorResidentSharedBytes(int bx) {
+    return bx == 32 ? ResidentShape<32, 16, 16>::SHARED_BYTES : ResidentShape<16, 16, 16>::SHARED_BYTES;
+}
 
 }  // namespace firesim

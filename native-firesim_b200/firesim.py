@@ -62,6 +62,8 @@ def load_library() -> ctypes.CDLL:
         "fireCudaRegisterHdrBufferSlot": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
         "fireCudaSetPressureSolver": (b, [ctypes.c_int, ctypes.c_float]),
         "fireCudaSetPressurePath": (b, [ctypes.c_int]),
+        "fireCudaGetPressurePathUsed": (ctypes.c_int, []),
+        "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
         "fireCudaSetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -159,6 +161,14 @@ class FireSim:
     def set_pressure_path(self, path: int):
         """0 automatic, 1 one launch per half sweep, 2 shared-memory-resident."""
         self._check(self.lib.fireCudaSetPressurePath(path), "fireCudaSetPressurePath")
+
+    def set_resident_sor_fault(self, silent_brick: int = -1, wait_us: int = 1_000_000):
+        """Fault injection for the resident SOR's bounded neighbour waits."""
+        self._check(self.lib.fireCudaSetResidentSorFault(silent_brick, wait_us), "fireCudaSetResidentSorFault")
+
+    def pressure_path_used(self) -> int:
+        """Path of the latest SOR solve: 0 none yet, 1 per-launch graph, 2 resident."""
+        return int(self.lib.fireCudaGetPressurePathUsed())
 
     def shape_of(self, name: str):
         nx, ny, nz = self.nx, self.ny, self.nz

@@ -228,5 +228,46 @@ def test_sor_resident_equals_per_launch(dims, product, abi):
         sim.set("pressure", p0)
         sim.set("divergence", d0)
         sim.stages("pressure_sor", "pressure_sor", s, 0.0)
-        out.append(sim.get("pressure"))
-    np.testing.assert_array_equal(out[0], out[1])
+        first = sim.get("pressure")
+        assert sim.pressure_path_used() == path
+        # A second solve in the same scene: the neighbour flags' epochs advance.
+        sim.stages("pressure_sor", "pressure_sor", s, 0.0)
+        out.append((first, sim.get("pressure")))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+def test_resident_sor_wait_runs_out_and_reports(product, abi):
+    """Failure detection of the resident SOR without a GPU fault: brick 5 is told
+    (from the host) never to announce its half sweeps, so its neighbours' waits
+    run out after 2 ms; the solve returns, the stage call reports the timed-out
+    brick, and the next solve on the same scene is correct again."""
+    nx, ny, nz = 64, 64, 64
+    rng = np.random.default_rng(11)
+    p0 = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    d0 = (0.3 * rng.standard_normal((nz, ny, nx))).astype(np.float32)
+    s = abi.FireSettings()
+    ref = product.FireSim(32, 16, nx, ny, nz)
+    ref.set_pressure_solver(20, 1.8)
+    ref.set_pressure_path(1)
+    ref.set("pressure", p0)
+    ref.set("divergence", d0)
+    ref.stages("pressure_sor", "pressure_sor", s, 0.0)
+    expect = ref.get("pressure")
+    ref.close()
+
+    sim = product.FireSim(32, 16, nx, ny, nz)
+    sim.set_pressure_solver(20, 1.8)
+    sim.set_pressure_path(2)
+    sim.set_resident_sor_fault(5, 2000)
+    sim.set("pressure", p0)
+    sim.set("divergence", d0)
+    with pytest.raises(product.firesim.FireSimError, match="timed out waiting for a neighbour"):
+        sim.stages("pressure_sor", "pressure_sor", s, 0.0)
+    sim.synchronize()  # the failure is reported once
+    sim.set_resident_sor_fault(-1, 1_000_000)
+    sim.set("pressure", p0)
+    sim.set("divergence", d0)
+    sim.stages("pressure_sor", "pressure_sor", s, 0.0)
+    assert sim.pressure_path_used() == 2
+    np.testing.assert_array_equal(sim.get("pressure"), expect)
