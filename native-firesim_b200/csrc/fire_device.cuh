@@ -139,7 +139,9 @@ __device__ __forceinline__ float valueNoise3(float px, float py, float pz) {
     return noiseLerp(noiseLerp(c00, c10, uy), noiseLerp(c01, c11, uy), uz);
 }
 
-// Five octaves (src/fire_cuda.cu:423-432).
+// Five octaves (src/fire_cuda.cu:423-432).  Inlined: its callers combine the
+// result with other terms, and the fused multiply-adds the compiler forms
+// there match the reference's build only in the inlined form.
 __device__ __forceinline__ float fbm(float px, float py) {
     float sum = 0.0f;
     float amp = 0.5f;
@@ -153,11 +155,16 @@ __device__ __forceinline__ float fbm(float px, float py) {
     return sum;
 }
 
-// Three octaves, rescaled and saturated (src/fire_cuda.cu:434-443).
-__device__ __forceinline__ float fbm3(float px, float py, float pz) {
+// Three octaves, rescaled and saturated (src/fire_cuda.cu:434-443).  Kept out
+// of line with a rolled octave loop, so one copy of the hash (and of sinf with
+// its large-argument path) serves every call site: inlined and unrolled, the
+// raymarch's four fbm3 calls put 96 copies of sinf in its sample loop, which
+// then stalls on instruction fetch.  The result is the same bits either way
+// (its callers only saturate or offset it).
+static __device__ __noinline__ float fbm3(float px, float py, float pz) {
     float sum = 0.0f;
     float amp = 0.5f;
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         sum = __fmaf_rn(amp, valueNoise3(px, py, pz), sum);
         px = __fmaf_rn(px, 2.03f, 17.7f);
