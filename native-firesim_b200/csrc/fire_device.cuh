@@ -117,6 +117,12 @@ __device__ __forceinline__ float hash31(float x, float y, float z) {
 __device__ __forceinline__ float noiseLerp(float a, float b, float t) { return __fmaf_rn(b - a, t, a); }
 __device__ __forceinline__ float smoothWeight(float f) { return f * f * (3.0f - 2.0f * f); }
 
+// Bilinear blend of the four lattice hashes around (px, py) with weights from the fractions.
+__device__ __forceinline__ float valueNoiseFromCorners(float a, float b, float c, float d, float fx, float fy) {
+    const float ux = smoothWeight(fx), uy = smoothWeight(fy);
+    return noiseLerp(noiseLerp(a, b, ux), noiseLerp(c, d, ux), uy);
+}
+
 __device__ __forceinline__ float valueNoise(float px, float py) {
     const float ix = floorf(px), iy = floorf(py);
     const float fx = fracf(px), fy = fracf(py);
@@ -124,8 +130,7 @@ __device__ __forceinline__ float valueNoise(float px, float py) {
     const float b = hash21(ix + 1.0f, iy);
     const float c = hash21(ix, iy + 1.0f);
     const float d = hash21(ix + 1.0f, iy + 1.0f);
-    const float ux = smoothWeight(fx), uy = smoothWeight(fy);
-    return noiseLerp(noiseLerp(a, b, ux), noiseLerp(c, d, ux), uy);
+    return valueNoiseFromCorners(a, b, c, d, fx, fy);
 }
 
 __device__ __forceinline__ float valueNoise3(float px, float py, float pz) {
@@ -173,6 +178,55 @@ static __device__ __noinline__ float fbm3(float px, float py, float pz) {
         amp *= 0.5f;
     }
     return saturate(sum * 1.142857f);
+}
+
+// --- hash lattices of 2D fbm call sites ---------------------------------------
+// A 2D fbm evaluated at every cell of the grid hashes the same integer
+// lattice points many times over (at the lowest octave a lattice cell spans
+// ten grid cells).  A HashLattice2 holds hash21 at every lattice point one
+// call site can reach in this step, per octave; fbmLattice reads its four
+// corners there instead of evaluating four sines.  The values are the same
+// bits (hash21 of the same integral coordinates), so fbmLattice(px, py, L)
+// equals fbm(px, py) exactly.  A corner outside the table, or a table with
+// no storage, is hashed directly.
+constexpr int kFbmOctaves = 5;
+struct HashLattice2 {
+    const float* values;  // octave o: sx[o] * sy[o] values at offset[o], x fastest
+    int ox[kFbmOctaves], oy[kFbmOctaves];  // lattice coordinate of entry (0, 0)
+    int sx[kFbmOctaves], sy[kFbmOctaves];
+    int offset[kFbmOctaves];
+};
+
+static __device__ __noinline__ float hash21OutOfLine(float x, float y) { return hash21(x, y); }
+
+__device__ __forceinline__ float fbmLattice(float px, float py, const HashLattice2& L) {
+    float sum = 0.0f;
+    float amp = 0.5f;
+#pragma unroll
+    for (int i = 0; i < kFbmOctaves; ++i) {
+        const float ix = floorf(px), iy = floorf(py);
+        const float fx = fracf(px), fy = fracf(py);
+        const int tx = static_cast<int>(ix) - L.ox[i];
+        const int ty = static_cast<int>(iy) - L.oy[i];
+        float a, b, c, d;
+        if (L.values != nullptr && tx >= 0 && tx < L.sx[i] - 1 && ty >= 0 && ty < L.sy[i] - 1) {
+            const float* q = L.values + L.offset[i] + ty * L.sx[i] + tx;
+            a = __ldg(q);
+            b = __ldg(q + 1);
+            c = __ldg(q + L.sx[i]);
+            d = __ldg(q + L.sx[i] + 1);
+        } else {
+            a = hash21OutOfLine(ix, iy);
+            b = hash21OutOfLine(ix + 1.0f, iy);
+            c = hash21OutOfLine(ix, iy + 1.0f);
+            d = hash21OutOfLine(ix + 1.0f, iy + 1.0f);
+        }
+        sum = __fmaf_rn(amp, valueNoiseFromCorners(a, b, c, d, fx, fy), sum);
+        px = __fmaf_rn(px, 2.03f, 17.7f);
+        py = __fmaf_rn(py, 2.01f, -9.2f);
+        amp *= 0.5f;
+    }
+    return sum;
 }
 
 // --- lattice sampling -------------------------------------------------------

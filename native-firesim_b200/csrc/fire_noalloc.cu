@@ -94,7 +94,9 @@ extern "C" bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float 
     const int bx = nx <= 32 ? 32 : (nx <= 64 ? 64 : 128);
     const dim3 grid((nx + bx - 1) / bx, ny, nz);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    firesim::forceContributions<<<grid, bx, 0, s>>>(scratch, in, vel, p);
+    // No lattice storage here: every curl-noise corner is hashed in place.
+    const firesim::HashLattice2 noLattice{};
+    firesim::forceContributions<<<grid, bx, 0, s>>>(scratch, in, vel, p, noLattice, noLattice);
     firesim::forceProjectSetup<<<grid, bx, 0, s>>>(uOut, vOut, wOut, divergence, pressure, scratch, vel, p);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(std::string("force pass launch: ") + cudaGetErrorString(e));

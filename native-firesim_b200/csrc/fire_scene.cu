@@ -66,7 +66,7 @@ void Scene::release() {
     }
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
-                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorSync_};
+                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorSync_, curlLattice_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
@@ -74,6 +74,7 @@ void Scene::release() {
     if (sorHostStatus_ != nullptr) cudaFreeHost(sorHostStatus_);
     sorSync_ = nullptr;
     sorHostStatus_ = nullptr;
+    curlLattice_ = nullptr;
     for (cudaEvent_t& e : events_) {
         if (e != nullptr) cudaEventDestroy(e);
         e = nullptr;
@@ -150,6 +151,17 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
          check("clear SOR flags", cudaMemsetAsync(sorSync_, 0, sorFlagLines_ * kResidentFlagStride * sizeof(unsigned), stream), err) &&
          check("cudaHostAlloc SOR status", cudaHostAlloc(reinterpret_cast<void**>(&sorHostStatus_), sizeof(unsigned), cudaHostAllocMapped), err);
     if (ok) *sorHostStatus_ = 0;
+    {
+        // Lattice sizes do not depend on time: plan at t = 0 with one extra
+        // lattice cell of slack per axis.
+        FrameParams p0{};
+        HashLattice2 a, b;
+        curlCapacity_[0] = curlCapacity_[1] = 1u << 30;
+        curlLattices(p0, a, b);
+        curlCapacity_[0] = static_cast<size_t>(a.offset[kFbmOctaves - 1] + (a.sx[kFbmOctaves - 1] + 1) * (a.sy[kFbmOctaves - 1] + 1)) + 4096;
+        curlCapacity_[1] = static_cast<size_t>(b.offset[kFbmOctaves - 1] + (b.sx[kFbmOctaves - 1] + 1) * (b.sy[kFbmOctaves - 1] + 1)) + 4096;
+        ok = ok && alloc(reinterpret_cast<void**>(&curlLattice_), (curlCapacity_[0] + curlCapacity_[1]) * sizeof(float), "cudaMalloc curl lattices", err);
+    }
     for (int i = 0; i < 9 && ok; ++i) {
         ok = check("cudaEventCreate", cudaEventCreate(&events_[i]), err);
     }
@@ -386,6 +398,45 @@ bool Scene::runMetrics(const FrameParams& p, std::string& err) {
     return check("metrics readback", cudaMemcpyAsync(metricHost_, metricDevice_, sizeof(MetricPartial), cudaMemcpyDeviceToHost, stream), err);
 }
 
+namespace {
+
+// Lattice of one 2D fbm call site whose octave-0 inputs lie in
+// [pxLo, pxHi] x [pyLo, pyHi]; later octaves map the range through the octave
+// step (x * 2.03 + 17.7, y * 2.01 - 9.2, src/fire_cuda.cu:423-432), widened by
+// one lattice cell per octave for rounding.  Entries past the edges are
+// hashed in place by fbmLattice, so the margins only affect speed.
+int planLattice(double pxLo, double pxHi, double pyLo, double pyHi, HashLattice2& L) {
+    int offset = 0;
+    for (int o = 0; o < kFbmOctaves; ++o) {
+        L.ox[o] = static_cast<int>(std::floor(pxLo)) - 2;
+        L.oy[o] = static_cast<int>(std::floor(pyLo)) - 2;
+        L.sx[o] = static_cast<int>(std::floor(pxHi)) - L.ox[o] + 4;
+        L.sy[o] = static_cast<int>(std::floor(pyHi)) - L.oy[o] + 4;
+        L.offset[o] = offset;
+        offset += L.sx[o] * L.sy[o];
+        pxLo = pxLo * 2.03 + 17.7 - 1.0;
+        pxHi = pxHi * 2.03 + 17.7 + 1.0;
+        pyLo = pyLo * 2.01 - 9.2 - 1.0;
+        pyHi = pyHi * 2.01 - 9.2 + 1.0;
+    }
+    return offset;
+}
+
+}  // namespace
+
+// The curl noise of forceContributions hashes, per cell at (u, v, w) in [0, 1]^3,
+//   A: (u * 9 + w * 3.7 + t * 0.22, v * 13 - t * 0.31)
+//   B: (w * 10 - t * 0.19, u * 8 + v * 5.5 + t * 0.27)        (src/fire_cuda.cu:1156-1157)
+bool Scene::curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b) const {
+    const double t = p.time;
+    const int na = planLattice(t * 0.22 - 1.0, 12.7 + t * 0.22 + 1.0, -t * 0.31 - 1.0, 13.0 - t * 0.31 + 1.0, a);
+    const int nb = planLattice(-t * 0.19 - 1.0, 10.0 - t * 0.19 + 1.0, t * 0.27 - 1.0, 13.5 + t * 0.27 + 1.0, b);
+    const bool fits = curlLattice_ != nullptr && static_cast<size_t>(na) <= curlCapacity_[0] && static_cast<size_t>(nb) <= curlCapacity_[1];
+    a.values = fits ? curlLattice_ : nullptr;
+    b.values = fits ? curlLattice_ + curlCapacity_[0] : nullptr;
+    return fits;
+}
+
 bool Scene::runStages(int first, int last, const FrameParams& p, std::string& err) {
     if (first < 0 || last > kReset || first > last) {
         err = "stage range out of order";
@@ -412,8 +463,12 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                 cur_ = 1 - cur_;
                 s = kForce;
                 break;
-            case kForce:
-                forceContributions<<<cells, bx, 0, stream>>>(contrib_, scalarsIn(), velocity(), p); ++launches_;
+            case kForce: {
+                HashLattice2 curlA{}, curlB{};
+                if (curlLattices(p, curlA, curlB)) {
+                    hashLatticeBuild<<<dim3(64, 2), 256, 0, stream>>>(curlA, curlB); ++launches_;
+                }
+                forceContributions<<<cells, bx, 0, stream>>>(contrib_, scalarsIn(), velocity(), p, curlA, curlB); ++launches_;
                 if (last >= kDivergence) {
                     forceProjectSetup<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], divergence_,
                                                                pressure_, contrib_, velocity(), p); ++launches_;
@@ -425,6 +480,7 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                     s = kVelocityBoundary;
                 }
                 break;
+            }
             case kVelocityBoundary:
                 velocityBoundary<<<faces, bxFace, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], p, 1); ++launches_;
                 s = kDivergence;

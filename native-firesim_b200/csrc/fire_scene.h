@@ -120,6 +120,10 @@ private:
     int pressurePath_ = 0;
     int lastPressurePath_ = 0;
     cudaGraphExec_t sorExec_ = nullptr;
+    // hash21 lattices of the two curl-noise fbm call sites of the force pass.
+    bool curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b) const;
+    float* curlLattice_ = nullptr;
+    size_t curlCapacity_[2] = {0, 0};
     unsigned* sorSync_ = nullptr;        // device: [0] status, then one flag line per brick
     unsigned* sorHostStatus_ = nullptr;  // host-mapped: brick + 1 of a wait that ran out
     size_t sorFlagLines_ = 0;

@@ -371,10 +371,29 @@ __global__ void __launch_bounds__(128) advectReact(ScalarFields out, ScalarField
 }
 
 // ---------------------------------------------------------------------------
+// hash21 at every entry of the curl-noise lattices of this step (blockIdx.y
+// selects the table).  The same function as the direct evaluation, so every
+// table entry is the same bits as hashing its lattice point in place.
+__global__ void __launch_bounds__(256) hashLatticeBuild(HashLattice2 a, HashLattice2 b) {
+    const HashLattice2& L = blockIdx.y == 0 ? a : b;
+    float* out = const_cast<float*>(L.values);
+    const int total = L.offset[kFbmOctaves - 1] + L.sx[kFbmOctaves - 1] * L.sy[kFbmOctaves - 1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int o = 0;
+        while (o + 1 < kFbmOctaves && i >= L.offset[o + 1]) ++o;
+        const int local = i - L.offset[o];
+        const int tx = local % L.sx[o];
+        const int ty = local / L.sx[o];
+        out[i] = hash21(static_cast<float>(L.ox[o] + tx), static_cast<float>(L.oy[o] + ty));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // src/fire_cuda.cu:1128-1183 -- per-cell forcing.  Every face is read before
 // any force is added; the per-cell increments go to `contrib` and the faces
 // gather them (lower cell first), which makes the result deterministic.
-__global__ void __launch_bounds__(128) forceContributions(float4* __restrict__ contrib, ScalarFieldsIn s, Velocity vel, FrameParams p) {
+__global__ void __launch_bounds__(128) forceContributions(float4* __restrict__ contrib, ScalarFieldsIn s, Velocity vel, FrameParams p,
+                                                         HashLattice2 curlA, HashLattice2 curlB) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
@@ -405,8 +424,8 @@ __global__ void __launch_bounds__(128) forceContributions(float4* __restrict__ c
     const float curlY = (uR - uL) - (wF - wB);
     const float curlZ = (vU - vD) - (uR - uL);
     const float curlMagnitude = fabsf(curlX) + fabsf(curlY) + fabsf(curlZ);
-    const float curlNoiseA = fbm(u * 9.0f + w * 3.7f + p.time * 0.22f, v * 13.0f - p.time * 0.31f) - 0.5f;
-    const float curlNoiseB = fbm(w * 10.0f - p.time * 0.19f, u * 8.0f + v * 5.5f + p.time * 0.27f) - 0.5f;
+    const float curlNoiseA = fbmLattice(u * 9.0f + w * 3.7f + p.time * 0.22f, v * 13.0f - p.time * 0.31f, curlA) - 0.5f;
+    const float curlNoiseB = fbmLattice(w * 10.0f - p.time * 0.19f, u * 8.0f + v * 5.5f + p.time * 0.27f, curlB) - 0.5f;
     const float thermalActivity = smoothstepf(0.04f, 4.20f, h + sv * 0.28f);
     const float upperDrag = smoothstepf(0.26f, 0.94f, v);
     const float lesGain = sqrtf(fmaxf(0.0f, k)) * (0.30f + c * 0.54f);
