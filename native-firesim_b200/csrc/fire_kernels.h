@@ -54,7 +54,8 @@ __global__ void fuelBedTables(float* material, float* breathing, FrameParams p, 
 __global__ void resetCells(ScalarFields out, float* pressure, float* divergence, float* divergenceAfter, const float* material,
                            const float* breathing, FrameParams p);
 __global__ void advectVelocity(float* uOut, float* vOut, float* wOut, Velocity vel, FrameParams p);
-__global__ void advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel, const float* material, const float* breathing, FrameParams p);
+__global__ void advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel, const float* material, const float* breathing, FrameParams p,
+                            HashLattice2 sourceLattice);
 __global__ void hashLatticeBuild(HashLattice2 a, HashLattice2 b);
 __global__ void forceContributions(float4* contrib, ScalarFieldsIn s, Velocity vel, FrameParams p, HashLattice2 curlA, HashLattice2 curlB);
 __global__ void forceApply(float* uOut, float* vOut, float* wOut, const float4* contrib, Velocity vel, FrameParams p);

@@ -66,7 +66,7 @@ void Scene::release() {
     }
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
-                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorSync_, curlLattice_};
+                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorSync_, curlLattice_, sourceLattice_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
@@ -75,6 +75,7 @@ void Scene::release() {
     sorSync_ = nullptr;
     sorHostStatus_ = nullptr;
     curlLattice_ = nullptr;
+    sourceLattice_ = nullptr;
     for (cudaEvent_t& e : events_) {
         if (e != nullptr) cudaEventDestroy(e);
         e = nullptr;
@@ -161,6 +162,12 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
         curlCapacity_[0] = static_cast<size_t>(a.offset[kFbmOctaves - 1] + (a.sx[kFbmOctaves - 1] + 1) * (a.sy[kFbmOctaves - 1] + 1)) + 4096;
         curlCapacity_[1] = static_cast<size_t>(b.offset[kFbmOctaves - 1] + (b.sx[kFbmOctaves - 1] + 1) * (b.sy[kFbmOctaves - 1] + 1)) + 4096;
         ok = ok && alloc(reinterpret_cast<void**>(&curlLattice_), (curlCapacity_[0] + curlCapacity_[1]) * sizeof(float), "cudaMalloc curl lattices", err);
+        HashLattice2 src;
+        sourceCapacity_ = 1u << 30;
+        sourceLattice(p0, src);
+        sourceCapacity_ =
+            static_cast<size_t>(src.offset[kFbmOctaves - 1] + (src.sx[kFbmOctaves - 1] + 1) * (src.sy[kFbmOctaves - 1] + 1)) + 4096;
+        ok = ok && alloc(reinterpret_cast<void**>(&sourceLattice_), sourceCapacity_ * sizeof(float), "cudaMalloc source lattice", err);
     }
     for (int i = 0; i < 9 && ok; ++i) {
         ok = check("cudaEventCreate", cudaEventCreate(&events_[i]), err);
@@ -426,7 +433,7 @@ int planLattice(double pxLo, double pxHi, double pyLo, double pyHi, HashLattice2
 
 // The curl noise of forceContributions hashes, per cell at (u, v, w) in [0, 1]^3,
 //   A: (u * 9 + w * 3.7 + t * 0.22, v * 13 - t * 0.31)
-//   B: (w * 10 - t * 0.19, u * 8 + v * 5.5 + t * 0.27)        (src/fire_cuda.cu:1156-1157)
+//   B: (w * 10 - t * 0.19, u * 8 + v * 5.5 + t * 0.27)        (src/fire_cuda.cu:1164-1165)
 bool Scene::curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b) const {
     const double t = p.time;
     const int na = planLattice(t * 0.22 - 1.0, 12.7 + t * 0.22 + 1.0, -t * 0.31 - 1.0, 13.0 - t * 0.31 + 1.0, a);
@@ -434,6 +441,17 @@ bool Scene::curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b)
     const bool fits = curlLattice_ != nullptr && static_cast<size_t>(na) <= curlCapacity_[0] && static_cast<size_t>(nb) <= curlCapacity_[1];
     a.values = fits ? curlLattice_ : nullptr;
     b.values = fits ? curlLattice_ + curlCapacity_[0] : nullptr;
+    return fits;
+}
+
+// The fuel-bed source noise of advectReact hashes, per cell at height v in [0, 1]
+// and world position X in [-1.05, 1.05], Z in [-0.82, 0.82],
+//   (X * 13 + Z * 3 + t * 0.38, v * 31 + Z * 11)               (src/fire_cuda.cu:1023)
+bool Scene::sourceLattice(const FrameParams& p, HashLattice2& l) const {
+    const double t = p.time;
+    const int n = planLattice(-13.65 - 2.46 + t * 0.38 - 1.0, 13.65 + 2.46 + t * 0.38 + 1.0, -9.02 - 1.0, 31.0 + 9.02 + 1.0, l);
+    const bool fits = sourceLattice_ != nullptr && static_cast<size_t>(n) <= sourceCapacity_;
+    l.values = fits ? sourceLattice_ : nullptr;
     return fits;
 }
 
@@ -459,7 +477,13 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                 break;
             case kAdvectReact:
                 if (!ensureMaterial(p, err)) return false;
-                advectReact<<<cells, bx, 0, stream>>>(scalarsOut(), scalarsIn(), velocity(), material_, breathing_, p); ++launches_;
+            {
+                HashLattice2 srcLattice{};
+                if (sourceLattice(p, srcLattice)) {
+                    hashLatticeBuild<<<dim3(256, 1), 256, 0, stream>>>(srcLattice, srcLattice); ++launches_;
+                }
+                advectReact<<<cells, bx, 0, stream>>>(scalarsOut(), scalarsIn(), velocity(), material_, breathing_, p, srcLattice); ++launches_;
+            }
                 cur_ = 1 - cur_;
                 s = kForce;
                 break;

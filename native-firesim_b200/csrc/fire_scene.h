@@ -124,6 +124,10 @@ private:
     bool curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b) const;
     float* curlLattice_ = nullptr;
     size_t curlCapacity_[2] = {0, 0};
+    // hash21 lattice of the fuel-bed source noise of the advect/react pass.
+    bool sourceLattice(const FrameParams& p, HashLattice2& l) const;
+    float* sourceLattice_ = nullptr;
+    size_t sourceCapacity_ = 0;
     unsigned* sorSync_ = nullptr;        // device: [0] status, then one flag line per brick
     unsigned* sorHostStatus_ = nullptr;  // host-mapped: brick + 1 of a wait that ran out
     size_t sorFlagLines_ = 0;

@@ -205,7 +205,7 @@ __device__ __forceinline__ float macCormack(float firstOrder, float lo, float hi
 // src/fire_cuda.cu:934-1126 -- advection of the ten scalars plus the reaction network.
 __global__ void __launch_bounds__(128) advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel,
                                                    const float* __restrict__ material, const float* __restrict__ breathing,
-                                                   FrameParams p) {
+                                                   FrameParams p, HashLattice2 sourceLattice) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
@@ -269,7 +269,13 @@ __global__ void __launch_bounds__(128) advectReact(ScalarFields out, ScalarField
     const float worldX = (u - 0.50f) * 2.10f;
     const float worldZ = (w - 0.50f) * 1.64f;
     const float mat = __ldg(material + z * p.nx + x);
-    const float sourceNoise = 0.70f + 0.48f * fbm(worldX * 13.0f + worldZ * 3.0f + p.time * 0.38f, v * 31.0f + worldZ * 11.0f);
+    // The source noise only matters where the bed profile or the char release
+    // is non-zero: elsewhere it multiplies a zero, and the zero (with its sign)
+    // is the same for any finite positive noise.  It is evaluated lazily, at
+    // most once, from this step's hash lattice.
+    auto evalSourceNoise = [&]() {
+        return 0.70f + 0.48f * fbmLattice(worldX * 13.0f + worldZ * 3.0f + p.time * 0.38f, v * 31.0f + worldZ * 11.0f, sourceLattice);
+    };
     const float exposedChar = saturate(charMass / fmaxf(0.055f, charMass + ash * 1.75f));
     const float charEdges = smoothstepf(0.06f, 0.78f, mat) * smoothstepf(0.92f, 0.02f, ash);
     const float gasFeed = sc == 2 ? 1.18f : exposedChar * charEdges;
@@ -277,13 +283,23 @@ __global__ void __launch_bounds__(128) advectReact(ScalarFields out, ScalarField
     const float sceneFuelGain = sc == 2 ? 0.46f : (sc == 1 ? 1.18f : 1.0f);
     const float sceneHeatGain = sc == 2 ? 1.18f : (sc == 1 ? 1.08f : 1.0f);
     const float sceneSootGain = sc == 2 ? 0.18f : (sc == 1 ? 1.22f : 1.0f);
-    const float bed = fuelBedSourceFrom(mat, __ldg(breathing + z * p.nx + x), v, p) * sourceNoise * gasFeed * p.intensity;
+    const float bedProfile = fuelBedSourceFrom(mat, __ldg(breathing + z * p.nx + x), v, p);
+    float sourceNoise = 1.0f;
+    bool haveSourceNoise = false;
+    if (bedProfile != 0.0f) {
+        sourceNoise = evalSourceNoise();
+        haveSourceNoise = true;
+    }
+    const float bed = bedProfile * sourceNoise * gasFeed * p.intensity;
     const float ambientK = 293.0f;
     float tempK = ambientK + heat * 335.0f;
     const float radiativeFeedback = smoothstepf(430.0f, 980.0f, tempK);
     const float solidOxygen = saturate(oxygen * 1.28f - soot * 0.030f);
     const float heatFlux = saturate((tempK - 405.0f) / 900.0f) + bed * 0.34f + sootOptics * 0.024f;
     const float charRelease = fminf(charMass, charMass * heatFlux * solidOxygen * (0.14f + radiativeFeedback * 1.38f) * p.dt);
+    if (!haveSourceNoise && charRelease != 0.0f) {
+        sourceNoise = evalSourceNoise();
+    }
     pyrolysisRate += (bed * (0.34f + radiativeFeedback * 1.05f) * p.dt + charRelease * (2.45f + sourceNoise * 0.72f)) * scenePyrolysisGain;
     charMass += mat * p.dt * (sc == 2 ? 0.00005f : (sc == 1 ? 0.050f : 0.026f));
     charMass -= charRelease * 0.92f;
