@@ -162,7 +162,8 @@ STAGE_BYTES_PER_CELL = {
 
 
 def stage_timings(pkg, sim, args, settings, iters: int = 3) -> dict:
-    """Average device time of each stage range, from CUDA events on the scene stream."""
+    """Device time of each stage range (best of `iters`), from CUDA events on the scene stream
+    around the queued stages."""
     import torch
     ext = torch.cuda.ExternalStream(sim.stream())
     ranges = {
@@ -181,11 +182,16 @@ def stage_timings(pkg, sim, args, settings, iters: int = 3) -> dict:
         ms = []
         for _ in range(iters):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            # A spin kernel holds the stream while the host queues the events and the
+            # stage, so the interval holds the stage's kernels and not the host's latency.
+            with torch.cuda.stream(ext):
+                torch.cuda._sleep(400_000)
             e0.record(ext)
-            sim.stages(a, b, settings, t_render if name in ("render", "embers") else t_sim)
+            sim.stages(a, b, settings, t_render if name in ("render", "embers") else t_sim, wait=False)
             e1.record(ext)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+        sim.synchronize()
         out[name] = min(ms)
     return out
 

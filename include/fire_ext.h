@@ -123,6 +123,12 @@ FIRE_API bool fireCudaSetField(int field, const void* host, size_t bytes);
  * The clocks are not advanced. */
 FIRE_API bool fireCudaRunStages(int first, int last, const FireSettings* settings, float time);
 
+/* As fireCudaRunStages, but returns once the stages are queued on the scene's
+ * stream (fireCudaGetStream) instead of waiting for them; errors the GPU
+ * reports surface at the next fireCudaSynchronize.  Lets a caller bracket a
+ * stage range with its own events on that stream. */
+FIRE_API bool fireCudaRunStagesAsync(int first, int last, const FireSettings* settings, float time);
+
 /* Simulation clock, render clock and frame index of the singleton scene. */
 FIRE_API bool fireCudaGetTimes(float* simTime, float* renderTime, int* frameIndex);
 FIRE_API bool fireCudaSetTimes(float simTime, float renderTime, int frameIndex);

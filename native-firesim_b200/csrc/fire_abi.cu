@@ -242,6 +242,15 @@ bool fireCudaRunStages(int first, int last, const FireSettings* settings, float 
     return true;
 }
 
+bool fireCudaRunStagesAsync(int first, int last, const FireSettings* settings, float time) {
+    if (!requireScene()) return false;
+    if (settings == nullptr) return fail("Settings pointer was null.");
+    std::string err;
+    const firesim::FrameParams p = g_scene->paramsFrom(*settings, time);
+    if (!g_scene->runStages(first, last, p, err)) return fail(err);
+    return true;
+}
+
 bool fireCudaGetTimes(float* simTime, float* renderTime, int* frameIndex) {
     if (!requireScene()) return false;
     if (simTime) *simTime = g_scene->simTime;

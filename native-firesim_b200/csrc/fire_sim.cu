@@ -749,21 +749,128 @@ __device__ __forceinline__ void residentHaloCell(int i, int c, int ox, int oy, i
     gi = (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) ? (gz * g.ny + gy) * g.nx + gx : -1;
 }
 
+// Face cells of one colour in a brick, updated after the halo has arrived:
+// both z faces (all k, y), both y faces (inner z), and in every inner (y, z)
+// row the one x-face cell of that colour (x = 0 when the row's offset is 0,
+// else x = BX - 1).  All other cells of the colour are the brick interior,
+// whose neighbours all lie in the brick.
+template <int BX, int BY, int BZ>
+struct ResidentFaces {
+    static constexpr int KX = BX / 2;
+    static constexpr int FZ = 2 * KX * BY;
+    static constexpr int FY = 2 * KX * (BZ - 2);
+    static constexpr int FX = (BY - 2) * (BZ - 2);
+    static constexpr int COUNT = FZ + FY + FX;
+    static constexpr int PER_THREAD = (COUNT + KX * BY - 1) / (KX * BY);
+};
+
+// Row y of thread t in the conflict-free warp mapping (see ResidentShape), and its inverse.
+template <int BX, int BY, int BZ>
+__device__ __forceinline__ void residentColumn(int t, int& k, int& y) {
+    using S = ResidentShape<BX, BY, BZ>;
+    const int lane = t & 31, warp = t >> 5;
+    k = lane % S::KX;
+    y = (warp >> 1) * 2 * S::RPW + (warp & 1) + 2 * (lane / S::KX);
+}
+template <int BX, int BY, int BZ>
+__device__ __forceinline__ int residentOwner(int k, int y) {
+    using S = ResidentShape<BX, BY, BZ>;
+    const int q = y / (2 * S::RPW), rem = y % (2 * S::RPW);
+    return (2 * q + (rem & 1)) * 32 + (rem >> 1) * S::KX + k;
+}
+
+// (k, y, z) of face cell i of colour c, packed k | y << 8 | z << 16.
+template <int BX, int BY, int BZ>
+__device__ __forceinline__ int residentFaceCell(int i, int c) {
+    using F = ResidentFaces<BX, BY, BZ>;
+    int k, y, z;
+    if (i < F::FZ) {
+        const int side = i / (F::KX * BY);
+        residentColumn<BX, BY, BZ>(i % (F::KX * BY), k, y);
+        z = side ? BZ - 1 : 0;
+    } else if (i < F::FZ + F::FY) {
+        const int j = i - F::FZ;
+        const int side = j / (F::KX * (BZ - 2));
+        const int r = j % (F::KX * (BZ - 2));
+        k = r % F::KX;
+        z = 1 + r / F::KX;
+        y = side ? BY - 1 : 0;
+    } else {
+        const int j = i - F::FZ - F::FY;
+        y = 1 + j % (BY - 2);
+        z = 1 + j / (BY - 2);
+        k = ((c + y + z) & 1) ? F::KX - 1 : 0;
+    }
+    return k | (y << 8) | (z << 16);
+}
+
+// Interior cells of colour C in z0 <= z < z1 of this thread's column.  Their
+// neighbours all lie in the brick; only in a brick that the grid's upper
+// walls cut (FULL == false) can a neighbour lie past a wall.
+template <int BX, int BY, int BZ, int C, int Z0, int Z1, bool FULL>
+__device__ __forceinline__ void residentInterior(float* planes, const float* divs, int k, int y, int ox, int oy, int oz, const Grid& g,
+                                                 float omega) {
+    using S = ResidentShape<BX, BY, BZ>;
+    constexpr int O = 1 - C;
+    if (y == 0 || y == BY - 1) return;
+    const int gy = oy + y;
+    if (!FULL && gy >= g.ny) return;
+#pragma unroll
+    for (int z = Z0; z < Z1; ++z) {
+        const int s = (C + y + z) & 1;
+        const int x = 2 * k + s;
+        if (x == 0 || x == BX - 1) continue;
+        const int gx = ox + x, gz = oz + z;
+        if (!FULL && (gx >= g.nx || gz >= g.nz)) continue;
+        const float self = planes[S::pidx(C, z, y, k)];
+        const float pL = planes[S::pidx(O, z, y, k + s - 1)];
+        const float pR = (!FULL && gx == g.nx - 1) ? self : planes[S::pidx(O, z, y, k + s)];
+        const float pD = planes[S::pidx(O, z, y - 1, k)];
+        const float pU = (!FULL && gy == g.ny - 1) ? self : planes[S::pidx(O, z, y + 1, k)];
+        const float pB = planes[S::pidx(O, z - 1, y, k)];
+        const float pF = (!FULL && gz == g.nz - 1) ? self : planes[S::pidx(O, z + 1, y, k)];
+        const float d = divs[S::didx(C, z, threadIdx.x)];
+        const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
+        planes[S::pidx(C, z, y, k)] = self + omega * (projected - self);
+    }
+}
+
+template <int BX, int BY, int BZ, int C, int Z0, int Z1>
+__device__ __forceinline__ void residentInteriorAny(bool full, float* planes, const float* divs, int k, int y, int ox, int oy, int oz,
+                                                    const Grid& g, float omega) {
+    if (full) {
+        residentInterior<BX, BY, BZ, C, Z0, Z1, true>(planes, divs, k, y, ox, oy, oz, g, omega);
+    } else {
+        residentInterior<BX, BY, BZ, C, Z0, Z1, false>(planes, divs, k, y, ox, oy, oz, g, omega);
+    }
+}
+
 }  // namespace
 
+// One half sweep h (colour c) of a brick runs as
+//   interior cells, first half of z
+//   wait for the face neighbours' flags of half sweep h - 1; issue the loads
+//     of their updated face cells (colour 1 - c) into registers
+//   interior cells, second half of z      (hides the loads' latency)
+//   halo registers -> shared memory; barrier
+//   face cells, each also written to global p; barrier; announce h
+// so the neighbour wait and the halo transfer overlap the interior update.
 template <int BX, int BY, int BZ>
 __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g,
                                                                ResidentBrick r, ResidentSync sync, int iterations, float omega) {
     using S = ResidentShape<BX, BY, BZ>;
+    using F = ResidentFaces<BX, BY, BZ>;
     constexpr int KX = S::KX;
+    constexpr int ZMID = BZ / 2;
     extern __shared__ float smem[];
     float* planes = smem;                // [2][EZ][EY][EX]
-    float* divs = smem + 2 * S::PLANE;   // [2][BZ][BY][KX]
+    float* divs = smem + 2 * S::PLANE;   // [2][BZ][THREADS]
     const int brick = blockIdx.x;
     const int bi = brick % r.nbx, bj = (brick / r.nbx) % r.nby, bk = brick / (r.nbx * r.nby);
     const int ox = bi * BX;
     const int oy = bj * BY;
     const int oz = bk * BZ;
+    const bool full = ox + BX <= g.nx && oy + BY <= g.ny && oz + BZ <= g.nz;
     // Threads 0..5 each watch one face neighbour (-x, +x, -y, +y, -z, +z).
     int watched = -1;
     if (threadIdx.x < 6) {
@@ -773,13 +880,12 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             watched = (nk * r.nby + nj) * r.nbx + ni;
         }
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int k = lane % KX;
-    const int y = (warp >> 1) * 2 * S::RPW + (warp & 1) + 2 * (lane / KX);
+    int k, y;
+    residentColumn<BX, BY, BZ>(threadIdx.x, k, y);
     const int gy = oy + y;
 
-    // This thread's halo cells of each colour, fixed for the whole solve.
-    int haloG[2][S::PER_THREAD], haloS[2][S::PER_THREAD];
+    // This thread's halo cells and face cells of each colour, fixed for the whole solve.
+    int haloG[2][S::PER_THREAD], haloS[2][S::PER_THREAD], face[2][F::PER_THREAD];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
 #pragma unroll
@@ -791,18 +897,12 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                 residentHaloCell<BX, BY, BZ>(i, c, ox, oy, oz, g, haloG[c][j], haloS[c][j]);
             }
         }
+#pragma unroll
+        for (int j = 0; j < F::PER_THREAD; ++j) {
+            const int i = threadIdx.x + j * S::THREADS;
+            face[c][j] = i < F::COUNT ? residentFaceCell<BX, BY, BZ>(i, c) : -1;
+        }
     }
-    auto loadHalo = [&](int c) {
-        float v[S::PER_THREAD];
-#pragma unroll
-        for (int j = 0; j < S::PER_THREAD; ++j) {
-            v[j] = haloG[c][j] >= 0 ? __ldcg(pressure + haloG[c][j]) : 0.0f;
-        }
-#pragma unroll
-        for (int j = 0; j < S::PER_THREAD; ++j) {
-            if (haloG[c][j] >= 0) planes[haloS[c][j]] = v[j];
-        }
-    };
 
     // Load both colours of the brick column, then the halo.
 #pragma unroll 4
@@ -818,58 +918,86 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             }
         }
     }
-    loadHalo(0);
-    loadHalo(1);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+        for (int j = 0; j < S::PER_THREAD; ++j) {
+            if (haloG[c][j] >= 0) planes[haloS[c][j]] = __ldcg(pressure + haloG[c][j]);
+        }
+    }
     __syncthreads();
 
-    const bool yFace = y == 0 || y == BY - 1;
-    const bool yIn = gy < g.ny;
     for (int it = 0; it < iterations; ++it) {
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             const int o = 1 - c;
+            const int h = 2 * it + c;
             const bool last = it == iterations - 1 && c == 1;
+            if (c == 0) {
+                residentInteriorAny<BX, BY, BZ, 0, 1, ZMID>(full, planes, divs, k, y, ox, oy, oz, g, omega);
+            } else {
+                residentInteriorAny<BX, BY, BZ, 1, 1, ZMID>(full, planes, divs, k, y, ox, oy, oz, g, omega);
+            }
+            float haloV[S::PER_THREAD];
+            if (h > 0) {
+                bool failed = false;
+                if (watched >= 0) {
+                    failed = !residentWait(sync.flags + watched * kResidentFlagStride, sync.epoch + static_cast<unsigned>(h), sync, brick);
+                    __threadfence();
+                }
+                if (__syncthreads_or(failed)) {
+                    return;
+                }
 #pragma unroll
-            for (int z = 0; z < BZ; ++z) {
-                const int s = (c + y + z) & 1;
-                const int x = 2 * k + s;
-                const int gx = ox + x, gz = oz + z;
-                if (gx < g.nx && yIn && gz < g.nz) {
-                    const float self = planes[S::pidx(c, z, y, k)];
-                    const float pL = gx == 0 ? self : planes[S::pidx(o, z, y, k + s - 1)];
-                    const float pR = gx == g.nx - 1 ? self : planes[S::pidx(o, z, y, k + s)];
-                    const float pD = gy == 0 ? self : planes[S::pidx(o, z, y - 1, k)];
-                    const float pU = gy == g.ny - 1 ? self : planes[S::pidx(o, z, y + 1, k)];
-                    const float pB = gz == 0 ? self : planes[S::pidx(o, z - 1, y, k)];
-                    const float pF = gz == g.nz - 1 ? self : planes[S::pidx(o, z + 1, y, k)];
-                    const float d = divs[S::didx(c, z, threadIdx.x)];
-                    const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
-                    const float next = self + omega * (projected - self);
-                    planes[S::pidx(c, z, y, k)] = next;
-                    if (!last && (yFace || z == 0 || z == BZ - 1 || x == 0 || x == BX - 1)) {
-                        __stcg(pressure + (gz * g.ny + gy) * g.nx + gx, next);
-                    }
+                for (int j = 0; j < S::PER_THREAD; ++j) {
+                    haloV[j] = haloG[o][j] >= 0 ? __ldcg(pressure + haloG[o][j]) : 0.0f;
+                }
+            }
+            if (c == 0) {
+                residentInteriorAny<BX, BY, BZ, 0, ZMID, BZ - 1>(full, planes, divs, k, y, ox, oy, oz, g, omega);
+            } else {
+                residentInteriorAny<BX, BY, BZ, 1, ZMID, BZ - 1>(full, planes, divs, k, y, ox, oy, oz, g, omega);
+            }
+            if (h > 0) {
+#pragma unroll
+                for (int j = 0; j < S::PER_THREAD; ++j) {
+                    if (haloG[o][j] >= 0) planes[haloS[o][j]] = haloV[j];
+                }
+            }
+            __syncthreads();
+            // Face cells, with the walls of the grid.
+#pragma unroll
+            for (int j = 0; j < F::PER_THREAD; ++j) {
+                const int cell = face[c][j];
+                if (cell < 0) continue;
+                const int fk = cell & 0xff, fy = (cell >> 8) & 0xff, fz = cell >> 16;
+                const int s = (c + fy + fz) & 1;
+                const int fx = 2 * fk + s;
+                const int gx = ox + fx, fgy = oy + fy, gz = oz + fz;
+                if (gx >= g.nx || fgy >= g.ny || gz >= g.nz) continue;
+                const float self = planes[S::pidx(c, fz, fy, fk)];
+                const float pL = gx == 0 ? self : planes[S::pidx(o, fz, fy, fk + s - 1)];
+                const float pR = gx == g.nx - 1 ? self : planes[S::pidx(o, fz, fy, fk + s)];
+                const float pD = fgy == 0 ? self : planes[S::pidx(o, fz, fy - 1, fk)];
+                const float pU = fgy == g.ny - 1 ? self : planes[S::pidx(o, fz, fy + 1, fk)];
+                const float pB = gz == 0 ? self : planes[S::pidx(o, fz - 1, fy, fk)];
+                const float pF = gz == g.nz - 1 ? self : planes[S::pidx(o, fz + 1, fy, fk)];
+                const float d = divs[S::didx(c, fz, residentOwner<BX, BY, BZ>(fk, fy))];
+                const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
+                const float next = self + omega * (projected - self);
+                planes[S::pidx(c, fz, fy, fk)] = next;
+                if (!last) {
+                    __stcg(pressure + (gz * g.ny + fgy) * g.nx + gx, next);
                 }
             }
             if (last) {
                 break;
             }
-            const unsigned target = sync.epoch + static_cast<unsigned>(2 * it + c + 1);
             __syncthreads();
             if (threadIdx.x == 0 && brick != sync.silentBrick) {
                 __threadfence();
-                storeVolatile(sync.flags + brick * kResidentFlagStride, target);
+                storeVolatile(sync.flags + brick * kResidentFlagStride, sync.epoch + static_cast<unsigned>(h + 1));
             }
-            bool failed = false;
-            if (watched >= 0) {
-                failed = !residentWait(sync.flags + watched * kResidentFlagStride, target, sync, brick);
-                __threadfence();
-            }
-            if (__syncthreads_or(failed)) {
-                return;
-            }
-            loadHalo(c);
-            __syncthreads();
         }
     }
     __syncthreads();

@@ -68,6 +68,7 @@ def load_library() -> ctypes.CDLL:
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
         "fireCudaSetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
         "fireCudaRunStages": (b, [ctypes.c_int, ctypes.c_int, S, ctypes.c_float]),
+        "fireCudaRunStagesAsync": (b, [ctypes.c_int, ctypes.c_int, S, ctypes.c_float]),
         "fireCudaGetTimes": (b, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]),
         "fireCudaSetTimes": (b, [ctypes.c_float, ctypes.c_float, ctypes.c_int]),
         "fireCudaGetStream": (b, [ctypes.POINTER(ctypes.c_void_p)]),
@@ -190,9 +191,11 @@ class FireSim:
         a = np.ascontiguousarray(arr, dtype=dtype).reshape(self.shape_of(name))
         self._check(self.lib.fireCudaSetField(abi.FIELDS[name], a.ctypes.data, a.nbytes), f"set {name}")
 
-    def stages(self, first: str, last: str, settings, time: float) -> None:
+    def stages(self, first: str, last: str, settings, time: float, wait: bool = True) -> None:
+        """Runs stages first..last; with wait=False only queues them on stream()."""
         s = abi.STAGES
-        self._check(self.lib.fireCudaRunStages(s[first], s[last], ctypes.byref(settings), time), f"stages {first}..{last}")
+        fn = self.lib.fireCudaRunStages if wait else self.lib.fireCudaRunStagesAsync
+        self._check(fn(s[first], s[last], ctypes.byref(settings), time), f"stages {first}..{last}")
 
     def times(self):
         t, r, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
