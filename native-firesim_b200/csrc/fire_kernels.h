@@ -29,23 +29,24 @@ struct ResidentBrick {
     int bx, by, bz;     // brick extent, all even
     int nbx, nby, nbz;  // bricks per axis
 };
-// Neighbour-to-neighbour synchronisation of the resident SOR.  Brick b
-// announces that its face cells of half sweep h are in global memory by
-// storing epoch + h + 1 into flags[b * kResidentFlagStride]; its six
-// neighbours wait for that value before reading them.  Every wait gives up
-// after waitNs nanoseconds (or kResidentMaxPolls polls), records epoch + 1 in
-// *status so the other bricks stop waiting too, writes brick + 1 into the
-// host-mapped *hostStatus and returns.  silentBrick >= 0 is a host-side fault
-// injection: that brick never announces, so its neighbours' waits run out.
+// Brick-to-brick exchange of the resident SOR.  After half sweep h a brick
+// publishes each of its face cells as one 64-bit word into exchange[cell]:
+// the value's bits in the high half, epoch + h + 1 in the low half.  A
+// neighbour that needs the cell for half sweep h + 1 polls that word until
+// the tag matches; value and tag travel in one single-copy-atomic store, so
+// there is no separate flag and no fence.  Every poll gives up after waitNs
+// nanoseconds (or kResidentMaxPolls polls), records epoch + 1 in *status so
+// the other bricks stop waiting too, writes brick + 1 into the host-mapped
+// *hostStatus and returns.  silentBrick >= 0 is a host-side fault injection:
+// that brick never publishes, so its neighbours' polls run out.
 struct ResidentSync {
-    unsigned* flags;
+    unsigned long long* exchange;  // one word per grid cell (only face cells are written)
     unsigned* status;
     unsigned* hostStatus;
     unsigned epoch;
     int silentBrick;
     unsigned long long waitNs;
 };
-constexpr int kResidentFlagStride = 32;  // one 128-byte line per brick
 constexpr unsigned kResidentMaxPolls = 1u << 24;
 constexpr int kMetricThreads = 128;
 

@@ -66,13 +66,14 @@ void Scene::release() {
     }
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
-                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorSync_, curlLattice_, sourceLattice_};
+                    shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
     if (metricHost_ != nullptr) cudaFreeHost(metricHost_);
     if (sorHostStatus_ != nullptr) cudaFreeHost(sorHostStatus_);
-    sorSync_ = nullptr;
+    sorStatus_ = nullptr;
+    sorExchange_ = nullptr;
     sorHostStatus_ = nullptr;
     curlLattice_ = nullptr;
     sourceLattice_ = nullptr;
@@ -146,10 +147,11 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
          alloc(reinterpret_cast<void**>(&partials_), kMetricBlocks * sizeof(MetricPartial), "cudaMalloc metric partials", err) &&
          alloc(reinterpret_cast<void**>(&metricDevice_), sizeof(MetricPartial), "cudaMalloc metrics", err) &&
          check("cudaMallocHost metrics", cudaMallocHost(reinterpret_cast<void**>(&metricHost_), sizeof(MetricPartial)), err);
-    // Flag lines for the largest brick plan (16^3 bricks) plus the status line.
-    sorFlagLines_ = 1 + static_cast<size_t>((nx + 15) / 16) * ((ny + 15) / 16) * ((nz + 15) / 16);
-    ok = ok && alloc(reinterpret_cast<void**>(&sorSync_), sorFlagLines_ * kResidentFlagStride * sizeof(unsigned), "cudaMalloc SOR flags", err) &&
-         check("clear SOR flags", cudaMemsetAsync(sorSync_, 0, sorFlagLines_ * kResidentFlagStride * sizeof(unsigned), stream), err) &&
+    // Resident SOR: the tagged exchange words (zero tags never match) and the failure status.
+    ok = ok && alloc(reinterpret_cast<void**>(&sorExchange_), cells_ * sizeof(unsigned long long), "cudaMalloc SOR exchange", err) &&
+         check("clear SOR exchange", cudaMemsetAsync(sorExchange_, 0, cells_ * sizeof(unsigned long long), stream), err) &&
+         alloc(reinterpret_cast<void**>(&sorStatus_), sizeof(unsigned), "cudaMalloc SOR status", err) &&
+         check("clear SOR status", cudaMemsetAsync(sorStatus_, 0, sizeof(unsigned), stream), err) &&
          check("cudaHostAlloc SOR status", cudaHostAlloc(reinterpret_cast<void**>(&sorHostStatus_), sizeof(unsigned), cudaHostAllocMapped), err);
     if (ok) *sorHostStatus_ = 0;
     {
@@ -345,7 +347,7 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
             Grid g{nx, ny, nz};
             int iterations = pressureIterations;
             float omega = pressureOmega;
-            ResidentSync sync{sorSync_ + kResidentFlagStride, sorSync_, sorHostStatus_, sorEpoch_, sorSilentBrick_, sorWaitNs_};
+            ResidentSync sync{sorExchange_, sorStatus_, sorHostStatus_, sorEpoch_, sorSilentBrick_, sorWaitNs_};
             sorEpoch_ += 2u * static_cast<unsigned>(iterations);
             void* args[] = {&pressure_, &divergence_, &g, &r, &sync, &iterations, &omega};
             const unsigned bricks = static_cast<unsigned>(r.nbx * r.nby * r.nbz);

@@ -128,9 +128,9 @@ private:
     bool sourceLattice(const FrameParams& p, HashLattice2& l) const;
     float* sourceLattice_ = nullptr;
     size_t sourceCapacity_ = 0;
-    unsigned* sorSync_ = nullptr;        // device: [0] status, then one flag line per brick
+    unsigned* sorStatus_ = nullptr;               // device: failure tag of the resident SOR
+    unsigned long long* sorExchange_ = nullptr;   // device: one tagged word per cell (face cells)
     unsigned* sorHostStatus_ = nullptr;  // host-mapped: brick + 1 of a wait that ran out
-    size_t sorFlagLines_ = 0;
     unsigned sorEpoch_ = 0;
     int sorSilentBrick_ = -1;
     unsigned long long sorWaitNs_ = 1000000000ull;

@@ -637,17 +637,16 @@ namespace firesim {
 // colour pattern equals the global one) and keeps its p and div in shared
 // memory, split by colour: for colour c, row (y, z) holds the cells
 // x = 2k + ((c + y + z) & 1), k = 0..BX/2-1, so a cell's x/y/z-neighbour reads
-// of the other colour are unit-stride.  Thread t owns the column
-// (k = t % KX, y = t / KX) of both colours and walks z.  A half sweep writes
-// its updated face cells straight to global p and announces them through the
-// brick's flag (ResidentSync); each brick then waits for its six neighbours'
-// flags only -- no grid-wide barrier -- and reads their updated face cells
-// into its one-cell halo, all of a thread's halo loads in flight at once.
-// The cooperative launch guarantees that all bricks are resident, so every
-// wait is for a running CTA; each wait is still bounded in time.  Walls are
-// Neumann through the clamped neighbour (the cell itself), as in
-// sorPressureParityKernel.  Per-cell arithmetic is identical to sorHalfSweep,
-// so the result is bit-identical to the per-launch path.
+// of the other colour are unit-stride.  Each thread owns one (k, y) column
+// of both colours and walks z.  A half sweep publishes its updated face cells
+// as tagged 64-bit words (value, half sweep) in an exchange array
+// (ResidentSync); a neighbour that needs them polls those words until the tag
+// matches -- no grid-wide barrier, no flags, no fences -- and copies them into
+// its one-cell halo.  The cooperative launch guarantees that all bricks are
+// resident, so every poll is for a running CTA; each poll is still bounded in
+// time.  Walls are Neumann through the clamped neighbour (the cell itself), as
+// in sorPressureParityKernel.  Per-cell arithmetic is identical to
+// sorHalfSweep, so the result is bit-identical to the per-launch path.
 namespace {
 
 __device__ __forceinline__ unsigned loadVolatile(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
@@ -658,13 +657,24 @@ __device__ __forceinline__ unsigned long long globalTimerNs() {
     return t;
 }
 
-// Bounded wait until *flag has reached target (wrap-safe).  False when the
-// wait ran out or another brick's wait already did.
-__device__ bool residentWait(const unsigned* flag, unsigned target, const ResidentSync& sync, int brick) {
+__device__ __forceinline__ unsigned long long loadExchange(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void storeExchange(unsigned long long* p, float value, unsigned tag) {
+    const unsigned long long v = (static_cast<unsigned long long>(__float_as_uint(value)) << 32) | tag;
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Bounded poll until the exchange word at p carries tag `want`; the word is
+// returned in w.  False when the poll ran out or another brick's did.
+__device__ bool residentAwait(const unsigned long long* p, unsigned want, const ResidentSync& sync, int brick, unsigned long long& w) {
     const unsigned failTag = sync.epoch + 1u;
     unsigned long long start = 0;
     for (unsigned n = 0; n < kResidentMaxPolls; ++n) {
-        if (static_cast<int>(loadVolatile(flag) - target) >= 0) {
+        w = loadExchange(p);
+        if (static_cast<unsigned>(w) == want) {
             return true;
         }
         if ((n & 15u) == 15u) {
@@ -849,12 +859,12 @@ __device__ __forceinline__ void residentInteriorAny(bool full, float* planes, co
 
 // One half sweep h (colour c) of a brick runs as
 //   interior cells, first half of z
-//   wait for the face neighbours' flags of half sweep h - 1; issue the loads
-//     of their updated face cells (colour 1 - c) into registers
+//   issue the loads of the neighbours' face cells (colour 1 - c) of half
+//     sweep h - 1 from the tagged exchange words
 //   interior cells, second half of z      (hides the loads' latency)
-//   halo registers -> shared memory; barrier
-//   face cells, each also written to global p; barrier; announce h
-// so the neighbour wait and the halo transfer overlap the interior update.
+//   words whose tag is not yet h: poll until it is; values -> halo; barrier
+//   face cells, each also published as a tagged word; barrier
+// so the exchange overlaps the interior update and costs one L2 round trip.
 template <int BX, int BY, int BZ>
 __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g,
                                                                ResidentBrick r, ResidentSync sync, int iterations, float omega) {
@@ -871,15 +881,7 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
     const int oy = bj * BY;
     const int oz = bk * BZ;
     const bool full = ox + BX <= g.nx && oy + BY <= g.ny && oz + BZ <= g.nz;
-    // Threads 0..5 each watch one face neighbour (-x, +x, -y, +y, -z, +z).
-    int watched = -1;
-    if (threadIdx.x < 6) {
-        const int axis = threadIdx.x >> 1, step = (threadIdx.x & 1) ? 1 : -1;
-        const int ni = bi + (axis == 0 ? step : 0), nj = bj + (axis == 1 ? step : 0), nk = bk + (axis == 2 ? step : 0);
-        if (ni >= 0 && ni < r.nbx && nj >= 0 && nj < r.nby && nk >= 0 && nk < r.nbz) {
-            watched = (nk * r.nby + nj) * r.nbx + ni;
-        }
-    }
+    const bool silent = brick == sync.silentBrick;
     int k, y;
     residentColumn<BX, BY, BZ>(threadIdx.x, k, y);
     const int gy = oy + y;
@@ -938,19 +940,13 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             } else {
                 residentInteriorAny<BX, BY, BZ, 1, 1, ZMID>(full, planes, divs, k, y, ox, oy, oz, g, omega);
             }
-            float haloV[S::PER_THREAD];
+            // The neighbours' face cells of colour o from half sweep h - 1, in flight during the second half.
+            unsigned long long haloW[S::PER_THREAD];
+            const unsigned want = sync.epoch + static_cast<unsigned>(h);
             if (h > 0) {
-                bool failed = false;
-                if (watched >= 0) {
-                    failed = !residentWait(sync.flags + watched * kResidentFlagStride, sync.epoch + static_cast<unsigned>(h), sync, brick);
-                    __threadfence();
-                }
-                if (__syncthreads_or(failed)) {
-                    return;
-                }
 #pragma unroll
                 for (int j = 0; j < S::PER_THREAD; ++j) {
-                    haloV[j] = haloG[o][j] >= 0 ? __ldcg(pressure + haloG[o][j]) : 0.0f;
+                    haloW[j] = haloG[o][j] >= 0 ? loadExchange(sync.exchange + haloG[o][j]) : 0ull;
                 }
             }
             if (c == 0) {
@@ -958,13 +954,22 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             } else {
                 residentInteriorAny<BX, BY, BZ, 1, ZMID, BZ - 1>(full, planes, divs, k, y, ox, oy, oz, g, omega);
             }
+            bool failed = false;
             if (h > 0) {
 #pragma unroll
                 for (int j = 0; j < S::PER_THREAD; ++j) {
-                    if (haloG[o][j] >= 0) planes[haloS[o][j]] = haloV[j];
+                    if (haloG[o][j] >= 0) {
+                        unsigned long long w = haloW[j];
+                        if (static_cast<unsigned>(w) != want && !failed) {
+                            failed = !residentAwait(sync.exchange + haloG[o][j], want, sync, brick, w);
+                        }
+                        planes[haloS[o][j]] = __uint_as_float(static_cast<unsigned>(w >> 32));
+                    }
                 }
             }
-            __syncthreads();
+            if (__syncthreads_or(failed)) {
+                return;
+            }
             // Face cells, with the walls of the grid.
 #pragma unroll
             for (int j = 0; j < F::PER_THREAD; ++j) {
@@ -986,18 +991,14 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                 const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
                 const float next = self + omega * (projected - self);
                 planes[S::pidx(c, fz, fy, fk)] = next;
-                if (!last) {
-                    __stcg(pressure + (gz * g.ny + fgy) * g.nx + gx, next);
+                if (!last && !silent) {
+                    storeExchange(sync.exchange + (gz * g.ny + fgy) * g.nx + gx, next, sync.epoch + static_cast<unsigned>(h + 1));
                 }
             }
             if (last) {
                 break;
             }
             __syncthreads();
-            if (threadIdx.x == 0 && brick != sync.silentBrick) {
-                __threadfence();
-                storeVolatile(sync.flags + brick * kResidentFlagStride, sync.epoch + static_cast<unsigned>(h + 1));
-            }
         }
     }
     __syncthreads();
