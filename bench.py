@@ -155,7 +155,7 @@ STAGE_BYTES_PER_CELL = {
     "advect_velocity": 24.0,          # read 3 faces + write 3 faces (velocity gathers hit L1/L2)
     "advect_react": 40.0 * 2 + 12.0,  # read + write the 10 scalars, read the 3 faces
     "force_project": 16.0 + 12.0 * 2 + 16.0 + 8.0,  # read heat/soot/k/progress, read+write faces, force scratch w+r, div+p
-    "pressure_sor": 6.0,              # per half-sweep: 12 B/cell per iteration (read p, write p, read div)
+    "pressure_sor": 6.0,              # per half sweep: 12 B/cell per iteration (read p, write p, read div)
     "subtract_walls": 4.0 + 24.0,     # read p, read+write faces
     "light": 0.0,                     # quarter-resolution grid, small
 }
@@ -352,7 +352,7 @@ def main() -> int:
     per_step_ms = {k: (v / args.render_every if k in ("render", "embers") else v) for k, v in st.items()}
     dominant = max(per_step_ms, key=per_step_ms.get)
     peaks, peak_src = measured_peaks()
-    roofline = roofline_block(dominant, st, args, cells, peaks, peak_src)
+    roofline = roofline_block(dominant, st, args, cells, peaks, peak_src, sim.pressure_path_used())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -381,12 +381,25 @@ def ctypes_sizeof_settings(abi) -> int:
     return ctypes.sizeof(abi.FireSettings)
 
 
-def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str) -> dict:
-    """achieved = algorithmic bytes of one launch / that launch's average device time."""
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the
+# dominant kernel, from one ncu capture of this workload (128^3, SOR 60).
+NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): None}
+
+
+def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str, sor_path: int) -> dict:
+    """achieved = algorithmic bytes of one launch / that launch's device time.
+
+    The pressure solve's algorithmic bytes are those of the global-memory
+    formulation, 12 B per cell per iteration (read p, write p, read div).  The
+    resident path runs the whole solve as one launch, so its launch carries
+    all N iterations; the per-launch path has one launch per half sweep."""
+    traffic = None
     if dominant == "pressure_sor":
-        launches = 2 * args.sor_iters
+        resident = sor_path == 2
+        launches = 1 if resident else 2 * args.sor_iters
         per_launch_ms = st["pressure_sor"] / launches
-        bytes_per_launch = STAGE_BYTES_PER_CELL["pressure_sor"] * cells
+        bytes_per_launch = 12.0 * args.sor_iters * cells / launches
+        traffic = NCU_TRAFFIC_BYTES.get(("pressure_sor", "resident" if resident else "graph", args.grid, args.sor_iters))
     elif dominant in STAGE_BYTES_PER_CELL and STAGE_BYTES_PER_CELL[dominant] > 0:
         per_launch_ms = st[dominant]
         bytes_per_launch = STAGE_BYTES_PER_CELL[dominant] * cells
@@ -397,7 +410,7 @@ def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     return {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
             "bytes_per_launch": bytes_per_launch, "launch_ms": per_launch_ms}
 
 

@@ -176,7 +176,7 @@ bool fireCudaGetDiagnostics(FireCudaDiagnostics* diagnostics) {
     out.computeMajor = props.major;
     out.computeMinor = props.minor;
     out.totalGlobalMem = static_cast<uint64_t>(props.totalGlobalMem);
-    std::snprintf(out.deviceName, sizeof(out.deviceName), "%s", props.name);
+    std::snprintf(out.deviceName, sizeof(out.deviceName), "%.*s", static_cast<int>(sizeof(out.deviceName) - 1), props.name);
     *diagnostics = out;
     return true;
 }

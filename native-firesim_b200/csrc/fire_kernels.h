@@ -78,7 +78,18 @@ __global__ void lightPropagate(float4* outLight, const float4* inLight, const fl
                                float decay);
 
 // fire_render.cu
-__global__ void raymarch(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p);
+// Work list of the raymarch: 8x4-pixel tiles taken by warps from *counter
+// (zeroed before each launch), in the order of `order` (tile ids, x fastest).
+constexpr int kRayTileW = 8, kRayTileH = 4;
+struct RayTiles {
+    int* counter;
+    const int* order;
+    int tilesX;
+    int count;
+};
+__global__ void hashLattice3Build(RenderLattices lat);
+__global__ void raymarch(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p, RayTiles tiles,
+                         RenderLattices lat);
 __global__ void emberSetup(EmberSplat* embers, ScalarFieldsIn s, Velocity vel, FrameParams p);
 __global__ void emberGather(float4* hdr, const EmberSplat* embers, FrameParams p);
 __global__ void tonemapOverlay(uint32_t* frame, const float4* hdr, FrameParams p, int doTonemap, int doOverlay);

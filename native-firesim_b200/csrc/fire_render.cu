@@ -306,15 +306,13 @@ __device__ __forceinline__ float3 debugHeatColor(float value) {  // src/fire_cud
 
 }  // namespace
 
-// src/fire_cuda.cu:1953-2244 -- one primary ray per pixel through the packed
-// field records; writes RGB and alpha = 1 to the internal HDR frame.
-__global__ void __launch_bounds__(128) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
-                                                const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= p.frameW || y >= p.frameH) {
-        return;
-    }
+namespace {
+
+// src/fire_cuda.cu:1953-2244 -- one primary ray through the packed field
+// records; writes RGB and alpha = 1 to pixel (x, y) of the internal HDR frame.
+__device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int y, const ScalarFieldsIn& s, const Velocity& vel,
+                                           const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
+                                           const RenderLattices& lat) {
     const Grid g{p.nx, p.ny, p.nz};
     const LightGrid L{p.lnx, p.lny, p.lnz};
     const float2 uv = make_float2((static_cast<float>(x) + 0.5f) / static_cast<float>(p.frameW),
@@ -357,8 +355,8 @@ __global__ void __launch_bounds__(128) raymarch(float4* __restrict__ out, Scalar
                 ++i;
                 continue;
             }
-            const float warpA = fbm3(fu * 7.0f + p.time * 0.18f, fv * 5.0f - p.time * 0.11f, fw * 9.0f + p.time * 0.07f) - 0.5f;
-            const float warpB = fbm3(fw * 8.0f - p.time * 0.14f, fu * 8.0f + p.time * 0.10f, fv * 6.0f - p.time * 0.08f) - 0.5f;
+            const float warpA = fbm3Lattice(fu * 7.0f + p.time * 0.18f, fv * 5.0f - p.time * 0.11f, fw * 9.0f + p.time * 0.07f, lat.warpA) - 0.5f;
+            const float warpB = fbm3Lattice(fw * 8.0f - p.time * 0.14f, fu * 8.0f + p.time * 0.10f, fv * 6.0f - p.time * 0.08f, lat.warpB) - 0.5f;
             const float warpGain = 0.028f + fv * 0.060f;
             const float wu = saturate(fu + warpA * warpGain);
             const float wv = saturate(fv + (warpA - warpB) * 0.020f);
@@ -389,8 +387,8 @@ __global__ void __launch_bounds__(128) raymarch(float4* __restrict__ out, Scalar
             const float gradHeatZ = sampleHeat(s, g, wu, wv, ww + cellZ) - sampleHeat(s, g, wu, wv, ww - cellZ);
             const float frontGradient = sqrtf(gradHeatX * gradHeatX + gradHeatY * gradHeatY + gradHeatZ * gradHeatZ) + fabsf(fuel - coarseFuel) * 0.62f;
             const float reactionFront = smoothstepf(0.020f, 0.46f, frontGradient * 1.35f + fuel * oxygen * 0.040f + progress * 0.18f + pyrolysis * 0.080f);
-            const float fineNoise = fbm3(wu * 42.0f + p.time * 0.72f, wv * 54.0f - p.time * 1.28f, ww * 43.0f + p.time * 0.38f);
-            const float shearNoise = fbm3(wu * 15.0f - p.time * 0.72f, wv * 13.0f - p.time * 1.08f, ww * 17.0f + p.time * 0.32f);
+            const float fineNoise = fbm3Lattice(wu * 42.0f + p.time * 0.72f, wv * 54.0f - p.time * 1.28f, ww * 43.0f + p.time * 0.38f, lat.fine);
+            const float shearNoise = fbm3Lattice(wu * 15.0f - p.time * 0.72f, wv * 13.0f - p.time * 1.08f, ww * 17.0f + p.time * 0.32f, lat.shear);
             const float plumeNoise = saturate(fineNoise * 0.58f + shearNoise * 0.42f);
             const float holeNoise = saturate((1.0f - fineNoise) * 0.36f + shearNoise * 0.64f);
             const float lesBreakup = saturate(turbulenceEnergy * 0.48f + progress * 0.28f);
@@ -573,6 +571,54 @@ __global__ void __launch_bounds__(128) raymarch(float4* __restrict__ out, Scalar
     const float bloom = saturate(flameGlow * 0.10f) * (1.0f - saturate(smokeOcclusion * 0.95f));
     color = add3(color, mul3(make_float3(1.0f, 0.25f, 0.045f), bloom * bloom * 0.017f * p.reflectionGain));
     out[y * p.frameW + x] = make_float4(fmaxf(0.0f, color.x), fmaxf(0.0f, color.y), fmaxf(0.0f, color.z), 1.0f);
+}
+
+}  // namespace
+
+// hash31 at every entry of the raymarch's four fbm3 lattices of this frame
+// (blockIdx.y selects the lattice); the same function as the in-place hash.
+__global__ void __launch_bounds__(256) hashLattice3Build(RenderLattices lat) {
+    const HashLattice3& L = blockIdx.y == 0 ? lat.warpA : (blockIdx.y == 1 ? lat.warpB : (blockIdx.y == 2 ? lat.fine : lat.shear));
+    float* out = const_cast<float*>(L.values);
+    if (out == nullptr) return;
+    constexpr int last = kFbm3Octaves - 1;
+    const int total = L.offset[last] + L.sx[last] * L.sy[last] * L.sz[last];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int o = 0;
+        while (o + 1 < kFbm3Octaves && i >= L.offset[o + 1]) ++o;
+        const int local = i - L.offset[o];
+        const int tx = local % L.sx[o];
+        const int ty = (local / L.sx[o]) % L.sy[o];
+        const int tz = local / (L.sx[o] * L.sy[o]);
+        out[i] = hash31(static_cast<float>(L.ox[o] + tx), static_cast<float>(L.oy[o] + ty), static_cast<float>(L.oz[o] + tz));
+    }
+}
+
+// Rays through the flame cost many times more than rays that miss it, so a
+// static grid leaves most SMs idle while the last blocks finish.  Here every
+// warp repeatedly takes the next 8x4-pixel tile from a counter, in an order
+// that starts at the centre of the frame (where the fire box projects) and
+// ends at the corners, until no tile is left.
+__global__ void __launch_bounds__(128, 5) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+                                                   const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
+                                                   RayTiles tiles, RenderLattices lat) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) {
+            t = atomicAdd(tiles.counter, 1);
+        }
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= tiles.count) {
+            break;
+        }
+        const int tile = __ldg(tiles.order + t);
+        const int x = (tile % tiles.tilesX) * kRayTileW + (lane % kRayTileW);
+        const int y = (tile / tiles.tilesX) * kRayTileH + (lane / kRayTileW);
+        if (x < p.frameW && y < p.frameH) {
+            shadePixel(out, x, y, s, vel, lightF, shadowF, p, lat);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -870,7 +870,6 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                                                                ResidentBrick r, ResidentSync sync, int iterations, float omega) {
     using S = ResidentShape<BX, BY, BZ>;
     using F = ResidentFaces<BX, BY, BZ>;
-    constexpr int KX = S::KX;
     constexpr int ZMID = BZ / 2;
     extern __shared__ float smem[];
     float* planes = smem;                // [2][EZ][EY][EX]
