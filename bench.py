@@ -315,16 +315,23 @@ def main() -> int:
     torch.cuda.synchronize()
     sampler.start()
     launches0 = sim.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    for _ in range(args.steps):
+    # One event per step boundary on the scene stream: the whole interval is
+    # the timed region, the gaps give the per-step device latency.
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    marks[0].record(ext)
+    for i in range(args.steps):
         one_step()
-    e1.record(ext)
+        marks[i + 1].record(ext)
+    e0, e1 = marks[0], marks[-1]
     e1.synchronize()
     torch.cuda.synchronize()
     dist_barrier(world)
     clocks = sampler.stop()
     launches = sim.launch_count() - launches0
+    step_ms = np.array([marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)])
+    latency = {"unit": "ms", "p50": float(np.percentile(step_ms, 50)), "p95": float(np.percentile(step_ms, 95)),
+               "p99": float(np.percentile(step_ms, 99)), "max": float(step_ms.max()),
+               "note": "device time per step from events at step boundaries; steps that render a frame form the tail"}
     device_s = dist_max(e0.elapsed_time(e1) / 1e3, world)
     cells = args.grid ** 3
     value = cells * args.steps * world / device_s
@@ -336,21 +343,38 @@ def main() -> int:
         dist_barrier(world)
         sim.synchronize()
         t0 = time.perf_counter()
+        frame_marks = [t0]
         for _ in range(args.steps):
             one_step(host_bgra=host)
+            if (frame - 1) % args.render_every == args.render_every - 1:
+                frame_marks.append(time.perf_counter())  # the BGRA call returns with its frame on the host
         sim.synchronize()
         wall = dist_max(time.perf_counter() - t0, world)
+        frame_ms = np.diff(np.array(frame_marks)) * 1e3
         renders = sum(1 for f in range(frame - args.steps, frame) if f % args.render_every == args.render_every - 1)
         e2e = {"value": cells * args.steps * world / wall, "unit": "voxel-steps/s",
                "h2d_bytes_per_step": int(ctypes_sizeof_settings(abi)),
                "d2h_bytes_per_step": int(renders * args.frame * args.frame * 4 / args.steps),
                "ms_per_step": wall * 1e3 / args.steps}
+        if len(frame_ms):
+            e2e["frame_latency_ms"] = {"p50": float(np.percentile(frame_ms, 50)), "p95": float(np.percentile(frame_ms, 95)),
+                                       "p99": float(np.percentile(frame_ms, 99)),
+                                       "note": f"host wall time per BGRA frame: {args.render_every} steps + render + readback"}
 
     # Per-stage device times and the roofline of the dominant kernel.
     s = workload_settings(abi, frame, args)
     st = stage_timings(pkg, sim, args, s)
     per_step_ms = {k: (v / args.render_every if k in ("render", "embers") else v) for k, v in st.items()}
-    dominant = max(per_step_ms, key=per_step_ms.get)
+    # The stage pass renders the final, most developed fire; the timed region's
+    # own frames cost less.  Their mean extra device time over a plain step
+    # (from the step latencies) gives the render's share of the timed steps.
+    render_steps = [i for i in range(args.steps) if (args.warmup + i) % args.render_every == args.render_every - 1]
+    plain_steps = [i for i in range(args.steps) if i not in set(render_steps)]
+    if render_steps and plain_steps:
+        render_in_region_ms = float(np.mean(step_ms[render_steps]) - np.median(step_ms[plain_steps]))
+        per_step_ms["render_end_state"] = per_step_ms["render"]
+        per_step_ms["render"] = render_in_region_ms / args.render_every
+    dominant = max((k for k in per_step_ms if k != "render_end_state"), key=per_step_ms.get)
     peaks, peak_src = measured_peaks()
     roofline = roofline_block(dominant, st, args, cells, peaks, peak_src, sim.pressure_path_used())
 
@@ -366,7 +390,7 @@ def main() -> int:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural fuel bed + validation-harness settings)",
             "config": config_block(args), "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-            "roofline": roofline, "stage_ms": per_step_ms, "cpu_baseline": cpu,
+            "roofline": roofline, "stage_ms": per_step_ms, "step_latency": latency, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     sim.close()
@@ -383,7 +407,7 @@ def ctypes_sizeof_settings(abi) -> int:
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the
 # dominant kernel, from one ncu capture of this workload (128^3, SOR 60).
-NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): None}
+NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): 30157312 + 1525760}
 
 
 def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str, sor_path: int) -> dict:

@@ -98,6 +98,13 @@ FIRE_API bool fireCudaSetPressureSolver(int iterations, float omega);
  * fit). */
 FIRE_API bool fireCudaSetPressurePath(int path);
 
+/* Hash lattices (default on): fbm fields evaluated over the whole grid or
+ * frame read their sin hashes from a table built once per step or frame.
+ * Off, every corner is hashed in place.  The results are the same bits either
+ * way; the switch exists to test that and to measure the tables' effect.  No
+ * counterpart in the reference, which always hashes in place. */
+FIRE_API bool fireCudaSetHashLattices(int enabled);
+
 /* Path the latest SOR solve took: 0 = none yet (or no grid), 1 = one launch
  * per half sweep, 2 = shared-memory-resident. */
 FIRE_API int fireCudaGetPressurePathUsed(void);

@@ -176,7 +176,9 @@ bool fireCudaGetDiagnostics(FireCudaDiagnostics* diagnostics) {
     out.computeMajor = props.major;
     out.computeMinor = props.minor;
     out.totalGlobalMem = static_cast<uint64_t>(props.totalGlobalMem);
-    std::snprintf(out.deviceName, sizeof(out.deviceName), "%.*s", static_cast<int>(sizeof(out.deviceName) - 1), props.name);
+    const size_t nameLen = strnlen(props.name, sizeof(out.deviceName) - 1);
+    std::memcpy(out.deviceName, props.name, nameLen);
+    out.deviceName[nameLen] = '\0';
     *diagnostics = out;
     return true;
 }
@@ -196,6 +198,12 @@ bool fireCudaSetPressurePath(int path) {
     if (!requireScene()) return false;
     std::string err;
     if (!g_scene->setPressurePath(path, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaSetHashLattices(int enabled) {
+    if (!requireScene()) return false;
+    g_scene->setHashLattices(enabled != 0);
     return true;
 }
 

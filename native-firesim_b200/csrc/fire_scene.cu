@@ -480,7 +480,8 @@ bool Scene::curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b)
     const double t = p.time;
     const int na = planLattice(t * 0.22 - 1.0, 12.7 + t * 0.22 + 1.0, -t * 0.31 - 1.0, 13.0 - t * 0.31 + 1.0, a);
     const int nb = planLattice(-t * 0.19 - 1.0, 10.0 - t * 0.19 + 1.0, t * 0.27 - 1.0, 13.5 + t * 0.27 + 1.0, b);
-    const bool fits = curlLattice_ != nullptr && static_cast<size_t>(na) <= curlCapacity_[0] && static_cast<size_t>(nb) <= curlCapacity_[1];
+    const bool fits = latticesEnabled_ && curlLattice_ != nullptr && static_cast<size_t>(na) <= curlCapacity_[0] &&
+                      static_cast<size_t>(nb) <= curlCapacity_[1];
     a.values = fits ? curlLattice_ : nullptr;
     b.values = fits ? curlLattice_ + curlCapacity_[0] : nullptr;
     return fits;
@@ -492,7 +493,7 @@ bool Scene::curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b)
 bool Scene::sourceLattice(const FrameParams& p, HashLattice2& l) const {
     const double t = p.time;
     const int n = planLattice(-13.65 - 2.46 + t * 0.38 - 1.0, 13.65 + 2.46 + t * 0.38 + 1.0, -9.02 - 1.0, 31.0 + 9.02 + 1.0, l);
-    const bool fits = sourceLattice_ != nullptr && static_cast<size_t>(n) <= sourceCapacity_;
+    const bool fits = latticesEnabled_ && sourceLattice_ != nullptr && static_cast<size_t>(n) <= sourceCapacity_;
     l.values = fits ? sourceLattice_ : nullptr;
     return fits;
 }
@@ -540,7 +541,7 @@ bool Scene::renderLattices(const FrameParams& p, RenderLattices& lat) const {
         {{-0.72 * t, 15.0 - 0.72 * t}, {-1.08 * t, 13.0 - 1.08 * t}, {0.32 * t, 17.0 + 0.32 * t}},
     };
     HashLattice3* sites[4] = {&lat.warpA, &lat.warpB, &lat.fine, &lat.shear};
-    bool fits = renderLattice_ != nullptr;
+    bool fits = latticesEnabled_ && renderLattice_ != nullptr;
     size_t base = 0;
     for (int i = 0; i < 4; ++i) {
         double lo[3], hi[3];

@@ -64,6 +64,8 @@ public:
     // Fault injection for the resident SOR's bounded waits: brick `silentBrick`
     // (-1 = none) never announces its half sweeps; each wait gives up after waitUs.
     bool setResidentFault(int silentBrick, long long waitUs, std::string& err);
+    // Hash lattices on (default) or off: off hashes every fbm corner in place (same bits, slower).
+    void setHashLattices(bool enabled) { latticesEnabled_ = enabled; }
     bool synchronize(std::string& err);
     // After a host sync: fails once with "timed out" if a resident SOR wait ran out since the last check.
     bool checkSolverStatus(std::string& err);
@@ -121,6 +123,7 @@ private:
     int lastPressurePath_ = 0;
     cudaGraphExec_t sorExec_ = nullptr;
     // hash21 lattices of the two curl-noise fbm call sites of the force pass.
+    bool latticesEnabled_ = true;
     bool curlLattices(const FrameParams& p, HashLattice2& a, HashLattice2& b) const;
     float* curlLattice_ = nullptr;
     size_t curlCapacity_[2] = {0, 0};

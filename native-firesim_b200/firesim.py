@@ -63,6 +63,7 @@ def load_library() -> ctypes.CDLL:
         "fireCudaSetPressureSolver": (b, [ctypes.c_int, ctypes.c_float]),
         "fireCudaSetPressurePath": (b, [ctypes.c_int]),
         "fireCudaGetPressurePathUsed": (ctypes.c_int, []),
+        "fireCudaSetHashLattices": (b, [ctypes.c_int]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -166,6 +167,10 @@ class FireSim:
     def set_resident_sor_fault(self, silent_brick: int = -1, wait_us: int = 1_000_000):
         """Fault injection for the resident SOR's bounded neighbour waits."""
         self._check(self.lib.fireCudaSetResidentSorFault(silent_brick, wait_us), "fireCudaSetResidentSorFault")
+
+    def set_hash_lattices(self, enabled: bool):
+        """Hash-lattice tables for the fbm fields on (default) or off (in-place hashing, same bits)."""
+        self._check(self.lib.fireCudaSetHashLattices(1 if enabled else 0), "fireCudaSetHashLattices")
 
     def pressure_path_used(self) -> int:
         """Path of the latest SOR solve: 0 none yet, 1 per-launch graph, 2 resident."""
