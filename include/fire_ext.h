@@ -98,6 +98,18 @@ FIRE_API bool fireCudaSetPressureSolver(int iterations, float omega);
  * fit). */
 FIRE_API bool fireCudaSetPressurePath(int path);
 
+/* Scene/emitter contract.  Writes the emitter fields of *settings
+ * (emitterCenterX/Z, emitterHeightNorm, emitterHeightBandNorm, emitterRadius,
+ * burnerCenterCount, burnerCenterX/Y/Z) for scene `sceneId` (clamped to 0..2)
+ * as the reference's worker does before each frame: from
+ * <fireScenesDir>/<room|campfire|gas-burner-aver1>/scene.json and, for scenes
+ * 1 and 2, emitter-mask.json beside it.  Replaces loadSceneEmitterParams +
+ * applySceneEmitterParams (src/main.cpp:1397-1476, :433-447), whose directory
+ * is the fixed relative path assets/fire-scenes.  A NULL or unreadable
+ * directory gives the reference's built-in values for the scene.  Host only;
+ * touches no GPU state. */
+FIRE_API bool fireCudaApplySceneContract(int sceneId, const char* fireScenesDir, FireSettings* settings);
+
 /* Hash lattices (default on): fbm fields evaluated over the whole grid or
  * frame read their sin hashes from a table built once per step or frame.
  * Off, every corner is hashed in place.  The results are the same bits either

@@ -114,14 +114,17 @@ CANONICAL = dict(cinematicMode=1, raymarchSteps=104, emberCount=176, exposure=0.
 
 
 def validation_settings(frame: int, scene: int = 0, width: int = 960, height: int = 540,
-                        pool_fire: bool = False) -> FireSettings:
+                        pool_fire: bool = False, fire_scenes_dir=None) -> FireSettings:
     """FireSettings of frame `frame` of the reference's validation harness.
 
     Restates src/main.cpp:4284-4311 (runValidation): deterministic mouse/wind
     motion, canonical constants, then the validation floors for turbulence,
     smoke and intensity and the fixed validation camera.  Scene emitter
     parameters are the built-in defaults of SceneEmitterParams
-    (src/main.cpp:173, used when no scene contract is loaded).
+    (src/main.cpp:173, used when no scene contract is loaded); with
+    `fire_scenes_dir` they come from the scene's contract files, applied at the
+    same point as the reference's applySceneEmitterParams (:4305), through
+    fireCudaApplySceneContract.
     """
     import numpy as np
     f = np.float32
@@ -141,6 +144,9 @@ def validation_settings(frame: int, scene: int = 0, width: int = 960, height: in
     s.detail = 0.98
     for k, v in CANONICAL.items():
         setattr(s, k, v)
+    if fire_scenes_dir is not None:
+        from . import firesim  # noqa: PLC0415
+        firesim.apply_scene_contract(scene, fire_scenes_dir, s)
     s.turbulence = max(s.turbulence, f32(1.08))
     s.smoke = max(s.smoke, f32(1.02))
     s.intensity = max(s.intensity, f32(1.18))

@@ -1,6 +1,7 @@
 """Build recipe for native-firesim_b200/libfiresim_b200.so (sm_100a).
 
-Compiles every csrc/*.cu with nvcc for compute_100a/sm_100a (-O3 -lineinfo),
+Compiles every csrc/*.cu (and the host-only csrc/*.cpp) with nvcc for
+compute_100a/sm_100a (-O3 -lineinfo),
 in parallel, and links them into one shared library next to this file.
 nvcc cross-compiles without a GPU, so this runs on a CPU-only host.
 
@@ -29,7 +30,7 @@ def _nvcc() -> str:
 
 
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def headers() -> list[Path]:

@@ -64,6 +64,7 @@ def load_library() -> ctypes.CDLL:
         "fireCudaSetPressurePath": (b, [ctypes.c_int]),
         "fireCudaGetPressurePathUsed": (ctypes.c_int, []),
         "fireCudaSetHashLattices": (b, [ctypes.c_int]),
+        "fireCudaApplySceneContract": (b, [ctypes.c_int, ctypes.c_char_p, S]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -220,3 +221,12 @@ class FireSim:
 
     def set_times(self, sim_time: float, render_time: float, frame_index: int) -> None:
         self._check(self.lib.fireCudaSetTimes(sim_time, render_time, frame_index), "set times")
+
+
+def apply_scene_contract(scene_id: int, fire_scenes_dir, settings) -> None:
+    """Fills the emitter fields of `settings` from the scene's contract files
+    (fireCudaApplySceneContract); None gives the built-in values."""
+    lib = load_library()
+    path = None if fire_scenes_dir is None else str(fire_scenes_dir).encode()
+    if not lib.fireCudaApplySceneContract(scene_id, path, ctypes.byref(settings)):
+        raise FireSimError(f"fireCudaApplySceneContract: {last_error()}")

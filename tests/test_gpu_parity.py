@@ -296,3 +296,25 @@ def test_hash_lattices_equal_in_place_hashing(scene, product, abi):
         np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32), err_msg=f"hdr frame {f}")
     for n in out[0][1]:
         np.testing.assert_array_equal(out[0][1][n].view(np.uint32), out[1][1][n].view(np.uint32), err_msg=n)
+
+
+@pytest.mark.parametrize("scene", [1, 2])
+def test_scene_contract_frames_vs_oracle(scene, product, abi, oracle_mod):
+    """The validation harness with the scene's contract applied (the emitter of
+    the campfire bed, the selected gas burner): 4 steps on the product and on
+    the CPU oracle from the same settings, compared per field in the
+    trajectory class."""
+    from pathlib import Path
+    contracts = Path(__file__).resolve().parent / "golden" / "scene_contracts"
+    nx, ny, nz = 32, 36, 24
+    sim = product.FireSim(48, 32, nx, ny, nz)
+    o = oracle_mod.OracleFire(abi, 48, 32, nx, ny, nz)
+    for f in range(4):
+        s = abi.validation_settings(f, scene=scene, width=48, height=32, fire_scenes_dir=contracts)
+        assert s.burnerCenterCount == (1 if scene == 2 else 0)
+        sim.step(s)
+        o.step(s, mode=2)  # advance without rendering, as fireCudaStepD3D11
+    sim.synchronize()
+    for n in STATE_FIELDS[:10] + ["u", "v", "w"]:
+        T.check_field(f"contract{scene}/{n}", sim.get(n), o.get(n), T.TRAJECTORY)
+    assert sim.get("heat").sum() > 0.0
