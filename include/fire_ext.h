@@ -187,6 +187,77 @@ FIRE_API bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float ti
                                           const float* u, const float* v, const float* w, float* uOut, float* vOut,
                                           float* wOut, float* divergence, float* pressure, void* stream);
 
+/* ---- Independent scenes, batched steps, serving ------------------------
+ * No counterpart in the reference, whose scene is one process-wide singleton
+ * (src/fire_cuda.cu:116-195).  A FireScene owns its fields, its stream and
+ * its output; work queued on different scenes may overlap on the GPU.  The
+ * entry points below return false and set fireCudaLastError() like the
+ * others; they are meant to be called from one host thread. */
+typedef struct FireScene FireScene;
+
+/* Creates a scene on `device` with an nx*ny*nz grid and a frameW*frameH HDR
+ * frame, reset as by fireCudaReset.  NULL on failure. */
+FIRE_API FireScene* fireSceneCreate(int device, int frameW, int frameH, int nx, int ny, int nz);
+/* Waits for the scene's queued work and frees it. */
+FIRE_API void fireSceneDestroy(FireScene* scene);
+/* Device memory the scene holds, in bytes (for admission against a budget). */
+FIRE_API size_t fireSceneDeviceBytes(const FireScene* scene);
+FIRE_API bool fireSceneSetPressureSolver(FireScene* scene, int iterations, float omega);
+/* Caller-owned device HDR buffer the scene renders into (as fireCudaRegisterHdrBufferSlot). */
+FIRE_API bool fireSceneSetHdrBuffer(FireScene* scene, void* devicePtr, size_t pitchBytes, int format);
+/* Queues one step (render = 0) or one step and a render into the HDR buffer
+ * (render != 0) on the scene's stream; returns without waiting. */
+FIRE_API bool fireSceneStep(FireScene* scene, const FireSettings* settings, int render);
+FIRE_API bool fireSceneSynchronize(FireScene* scene);
+FIRE_API bool fireSceneGetStream(FireScene* scene, void** stream);
+/* Waits for the scene, then copies one field (FIRE_FIELD_*), as fireCudaGetField. */
+FIRE_API bool fireSceneGetField(FireScene* scene, int field, void* host, size_t bytes);
+
+/* One sub-step of n scenes: queues fireSceneStep(scenes[i], &settings[i],
+ * render ? render[i] : 0) for every scene, each on its own stream, so the
+ * scenes' kernels run side by side on the GPU. */
+FIRE_API bool fireBatchStep(FireScene* const* scenes, const FireSettings* settings, const int* render, int n);
+
+/* A serving loop over FireScenes: requests arrive over time, are admitted
+ * while the device memory of the admitted scenes stays within a budget, and
+ * every admitted scene advances one step per round (continuous batching:
+ * a request that arrives while others run joins at the next round, and a
+ * finished scene leaves and frees its memory at once). */
+typedef struct FireServer FireServer;
+typedef struct FireServeRequest {
+    int id;
+    int nx, ny, nz;             /* grid */
+    int frameW, frameH;         /* HDR frame of the scene */
+    int steps;                  /* steps to run */
+    int renderEvery;            /* render after every renderEvery-th step (0 = never) */
+    int sorIterations;          /* 0 = library default */
+    float sorOmega;
+    double arrivalSeconds;      /* arrival time, from the start of fireServerRun */
+    FireSettings settings;      /* per-step settings (reset on the first step) */
+    float* resultHeat;          /* optional host buffer (nx*ny*nz floats): final heat */
+    float* resultHdr;           /* optional host buffer (frameW*frameH*4 floats): last frame */
+} FireServeRequest;
+typedef struct FireServeReport {
+    int submitted, completed, admittedPeak;
+    double seconds;             /* wall time of the run */
+    double voxelSteps;          /* sum over completed steps of nx*ny*nz */
+    double stepMsP50, stepMsP95, stepMsP99, stepMsMax;     /* per scene step, see fireServerRun */
+    double frameMsP50, frameMsP95, frameMsP99;             /* per rendered frame */
+    double queueMsP50, queueMsP99;                         /* arrival to admission */
+    size_t deviceBytesPeak;
+} FireServeReport;
+
+FIRE_API FireServer* fireServerCreate(int device, size_t budgetBytes);
+FIRE_API void fireServerDestroy(FireServer* server);
+/* Adds a request; it is admitted no earlier than its arrivalSeconds. */
+FIRE_API bool fireServerSubmit(FireServer* server, const FireServeRequest* request);
+/* Runs rounds until every submitted request has completed or `maxSeconds`
+ * of wall time have passed.  Step latency is the device time between the
+ * completions of a scene's consecutive steps (its first step: from its
+ * admission), measured with events on the scene's stream; it contains the
+ * time the scene shares the GPU with the others. */
+FIRE_API bool fireServerRun(FireServer* server, double maxSeconds, FireServeReport* report);
+
 /* Name of the build and its compute capability target, for diagnostics. */
 FIRE_API const char* fireCudaBuildInfo(void);
 

@@ -113,6 +113,31 @@ CANONICAL = dict(cinematicMode=1, raymarchSteps=104, emberCount=176, exposure=0.
                  smokeDarkness=1.26, intensity=1.42, smoke=0.96, turbulence=1.34, renderDebugMode=0)
 
 
+class FireServeRequest(ctypes.Structure):
+    """include/fire_ext.h FireServeRequest."""
+    _fields_ = [
+        ("id", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("frameW", ctypes.c_int), ("frameH", ctypes.c_int), ("steps", ctypes.c_int), ("renderEvery", ctypes.c_int),
+        ("sorIterations", ctypes.c_int), ("sorOmega", ctypes.c_float), ("arrivalSeconds", ctypes.c_double),
+        ("settings", FireSettings), ("resultHeat", ctypes.c_void_p), ("resultHdr", ctypes.c_void_p),
+    ]
+
+
+class FireServeReport(ctypes.Structure):
+    """include/fire_ext.h FireServeReport."""
+    _fields_ = [
+        ("submitted", ctypes.c_int), ("completed", ctypes.c_int), ("admittedPeak", ctypes.c_int),
+        ("seconds", ctypes.c_double), ("voxelSteps", ctypes.c_double),
+        ("stepMsP50", ctypes.c_double), ("stepMsP95", ctypes.c_double), ("stepMsP99", ctypes.c_double),
+        ("stepMsMax", ctypes.c_double), ("frameMsP50", ctypes.c_double), ("frameMsP95", ctypes.c_double),
+        ("frameMsP99", ctypes.c_double), ("queueMsP50", ctypes.c_double), ("queueMsP99", ctypes.c_double),
+        ("deviceBytesPeak", ctypes.c_size_t),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def validation_settings(frame: int, scene: int = 0, width: int = 960, height: int = 540,
                         pool_fire: bool = False, fire_scenes_dir=None) -> FireSettings:
     """FireSettings of frame `frame` of the reference's validation harness.

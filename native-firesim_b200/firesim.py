@@ -65,6 +65,20 @@ def load_library() -> ctypes.CDLL:
         "fireCudaGetPressurePathUsed": (ctypes.c_int, []),
         "fireCudaSetHashLattices": (b, [ctypes.c_int]),
         "fireCudaApplySceneContract": (b, [ctypes.c_int, ctypes.c_char_p, S]),
+        "fireSceneCreate": (ctypes.c_void_p, [ctypes.c_int] * 6),
+        "fireSceneDestroy": (None, [ctypes.c_void_p]),
+        "fireSceneDeviceBytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+        "fireSceneSetPressureSolver": (b, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]),
+        "fireSceneSetHdrBuffer": (b, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
+        "fireSceneStep": (b, [ctypes.c_void_p, S, ctypes.c_int]),
+        "fireSceneSynchronize": (b, [ctypes.c_void_p]),
+        "fireSceneGetStream": (b, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+        "fireSceneGetField": (b, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
+        "fireBatchStep": (b, [ctypes.POINTER(ctypes.c_void_p), S, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+        "fireServerCreate": (ctypes.c_void_p, [ctypes.c_int, ctypes.c_size_t]),
+        "fireServerDestroy": (None, [ctypes.c_void_p]),
+        "fireServerSubmit": (b, [ctypes.c_void_p, ctypes.POINTER(abi.FireServeRequest)]),
+        "fireServerRun": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(abi.FireServeReport)]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -230,3 +244,100 @@ def apply_scene_contract(scene_id: int, fire_scenes_dir, settings) -> None:
     path = None if fire_scenes_dir is None else str(fire_scenes_dir).encode()
     if not lib.fireCudaApplySceneContract(scene_id, path, ctypes.byref(settings)):
         raise FireSimError(f"fireCudaApplySceneContract: {last_error()}")
+
+
+class Scene:
+    """A FireScene handle (fireSceneCreate ...): an independent scene with its
+    own fields and stream; many of them run side by side on one GPU."""
+
+    def __init__(self, frame_w: int, frame_h: int, nx: int, ny: int, nz: int, device: int = 0):
+        self.lib = load_library()
+        self.h = self.lib.fireSceneCreate(device, frame_w, frame_h, nx, ny, nz)
+        if not self.h:
+            raise FireSimError(f"fireSceneCreate: {last_error()}")
+        self.nx, self.ny, self.nz, self.frame_w, self.frame_h = nx, ny, nz, frame_w, frame_h
+
+    def _check(self, ok, what):
+        if not ok:
+            raise FireSimError(f"{what}: {last_error()}")
+
+    def close(self):
+        if self.h:
+            self.lib.fireSceneDestroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 -- interpreter shutdown
+            pass
+
+    def device_bytes(self) -> int:
+        return int(self.lib.fireSceneDeviceBytes(self.h))
+
+    def set_pressure_solver(self, iterations: int, omega: float):
+        self._check(self.lib.fireSceneSetPressureSolver(self.h, iterations, omega), "fireSceneSetPressureSolver")
+
+    def set_hdr_buffer(self, device_ptr: int, pitch_bytes: int, fmt: int = 0):
+        self._check(self.lib.fireSceneSetHdrBuffer(self.h, device_ptr, pitch_bytes, fmt), "fireSceneSetHdrBuffer")
+
+    def step(self, settings, render: bool = False):
+        self._check(self.lib.fireSceneStep(self.h, ctypes.byref(settings), 1 if render else 0), "fireSceneStep")
+
+    def synchronize(self):
+        self._check(self.lib.fireSceneSynchronize(self.h), "fireSceneSynchronize")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.fireSceneGetStream(self.h, ctypes.byref(s)), "fireSceneGetStream")
+        return s.value or 0
+
+    def get(self, name: str) -> np.ndarray:
+        shape = {"u": (self.nz, self.ny, self.nx + 1), "v": (self.nz, self.ny + 1, self.nx),
+                 "w": (self.nz + 1, self.ny, self.nx)}.get(name, (self.nz, self.ny, self.nx))
+        out = np.empty(shape, dtype=np.float32)
+        self._check(self.lib.fireSceneGetField(self.h, abi.FIELDS[name], out.ctypes.data, out.nbytes), f"get {name}")
+        return out
+
+
+def batch_step(scenes, settings, render=None) -> None:
+    """fireBatchStep: one queued step of every scene (settings[i] for scenes[i])."""
+    lib = load_library()
+    n = len(scenes)
+    handles = (ctypes.c_void_p * n)(*[s.h for s in scenes])
+    arr = (abi.FireSettings * n)(*settings)
+    flags = None if render is None else (ctypes.c_int * n)(*[1 if r else 0 for r in render])
+    if not lib.fireBatchStep(handles, arr, flags, n):
+        raise FireSimError(f"fireBatchStep: {last_error()}")
+
+
+class Server:
+    """fireServer*: requests arrive over time, are admitted within a device-memory
+    budget and all admitted scenes advance one step per round."""
+
+    def __init__(self, budget_bytes: int, device: int = 0):
+        self.lib = load_library()
+        self.h = self.lib.fireServerCreate(device, budget_bytes)
+        if not self.h:
+            raise FireSimError(f"fireServerCreate: {last_error()}")
+
+    def submit(self, request) -> None:
+        if not self.lib.fireServerSubmit(self.h, ctypes.byref(request)):
+            raise FireSimError(f"fireServerSubmit: {last_error()}")
+
+    def run(self, max_seconds: float) -> dict:
+        rep = abi.FireServeReport()
+        if not self.lib.fireServerRun(self.h, max_seconds, ctypes.byref(rep)):
+            raise FireSimError(f"fireServerRun: {last_error()}")
+        return rep.as_dict()
+
+    def close(self):
+        if self.h:
+            self.lib.fireServerDestroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass

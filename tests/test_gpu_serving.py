@@ -1,0 +1,135 @@
+"""Independent scenes, batched steps and the serving loop (needs a GPU).
+
+Scenes share nothing on the device, so a scene's result must be the same bits
+whether it runs through the singleton ABI, through its own FireScene handle,
+side by side with others in fireBatchStep, or admitted by the server into a
+mix of requests that arrive over time.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(24, 28, 20), (32, 32, 32), (40, 24, 36)]
+
+
+def _settings(abi, f, scene=0, w=64, h=48):
+    s = abi.validation_settings(f, scene=scene, width=w, height=h)
+    s.reset = 1 if f == 0 else 0
+    return s
+
+
+def _alone(pkg, abi, dims, steps, render_every, scene=0, settings=None):
+    import torch
+    nx, ny, nz = dims
+    sc = pkg.Scene(64, 48, nx, ny, nz)
+    hdr = torch.zeros((48, 64, 4), dtype=torch.float32, device="cuda")
+    sc.set_hdr_buffer(hdr.data_ptr(), 64 * 16, 0)
+    for f in range(steps):
+        s = settings(f) if settings else _settings(abi, f, scene)
+        sc.step(s, render=render_every > 0 and f % render_every == render_every - 1)
+    sc.synchronize()
+    out = {n: sc.get(n) for n in ("heat", "fuel", "soot", "u", "v", "w", "pressure")}
+    torch.cuda.synchronize()
+    out["hdr"] = hdr.cpu().numpy()
+    sc.close()
+    return out
+
+
+def test_scene_handle_equals_singleton(pkg, abi):
+    """A FireScene steps exactly like the reference-style singleton."""
+    nx, ny, nz = SIZES[1]
+    sim = pkg.FireSim(64, 48, nx, ny, nz)
+    for f in range(6):
+        sim.step(_settings(abi, f))
+    sim.synchronize()
+    want = {n: sim.get(n) for n in ("heat", "fuel", "soot", "u", "v", "w", "pressure")}
+    sim.close()
+    got = _alone(pkg, abi, SIZES[1], 6, 0)
+    for n, a in want.items():
+        np.testing.assert_array_equal(got[n].view(np.uint32), a.view(np.uint32), err_msg=n)
+
+
+def test_batch_step_equals_alone(pkg, abi):
+    """Three scenes of different sizes and scenes, stepped together with fireBatchStep
+    (a render every 3rd step), equal each scene stepped alone."""
+    import torch
+    scenes = [pkg.Scene(64, 48, *d) for d in SIZES]
+    hdrs = [torch.zeros((48, 64, 4), dtype=torch.float32, device="cuda") for _ in SIZES]
+    for sc, hdr in zip(scenes, hdrs):
+        sc.set_hdr_buffer(hdr.data_ptr(), 64 * 16, 0)
+    for f in range(7):
+        pkg.batch_step(scenes, [_settings(abi, f, scene=i) for i in range(3)], render=[f % 3 == 2] * 3)
+    for i, (sc, hdr) in enumerate(zip(scenes, hdrs)):
+        sc.synchronize()
+        alone = _alone(pkg, abi, SIZES[i], 7, 3, scene=i)
+        for n in ("heat", "fuel", "soot", "u", "v", "w", "pressure"):
+            np.testing.assert_array_equal(sc.get(n).view(np.uint32), alone[n].view(np.uint32), err_msg=f"scene {i} {n}")
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(hdr.cpu().numpy().view(np.uint32), alone["hdr"].view(np.uint32), err_msg=f"scene {i} hdr")
+        sc.close()
+
+
+def _request(abi, rid, dims, steps, arrival, scene, render_every=4):
+    r = abi.FireServeRequest()
+    r.id = rid
+    r.nx, r.ny, r.nz = dims
+    r.frameW, r.frameH = 64, 48
+    r.steps = steps
+    r.renderEvery = render_every
+    r.arrivalSeconds = arrival
+    r.settings = _settings(abi, 1, scene=scene)
+    return r
+
+
+def test_server_results_equal_alone(pkg, abi):
+    """Six requests of three sizes arrive over 60 ms; every one completes, and each
+    request's final heat field and last frame equal the same request run alone."""
+    server = pkg.Server(budget_bytes=64 << 30)
+    reqs, heats, hdrs = [], [], []
+    for i in range(6):
+        dims = SIZES[i % 3]
+        r = _request(abi, i, dims, steps=6 + 2 * i, arrival=0.01 * i, scene=i % 3)
+        heat = np.zeros(dims[::-1], dtype=np.float32)
+        hdr = np.zeros((48, 64, 4), dtype=np.float32)
+        r.resultHeat, r.resultHdr = heat.ctypes.data, hdr.ctypes.data
+        reqs.append(r)
+        heats.append(heat)
+        hdrs.append(hdr)
+        server.submit(r)
+    rep = server.run(60.0)
+    server.close()
+    assert rep["submitted"] == 6 and rep["completed"] == 6
+    assert rep["voxelSteps"] == sum((6 + 2 * i) * np.prod(SIZES[i % 3]) for i in range(6))
+    assert 0 < rep["stepMsP50"] <= rep["stepMsP99"] <= rep["stepMsMax"]
+    for i, r in enumerate(reqs):
+        base = r.settings
+
+        def per_step(f, base=base):
+            s = abi.FireSettings.from_buffer_copy(base)
+            s.reset = 1 if f == 0 else 0
+            return s
+
+        alone = _alone(pkg, abi, SIZES[i % 3], r.steps, 4, settings=per_step)
+        np.testing.assert_array_equal(heats[i].view(np.uint32), alone["heat"].view(np.uint32), err_msg=f"request {i} heat")
+        np.testing.assert_array_equal(hdrs[i].view(np.uint32), alone["hdr"].view(np.uint32), err_msg=f"request {i} hdr")
+
+
+def test_server_respects_budget(pkg, abi):
+    """With room for about two scenes at a time, the server never holds more than
+    its budget and still completes every request, later ones after a queue wait."""
+    probe = pkg.Scene(64, 48, *SIZES[1])
+    per_scene = probe.device_bytes() + 64 * 48 * 16
+    probe.close()
+    budget = int(2.5 * per_scene)
+    server = pkg.Server(budget_bytes=budget)
+    for i in range(5):
+        server.submit(_request(abi, i, SIZES[1], steps=8, arrival=0.0, scene=0))
+    rep = server.run(60.0)
+    server.close()
+    assert rep["completed"] == 5
+    assert rep["admittedPeak"] <= 2
+    assert rep["deviceBytesPeak"] <= budget
+    assert rep["queueMsP99"] > 0.0
