@@ -28,6 +28,7 @@ from __future__ import annotations
 import argparse
 import importlib.util
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -249,6 +250,134 @@ def config_block(args) -> dict:
             "l2": "per-step state (~270 MB at 128^3) exceeds the 126 MB L2; no flush", "parallelism": "replicas"}
 
 
+class SplitMix64:
+    """SplitMix64 (Steele, Lea, Flood 2014): the host RNG of the batched and serving draws."""
+
+    def __init__(self, seed: int):
+        self.state = seed & 0xFFFFFFFFFFFFFFFF
+
+    def next(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        return z ^ (z >> 31)
+
+    def uniform(self, lo: float = 0.0, hi: float = 1.0) -> float:
+        return lo + (hi - lo) * (self.next() >> 11) * (1.0 / (1 << 53))
+
+    def normal(self) -> float:
+        u1, u2 = max(self.uniform(), 1e-300), self.uniform()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+def scene_settings(abi, rng: SplitMix64, dims, frame_w: int, frame_h: int, radius_cells: tuple, wind: float):
+    """Per-scene settings of the batched and serving mixes on the reference's physics:
+    validation-harness settings with the emitter centre drawn in the middle half of
+    the floor, its radius drawn in cells (converted to the 2.1 m wide domain) and
+    the wind drawn per scene (the reference's wind acts along x only)."""
+    nx = dims[0]
+    s = abi.validation_settings(1, scene=0, width=frame_w, height=frame_h)
+    s.reset = 0
+    s.emitterCenterX = rng.uniform(-0.25, 0.25) * 2.10
+    s.emitterCenterZ = rng.uniform(-0.25, 0.25) * 1.64
+    s.emitterRadius = rng.uniform(*radius_cells) / nx * 2.10
+    s.wind = wind
+    return s
+
+
+def run_batched(args, pkg) -> None:
+    """48 independent scenes of mixed sizes stepped together (fireBatchStep)."""
+    import torch
+    abi = pkg.abi
+    rng = SplitMix64(11)
+    sizes = [(48, 48, 48), (64, 64, 64), (96, 96, 96), (128, 64, 64), (160, 96, 96)]
+    dims = [sizes[rng.next() % len(sizes)] for _ in range(args.scenes)]
+    scenes, settings, hdrs = [], [], []
+    for d in dims:
+        sc = pkg.Scene(256, 256, *d)
+        sc.set_pressure_solver(40, 1.8)
+        hdr = torch.zeros((256, 256, 4), dtype=torch.float32, device="cuda")
+        sc.set_hdr_buffer(hdr.data_ptr(), 256 * 16, 0)
+        scenes.append(sc)
+        hdrs.append(hdr)
+        s = scene_settings(abi, rng, d, 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
+        s.raymarchSteps = 64
+        settings.append(s)
+    voxels = sum(int(np.prod(d)) for d in dims)
+
+    def sub_step(i):
+        for s in settings:
+            s.reset = 1 if i == 0 else 0
+        pkg.batch_step(scenes, settings, render=[(i % args.render_every) == args.render_every - 1] * len(scenes))
+
+    for i in range(args.warmup):
+        sub_step(i)
+    for sc in scenes:
+        sc.synchronize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        sub_step(i)
+    for sc in scenes:
+        sc.synchronize()
+    wall = time.perf_counter() - t0
+    line = {"metric": "voxel-steps/s", "mode": "batched", "value": voxels * args.steps / wall, "unit": "voxel-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_sub_step": wall * 1e3 / args.steps,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (SplitMix64 seed 11 draws)",
+            "config": {"workload": f"{args.scenes} independent scenes, sizes drawn from {sizes}, reference physics FP32, "
+                                   f"SOR 40 iterations omega 1.8, 256x256 render (64 samples) every {args.render_every} steps, "
+                                   "one fireBatchStep per sub-step, each scene on its own stream",
+                       "voxels_per_sub_step": voxels, "timing": "host wall clock around the sub-steps, synchronised on all scenes"}}
+    print(json.dumps(line), flush=True)
+    for sc in scenes:
+        sc.close()
+
+
+def run_serve(args, pkg) -> None:
+    """Poisson arrivals of scene requests into the FireServer loop."""
+    abi = pkg.abi
+    rng = SplitMix64(args.seed)
+    server = pkg.Server(budget_bytes=int(args.budget_gb * (1 << 30)))
+    server.set_limits(int(args.max_active_mvoxels * 1e6))
+    t, n = 0.0, 0
+    keep = []
+    while True:
+        t += -math.log(max(rng.uniform(), 1e-300)) / args.rate
+        if t > args.arrival_seconds:
+            break
+        edge = int(round(min(192.0, max(32.0, 96.0 * math.exp(0.4 * rng.normal()))) / 16.0)) * 16
+        r = abi.FireServeRequest()
+        r.id = n
+        r.nx = r.ny = r.nz = edge
+        r.frameW = r.frameH = 256
+        r.steps = 30 + int(rng.uniform() * 271)
+        r.renderEvery = 4
+        r.sorIterations, r.sorOmega = 40, 1.8
+        r.arrivalSeconds = t
+        r.settings = scene_settings(abi, rng, (edge, edge, edge), 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
+        r.settings.raymarchSteps = 64
+        server.submit(r)
+        keep.append(r)
+        n += 1
+    rep = server.run(args.serve_seconds)
+    server.close()
+    line = {"metric": "voxel-steps/s", "mode": "serve", "value": rep["voxelSteps"] / max(rep["seconds"], 1e-9),
+            "unit": "voxel-steps/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (SplitMix64 draws)",
+            "latency_ms": {"step_p50": rep["stepMsP50"], "step_p95": rep["stepMsP95"], "step_p99": rep["stepMsP99"],
+                           "step_max": rep["stepMsMax"], "frame_p50": rep["frameMsP50"], "frame_p95": rep["frameMsP95"],
+                           "frame_p99": rep["frameMsP99"], "queue_p50": rep["queueMsP50"], "queue_p99": rep["queueMsP99"]},
+            "requests": {"submitted": rep["submitted"], "completed": rep["completed"], "admitted_peak": rep["admittedPeak"]},
+            "device_bytes_peak": rep["deviceBytesPeak"], "seconds": rep["seconds"],
+            "config": {"workload": f"Poisson arrivals at {args.rate}/s for {args.arrival_seconds} s; cubic edge log-normal "
+                                   "(median 96, sigma 0.4) clamped to [32, 192], multiple of 16; steps U[30, 300]; "
+                                   "reference physics FP32, SOR 40; 256x256 render (64 samples) every 4 steps; "
+                                   f"HBM budget {args.budget_gb} GB; at most {args.max_active_mvoxels} M active cells; "
+                                   f"run bounded at {args.serve_seconds} s",
+                       "latency": "device time between a scene's consecutive step completions, events on its stream"}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -264,6 +393,17 @@ def main() -> int:
     ap.add_argument("--reference-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="single", choices=["single", "batched", "serve"],
+                    help="single: the 128^3 scene (the headline line); batched: --scenes scenes per fireBatchStep; "
+                         "serve: Poisson requests into the FireServer loop")
+    ap.add_argument("--scenes", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--arrival-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--max-active-mvoxels", type=float, default=24.0,
+                    help="serve: admit while the admitted scenes hold at most this many million cells (0 = no limit)")
+    ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--sor-path", default="auto", choices=["auto", "graph", "resident"],
                     help="pressure SOR: per-launch half sweeps in a CUDA graph, one cooperative resident launch, or auto")
     args = ap.parse_args()
@@ -278,6 +418,14 @@ def main() -> int:
     import torch
     torch.cuda.set_device(local)
     pkg = load_package()
+    if args.mode != "single":
+        if rank == 0:
+            if args.mode == "batched":
+                run_batched(args, pkg)
+            else:
+                run_serve(args, pkg)
+        dist_barrier(world)
+        return 0
     abi = pkg.abi
     lib = pkg.load_library()
     if not lib.fireCudaSelectDevice(local):

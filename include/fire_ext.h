@@ -247,8 +247,18 @@ typedef struct FireServeReport {
     size_t deviceBytesPeak;
 } FireServeReport;
 
+/* A finished scene stays in a pool, by grid and frame shape, for the next
+ * request of that shape (its first step resets it), so steady serving neither
+ * allocates nor frees device memory; pooled scenes count toward the budget and
+ * are freed, oldest first, when an admission needs their room. */
 FIRE_API FireServer* fireServerCreate(int device, size_t budgetBytes);
 FIRE_API void fireServerDestroy(FireServer* server);
+/* Latency control: admit a request only while the admitted scenes hold at
+ * most maxActiveVoxels cells (0 = no limit); every round steps all of them,
+ * so this bounds the round time and with it the step latency.  Requests
+ * beyond it wait in arrival order (their wait is queueMs). */
+FIRE_API bool fireServerSetLimits(FireServer* server, long long maxActiveVoxels);
+
 /* Adds a request; it is admitted no earlier than its arrivalSeconds. */
 FIRE_API bool fireServerSubmit(FireServer* server, const FireServeRequest* request);
 /* Runs rounds until every submitted request has completed or `maxSeconds`

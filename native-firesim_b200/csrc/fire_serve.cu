@@ -166,11 +166,15 @@ constexpr int kStepsInFlight = 2;
 
 }  // namespace
 
+using Shape = std::tuple<int, int, int, int, int>;  // nx, ny, nz, frameW, frameH
+
 struct FireServer {
     int device = 0;
     size_t budget = 0;
+    long long maxActiveVoxels = 0;
     std::vector<FireServeRequest> pending;  // sorted by arrival when the run starts
-    std::map<std::tuple<int, int, int, int, int>, size_t> bytesByShape;  // measured scene + frame bytes
+    std::map<Shape, size_t> bytesByShape;   // measured scene + frame bytes
+    std::deque<std::unique_ptr<Active>> pool;  // finished scenes, oldest first
 };
 
 namespace {
@@ -201,6 +205,8 @@ void releaseActive(Active& a) {
 
 size_t frameBytes(const FireServeRequest& r) { return static_cast<size_t>(r.frameW) * r.frameH * sizeof(float) * 4; }
 
+Shape shapeOf(const FireServeRequest& r) { return std::make_tuple(r.nx, r.ny, r.nz, r.frameW, r.frameH); }
+
 }  // namespace
 
 extern "C" FireServer* fireServerCreate(int device, size_t budgetBytes) {
@@ -211,7 +217,18 @@ extern "C" FireServer* fireServerCreate(int device, size_t budgetBytes) {
     return s;
 }
 
-extern "C" void fireServerDestroy(FireServer* server) { delete server; }
+extern "C" void fireServerDestroy(FireServer* server) {
+    if (server == nullptr) return;
+    cudaSetDevice(server->device);
+    for (auto& a : server->pool) releaseActive(*a);
+    delete server;
+}
+
+extern "C" bool fireServerSetLimits(FireServer* server, long long maxActiveVoxels) {
+    if (server == nullptr || maxActiveVoxels < 0) return fail("fireServerSetLimits: null server or negative limit.");
+    server->maxActiveVoxels = maxActiveVoxels;
+    return true;
+}
 
 extern "C" bool fireServerSubmit(FireServer* server, const FireServeRequest* request) {
     if (server == nullptr || request == nullptr) return fail("fireServerSubmit: null server or request.");
@@ -235,6 +252,8 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
     std::vector<double> stepMs, frameMs, queueMs;
     std::vector<std::unique_ptr<Active>> active;
     size_t inUse = 0;
+    for (auto& p : server->pool) inUse += p->bytes;
+    long long activeVoxels = 0;
     std::string err;
     bool ok = true;
     const auto t0 = std::chrono::steady_clock::now();
@@ -243,43 +262,72 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
     while (ok && (!waiting.empty() || !active.empty())) {
         const double t = now();
         if (t > maxSeconds) break;
-        // Admission: in arrival order, while the budget holds.
+        // Admission: in arrival order, while the voxel limit and the budget hold.
         while (!waiting.empty() && waiting.front().arrivalSeconds <= t) {
             const FireServeRequest& r = waiting.front();
-            const auto shape = std::make_tuple(r.nx, r.ny, r.nz, r.frameW, r.frameH);
-            const auto known = server->bytesByShape.find(shape);
-            if (known != server->bytesByShape.end() && inUse + known->second > server->budget && !active.empty()) break;
-            auto a = std::make_unique<Active>();
-            a->req = r;
-            a->scene = makeScene(server->device, r.frameW, r.frameH, r.nx, r.ny, r.nz, err);
-            if (!a->scene) {
-                ok = fail(err);
-                break;
+            const long long voxels = static_cast<long long>(r.nx) * r.ny * r.nz;
+            if (server->maxActiveVoxels > 0 && !active.empty() && activeVoxels + voxels > server->maxActiveVoxels) break;
+            const Shape shape = shapeOf(r);
+            // A pooled scene of this shape is taken as it is.
+            std::unique_ptr<Active> a;
+            for (auto it = server->pool.begin(); it != server->pool.end(); ++it) {
+                if (shapeOf((*it)->req) == shape) {
+                    a = std::move(*it);
+                    server->pool.erase(it);
+                    break;
+                }
             }
+            if (!a) {
+                // A new scene: make room by freeing pooled scenes, oldest first.
+                const auto known = server->bytesByShape.find(shape);
+                const size_t need = known != server->bytesByShape.end() ? known->second : 0;
+                while (!server->pool.empty() && inUse + need > server->budget) {
+                    inUse -= server->pool.front()->bytes;
+                    releaseActive(*server->pool.front());
+                    server->pool.pop_front();
+                }
+                if (known != server->bytesByShape.end() && inUse + need > server->budget && !active.empty()) break;
+                a = std::make_unique<Active>();
+                a->scene = makeScene(server->device, r.frameW, r.frameH, r.nx, r.ny, r.nz, err);
+                if (!a->scene) {
+                    ok = fail(err);
+                    break;
+                }
+                if (cudaMalloc(&a->hdr, frameBytes(r)) != cudaSuccess) {
+                    cudaGetLastError();
+                    ok = fail("fireServerRun: cudaMalloc of a scene's HDR frame failed.");
+                    break;
+                }
+                if (!a->scene->registerHdrSlot(0, a->hdr, static_cast<size_t>(r.frameW) * 16, FIRE_HDR_RGBA32F, err) ||
+                    !a->scene->setActiveSlot(0, err)) {
+                    ok = fail(err);
+                    break;
+                }
+                a->bytes = a->scene->deviceBytes() + frameBytes(r);
+                server->bytesByShape[shape] = a->bytes;
+                if (inUse + a->bytes > server->budget && !active.empty()) {
+                    // The first scene of this shape did not fit after all: give it back.
+                    releaseActive(*a);
+                    break;
+                }
+                inUse += a->bytes;
+            } else {
+                // A pooled scene starts like a new one: clocks and fields reset, frame cleared.
+                if (!a->scene->reset(err) ||
+                    cudaMemsetAsync(a->hdr, 0, frameBytes(a->req), a->scene->stream) != cudaSuccess) {
+                    ok = fail(err.empty() ? std::string("fireServerRun: clearing a pooled scene failed.") : err);
+                    break;
+                }
+            }
+            a->req = r;
+            a->queued = 0;
             if (r.sorIterations > 0 && !a->scene->setPressureSolver(r.sorIterations, r.sorOmega, err)) {
                 ok = fail(err);
                 break;
             }
-            if (cudaMalloc(&a->hdr, frameBytes(r)) != cudaSuccess) {
-                cudaGetLastError();
-                ok = fail("fireServerRun: cudaMalloc of a scene's HDR frame failed.");
-                break;
-            }
-            if (!a->scene->registerHdrSlot(0, a->hdr, static_cast<size_t>(r.frameW) * 16, FIRE_HDR_RGBA32F, err) ||
-                !a->scene->setActiveSlot(0, err)) {
-                ok = fail(err);
-                break;
-            }
-            a->bytes = a->scene->deviceBytes() + frameBytes(r);
-            server->bytesByShape[shape] = a->bytes;
-            if (inUse + a->bytes > server->budget && !active.empty()) {
-                // First scene of this shape did not fit after all: give it back.
-                releaseActive(*a);
-                break;
-            }
             a->last = takeEvent(*a);
             cudaEventRecord(a->last, a->scene->stream);
-            inUse += a->bytes;
+            activeVoxels += voxels;
             rep.deviceBytesPeak = std::max(rep.deviceBytesPeak, inUse);
             queueMs.push_back((t - r.arrivalSeconds) * 1e3);
             waiting.pop_front();
@@ -339,8 +387,12 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
                     ok = fail("fireServerRun: copy of a finished scene's frame failed.");
                     break;
                 }
-                inUse -= a.bytes;
-                releaseActive(a);
+                activeVoxels -= static_cast<long long>(a.req.nx) * a.req.ny * a.req.nz;
+                if (a.last) {
+                    a.spare.push_back(a.last);
+                    a.last = nullptr;
+                }
+                server->pool.push_back(std::move(active[i]));
                 active.erase(active.begin() + static_cast<long>(i));
                 ++rep.completed;
             } else {
@@ -357,7 +409,10 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
             }
         }
     }
-    for (auto& ap : active) releaseActive(*ap);
+    for (auto& ap : active) {
+        inUse -= ap->bytes;
+        releaseActive(*ap);
+    }
     rep.seconds = now();
     rep.stepMsP50 = percentile(stepMs, 0.50);
     rep.stepMsP95 = percentile(stepMs, 0.95);

@@ -78,6 +78,7 @@ def load_library() -> ctypes.CDLL:
         "fireServerCreate": (ctypes.c_void_p, [ctypes.c_int, ctypes.c_size_t]),
         "fireServerDestroy": (None, [ctypes.c_void_p]),
         "fireServerSubmit": (b, [ctypes.c_void_p, ctypes.POINTER(abi.FireServeRequest)]),
+        "fireServerSetLimits": (b, [ctypes.c_void_p, ctypes.c_longlong]),
         "fireServerRun": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(abi.FireServeReport)]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
@@ -320,6 +321,11 @@ class Server:
         self.h = self.lib.fireServerCreate(device, budget_bytes)
         if not self.h:
             raise FireSimError(f"fireServerCreate: {last_error()}")
+
+    def set_limits(self, max_active_voxels: int) -> None:
+        """Admit only while the admitted scenes hold at most this many cells (0 = no limit)."""
+        if not self.lib.fireServerSetLimits(self.h, max_active_voxels):
+            raise FireSimError(f"fireServerSetLimits: {last_error()}")
 
     def submit(self, request) -> None:
         if not self.lib.fireServerSubmit(self.h, ctypes.byref(request)):

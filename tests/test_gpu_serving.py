@@ -133,3 +133,40 @@ def test_server_respects_budget(pkg, abi):
     assert rep["admittedPeak"] <= 2
     assert rep["deviceBytesPeak"] <= budget
     assert rep["queueMsP99"] > 0.0
+
+
+def test_server_pool_and_voxel_limit(pkg, abi):
+    """With room for one active scene at a time (by cells), eight requests of two
+    shapes run one after another; finished scenes are reused from the pool, and
+    every request's result equals the same request run alone."""
+    server = pkg.Server(budget_bytes=64 << 30)
+    server.set_limits(int(np.prod(SIZES[2])))
+    reqs, heats = [], []
+    for i in range(8):
+        dims = SIZES[i % 2]
+        r = _request(abi, i, dims, steps=5 + i, arrival=0.0, scene=i % 3)
+        heat = np.zeros(dims[::-1], dtype=np.float32)
+        r.resultHeat = heat.ctypes.data
+        reqs.append(r)
+        heats.append(heat)
+        server.submit(r)
+    rep = server.run(60.0)
+    assert rep["completed"] == 8 and rep["admittedPeak"] == 1
+    # A second run on the same server starts from the pool.
+    again = _request(abi, 8, SIZES[0], steps=5, arrival=0.0, scene=0)
+    heat_again = np.zeros(SIZES[0][::-1], dtype=np.float32)
+    again.resultHeat = heat_again.ctypes.data
+    server.submit(again)
+    assert server.run(60.0)["completed"] == 1
+    server.close()
+    for i, r in enumerate(reqs + [again]):
+        base = r.settings
+
+        def per_step(f, base=base):
+            s = abi.FireSettings.from_buffer_copy(base)
+            s.reset = 1 if f == 0 else 0
+            return s
+
+        alone = _alone(pkg, abi, (r.nx, r.ny, r.nz), r.steps, 4, settings=per_step)
+        got = heats[i] if i < 8 else heat_again
+        np.testing.assert_array_equal(got.view(np.uint32), alone["heat"].view(np.uint32), err_msg=f"request {i}")
