@@ -117,6 +117,21 @@ FIRE_API bool fireCudaApplySceneContract(int sceneId, const char* fireScenesDir,
  * counterpart in the reference, which always hashes in place. */
 FIRE_API bool fireCudaSetHashLattices(int enabled);
 
+/* Residual-gated pressure solve (SOR policy; the reference always runs a
+ * fixed count, src/fire_cuda.cu:3280-3284).  With maxResidual > 0 the
+ * shared-memory-resident solve runs in chunks of checkEvery iterations; after
+ * each chunk the residual r = div + (six neighbours, clamped at the walls) - 6p
+ * is reduced in a fixed order (max |r| in FP32, L2 in FP64) and once
+ * max |r| <= maxResidual the remaining chunks return at once, up to the
+ * iteration count of fireCudaSetPressureSolver.  The host does not wait.
+ * maxResidual = 0 restores the fixed count.  A gated solve that runs m
+ * iterations gives the same bits as a fixed solve of m iterations.  The
+ * per-launch path (fireCudaSetPressurePath(1)) ignores the tolerance. */
+FIRE_API bool fireCudaSetPressureTolerance(double maxResidual, int checkEvery);
+/* Iterations run, max |r| and L2 residual of the latest gated solve (waits
+ * for the scene's stream); after a fixed-count solve: the count and -1. */
+FIRE_API bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Residual);
+
 /* Path the latest SOR solve took: 0 = none yet (or no grid), 1 = one launch
  * per half sweep, 2 = shared-memory-resident. */
 FIRE_API int fireCudaGetPressurePathUsed(void);

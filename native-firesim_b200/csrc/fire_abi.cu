@@ -207,6 +207,21 @@ bool fireCudaSetHashLattices(int enabled) {
     return true;
 }
 
+bool fireCudaSetPressureTolerance(double maxResidual, int checkEvery) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->setPressureTolerance(maxResidual, checkEvery, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Residual) {
+    if (!requireScene()) return false;
+    if (iterations == nullptr || maxResidual == nullptr || l2Residual == nullptr) return fail("Pressure stats pointer was null.");
+    std::string err;
+    if (!g_scene->pressureStats(*iterations, *maxResidual, *l2Residual, err)) return fail(err);
+    return true;
+}
+
 int fireCudaGetPressurePathUsed(void) { return g_scene ? g_scene->lastPressurePath() : 0; }
 
 bool fireCudaSetResidentSorFault(int silentBrick, long long waitUs) {

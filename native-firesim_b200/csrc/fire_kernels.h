@@ -46,7 +46,22 @@ struct ResidentSync {
     unsigned epoch;
     int silentBrick;
     unsigned long long waitNs;
+    const int* skip;               // non-null and non-zero: the solve has converged, return at once
 };
+
+// Residual gate of a solve run in chunks: after each chunk the residual
+// r = div + (sum of the six neighbours) - 6 p (neighbours clamped at the walls,
+// as in the update) is reduced in a fixed order, and the chunks after the one
+// that reached max |r| <= tolerance return at once.
+struct SorGate {
+    int converged;
+    int iterations;      // iterations run
+    float maxResidual;   // max |r| after the last chunk run
+    int pad;
+    double l2Residual;   // sqrt(sum r^2), accumulated in FP64
+};
+constexpr int kResidualBlocks = 296;
+constexpr int kResidualThreads = 256;
 constexpr unsigned kResidentMaxPolls = 1u << 24;
 constexpr int kMetricThreads = 128;
 
@@ -65,6 +80,10 @@ __global__ void forceProjectSetup(float* uOut, float* vOut, float* wOut, float* 
 __global__ void velocityBoundary(float* u, float* v, float* w, FrameParams p, int clampValues);
 __global__ void divergenceOf(float* divergence, float* pressureOrNull, Velocity vel, FrameParams p);
 __global__ void sorHalfSweep(float* pressure, const float* divergence, Grid g, int parity, float omega);
+__global__ void sorResidualPartials(const float* pressure, const float* divergence, Grid g, const SorGate* gate, double* partialSq,
+                                    float* partialMax);
+__global__ void sorResidualFinal(SorGate* gate, const double* partialSq, const float* partialMax, int partials, float tolerance,
+                                 int chunkIterations);
 // The sorResident<BX, 16, 16> instantiation for brick width bx (32 or 16),
 // for cudaFuncSetAttribute / cudaLaunchCooperativeKernel.
 const void* sorResidentKernel(int bx);

@@ -67,7 +67,7 @@ void Scene::release() {
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
                     shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_,
-                    rayTileOrder_, rayTileCounter_, renderLattice_};
+                    rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
@@ -78,6 +78,9 @@ void Scene::release() {
     rayTileOrder_ = nullptr;
     rayTileCounter_ = nullptr;
     renderLattice_ = nullptr;
+    sorGate_ = nullptr;
+    residualSq_ = nullptr;
+    residualMax_ = nullptr;
     sorHostStatus_ = nullptr;
     curlLattice_ = nullptr;
     sourceLattice_ = nullptr;
@@ -174,6 +177,10 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
              check("raymarch occupancy", cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, raymarch, 128, 0), err);
         rayBlocks_ = std::max(1, sms * std::max(1, perSm));
     }
+    ok = ok && alloc(reinterpret_cast<void**>(&sorGate_), sizeof(SorGate), "cudaMalloc SOR gate", err) &&
+         check("clear SOR gate", cudaMemsetAsync(sorGate_, 0, sizeof(SorGate), stream), err) &&
+         alloc(reinterpret_cast<void**>(&residualSq_), kResidualBlocks * sizeof(double), "cudaMalloc residual partials", err) &&
+         alloc(reinterpret_cast<void**>(&residualMax_), kResidualBlocks * sizeof(float), "cudaMalloc residual maxima", err);
     // Resident SOR: the tagged exchange words (zero tags never match) and the failure status.
     ok = ok && alloc(reinterpret_cast<void**>(&sorExchange_), cells_ * sizeof(unsigned long long), "cudaMalloc SOR exchange", err) &&
          check("clear SOR exchange", cudaMemsetAsync(sorExchange_, 0, cells_ * sizeof(unsigned long long), stream), err) &&
@@ -385,17 +392,32 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
         int threads = 0;
         if (residentPlan(r, smem, threads)) {
             Grid g{nx, ny, nz};
-            int iterations = pressureIterations;
             float omega = pressureOmega;
-            ResidentSync sync{sorExchange_, sorStatus_, sorHostStatus_, sorEpoch_, sorSilentBrick_, sorWaitNs_};
-            sorEpoch_ += 2u * static_cast<unsigned>(iterations);
-            void* args[] = {&pressure_, &divergence_, &g, &r, &sync, &iterations, &omega};
             const unsigned bricks = static_cast<unsigned>(r.nbx * r.nby * r.nbz);
             void* fn = const_cast<void*>(sorResidentKernel(r.bx));
-            if (!check("SOR cooperative launch", cudaLaunchCooperativeKernel(fn, dim3(bricks), dim3(threads), args, smem, stream), err)) {
-                return false;
+            const bool gated = pressureTolerance_ > 0.0;
+            const int chunk = gated ? std::max(1, std::min(pressureCheckEvery_, pressureIterations)) : pressureIterations;
+            if (gated && !check("clear SOR gate", cudaMemsetAsync(sorGate_, 0, sizeof(SorGate), stream), err)) return false;
+            for (int done = 0; done < pressureIterations; done += chunk) {
+                int iterations = std::min(chunk, pressureIterations - done);
+                ResidentSync sync{sorExchange_, sorStatus_, sorHostStatus_, sorEpoch_, sorSilentBrick_, sorWaitNs_,
+                                  gated ? &sorGate_->converged : nullptr};
+                sorEpoch_ += 2u * static_cast<unsigned>(iterations);
+                void* args[] = {&pressure_, &divergence_, &g, &r, &sync, &iterations, &omega};
+                if (!check("SOR cooperative launch", cudaLaunchCooperativeKernel(fn, dim3(bricks), dim3(threads), args, smem, stream), err)) {
+                    return false;
+                }
+                ++launches_;
+                if (gated) {
+                    sorResidualPartials<<<kResidualBlocks, kResidualThreads, 0, stream>>>(pressure_, divergence_, g, sorGate_, residualSq_,
+                                                                                        residualMax_);
+                    sorResidualFinal<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks,
+                                                           static_cast<float>(pressureTolerance_), iterations);
+                    launches_ += 2;
+                    if (!check("SOR residual launch", cudaGetLastError(), err)) return false;
+                }
             }
-            ++launches_;
+            lastSolveGated_ = gated;
             lastPressurePath_ = 2;
             return true;
         }
@@ -432,6 +454,7 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
         sorOmega_ = pressureOmega;
     }
     launches_ += 2ull * static_cast<unsigned long long>(pressureIterations);
+    lastSolveGated_ = false;
     lastPressurePath_ = 1;
     return check("SOR graph launch", cudaGraphLaunch(sorExec_, stream), err);
 }
@@ -805,6 +828,13 @@ bool Scene::fillMetrics(FireCudaFrameMetrics* out, std::string& err) {
     o.gridY = ny;
     o.gridZ = nz;
     o.pressureIterations = pressureIterations;
+    if (lastSolveGated_) {
+        int it = 0;
+        float mr = 0.0f;
+        double l2 = 0.0;
+        if (!pressureStats(it, mr, l2, err)) return false;
+        o.pressureIterations = it;
+    }
     o.invalidCells = m.invalidCells;
     o.timeSeconds = simTime;
     o.gpuSolveMs = solveMs;
@@ -985,6 +1015,34 @@ bool Scene::checkSolverStatus(std::string& err) {
     *sorHostStatus_ = 0;
     err = "resident SOR: brick " + std::to_string(st - 1) + " timed out waiting for a neighbour's half sweep";
     return false;
+}
+
+bool Scene::setPressureTolerance(double tolerance, int checkEvery, std::string& err) {
+    if (!(tolerance >= 0.0) || checkEvery < 1) {
+        err = "pressure tolerance must be >= 0 and the check interval >= 1";
+        return false;
+    }
+    pressureTolerance_ = tolerance;
+    pressureCheckEvery_ = checkEvery;
+    return true;
+}
+
+bool Scene::pressureStats(int& iterations, float& maxResidual, double& l2Residual, std::string& err) {
+    if (!lastSolveGated_) {
+        iterations = pressureIterations;
+        maxResidual = -1.0f;
+        l2Residual = -1.0;
+        return true;
+    }
+    SorGate gate{};
+    if (!check("pressure stats sync", cudaStreamSynchronize(stream), err) ||
+        !check("pressure stats copy", cudaMemcpy(&gate, sorGate_, sizeof(gate), cudaMemcpyDeviceToHost), err)) {
+        return false;
+    }
+    iterations = gate.iterations;
+    maxResidual = gate.maxResidual;
+    l2Residual = gate.l2Residual;
+    return true;
 }
 
 bool Scene::setResidentFault(int silentBrick, long long waitUs, std::string& err) {

@@ -64,6 +64,11 @@ public:
     // Fault injection for the resident SOR's bounded waits: brick `silentBrick`
     // (-1 = none) never announces its half sweeps; each wait gives up after waitUs.
     bool setResidentFault(int silentBrick, long long waitUs, std::string& err);
+    // Residual-gated solve: stop once max |r| <= tolerance, checked every checkEvery iterations
+    // (tolerance 0 = the fixed iteration count).
+    bool setPressureTolerance(double tolerance, int checkEvery, std::string& err);
+    // Iterations run, max |r| and the FP64 L2 residual of the latest gated solve (waits for the stream).
+    bool pressureStats(int& iterations, float& maxResidual, double& l2Residual, std::string& err);
     // Hash lattices on (default) or off: off hashes every fbm corner in place (same bits, slower).
     void setHashLattices(bool enabled) { latticesEnabled_ = enabled; }
     bool synchronize(std::string& err);
@@ -139,6 +144,12 @@ private:
     int* rayTileOrder_ = nullptr;
     int* rayTileCounter_ = nullptr;
     int rayTilesX_ = 0, rayTileCount_ = 0, rayBlocks_ = 0;
+    double pressureTolerance_ = 0.0;
+    int pressureCheckEvery_ = 10;
+    bool lastSolveGated_ = false;
+    SorGate* sorGate_ = nullptr;
+    double* residualSq_ = nullptr;
+    float* residualMax_ = nullptr;
     unsigned* sorStatus_ = nullptr;               // device: failure tag of the resident SOR
     unsigned long long* sorExchange_ = nullptr;   // device: one tagged word per cell (face cells)
     unsigned* sorHostStatus_ = nullptr;  // host-mapped: brick + 1 of a wait that ran out

@@ -871,6 +871,9 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
     using S = ResidentShape<BX, BY, BZ>;
     using F = ResidentFaces<BX, BY, BZ>;
     constexpr int ZMID = BZ / 2;
+    if (sync.skip != nullptr && *reinterpret_cast<const volatile int*>(sync.skip) != 0) {
+        return;  // an earlier chunk of this solve converged (the same word for every block)
+    }
     extern __shared__ float smem[];
     float* planes = smem;                // [2][EZ][EY][EX]
     float* divs = smem + 2 * S::PLANE;   // [2][BZ][THREADS]
@@ -1012,6 +1015,66 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             }
         }
     }
+}
+
+// Residual of the red-black system, per block over a fixed set of cells
+// (grid-stride with a fixed grid), so the reduction order never changes.
+__global__ void __launch_bounds__(kResidualThreads) sorResidualPartials(const float* __restrict__ pressure,
+                                                                       const float* __restrict__ divergence, Grid g,
+                                                                       const SorGate* gate, double* __restrict__ partialSq,
+                                                                       float* __restrict__ partialMax) {
+    if (gate->converged) return;
+    __shared__ double sq[kResidualThreads];
+    __shared__ float mx[kResidualThreads];
+    const long long cells = static_cast<long long>(g.nx) * g.ny * g.nz;
+    double s = 0.0;
+    float m = 0.0f;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < cells;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % g.nx);
+        const int y = static_cast<int>((i / g.nx) % g.ny);
+        const int z = static_cast<int>(i / (static_cast<long long>(g.nx) * g.ny));
+        const float self = __ldg(pressure + i);
+        const float pL = x > 0 ? __ldg(pressure + i - 1) : self;
+        const float pR = x < g.nx - 1 ? __ldg(pressure + i + 1) : self;
+        const float pD = y > 0 ? __ldg(pressure + i - g.nx) : self;
+        const float pU = y < g.ny - 1 ? __ldg(pressure + i + g.nx) : self;
+        const long long plane = static_cast<long long>(g.nx) * g.ny;
+        const float pB = z > 0 ? __ldg(pressure + i - plane) : self;
+        const float pF = z < g.nz - 1 ? __ldg(pressure + i + plane) : self;
+        const float r = __fsub_rn(__ldg(divergence + i) + pL + pR + pD + pU + pB + pF, __fmul_rn(6.0f, self));
+        m = fmaxf(m, fabsf(r));
+        s += static_cast<double>(r) * static_cast<double>(r);
+    }
+    sq[threadIdx.x] = s;
+    mx[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kResidualThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sq[threadIdx.x] += sq[threadIdx.x + w];
+            mx[threadIdx.x] = fmaxf(mx[threadIdx.x], mx[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partialSq[blockIdx.x] = sq[0];
+        partialMax[blockIdx.x] = mx[0];
+    }
+}
+
+__global__ void sorResidualFinal(SorGate* gate, const double* __restrict__ partialSq, const float* __restrict__ partialMax, int partials,
+                                 float tolerance, int chunkIterations) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || gate->converged) return;
+    double s = 0.0;
+    float m = 0.0f;
+    for (int b = 0; b < partials; ++b) {
+        s += partialSq[b];
+        m = fmaxf(m, partialMax[b]);
+    }
+    gate->iterations += chunkIterations;
+    gate->maxResidual = m;
+    gate->l2Residual = sqrt(s);
+    if (m <= tolerance) gate->converged = 1;
 }
 
 const void* sorResidentKernel(int bx) {

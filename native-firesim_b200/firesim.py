@@ -64,6 +64,8 @@ def load_library() -> ctypes.CDLL:
         "fireCudaSetPressurePath": (b, [ctypes.c_int]),
         "fireCudaGetPressurePathUsed": (ctypes.c_int, []),
         "fireCudaSetHashLattices": (b, [ctypes.c_int]),
+        "fireCudaSetPressureTolerance": (b, [ctypes.c_double, ctypes.c_int]),
+        "fireCudaGetPressureStats": (b, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
         "fireCudaApplySceneContract": (b, [ctypes.c_int, ctypes.c_char_p, S]),
         "fireSceneCreate": (ctypes.c_void_p, [ctypes.c_int] * 6),
         "fireSceneDestroy": (None, [ctypes.c_void_p]),
@@ -183,6 +185,16 @@ class FireSim:
     def set_resident_sor_fault(self, silent_brick: int = -1, wait_us: int = 1_000_000):
         """Fault injection for the resident SOR's bounded neighbour waits."""
         self._check(self.lib.fireCudaSetResidentSorFault(silent_brick, wait_us), "fireCudaSetResidentSorFault")
+
+    def set_pressure_tolerance(self, max_residual: float, check_every: int = 10):
+        """Residual-gated SOR: stop once max |r| <= max_residual (0 = fixed iteration count)."""
+        self._check(self.lib.fireCudaSetPressureTolerance(max_residual, check_every), "fireCudaSetPressureTolerance")
+
+    def pressure_stats(self):
+        """(iterations, max |r|, L2 residual) of the latest gated solve."""
+        it, mr, l2 = ctypes.c_int(), ctypes.c_float(), ctypes.c_double()
+        self._check(self.lib.fireCudaGetPressureStats(ctypes.byref(it), ctypes.byref(mr), ctypes.byref(l2)), "fireCudaGetPressureStats")
+        return it.value, mr.value, l2.value
 
     def set_hash_lattices(self, enabled: bool):
         """Hash-lattice tables for the fbm fields on (default) or off (in-place hashing, same bits)."""

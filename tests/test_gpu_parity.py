@@ -318,3 +318,56 @@ def test_scene_contract_frames_vs_oracle(scene, product, abi, oracle_mod):
     for n in STATE_FIELDS[:10] + ["u", "v", "w"]:
         T.check_field(f"contract{scene}/{n}", sim.get(n), o.get(n), T.TRAJECTORY)
     assert sim.get("heat").sum() > 0.0
+
+
+
+def _residual(p, d):
+    """r = d + (six neighbours, clamped) - 6p in float32, summed in the kernel's order; max |r| and FP64 L2."""
+    f = np.float32
+    pad = np.pad(p, 1, mode="edge")
+    nb = [pad[1:-1, 1:-1, :-2], pad[1:-1, 1:-1, 2:], pad[1:-1, :-2, 1:-1], pad[1:-1, 2:, 1:-1], pad[:-2, 1:-1, 1:-1], pad[2:, 1:-1, 1:-1]]
+    acc = d.astype(f)
+    for n in nb:
+        acc = (acc + n).astype(f)
+    r = (acc - f(6.0) * p).astype(f)
+    return float(np.abs(r).max()), float(np.sqrt(np.sum(r.astype(np.float64) ** 2)))
+
+
+def test_pressure_tolerance_gates_the_solve(product, abi):
+    """The residual-gated solve stops at the first check with max |r| <= tolerance,
+    and its result equals a fixed solve of the same iteration count; a tolerance
+    never reached runs every iteration and equals the fixed solve."""
+    nx, ny, nz = 64, 48, 40
+    rng = np.random.default_rng(5)
+    p0 = np.zeros((nz, ny, nx), np.float32)
+    d0 = (0.2 * rng.standard_normal((nz, ny, nx))).astype(np.float32)
+    d0 -= d0.mean()
+    s = abi.FireSettings()
+
+    def solve(iters, tol, every=10):
+        sim = product.FireSim(32, 16, nx, ny, nz)
+        sim.set_pressure_solver(iters, 1.8)
+        sim.set_pressure_tolerance(tol, every)
+        sim.set("pressure", p0)
+        sim.set("divergence", d0)
+        sim.stages("pressure_sor", "pressure_sor", s, 0.0)
+        out = sim.get("pressure"), sim.pressure_stats(), sim.pressure_path_used()
+        sim.close()
+        return out
+
+    fixed, stats, path = solve(120, 0.0)
+    assert path == 2 and stats[0] == 120 and stats[1] == -1.0
+    never, stats_never, _ = solve(120, 1e-30)
+    assert stats_never[0] == 120
+    np.testing.assert_array_equal(never.view(np.uint32), fixed.view(np.uint32))
+    mx_ref, l2_ref = _residual(never, d0)
+    assert stats_never[1] == mx_ref
+    assert stats_never[2] == pytest.approx(l2_ref, rel=1e-6)
+    # A reachable tolerance: the residual after 40 iterations.
+    at40, _, _ = solve(40, 0.0)
+    tol = _residual(at40, d0)[0] * 1.01
+    gated, stats_gated, _ = solve(120, tol)
+    m = stats_gated[0]
+    assert m % 10 == 0 and m <= 40 and stats_gated[1] <= tol
+    fixed_m, _, _ = solve(m, 0.0)
+    np.testing.assert_array_equal(gated.view(np.uint32), fixed_m.view(np.uint32))
