@@ -348,35 +348,65 @@ bool Scene::setPressurePath(int path, std::string& err) {
 // 93 KB of shared memory, two CTAs per SM), or 16^3 bricks (128 threads, 67 KB)
 // when the larger ones do not fit co-resident; one CTA per brick.
 bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
+    if (planState_ != 0) {
+        r = plan_;
+        smemBytes = planSmem_;
+        threads = planThreads_;
+        return planState_ == 1;
+    }
+    planState_ = 2;
     int coop = 0, sms = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
+    // Both brick shapes, each kept only if all its bricks fit on the GPU at once.
+    struct Candidate {
+        ResidentBrick r;
+        size_t smem;
+        int threads;
+        long long bricks;
+        bool fits;
+    } cand[2];
     const int shapes[2][3] = {{32, 16, 16}, {16, 16, 16}};
-    for (const auto& sh : shapes) {
-        r.bx = sh[0];
-        r.by = sh[1];
-        r.bz = sh[2];
-        r.nbx = (nx + r.bx - 1) / r.bx;
-        r.nby = (ny + r.by - 1) / r.by;
-        r.nbz = (nz + r.bz - 1) / r.bz;
-        threads = (r.bx / 2) * r.by;
-        smemBytes = sorResidentSharedBytes(r.bx);
-        const void* fn = sorResidentKernel(r.bx);
+    for (int c = 0; c < 2; ++c) {
+        ResidentBrick b{};
+        b.bx = shapes[c][0];
+        b.by = shapes[c][1];
+        b.bz = shapes[c][2];
+        b.nbx = (nx + b.bx - 1) / b.bx;
+        b.nby = (ny + b.by - 1) / b.by;
+        b.nbz = (nz + b.bz - 1) / b.bz;
+        cand[c] = Candidate{b, sorResidentSharedBytes(b.bx), (b.bx / 2) * b.by, static_cast<long long>(b.nbx) * b.nby * b.nbz, false};
+        const void* fn = sorResidentKernel(b.bx);
         int perSm = 0;
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemBytes)) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, threads, smemBytes) != cudaSuccess) {
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cand[c].smem)) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, cand[c].threads, cand[c].smem) != cudaSuccess) {
             cudaGetLastError();
             continue;
         }
-        const long long bricks = static_cast<long long>(r.nbx) * r.nby * r.nbz;
-        if (bricks <= static_cast<long long>(perSm) * sms) {
-            return true;
-        }
+        cand[c].fits = cand[c].bricks <= static_cast<long long>(perSm) * sms;
     }
-    return false;
+    // The larger bricks when they give every SM at least one; the smaller ones
+    // when the larger would leave SMs idle (small grids) or do not fit.
+    int pick = -1;
+    if (cand[0].fits && cand[0].bricks >= sms) {
+        pick = 0;
+    } else if (cand[1].fits) {
+        pick = 1;
+    } else if (cand[0].fits) {
+        pick = 0;
+    }
+    if (pick < 0) return false;
+    plan_ = cand[pick].r;
+    planSmem_ = cand[pick].smem;
+    planThreads_ = cand[pick].threads;
+    planState_ = 1;
+    r = plan_;
+    smemBytes = planSmem_;
+    threads = planThreads_;
+    return true;
 }
 
 // src/fire_cuda.cu:3280-3284 -- 2N half sweeps.  When the grid fits, one

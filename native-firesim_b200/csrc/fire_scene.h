@@ -124,6 +124,10 @@ private:
     int activeSlot_ = 0;
     cudaEvent_t events_[9] = {};
     bool residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads);
+    int planState_ = 0;  // 0 not planned, 1 resident plan, 2 no resident plan
+    ResidentBrick plan_{};
+    size_t planSmem_ = 0;
+    int planThreads_ = 0;
     int pressurePath_ = 0;
     int lastPressurePath_ = 0;
     cudaGraphExec_t sorExec_ = nullptr;

@@ -203,7 +203,7 @@ __device__ __forceinline__ float macCormack(float firstOrder, float lo, float hi
 }  // namespace
 
 // src/fire_cuda.cu:934-1126 -- advection of the ten scalars plus the reaction network.
-__global__ void __launch_bounds__(128) advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel,
+__global__ void __launch_bounds__(128, 6) advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel,
                                                    const float* __restrict__ material, const float* __restrict__ breathing,
                                                    FrameParams p, HashLattice2 sourceLattice) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -825,23 +825,38 @@ __device__ __forceinline__ void residentInterior(float* planes, const float* div
     if (y == 0 || y == BY - 1) return;
     const int gy = oy + y;
     if (!FULL && gy >= g.ny) return;
+    // The two colour planes never overlap: stores to this colour cannot
+    // change the other colour's values, so their loads may run ahead.
+    float* __restrict__ mine = planes + C * S::PLANE;
+    const float* __restrict__ other = planes + O * S::PLANE;
+    const float* __restrict__ dv = divs;
+    auto at = [](int z, int yy, int kk) { return ((z + 1) * S::EY + (yy + 1)) * S::EX + (kk + 1); };
+    const int sy = (C + y) & 1;
+    // The other colour's (y, k) column at z - 1, z, z + 1 slides along z in
+    // registers: it is the back, front and one of the x neighbours.
+    float below = other[at(Z0 - 1, y, k)];
+    float centre = other[at(Z0, y, k)];
 #pragma unroll
     for (int z = Z0; z < Z1; ++z) {
-        const int s = (C + y + z) & 1;
+        const float above = other[at(z + 1, y, k)];
+        const int s = sy ^ (z & 1);
         const int x = 2 * k + s;
-        if (x == 0 || x == BX - 1) continue;
         const int gx = ox + x, gz = oz + z;
-        if (!FULL && (gx >= g.nx || gz >= g.nz)) continue;
-        const float self = planes[S::pidx(C, z, y, k)];
-        const float pL = planes[S::pidx(O, z, y, k + s - 1)];
-        const float pR = (!FULL && gx == g.nx - 1) ? self : planes[S::pidx(O, z, y, k + s)];
-        const float pD = planes[S::pidx(O, z, y - 1, k)];
-        const float pU = (!FULL && gy == g.ny - 1) ? self : planes[S::pidx(O, z, y + 1, k)];
-        const float pB = planes[S::pidx(O, z - 1, y, k)];
-        const float pF = (!FULL && gz == g.nz - 1) ? self : planes[S::pidx(O, z + 1, y, k)];
-        const float d = divs[S::didx(C, z, threadIdx.x)];
-        const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
-        planes[S::pidx(C, z, y, k)] = self + omega * (projected - self);
+        if (x != 0 && x != BX - 1 && (FULL || (gx < g.nx && gz < g.nz))) {
+            const float self = mine[at(z, y, k)];
+            const float side = other[at(z, y, s ? k + 1 : k - 1)];
+            const float pL = s ? centre : side;
+            const float pR = (!FULL && gx == g.nx - 1) ? self : (s ? side : centre);
+            const float pD = other[at(z, y - 1, k)];
+            const float pU = (!FULL && gy == g.ny - 1) ? self : other[at(z, y + 1, k)];
+            const float pB = below;
+            const float pF = (!FULL && gz == g.nz - 1) ? self : above;
+            const float d = dv[S::didx(C, z, threadIdx.x)];
+            const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
+            mine[at(z, y, k)] = self + omega * (projected - self);
+        }
+        below = centre;
+        centre = above;
     }
 }
 
@@ -973,6 +988,9 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                 return;
             }
             // Face cells, with the walls of the grid.
+            float* __restrict__ mineF = planes + c * S::PLANE;
+            const float* __restrict__ otherF = planes + o * S::PLANE;
+            const float* __restrict__ divF = divs;
 #pragma unroll
             for (int j = 0; j < F::PER_THREAD; ++j) {
                 const int cell = face[c][j];
@@ -982,17 +1000,17 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                 const int fx = 2 * fk + s;
                 const int gx = ox + fx, fgy = oy + fy, gz = oz + fz;
                 if (gx >= g.nx || fgy >= g.ny || gz >= g.nz) continue;
-                const float self = planes[S::pidx(c, fz, fy, fk)];
-                const float pL = gx == 0 ? self : planes[S::pidx(o, fz, fy, fk + s - 1)];
-                const float pR = gx == g.nx - 1 ? self : planes[S::pidx(o, fz, fy, fk + s)];
-                const float pD = fgy == 0 ? self : planes[S::pidx(o, fz, fy - 1, fk)];
-                const float pU = fgy == g.ny - 1 ? self : planes[S::pidx(o, fz, fy + 1, fk)];
-                const float pB = gz == 0 ? self : planes[S::pidx(o, fz - 1, fy, fk)];
-                const float pF = gz == g.nz - 1 ? self : planes[S::pidx(o, fz + 1, fy, fk)];
-                const float d = divs[S::didx(c, fz, residentOwner<BX, BY, BZ>(fk, fy))];
+                const float self = mineF[S::pidx(0, fz, fy, fk)];
+                const float pL = gx == 0 ? self : otherF[S::pidx(0, fz, fy, fk + s - 1)];
+                const float pR = gx == g.nx - 1 ? self : otherF[S::pidx(0, fz, fy, fk + s)];
+                const float pD = fgy == 0 ? self : otherF[S::pidx(0, fz, fy - 1, fk)];
+                const float pU = fgy == g.ny - 1 ? self : otherF[S::pidx(0, fz, fy + 1, fk)];
+                const float pB = gz == 0 ? self : otherF[S::pidx(0, fz - 1, fy, fk)];
+                const float pF = gz == g.nz - 1 ? self : otherF[S::pidx(0, fz + 1, fy, fk)];
+                const float d = divF[S::didx(c, fz, residentOwner<BX, BY, BZ>(fk, fy))];
                 const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
                 const float next = self + omega * (projected - self);
-                planes[S::pidx(c, fz, fy, fk)] = next;
+                mineF[S::pidx(0, fz, fy, fk)] = next;
                 if (!last && !silent) {
                     storeExchange(sync.exchange + (gz * g.ny + fgy) * g.nx + gx, next, sync.epoch + static_cast<unsigned>(h + 1));
                 }
