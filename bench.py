@@ -242,6 +242,7 @@ def run_reference(args, world: int, rank: int) -> None:
 def config_block(args) -> dict:
     return {"workload": f"reference frame pipeline (native-firesim physics, 10 scalars, MAC velocity), FP32, "
                         f"{args.grid}^3 grid, SOR {args.sor_iters} iterations omega {args.omega}, "
+                        f"{'FP16 storage, ' if args.precision == 'f16' else ''}"
                         f"{args.frame}x{args.frame} HDR raymarch every {args.render_every} steps "
                         f"({args.samples} samples requested, clamped to 120)",
             "grid": [args.grid] * 3, "frame": [args.frame, args.frame], "sor_iterations": args.sor_iters,
@@ -295,7 +296,7 @@ def run_batched(args, pkg) -> None:
     dims = [sizes[rng.next() % len(sizes)] for _ in range(args.scenes)]
     scenes, settings, hdrs = [], [], []
     for d in dims:
-        sc = pkg.Scene(256, 256, *d)
+        sc = pkg.Scene(256, 256, *d, precision=args.precision)
         sc.set_pressure_solver(40, 1.8)
         hdr = torch.zeros((256, 256, 4), dtype=torch.float32, device="cuda")
         sc.set_hdr_buffer(hdr.data_ptr(), 256 * 16, 0)
@@ -324,7 +325,7 @@ def run_batched(args, pkg) -> None:
     wall = time.perf_counter() - t0
     line = {"metric": "voxel-steps/s", "mode": "batched", "value": voxels * args.steps / wall, "unit": "voxel-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_sub_step": wall * 1e3 / args.steps,
-            "higher_is_better": True, "dtype": "f32", "data": "synthetic (SplitMix64 seed 11 draws)",
+            "higher_is_better": True, "dtype": args.precision, "data": "synthetic (SplitMix64 seed 11 draws)",
             "config": {"workload": f"{args.scenes} independent scenes, sizes drawn from {sizes}, reference physics FP32, "
                                    f"SOR 40 iterations omega 1.8, 256x256 render (64 samples) every {args.render_every} steps, "
                                    "one fireBatchStep per sub-step, each scene on its own stream",
@@ -338,7 +339,7 @@ def run_serve(args, pkg) -> None:
     """Poisson arrivals of scene requests into the FireServer loop."""
     abi = pkg.abi
     rng = SplitMix64(args.seed)
-    server = pkg.Server(budget_bytes=int(args.budget_gb * (1 << 30)))
+    server = pkg.Server(budget_bytes=int(args.budget_gb * (1 << 30)), precision=args.precision)
     server.set_limits(int(args.max_active_mvoxels * 1e6))
     t, n = 0.0, 0
     keep = []
@@ -363,7 +364,7 @@ def run_serve(args, pkg) -> None:
     rep = server.run(args.serve_seconds)
     server.close()
     line = {"metric": "voxel-steps/s", "mode": "serve", "value": rep["voxelSteps"] / max(rep["seconds"], 1e-9),
-            "unit": "voxel-steps/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (SplitMix64 draws)",
+            "unit": "voxel-steps/s", "n_gpus": 1, "higher_is_better": True, "dtype": args.precision, "data": "synthetic (SplitMix64 draws)",
             "latency_ms": {"step_p50": rep["stepMsP50"], "step_p95": rep["stepMsP95"], "step_p99": rep["stepMsP99"],
                            "step_max": rep["stepMsMax"], "frame_p50": rep["frameMsP50"], "frame_p95": rep["frameMsP95"],
                            "frame_p99": rep["frameMsP99"], "queue_p50": rep["queueMsP50"], "queue_p99": rep["queueMsP99"]},
@@ -393,6 +394,8 @@ def main() -> int:
     ap.add_argument("--reference-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16"],
+                    help="storage of the transported fields: f32 (the reference's) or f16 (FP32 arithmetic)")
     ap.add_argument("--mode", default="single", choices=["single", "batched", "serve"],
                     help="single: the 128^3 scene (the headline line); batched: --scenes scenes per fireBatchStep; "
                          "serve: Poisson requests into the FireServer loop")
@@ -427,10 +430,10 @@ def main() -> int:
         dist_barrier(world)
         return 0
     abi = pkg.abi
-    lib = pkg.load_library()
+    lib = pkg.load_library(args.precision)
     if not lib.fireCudaSelectDevice(local):
-        raise RuntimeError(pkg.firesim.last_error())
-    sim = pkg.FireSim(args.frame, args.frame, args.grid, args.grid, args.grid)
+        raise RuntimeError(pkg.firesim.last_error(lib))
+    sim = pkg.FireSim(args.frame, args.frame, args.grid, args.grid, args.grid, precision=args.precision)
     sim.set_pressure_solver(args.sor_iters, args.omega)
     sim.set_pressure_path({"auto": 0, "graph": 1, "resident": 2}[args.sor_path])
     hdr = torch.zeros((args.frame, args.frame, 4), dtype=torch.float32, device="cuda")
@@ -446,7 +449,7 @@ def main() -> int:
         if host_bgra is not None and render:
             ok = lib.fireCudaStepAndRender(host_bgra.ctypes.data, s)
             if not ok:
-                raise RuntimeError(pkg.firesim.last_error())
+                raise RuntimeError(pkg.firesim.last_error(lib))
         elif render:
             sim.step_and_render_hdr(s)
         else:
@@ -535,7 +538,8 @@ def main() -> int:
         line = {
             "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": device_s * 1e3 / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "f32" else "f16-storage/f32-arithmetic",
             "data": "synthetic (seeded procedural fuel bed + validation-harness settings)",
             "config": config_block(args), "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "roofline": roofline, "stage_ms": per_step_ms, "step_latency": latency, "cpu_baseline": cpu,

@@ -20,6 +20,9 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OBJ = HERE / "_build"
 LIB = HERE / "libfiresim_b200.so"
+# The FP16-storage variant: the same sources with -DFIRE_STORAGE_F16.
+OBJ_F16 = HERE / "_build_f16"
+LIB_F16 = HERE / "libfiresim_b200_f16.so"
 INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr"]
@@ -37,12 +40,12 @@ def headers() -> list[Path]:
     return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
 
 
-def _compile(src: Path, force: bool, verbose_ptxas: bool) -> tuple[Path, str]:
-    obj = OBJ / (src.stem + ".o")
+def _compile(src: Path, force: bool, verbose_ptxas: bool, f16: bool = False) -> tuple[Path, str]:
+    obj = (OBJ_F16 if f16 else OBJ) / (src.stem + ".o")
     newest_dep = max([src.stat().st_mtime] + [h.stat().st_mtime for h in headers()])
     if not force and obj.exists() and obj.stat().st_mtime >= newest_dep and not verbose_ptxas:
         return obj, ""
-    cmd = [_nvcc(), *ARCH, *CUFLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+    cmd = [_nvcc(), *ARCH, *CUFLAGS, *(["-DFIRE_STORAGE_F16"] if f16 else []), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
     if verbose_ptxas:
         cmd[1:1] = ["-Xptxas", "-v"]
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -51,25 +54,34 @@ def _compile(src: Path, force: bool, verbose_ptxas: bool) -> tuple[Path, str]:
     return obj, res.stderr
 
 
-def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True) -> Path:
-    OBJ.mkdir(parents=True, exist_ok=True)
+def _build_variant(f16: bool, force: bool, verbose_ptxas: bool, quiet: bool) -> Path:
+    objdir, lib = (OBJ_F16, LIB_F16) if f16 else (OBJ, LIB)
+    objdir.mkdir(parents=True, exist_ok=True)
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        results = list(ex.map(lambda s: _compile(s, force, verbose_ptxas), srcs))
+        results = list(ex.map(lambda s: _compile(s, force, verbose_ptxas, f16), srcs))
     if verbose_ptxas:
         for _, log in results:
             print(log)
     objs = [o for o, _ in results]
-    if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    if force or not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objs):
+        tmp = lib.with_suffix(".so.tmp")
         cmd = [_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
-        os.replace(tmp, LIB)
+        os.replace(tmp, lib)
         if not quiet:
-            print(f"linked {LIB}")
-    return LIB
+            print(f"linked {lib}")
+    return lib
+
+
+def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True, f16: bool = True) -> Path:
+    """Builds the FP32 library (returned) and, unless f16=False, the FP16-storage variant."""
+    lib = _build_variant(False, force, verbose_ptxas, quiet)
+    if f16:
+        _build_variant(True, force, False, quiet)
+    return lib
 
 
 def main() -> int:

@@ -13,6 +13,9 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#if defined(FIRE_STORAGE_F16)
+#include <cuda_fp16.h>
+#endif
 
 namespace firesim {
 
@@ -42,6 +45,62 @@ struct FrameParams {
     float burnerCenterX[4], burnerCenterY[4], burnerCenterZ[4];
 };
 
+// Storage of the transported fields.  The default build stores the ten
+// scalars and the three face grids in FP32.  The FIRE_STORAGE_F16 build
+// (libfiresim_b200_f16.so) stores them as IEEE half, converted on every load
+// and rounded to nearest on every store; all arithmetic stays FP32, and
+// pressure, divergence, forcing, light and frames stay FP32.  ldv/stv are the
+// only accessors of these buffers, so in the FP32 build they are the plain
+// loads and stores they replace.
+#if defined(FIRE_STORAGE_F16)
+struct __align__(8) Rec4 {
+    __half2 xy, zw;
+};
+using Rec2 = __half2;
+using FaceT = __half;
+constexpr bool kHalfStorage = true;
+#else
+using Rec4 = float4;
+using Rec2 = float2;
+using FaceT = float;
+constexpr bool kHalfStorage = false;
+#endif
+
+__device__ __forceinline__ float ldv(const float* p) { return __ldg(p); }
+__device__ __forceinline__ void stv(float* p, float v) { *p = v; }
+#if defined(FIRE_STORAGE_F16)
+__device__ __forceinline__ float4 ldv(const Rec4* p) {
+    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(p));
+    const float2 xy = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+    const float2 zw = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+    return make_float4(xy.x, xy.y, zw.x, zw.y);
+}
+__device__ __forceinline__ float2 ldv(const Rec2* p) { return __half22float2(__ldg(p)); }
+__device__ __forceinline__ float ldv(const __half* p) { return __half2float(__ldg(p)); }
+__device__ __forceinline__ void stv(Rec4* p, float4 v) {
+    Rec4 r;
+    r.xy = __floats2half2_rn(v.x, v.y);
+    r.zw = __floats2half2_rn(v.z, v.w);
+    *p = r;
+}
+__device__ __forceinline__ void stv(Rec2* p, float2 v) { *p = __floats2half2_rn(v.x, v.y); }
+__device__ __forceinline__ void stv(__half* p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ float4 ldv(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ float2 ldv(const float2* p) { return __ldg(p); }
+// Single components of a packed record.
+__device__ __forceinline__ float ldX(const Rec4* p) { return __half2float(__ldg(reinterpret_cast<const __half*>(p))); }
+__device__ __forceinline__ float ldW(const Rec4* p) { return __half2float(__ldg(reinterpret_cast<const __half*>(p) + 3)); }
+__device__ __forceinline__ float ldX(const Rec2* p) { return __half2float(__ldg(reinterpret_cast<const __half*>(p))); }
+#else
+__device__ __forceinline__ float4 ldv(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ float2 ldv(const float2* p) { return __ldg(p); }
+__device__ __forceinline__ void stv(float4* p, float4 v) { *p = v; }
+__device__ __forceinline__ void stv(float2* p, float2 v) { *p = v; }
+__device__ __forceinline__ float ldX(const float4* p) { return __ldg(&p->x); }
+__device__ __forceinline__ float ldW(const float4* p) { return __ldg(&p->w); }
+__device__ __forceinline__ float ldX(const float2* p) { return __ldg(&p->x); }
+#endif
+
 // Packed cell record of the ten transported scalars: every consumer gathers
 // many of them at the same trilinear corners, so one corner is three vector
 // loads instead of ten scalar ones.
@@ -49,14 +108,14 @@ struct FrameParams {
 //   b = (char, ash, pyrolysis, progress)
 //   c = (turbulenceEnergy, sootOptics)
 struct ScalarFields {
-    float4* a;
-    float4* b;
-    float2* c;
+    Rec4* a;
+    Rec4* b;
+    Rec2* c;
 };
 struct ScalarFieldsIn {
-    const float4* __restrict__ a;
-    const float4* __restrict__ b;
-    const float2* __restrict__ c;
+    const Rec4* __restrict__ a;
+    const Rec4* __restrict__ b;
+    const Rec2* __restrict__ c;
 };
 
 struct Cell10 {
@@ -64,9 +123,9 @@ struct Cell10 {
 };
 
 __device__ __forceinline__ Cell10 loadCell(const ScalarFieldsIn& s, int idx) {
-    const float4 a = __ldg(s.a + idx);
-    const float4 b = __ldg(s.b + idx);
-    const float2 c = __ldg(s.c + idx);
+    const float4 a = ldv(s.a + idx);
+    const float4 b = ldv(s.b + idx);
+    const float2 c = ldv(s.c + idx);
     return {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y};
 }
 
@@ -327,16 +386,18 @@ __device__ __forceinline__ Corners cornersOf(float u, float v, float w, int ex, 
     return c;
 }
 
-// Gather of one float lattice with row pitch sx and slice pitch sx*sy.
-__device__ __forceinline__ float gather1(const float* __restrict__ f, const Corners& c, int sx, int sy) {
-    const float c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
-    const float c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
-    const float c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
-    const float c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
-    const float c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
-    const float c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
-    const float c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
-    const float c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
+// Gather of one scalar lattice (float, or a half face grid) with row pitch sx
+// and slice pitch sx*sy.
+template <class T>
+__device__ __forceinline__ float gather1(const T* __restrict__ f, const Corners& c, int sx, int sy) {
+    const float c000 = ldv(f + (c.z0 * sy + c.y0) * sx + c.x0);
+    const float c100 = ldv(f + (c.z0 * sy + c.y0) * sx + c.x1);
+    const float c010 = ldv(f + (c.z0 * sy + c.y1) * sx + c.x0);
+    const float c110 = ldv(f + (c.z0 * sy + c.y1) * sx + c.x1);
+    const float c001 = ldv(f + (c.z1 * sy + c.y0) * sx + c.x0);
+    const float c101 = ldv(f + (c.z1 * sy + c.y0) * sx + c.x1);
+    const float c011 = ldv(f + (c.z1 * sy + c.y1) * sx + c.x0);
+    const float c111 = ldv(f + (c.z1 * sy + c.y1) * sx + c.x1);
     return lerpf(lerpf(lerpf(c000, c100, c.tx), lerpf(c010, c110, c.tx), c.ty),
                  lerpf(lerpf(c001, c101, c.tx), lerpf(c011, c111, c.tx), c.ty), c.tz);
 }
@@ -345,20 +406,20 @@ struct Grid {
     int nx, ny, nz;
 };
 
-__device__ __forceinline__ float sampleU(const float* __restrict__ u, const Grid& g, float a, float b, float c) {
+__device__ __forceinline__ float sampleU(const FaceT* __restrict__ u, const Grid& g, float a, float b, float c) {
     return gather1(u, cornersOf(a, b, c, g.nx, g.ny - 1, g.nz - 1), g.nx + 1, g.ny);
 }
-__device__ __forceinline__ float sampleV(const float* __restrict__ v, const Grid& g, float a, float b, float c) {
+__device__ __forceinline__ float sampleV(const FaceT* __restrict__ v, const Grid& g, float a, float b, float c) {
     return gather1(v, cornersOf(a, b, c, g.nx - 1, g.ny, g.nz - 1), g.nx, g.ny + 1);
 }
-__device__ __forceinline__ float sampleW(const float* __restrict__ w, const Grid& g, float a, float b, float c) {
+__device__ __forceinline__ float sampleW(const FaceT* __restrict__ w, const Grid& g, float a, float b, float c) {
     return gather1(w, cornersOf(a, b, c, g.nx - 1, g.ny - 1, g.nz), g.nx, g.ny);
 }
 
 struct Velocity {
-    const float* __restrict__ u;
-    const float* __restrict__ v;
-    const float* __restrict__ w;
+    const FaceT* __restrict__ u;
+    const FaceT* __restrict__ v;
+    const FaceT* __restrict__ w;
 };
 
 __device__ __forceinline__ float3 sampleVelocity(const Velocity& vel, const Grid& g, float a, float b, float c) {
@@ -376,35 +437,23 @@ __device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
 }
 __device__ __forceinline__ float2 lerp2v(float2 a, float2 b, float t) { return make_float2(lerpf(a.x, b.x, t), lerpf(a.y, b.y, t)); }
 
-template <class V>
-__device__ __forceinline__ V gatherVec(const V* __restrict__ f, const Corners& c, int sx, int sy);
+__device__ __forceinline__ float4 lerpv(float4 a, float4 b, float t) { return lerp4(a, b, t); }
+__device__ __forceinline__ float2 lerpv(float2 a, float2 b, float t) { return lerp2v(a, b, t); }
 
-template <>
-__device__ __forceinline__ float4 gatherVec<float4>(const float4* __restrict__ f, const Corners& c, int sx, int sy) {
-    const float4 c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
-    const float4 c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
-    const float4 c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
-    const float4 c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
-    const float4 c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
-    const float4 c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
-    const float4 c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
-    const float4 c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
-    return lerp4(lerp4(lerp4(c000, c100, c.tx), lerp4(c010, c110, c.tx), c.ty),
-                 lerp4(lerp4(c001, c101, c.tx), lerp4(c011, c111, c.tx), c.ty), c.tz);
-}
-
-template <>
-__device__ __forceinline__ float2 gatherVec<float2>(const float2* __restrict__ f, const Corners& c, int sx, int sy) {
-    const float2 c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
-    const float2 c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
-    const float2 c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
-    const float2 c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
-    const float2 c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
-    const float2 c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
-    const float2 c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
-    const float2 c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
-    return lerp2v(lerp2v(lerp2v(c000, c100, c.tx), lerp2v(c010, c110, c.tx), c.ty),
-                  lerp2v(lerp2v(c001, c101, c.tx), lerp2v(c011, c111, c.tx), c.ty), c.tz);
+// Gather of a packed lattice (float4 / float2, or a half record), blended
+// component-wise in FP32.
+template <class P>
+__device__ __forceinline__ auto gatherVec(const P* __restrict__ f, const Corners& c, int sx, int sy) -> decltype(ldv(f)) {
+    const auto c000 = ldv(f + (c.z0 * sy + c.y0) * sx + c.x0);
+    const auto c100 = ldv(f + (c.z0 * sy + c.y0) * sx + c.x1);
+    const auto c010 = ldv(f + (c.z0 * sy + c.y1) * sx + c.x0);
+    const auto c110 = ldv(f + (c.z0 * sy + c.y1) * sx + c.x1);
+    const auto c001 = ldv(f + (c.z1 * sy + c.y0) * sx + c.x0);
+    const auto c101 = ldv(f + (c.z1 * sy + c.y0) * sx + c.x1);
+    const auto c011 = ldv(f + (c.z1 * sy + c.y1) * sx + c.x0);
+    const auto c111 = ldv(f + (c.z1 * sy + c.y1) * sx + c.x1);
+    return lerpv(lerpv(lerpv(c000, c100, c.tx), lerpv(c010, c110, c.tx), c.ty),
+                 lerpv(lerpv(c001, c101, c.tx), lerpv(c011, c111, c.tx), c.ty), c.tz);
 }
 
 __device__ __forceinline__ Corners scalarCorners(const Grid& g, float u, float v, float w) {
@@ -424,7 +473,7 @@ __device__ __forceinline__ Cell10 sampleAll(const ScalarFieldsIn& s, const Grid&
 __device__ __forceinline__ float sampleHeat(const ScalarFieldsIn& s, const Grid& g, float u, float v, float w) {
     const Corners c = scalarCorners(g, u, v, w);
     const int sx = g.nx, sy = g.ny;
-    auto h = [&](int x, int y, int z) { return __ldg(&s.a[(z * sy + y) * sx + x].x); };
+    auto h = [&](int x, int y, int z) { return ldX(s.a + (z * sy + y) * sx + x); };
     return lerpf(lerpf(lerpf(h(c.x0, c.y0, c.z0), h(c.x1, c.y0, c.z0), c.tx), lerpf(h(c.x0, c.y1, c.z0), h(c.x1, c.y1, c.z0), c.tx), c.ty),
                  lerpf(lerpf(h(c.x0, c.y0, c.z1), h(c.x1, c.y0, c.z1), c.tx), lerpf(h(c.x0, c.y1, c.z1), h(c.x1, c.y1, c.z1), c.tx), c.ty),
                  c.tz);

@@ -69,15 +69,15 @@ constexpr int kMetricThreads = 128;
 __global__ void fuelBedTables(float* material, float* breathing, FrameParams p, int withMaterial);
 __global__ void resetCells(ScalarFields out, float* pressure, float* divergence, float* divergenceAfter, const float* material,
                            const float* breathing, FrameParams p);
-__global__ void advectVelocity(float* uOut, float* vOut, float* wOut, Velocity vel, FrameParams p);
+__global__ void advectVelocity(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, FrameParams p);
 __global__ void advectReact(ScalarFields out, ScalarFieldsIn in, Velocity vel, const float* material, const float* breathing, FrameParams p,
                             HashLattice2 sourceLattice);
 __global__ void hashLatticeBuild(HashLattice2 a, HashLattice2 b);
 __global__ void forceContributions(float4* contrib, ScalarFieldsIn s, Velocity vel, FrameParams p, HashLattice2 curlA, HashLattice2 curlB);
-__global__ void forceApply(float* uOut, float* vOut, float* wOut, const float4* contrib, Velocity vel, FrameParams p);
-__global__ void forceProjectSetup(float* uOut, float* vOut, float* wOut, float* divergence, float* pressure, const float4* contrib,
+__global__ void forceApply(FaceT* uOut, FaceT* vOut, FaceT* wOut, const float4* contrib, Velocity vel, FrameParams p);
+__global__ void forceProjectSetup(FaceT* uOut, FaceT* vOut, FaceT* wOut, float* divergence, float* pressure, const float4* contrib,
                                   Velocity vel, FrameParams p);
-__global__ void velocityBoundary(float* u, float* v, float* w, FrameParams p, int clampValues);
+__global__ void velocityBoundary(FaceT* u, FaceT* v, FaceT* w, FrameParams p, int clampValues);
 __global__ void divergenceOf(float* divergence, float* pressureOrNull, Velocity vel, FrameParams p);
 __global__ void sorHalfSweep(float* pressure, const float* divergence, Grid g, int parity, float omega);
 __global__ void sorResidualPartials(const float* pressure, const float* divergence, Grid g, const SorGate* gate, double* partialSq,
@@ -89,7 +89,7 @@ __global__ void sorResidualFinal(SorGate* gate, const double* partialSq, const f
 const void* sorResidentKernel(int bx);
 // Dynamic shared memory of that instantiation (padded colour planes + div).
 size_t sorResidentSharedBytes(int bx);
-__global__ void subtractWall(float* u, float* v, float* w, const float* pressure, FrameParams p, int doSubtract, int doWalls);
+__global__ void subtractWall(FaceT* u, FaceT* v, FaceT* w, const float* pressure, FrameParams p, int doSubtract, int doWalls);
 
 // fire_light.cu
 __global__ void lightBuild(float4* sceneLight, float* sceneShadow, ScalarFieldsIn s, FrameParams p);

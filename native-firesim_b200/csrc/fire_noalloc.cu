@@ -88,16 +88,19 @@ extern "C" bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float 
     dims.frameW = 1;
     dims.frameH = 1;
     const firesim::FrameParams p = dims.paramsFrom(*settings, time);
-    const firesim::ScalarFieldsIn in{static_cast<const float4*>(recordsA), static_cast<const float4*>(recordsB),
-                                     static_cast<const float2*>(recordsC)};
-    const firesim::Velocity vel{u, v, w};
+    // Records and faces in this build's storage format (float, or half in the FP16 build).
+    const firesim::ScalarFieldsIn in{static_cast<const firesim::Rec4*>(recordsA), static_cast<const firesim::Rec4*>(recordsB),
+                                     static_cast<const firesim::Rec2*>(recordsC)};
+    const firesim::Velocity vel{reinterpret_cast<const firesim::FaceT*>(u), reinterpret_cast<const firesim::FaceT*>(v),
+                                reinterpret_cast<const firesim::FaceT*>(w)};
     const int bx = nx <= 32 ? 32 : (nx <= 64 ? 64 : 128);
     const dim3 grid((nx + bx - 1) / bx, ny, nz);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // No lattice storage here: every curl-noise corner is hashed in place.
     const firesim::HashLattice2 noLattice{};
     firesim::forceContributions<<<grid, bx, 0, s>>>(scratch, in, vel, p, noLattice, noLattice);
-    firesim::forceProjectSetup<<<grid, bx, 0, s>>>(uOut, vOut, wOut, divergence, pressure, scratch, vel, p);
+    firesim::forceProjectSetup<<<grid, bx, 0, s>>>(reinterpret_cast<firesim::FaceT*>(uOut), reinterpret_cast<firesim::FaceT*>(vOut),
+                                                   reinterpret_cast<firesim::FaceT*>(wOut), divergence, pressure, scratch, vel, p);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(std::string("force pass launch: ") + cudaGetErrorString(e));
     return true;

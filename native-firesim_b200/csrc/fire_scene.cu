@@ -132,12 +132,12 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
     if (!check("cudaStreamCreate", cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), err)) return false;
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) {
-        ok = alloc(reinterpret_cast<void**>(&sa_[i]), cells_ * sizeof(float4), "cudaMalloc scalars a", err) &&
-             alloc(reinterpret_cast<void**>(&sb_[i]), cells_ * sizeof(float4), "cudaMalloc scalars b", err) &&
-             alloc(reinterpret_cast<void**>(&sc_[i]), cells_ * sizeof(float2), "cudaMalloc scalars c", err) &&
-             alloc(reinterpret_cast<void**>(&vel_[0][i]), nu_ * sizeof(float), "cudaMalloc u", err) &&
-             alloc(reinterpret_cast<void**>(&vel_[1][i]), nv_ * sizeof(float), "cudaMalloc v", err) &&
-             alloc(reinterpret_cast<void**>(&vel_[2][i]), nw_ * sizeof(float), "cudaMalloc w", err);
+        ok = alloc(reinterpret_cast<void**>(&sa_[i]), cells_ * sizeof(Rec4), "cudaMalloc scalars a", err) &&
+             alloc(reinterpret_cast<void**>(&sb_[i]), cells_ * sizeof(Rec4), "cudaMalloc scalars b", err) &&
+             alloc(reinterpret_cast<void**>(&sc_[i]), cells_ * sizeof(Rec2), "cudaMalloc scalars c", err) &&
+             alloc(reinterpret_cast<void**>(&vel_[0][i]), nu_ * sizeof(FaceT), "cudaMalloc u", err) &&
+             alloc(reinterpret_cast<void**>(&vel_[1][i]), nv_ * sizeof(FaceT), "cudaMalloc v", err) &&
+             alloc(reinterpret_cast<void**>(&vel_[2][i]), nw_ * sizeof(FaceT), "cudaMalloc w", err);
     }
     ok = ok && alloc(reinterpret_cast<void**>(&pressure_), cells_ * sizeof(float), "cudaMalloc pressure", err) &&
          alloc(reinterpret_cast<void**>(&divergence_), cells_ * sizeof(float), "cudaMalloc divergence", err) &&
@@ -731,8 +731,8 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                 bool ok = true;
                 for (int c = 0; c < 3 && ok; ++c) {
                     const size_t n = c == 0 ? nu_ : (c == 1 ? nv_ : nw_);
-                    ok = check("reset velocity", cudaMemsetAsync(vel_[c][0], 0, n * sizeof(float), stream), err) &&
-                         check("reset velocity", cudaMemsetAsync(vel_[c][1], 0, n * sizeof(float), stream), err);
+                    ok = check("reset velocity", cudaMemsetAsync(vel_[c][0], 0, n * sizeof(FaceT), stream), err) &&
+                         check("reset velocity", cudaMemsetAsync(vel_[c][1], 0, n * sizeof(FaceT), stream), err);
                 }
                 ok = ok && check("reset scene light", cudaMemsetAsync(light_, 0, lightCells_ * sizeof(float4), stream), err) &&
                      check("reset scene light next", cudaMemsetAsync(lightNext_, 0, lightCells_ * sizeof(float4), stream), err) &&
@@ -917,37 +917,69 @@ namespace {
 
 struct FieldView {
     void* base;
-    size_t count;    // elements of `stride` floats
-    int stride;      // floats per element in device memory
-    int component;   // float offset inside the element
+    size_t count;    // elements of `stride` values
+    int stride;      // values per element in device memory
+    int component;   // value offset inside the element
     int width;       // floats per element in the host layout
+    int valueBytes;  // bytes of one stored value: 4 (float), or 2 for the transported fields of the half build
 };
 
 }  // namespace
 
-static bool fieldView(int field, float4* sa, float4* sb, float2* sc, float* const vel[3], float* pressure, float* divergence,
+static bool fieldView(int field, Rec4* sa, Rec4* sb, Rec2* sc, FaceT* const vel[3], float* pressure, float* divergence,
                       float* divergenceAfter, float4* light, float* shadow, float4* hdr, uint32_t* bgra, size_t cells, size_t nu,
                       size_t nv, size_t nw, size_t lightCells, size_t pixels, FieldView& v) {
+    const int t = static_cast<int>(sizeof(FaceT));
     switch (field) {
-        case 0: case 1: case 2: case 3: v = {sa, cells, 4, field, 1}; return true;
-        case 4: case 5: case 6: case 7: v = {sb, cells, 4, field - 4, 1}; return true;
-        case 8: case 9: v = {sc, cells, 2, field - 8, 1}; return true;
-        case 10: v = {pressure, cells, 1, 0, 1}; return true;
-        case 11: v = {divergence, cells, 1, 0, 1}; return true;
-        case 12: v = {vel[0], nu, 1, 0, 1}; return true;
-        case 13: v = {vel[1], nv, 1, 0, 1}; return true;
-        case 14: v = {vel[2], nw, 1, 0, 1}; return true;
-        case 15: v = {light, lightCells, 4, 0, 4}; return true;
-        case 16: v = {shadow, lightCells, 1, 0, 1}; return true;
-        case 17: v = {hdr, pixels, 4, 0, 4}; return true;
-        case 18: v = {bgra, pixels, 1, 0, 1}; return true;
-        case 19: v = {divergenceAfter, cells, 1, 0, 1}; return true;
+        case 0: case 1: case 2: case 3: v = {sa, cells, 4, field, 1, t}; return true;
+        case 4: case 5: case 6: case 7: v = {sb, cells, 4, field - 4, 1, t}; return true;
+        case 8: case 9: v = {sc, cells, 2, field - 8, 1, t}; return true;
+        case 10: v = {pressure, cells, 1, 0, 1, 4}; return true;
+        case 11: v = {divergence, cells, 1, 0, 1, 4}; return true;
+        case 12: v = {vel[0], nu, 1, 0, 1, t}; return true;
+        case 13: v = {vel[1], nv, 1, 0, 1, t}; return true;
+        case 14: v = {vel[2], nw, 1, 0, 1, t}; return true;
+        case 15: v = {light, lightCells, 4, 0, 4, 4}; return true;
+        case 16: v = {shadow, lightCells, 1, 0, 1, 4}; return true;
+        case 17: v = {hdr, pixels, 4, 0, 4, 4}; return true;
+        case 18: v = {bgra, pixels, 1, 0, 1, 4}; return true;
+        case 19: v = {divergenceAfter, cells, 1, 0, 1, 4}; return true;
         default: return false;
     }
 }
 
+namespace {
+
+float storedToFloat(const unsigned char* p, int bytes) {
+    if (bytes == 4) {
+        float f;
+        std::memcpy(&f, p, 4);
+        return f;
+    }
+#if defined(FIRE_STORAGE_F16)
+    __half h;
+    std::memcpy(&h, p, 2);
+    return __half2float(h);
+#else
+    return 0.0f;
+#endif
+}
+
+void floatToStored(float f, unsigned char* p, int bytes) {
+    if (bytes == 4) {
+        std::memcpy(p, &f, 4);
+        return;
+    }
+#if defined(FIRE_STORAGE_F16)
+    const __half h = __float2half_rn(f);
+    std::memcpy(p, &h, 2);
+#endif
+}
+
+}  // namespace
+
 bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
-    float* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
+    FaceT* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
     FieldView v;
     if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_, bgra_,
                    cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
@@ -959,18 +991,22 @@ bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
         return false;
     }
     if (!check("field sync", cudaStreamSynchronize(stream), err)) return false;
-    if (v.width == v.stride) {
+    if (v.width == v.stride && v.valueBytes == 4) {
         return check("cudaMemcpy field", cudaMemcpy(host, v.base, bytes, cudaMemcpyDeviceToHost), err);
     }
-    std::vector<float> staging(v.count * v.stride);
-    if (!check("cudaMemcpy field", cudaMemcpy(staging.data(), v.base, staging.size() * 4, cudaMemcpyDeviceToHost), err)) return false;
+    std::vector<unsigned char> staging(v.count * v.stride * v.valueBytes);
+    if (!check("cudaMemcpy field", cudaMemcpy(staging.data(), v.base, staging.size(), cudaMemcpyDeviceToHost), err)) return false;
     float* out = static_cast<float*>(host);
-    for (size_t i = 0; i < v.count; ++i) out[i] = staging[i * v.stride + v.component];
+    for (size_t i = 0; i < v.count; ++i) {
+        for (int w = 0; w < v.width; ++w) {
+            out[i * v.width + w] = storedToFloat(staging.data() + (i * v.stride + v.component + w) * v.valueBytes, v.valueBytes);
+        }
+    }
     return true;
 }
 
 bool Scene::setField(int field, const void* host, size_t bytes, std::string& err) {
-    float* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
+    FaceT* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
     FieldView v;
     if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_, bgra_,
                    cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
@@ -982,14 +1018,18 @@ bool Scene::setField(int field, const void* host, size_t bytes, std::string& err
         return false;
     }
     if (!check("field sync", cudaStreamSynchronize(stream), err)) return false;
-    if (v.width == v.stride) {
+    if (v.width == v.stride && v.valueBytes == 4) {
         return check("cudaMemcpy field", cudaMemcpy(v.base, host, bytes, cudaMemcpyHostToDevice), err);
     }
-    std::vector<float> staging(v.count * v.stride);
-    if (!check("cudaMemcpy field", cudaMemcpy(staging.data(), v.base, staging.size() * 4, cudaMemcpyDeviceToHost), err)) return false;
+    std::vector<unsigned char> staging(v.count * v.stride * v.valueBytes);
+    if (!check("cudaMemcpy field", cudaMemcpy(staging.data(), v.base, staging.size(), cudaMemcpyDeviceToHost), err)) return false;
     const float* in = static_cast<const float*>(host);
-    for (size_t i = 0; i < v.count; ++i) staging[i * v.stride + v.component] = in[i];
-    return check("cudaMemcpy field", cudaMemcpy(v.base, staging.data(), staging.size() * 4, cudaMemcpyHostToDevice), err);
+    for (size_t i = 0; i < v.count; ++i) {
+        for (int w = 0; w < v.width; ++w) {
+            floatToStored(in[i * v.width + w], staging.data() + (i * v.stride + v.component + w) * v.valueBytes, v.valueBytes);
+        }
+    }
+    return check("cudaMemcpy field", cudaMemcpy(v.base, staging.data(), staging.size(), cudaMemcpyHostToDevice), err);
 }
 
 bool Scene::registerHdrSlot(int slot, void* ptr, size_t pitch, int format, std::string& err) {

@@ -98,11 +98,11 @@ private:
 
     unsigned long long launches_ = 0;
     size_t cells_ = 0, nu_ = 0, nv_ = 0, nw_ = 0, lightCells_ = 0, pixels_ = 0, deviceBytes_ = 0;
-    float4* sa_[2] = {};
-    float4* sb_[2] = {};
-    float2* sc_[2] = {};
+    Rec4* sa_[2] = {};
+    Rec4* sb_[2] = {};
+    Rec2* sc_[2] = {};
     int cur_ = 0;
-    float* vel_[3][2] = {};
+    FaceT* vel_[3][2] = {};
     int vcur_ = 0;
     float* pressure_ = nullptr;
     float* divergence_ = nullptr;

@@ -79,9 +79,9 @@ __global__ void __launch_bounds__(256) resetCells(ScalarFields out, float* __res
     const float progress = bed * (sc == 2 ? 0.11f : (sc == 1 ? 0.24f : 0.21f));
     const float turbulence = bed * (sc == 2 ? 0.012f : (sc == 1 ? 0.082f : 0.065f));
     const float sootOptics = bed * (sc == 2 ? 0.00050f : 0.018f) * sootScale;
-    out.a[idx] = make_float4(heat, fuel, 1.0f, soot);
-    out.b[idx] = make_float4(charMass, ash, pyrolysis, progress);
-    out.c[idx] = make_float2(turbulence, sootOptics);
+    stv(out.a + idx, make_float4(heat, fuel, 1.0f, soot));
+    stv(out.b + idx, make_float4(charMass, ash, pyrolysis, progress));
+    stv(out.c + idx, make_float2(turbulence, sootOptics));
     pressure[idx] = 0.0f;
     divergence[idx] = 0.0f;
     divergenceAfter[idx] = 0.0f;
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(256) resetCells(ScalarFields out, float* __res
 // ---------------------------------------------------------------------------
 // src/fire_cuda.cu:880-932 -- self-advection of the three face grids.  One
 // thread owns the u, v and w faces that share its (x, y, z) index.
-__global__ void __launch_bounds__(256) advectVelocity(float* __restrict__ uOut, float* __restrict__ vOut, float* __restrict__ wOut,
+__global__ void __launch_bounds__(256) advectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
                                                       Velocity vel, FrameParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) advectVelocity(float* __restrict__ uOut, 
             r = sampleU(vel.u, g, fu - c.x * back * kAdvectionScale, fv - c.y * back * kAdvectionScale,
                         fw - c.z * back * kAdvectionScale) * 0.995f;
         }
-        uOut[uAt(g, x, y, z)] = r;
+        stv(uOut + uAt(g, x, y, z), r);
     }
     if (x < p.nx && y <= p.ny && z < p.nz) {
         float r = 0.0f;
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) advectVelocity(float* __restrict__ uOut, 
             r = sampleV(vel.v, g, fu - c.x * back * kAdvectionScale, fv - c.y * back * kAdvectionScale,
                         fw - c.z * back * kAdvectionScale) * 0.996f;
         }
-        vOut[vAt(g, x, y, z)] = r;
+        stv(vOut + vAt(g, x, y, z), r);
     }
     if (x < p.nx && y < p.ny && z <= p.nz) {
         float r = 0.0f;
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256) advectVelocity(float* __restrict__ uOut, 
             r = sampleW(vel.w, g, fu - c.x * back * kAdvectionScale, fv - c.y * back * kAdvectionScale,
                         fw - c.z * back * kAdvectionScale) * 0.995f;
         }
-        wOut[wAt(g, x, y, z)] = r;
+        stv(wOut + wAt(g, x, y, z), r);
     }
 }
 
@@ -158,41 +158,27 @@ __device__ __forceinline__ float4 max4(float4 a, float4 b) {
 __device__ __forceinline__ float2 min2(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
 __device__ __forceinline__ float2 max2(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
 
-template <class V>
-__device__ __forceinline__ void gatherBounded(const V* __restrict__ f, const Corners& c, int sx, int sy, V& value, V& lo, V& hi);
+// First-order sample of a packed record and the componentwise min/max of its
+// eight corners (float4 / float2 records, or their half forms).
+__device__ __forceinline__ float4 minv(float4 a, float4 b) { return min4(a, b); }
+__device__ __forceinline__ float4 maxv(float4 a, float4 b) { return max4(a, b); }
+__device__ __forceinline__ float2 minv(float2 a, float2 b) { return min2(a, b); }
+__device__ __forceinline__ float2 maxv(float2 a, float2 b) { return max2(a, b); }
 
-template <>
-__device__ __forceinline__ void gatherBounded<float4>(const float4* __restrict__ f, const Corners& c, int sx, int sy, float4& value,
-                                                      float4& lo, float4& hi) {
-    const float4 c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
-    const float4 c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
-    const float4 c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
-    const float4 c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
-    const float4 c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
-    const float4 c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
-    const float4 c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
-    const float4 c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
-    value = lerp4(lerp4(lerp4(c000, c100, c.tx), lerp4(c010, c110, c.tx), c.ty),
-                  lerp4(lerp4(c001, c101, c.tx), lerp4(c011, c111, c.tx), c.ty), c.tz);
-    lo = min4(min4(min4(c000, c100), min4(c010, c110)), min4(min4(c001, c101), min4(c011, c111)));
-    hi = max4(max4(max4(c000, c100), max4(c010, c110)), max4(max4(c001, c101), max4(c011, c111)));
-}
-
-template <>
-__device__ __forceinline__ void gatherBounded<float2>(const float2* __restrict__ f, const Corners& c, int sx, int sy, float2& value,
-                                                      float2& lo, float2& hi) {
-    const float2 c000 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x0);
-    const float2 c100 = __ldg(f + (c.z0 * sy + c.y0) * sx + c.x1);
-    const float2 c010 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x0);
-    const float2 c110 = __ldg(f + (c.z0 * sy + c.y1) * sx + c.x1);
-    const float2 c001 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x0);
-    const float2 c101 = __ldg(f + (c.z1 * sy + c.y0) * sx + c.x1);
-    const float2 c011 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x0);
-    const float2 c111 = __ldg(f + (c.z1 * sy + c.y1) * sx + c.x1);
-    value = lerp2v(lerp2v(lerp2v(c000, c100, c.tx), lerp2v(c010, c110, c.tx), c.ty),
-                   lerp2v(lerp2v(c001, c101, c.tx), lerp2v(c011, c111, c.tx), c.ty), c.tz);
-    lo = min2(min2(min2(c000, c100), min2(c010, c110)), min2(min2(c001, c101), min2(c011, c111)));
-    hi = max2(max2(max2(c000, c100), max2(c010, c110)), max2(max2(c001, c101), max2(c011, c111)));
+template <class P, class V>
+__device__ __forceinline__ void gatherBounded(const P* __restrict__ f, const Corners& c, int sx, int sy, V& value, V& lo, V& hi) {
+    const V c000 = ldv(f + (c.z0 * sy + c.y0) * sx + c.x0);
+    const V c100 = ldv(f + (c.z0 * sy + c.y0) * sx + c.x1);
+    const V c010 = ldv(f + (c.z0 * sy + c.y1) * sx + c.x0);
+    const V c110 = ldv(f + (c.z0 * sy + c.y1) * sx + c.x1);
+    const V c001 = ldv(f + (c.z1 * sy + c.y0) * sx + c.x0);
+    const V c101 = ldv(f + (c.z1 * sy + c.y0) * sx + c.x1);
+    const V c011 = ldv(f + (c.z1 * sy + c.y1) * sx + c.x0);
+    const V c111 = ldv(f + (c.z1 * sy + c.y1) * sx + c.x1);
+    value = lerpv(lerpv(lerpv(c000, c100, c.tx), lerpv(c010, c110, c.tx), c.ty),
+                  lerpv(lerpv(c001, c101, c.tx), lerpv(c011, c111, c.tx), c.ty), c.tz);
+    lo = minv(minv(minv(c000, c100), minv(c010, c110)), minv(minv(c001, c101), minv(c011, c111)));
+    hi = maxv(maxv(maxv(c000, c100), maxv(c010, c110)), maxv(maxv(c001, c101), maxv(c011, c111)));
 }
 
 __device__ __forceinline__ float macCormack(float firstOrder, float lo, float hi, float current, float roundTrip, float blend) {
@@ -228,9 +214,9 @@ __global__ void __launch_bounds__(128, 6) advectReact(ScalarFields out, ScalarFi
     if (v > 0.18f && currentActivity < 0.00035f && cur.charMass < 0.00010f && cur.ash < 0.00010f && outsideInteractiveSource &&
         p.rightDown == 0) {
         // Cold-air early out (src/fire_cuda.cu:984-1001).
-        out.a[idx] = make_float4(0.0f, 0.0f, fminf(1.0f, cur.oxygen + (1.0f - cur.oxygen) * p.dt * 0.08f), 0.0f);
-        out.b[idx] = make_float4(cur.charMass, cur.ash, 0.0f, 0.0f);
-        out.c[idx] = make_float2(cur.turbulenceEnergy * fmaxf(0.0f, 1.0f - p.dt * 0.54f), 0.0f);
+        stv(out.a + idx, make_float4(0.0f, 0.0f, fminf(1.0f, cur.oxygen + (1.0f - cur.oxygen) * p.dt * 0.08f), 0.0f));
+        stv(out.b + idx, make_float4(cur.charMass, cur.ash, 0.0f, 0.0f));
+        stv(out.c + idx, make_float2(cur.turbulenceEnergy * fmaxf(0.0f, 1.0f - p.dt * 0.54f), 0.0f));
         return;
     }
     const float3 velHere = sampleVelocity(vel, g, u, v, w);
@@ -364,12 +350,12 @@ __global__ void __launch_bounds__(128, 6) advectReact(ScalarFields out, ScalarFi
     soot *= expf(-p.dt * (0.060f + v * 0.092f + oxygen * 0.028f + saturate(boundaryAir) * 0.96f + upperEntrainment * 0.22f));
     pyrolysisRate *= expf(-p.dt * (1.55f + v * 0.58f + saturate(boundaryAir) * 0.18f));
 
-    const float uL = __ldg(vel.u + uAt(g, x, y, z));
-    const float uR = __ldg(vel.u + uAt(g, x + 1, y, z));
-    const float vD = __ldg(vel.v + vAt(g, x, y, z));
-    const float vU = __ldg(vel.v + vAt(g, x, y + 1, z));
-    const float wB = __ldg(vel.w + wAt(g, x, y, z));
-    const float wF = __ldg(vel.w + wAt(g, x, y, z + 1));
+    const float uL = ldv(vel.u + uAt(g, x, y, z));
+    const float uR = ldv(vel.u + uAt(g, x + 1, y, z));
+    const float vD = ldv(vel.v + vAt(g, x, y, z));
+    const float vU = ldv(vel.v + vAt(g, x, y + 1, z));
+    const float wB = ldv(vel.w + wAt(g, x, y, z));
+    const float wF = ldv(vel.w + wAt(g, x, y, z + 1));
     const float shear = fabsf(uR - uL) + fabsf(vU - vD) + fabsf(wF - wB);
     const float flameActivity = saturate(progress * 0.64f + burnMass * 5.2f + heat * 0.065f);
     turbulenceEnergy += p.dt * (shear * (0.72f + progress * 0.06f) + flameActivity * p.turbulence * 0.62f + frontProduction * 0.085f + soot * 0.018f);
@@ -379,11 +365,11 @@ __global__ void __launch_bounds__(128, 6) advectReact(ScalarFields out, ScalarFi
     sootOptics = soot * (1.04f + 0.28f * sqrtf(fmaxf(0.0f, heat)) + 0.24f * ash + 0.46f * particleGrowth);
     sootOptics = lerpf(sootOptics, sootOptics * 0.48f, saturate(sootOxidation * 0.92f));
 
-    out.a[idx] = make_float4(fminf(8.8f, fmaxf(0.0f, heat)), fminf(5.5f, fmaxf(0.0f, fuel)), fminf(1.0f, fmaxf(0.0f, oxygen)),
-                             fminf(7.4f, fmaxf(0.0f, soot)));
-    out.b[idx] = make_float4(fminf(2.8f, fmaxf(0.0f, charMass)), fminf(1.9f, fmaxf(0.0f, ash)), fminf(3.6f, fmaxf(0.0f, pyrolysisRate)),
-                             fminf(3.4f, fmaxf(0.0f, progress)));
-    out.c[idx] = make_float2(fminf(4.2f, fmaxf(0.0f, turbulenceEnergy)), fminf(10.0f, fmaxf(0.0f, sootOptics)));
+    stv(out.a + idx, make_float4(fminf(8.8f, fmaxf(0.0f, heat)), fminf(5.5f, fmaxf(0.0f, fuel)), fminf(1.0f, fmaxf(0.0f, oxygen)),
+                             fminf(7.4f, fmaxf(0.0f, soot))));
+    stv(out.b + idx, make_float4(fminf(2.8f, fmaxf(0.0f, charMass)), fminf(1.9f, fmaxf(0.0f, ash)), fminf(3.6f, fmaxf(0.0f, pyrolysisRate)),
+                             fminf(3.4f, fmaxf(0.0f, progress))));
+    stv(out.c + idx, make_float2(fminf(4.2f, fmaxf(0.0f, turbulenceEnergy)), fminf(10.0f, fmaxf(0.0f, sootOptics))));
 }
 
 // ---------------------------------------------------------------------------
@@ -418,24 +404,24 @@ __global__ void __launch_bounds__(128) forceContributions(float4* __restrict__ c
     }
     const Grid g{p.nx, p.ny, p.nz};
     const int idx = sAt(g, x, y, z);
-    const float4 here = __ldg(s.a + idx);
+    const float4 here = ldv(s.a + idx);
     const float h = here.x;
     const float sv = here.w;
-    const float k = __ldg(&s.c[idx].x);
-    const float c = __ldg(&s.b[idx].w);
+    const float k = ldX(s.c + idx);
+    const float c = ldW(s.b + idx);
     const float u = cellCoord(x, p.nx);
     const float v = cellCoord(y, p.ny);
     const float w = cellCoord(z, p.nz);
-    auto heatAt = [&](int xx, int yy, int zz) { return __ldg(&s.a[sClamped(g, xx, yy, zz)].x); };
+    auto heatAt = [&](int xx, int yy, int zz) { return ldX(s.a + sClamped(g, xx, yy, zz)); };
     const float gradX = heatAt(x + 1, y, z) - heatAt(x - 1, y, z);
     const float gradY = heatAt(x, y + 1, z) - heatAt(x, y - 1, z);
     const float gradZ = heatAt(x, y, z + 1) - heatAt(x, y, z - 1);
-    const float uL = __ldg(vel.u + uAt(g, x, y, z));
-    const float uR = __ldg(vel.u + uAt(g, x + 1, y, z));
-    const float vD = __ldg(vel.v + vAt(g, x, y, z));
-    const float vU = __ldg(vel.v + vAt(g, x, y + 1, z));
-    const float wB = __ldg(vel.w + wAt(g, x, y, z));
-    const float wF = __ldg(vel.w + wAt(g, x, y, z + 1));
+    const float uL = ldv(vel.u + uAt(g, x, y, z));
+    const float uR = ldv(vel.u + uAt(g, x + 1, y, z));
+    const float vD = ldv(vel.v + vAt(g, x, y, z));
+    const float vU = ldv(vel.v + vAt(g, x, y + 1, z));
+    const float wB = ldv(vel.w + wAt(g, x, y, z));
+    const float wF = ldv(vel.w + wAt(g, x, y, z + 1));
     const float curlX = (wF - wB) - (vU - vD);
     const float curlY = (uR - uL) - (wF - wB);
     const float curlZ = (vU - vD) - (uR - uL);
@@ -465,24 +451,24 @@ namespace {
 
 // Velocity of one face after the force gather and, optionally, the boundary
 // clamp of src/fire_cuda.cu:1261-1291.
-__device__ __forceinline__ float forcedU(const float* __restrict__ u, const float4* __restrict__ contrib, const Grid& g, int x, int y,
+__device__ __forceinline__ float forcedU(const FaceT* __restrict__ u, const float4* __restrict__ contrib, const Grid& g, int x, int y,
                                          int z, bool clampWalls) {
-    float val = __ldg(u + uAt(g, x, y, z));
+    float val = ldv(u + uAt(g, x, y, z));
     if (x > 0) val += __ldg(&contrib[sAt(g, x - 1, y, z)].x);
     if (x < g.nx) val += __ldg(&contrib[sAt(g, x, y, z)].x);
     if (clampWalls) val = (x == 0 || x == g.nx) ? 0.0f : fminf(4.0f, fmaxf(-4.0f, val));
     return val;
 }
-__device__ __forceinline__ float forcedV(const float* __restrict__ v, const float4* __restrict__ contrib, const Grid& g, int x, int y,
+__device__ __forceinline__ float forcedV(const FaceT* __restrict__ v, const float4* __restrict__ contrib, const Grid& g, int x, int y,
                                          int z, bool clampWalls) {
-    float val = __ldg(v + vAt(g, x, y, z));
+    float val = ldv(v + vAt(g, x, y, z));
     if (y > 0) val += __ldg(&contrib[sAt(g, x, y - 1, z)].y);
     if (clampWalls) val = y == 0 ? 0.0f : fminf(6.4f, fmaxf(-0.9f, val));
     return val;
 }
-__device__ __forceinline__ float forcedW(const float* __restrict__ w, const float4* __restrict__ contrib, const Grid& g, int x, int y,
+__device__ __forceinline__ float forcedW(const FaceT* __restrict__ w, const float4* __restrict__ contrib, const Grid& g, int x, int y,
                                          int z, bool clampWalls) {
-    float val = __ldg(w + wAt(g, x, y, z));
+    float val = ldv(w + wAt(g, x, y, z));
     if (z > 0) val += __ldg(&contrib[sAt(g, x, y, z - 1)].z);
     if (z < g.nz) val += __ldg(&contrib[sAt(g, x, y, z)].z);
     if (clampWalls) val = (z == 0 || z == g.nz) ? 0.0f : fminf(4.0f, fmaxf(-4.0f, val));
@@ -492,21 +478,21 @@ __device__ __forceinline__ float forcedW(const float* __restrict__ w, const floa
 }  // namespace
 
 // The force gather alone (stage "force"): every face adds its cells' increments.
-__global__ void __launch_bounds__(256) forceApply(float* __restrict__ uOut, float* __restrict__ vOut, float* __restrict__ wOut,
+__global__ void __launch_bounds__(256) forceApply(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
                                                   const float4* __restrict__ contrib, Velocity vel, FrameParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
     const Grid g{p.nx, p.ny, p.nz};
-    if (x <= p.nx && y < p.ny && z < p.nz) uOut[uAt(g, x, y, z)] = forcedU(vel.u, contrib, g, x, y, z, false);
-    if (x < p.nx && y <= p.ny && z < p.nz) vOut[vAt(g, x, y, z)] = forcedV(vel.v, contrib, g, x, y, z, false);
-    if (x < p.nx && y < p.ny && z <= p.nz) wOut[wAt(g, x, y, z)] = forcedW(vel.w, contrib, g, x, y, z, false);
+    if (x <= p.nx && y < p.ny && z < p.nz) stv(uOut + uAt(g, x, y, z), forcedU(vel.u, contrib, g, x, y, z, false));
+    if (x < p.nx && y <= p.ny && z < p.nz) stv(vOut + vAt(g, x, y, z), forcedV(vel.v, contrib, g, x, y, z, false));
+    if (x < p.nx && y < p.ny && z <= p.nz) stv(wOut + wAt(g, x, y, z), forcedW(vel.w, contrib, g, x, y, z, false));
 }
 
 // Fused force gather + boundary clamp + divergence (+ pressure reset): one cell
 // per thread computes its six faces, writes the faces it owns (lower faces, and
 // the upper ones on the last layer) and div = -(sum of differences).
-__global__ void __launch_bounds__(256) forceProjectSetup(float* __restrict__ uOut, float* __restrict__ vOut, float* __restrict__ wOut,
+__global__ void __launch_bounds__(256) forceProjectSetup(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
                                                          float* __restrict__ divergence, float* __restrict__ pressure,
                                                          const float4* __restrict__ contrib, Velocity vel, FrameParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -522,12 +508,12 @@ __global__ void __launch_bounds__(256) forceProjectSetup(float* __restrict__ uOu
     const float vU = forcedV(vel.v, contrib, g, x, y + 1, z, true);
     const float wB = forcedW(vel.w, contrib, g, x, y, z, true);
     const float wF = forcedW(vel.w, contrib, g, x, y, z + 1, true);
-    uOut[uAt(g, x, y, z)] = uL;
-    vOut[vAt(g, x, y, z)] = vD;
-    wOut[wAt(g, x, y, z)] = wB;
-    if (x == p.nx - 1) uOut[uAt(g, x + 1, y, z)] = uR;
-    if (y == p.ny - 1) vOut[vAt(g, x, y + 1, z)] = vU;
-    if (z == p.nz - 1) wOut[wAt(g, x, y, z + 1)] = wF;
+    stv(uOut + uAt(g, x, y, z), uL);
+    stv(vOut + vAt(g, x, y, z), vD);
+    stv(wOut + wAt(g, x, y, z), wB);
+    if (x == p.nx - 1) stv(uOut + uAt(g, x + 1, y, z), uR);
+    if (y == p.ny - 1) stv(vOut + vAt(g, x, y + 1, z), vU);
+    if (z == p.nz - 1) stv(wOut + wAt(g, x, y, z + 1), wF);
     const float div = uR - uL + vU - vD + wF - wB;
     const int idx = sAt(g, x, y, z);
     divergence[idx] = -div;
@@ -535,26 +521,26 @@ __global__ void __launch_bounds__(256) forceProjectSetup(float* __restrict__ uOu
 }
 
 // src/fire_cuda.cu:1261-1317 -- wall zeroing, with (clampValues) or without the value clamps.
-__global__ void __launch_bounds__(256) velocityBoundary(float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+__global__ void __launch_bounds__(256) velocityBoundary(FaceT* __restrict__ u, FaceT* __restrict__ v, FaceT* __restrict__ w,
                                                         FrameParams p, int clampValues) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
     const Grid g{p.nx, p.ny, p.nz};
     if (x <= p.nx && y < p.ny && z < p.nz) {
-        float& f = u[uAt(g, x, y, z)];
-        if (x == 0 || x == p.nx) f = 0.0f;
-        else if (clampValues) f = fminf(4.0f, fmaxf(-4.0f, f));
+        FaceT* f = u + uAt(g, x, y, z);
+        if (x == 0 || x == p.nx) stv(f, 0.0f);
+        else if (clampValues) stv(f, fminf(4.0f, fmaxf(-4.0f, ldv(f))));
     }
     if (x < p.nx && y <= p.ny && z < p.nz) {
-        float& f = v[vAt(g, x, y, z)];
-        if (y == 0) f = 0.0f;
-        else if (clampValues) f = fminf(6.4f, fmaxf(-0.9f, f));
+        FaceT* f = v + vAt(g, x, y, z);
+        if (y == 0) stv(f, 0.0f);
+        else if (clampValues) stv(f, fminf(6.4f, fmaxf(-0.9f, ldv(f))));
     }
     if (x < p.nx && y < p.ny && z <= p.nz) {
-        float& f = w[wAt(g, x, y, z)];
-        if (z == 0 || z == p.nz) f = 0.0f;
-        else if (clampValues) f = fminf(4.0f, fmaxf(-4.0f, f));
+        FaceT* f = w + wAt(g, x, y, z);
+        if (z == 0 || z == p.nz) stv(f, 0.0f);
+        else if (clampValues) stv(f, fminf(4.0f, fmaxf(-4.0f, ldv(f))));
     }
 }
 
@@ -568,8 +554,8 @@ __global__ void __launch_bounds__(256) divergenceOf(float* __restrict__ divergen
         return;
     }
     const Grid g{p.nx, p.ny, p.nz};
-    const float div = __ldg(vel.u + uAt(g, x + 1, y, z)) - __ldg(vel.u + uAt(g, x, y, z)) + __ldg(vel.v + vAt(g, x, y + 1, z)) -
-                      __ldg(vel.v + vAt(g, x, y, z)) + __ldg(vel.w + wAt(g, x, y, z + 1)) - __ldg(vel.w + wAt(g, x, y, z));
+    const float div = ldv(vel.u + uAt(g, x + 1, y, z)) - ldv(vel.u + uAt(g, x, y, z)) + ldv(vel.v + vAt(g, x, y + 1, z)) -
+                      ldv(vel.v + vAt(g, x, y, z)) + ldv(vel.w + wAt(g, x, y, z + 1)) - ldv(vel.w + wAt(g, x, y, z));
     const int idx = sAt(g, x, y, z);
     divergence[idx] = -div;
     if (pressureOrNull != nullptr) pressureOrNull[idx] = 0.0f;
@@ -602,7 +588,7 @@ __global__ void __launch_bounds__(256) sorHalfSweep(float* __restrict__ pressure
 
 // src/fire_cuda.cu:1229-1245 + :1293-1317 -- u -= grad p on interior faces,
 // then the wall faces are zeroed (doSubtract / doWalls select either half).
-__global__ void __launch_bounds__(256) subtractWall(float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+__global__ void __launch_bounds__(256) subtractWall(FaceT* __restrict__ u, FaceT* __restrict__ v, FaceT* __restrict__ w,
                                                     const float* __restrict__ pressure, FrameParams p, int doSubtract, int doWalls) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -614,16 +600,16 @@ __global__ void __launch_bounds__(256) subtractWall(float* __restrict__ u, float
     const int idx = sAt(g, x, y, z);
     if (doSubtract) {
         const float pc = __ldg(pressure + idx);
-        if (x > 0) u[uAt(g, x, y, z)] -= pc - __ldg(pressure + idx - 1);
-        if (y > 0) v[vAt(g, x, y, z)] -= pc - __ldg(pressure + idx - g.nx);
-        if (z > 0) w[wAt(g, x, y, z)] -= pc - __ldg(pressure + idx - g.nx * g.ny);
+        if (x > 0) stv(u + uAt(g, x, y, z), ldv(u + uAt(g, x, y, z)) - (pc - __ldg(pressure + idx - 1)));
+        if (y > 0) stv(v + vAt(g, x, y, z), ldv(v + vAt(g, x, y, z)) - (pc - __ldg(pressure + idx - g.nx)));
+        if (z > 0) stv(w + wAt(g, x, y, z), ldv(w + wAt(g, x, y, z)) - (pc - __ldg(pressure + idx - g.nx * g.ny)));
     }
     if (doWalls) {
-        if (x == 0) u[uAt(g, 0, y, z)] = 0.0f;
-        if (x == p.nx - 1) u[uAt(g, p.nx, y, z)] = 0.0f;
-        if (y == 0) v[vAt(g, x, 0, z)] = 0.0f;
-        if (z == 0) w[wAt(g, x, y, 0)] = 0.0f;
-        if (z == p.nz - 1) w[wAt(g, x, y, p.nz)] = 0.0f;
+        if (x == 0) stv(u + uAt(g, 0, y, z), 0.0f);
+        if (x == p.nx - 1) stv(u + uAt(g, p.nx, y, z), 0.0f);
+        if (y == 0) stv(v + vAt(g, x, 0, z), 0.0f);
+        if (z == 0) stv(w + wAt(g, x, y, 0), 0.0f);
+        if (z == p.nz - 1) stv(w + wAt(g, x, y, p.nz), 0.0f);
     }
 }
 

@@ -19,23 +19,28 @@ from . import abi
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libfiresim_b200.so"
+# The same library built with FP16 storage of the transported fields (FP32 arithmetic).
+LIB_PATH_F16 = HERE / "libfiresim_b200_f16.so"
 
 
 class FireSimError(RuntimeError):
     pass
 
 
-_LIB = None
+_LIBS: dict = {}
 
 
-def load_library() -> ctypes.CDLL:
-    """Loads the in-tree library (build it with native-firesim_b200/build.py)."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
-    if not LIB_PATH.exists():
-        raise FireSimError(f"{LIB_PATH} is missing: run `python native-firesim_b200/build.py` first")
-    L = ctypes.CDLL(str(LIB_PATH))
+def load_library(precision: str = "f32") -> ctypes.CDLL:
+    """Loads the in-tree library (build it with native-firesim_b200/build.py):
+    precision "f32" (the reference's storage) or "f16" (FP16 storage)."""
+    if precision in _LIBS:
+        return _LIBS[precision]
+    if precision not in ("f32", "f16"):
+        raise FireSimError(f"unknown precision {precision!r}: 'f32' or 'f16'")
+    path = LIB_PATH if precision == "f32" else LIB_PATH_F16
+    if not path.exists():
+        raise FireSimError(f"{path} is missing: run `python native-firesim_b200/build.py` first")
+    L = ctypes.CDLL(str(path))
     S = ctypes.POINTER(abi.FireSettings)
     M = ctypes.POINTER(abi.FireCudaFrameMetrics)
     b = ctypes.c_bool
@@ -98,20 +103,21 @@ def load_library() -> ctypes.CDLL:
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    _LIB = L
+    _LIBS[precision] = L
     return L
 
 
-def last_error() -> str:
-    return load_library().fireCudaLastError().decode()
+def last_error(lib=None) -> str:
+    return (lib or load_library()).fireCudaLastError().decode()
 
 
 class FireSim:
     """The library's singleton scene on one GPU."""
 
     def __init__(self, frame_w: int, frame_h: int, nx: int | None = None, ny: int | None = None,
-                 nz: int | None = None, grid_request: tuple[int, int] | None = None):
-        self.lib = load_library()
+                 nz: int | None = None, grid_request: tuple[int, int] | None = None, precision: str = "f32"):
+        self.lib = load_library(precision)
+        self.precision = precision
         if grid_request is not None:
             ok = self.lib.fireCudaInitialize(frame_w, frame_h, grid_request[0], grid_request[1])
         else:
@@ -124,7 +130,7 @@ class FireSim:
 
     def _check(self, ok, what):
         if not ok:
-            raise FireSimError(f"{what}: {last_error()}")
+            raise FireSimError(f"{what}: {last_error(self.lib)}")
 
     def close(self):
         self.lib.fireCudaShutdown()
@@ -263,16 +269,16 @@ class Scene:
     """A FireScene handle (fireSceneCreate ...): an independent scene with its
     own fields and stream; many of them run side by side on one GPU."""
 
-    def __init__(self, frame_w: int, frame_h: int, nx: int, ny: int, nz: int, device: int = 0):
-        self.lib = load_library()
+    def __init__(self, frame_w: int, frame_h: int, nx: int, ny: int, nz: int, device: int = 0, precision: str = "f32"):
+        self.lib = load_library(precision)
         self.h = self.lib.fireSceneCreate(device, frame_w, frame_h, nx, ny, nz)
         if not self.h:
-            raise FireSimError(f"fireSceneCreate: {last_error()}")
+            raise FireSimError(f"fireSceneCreate: {last_error(self.lib)}")
         self.nx, self.ny, self.nz, self.frame_w, self.frame_h = nx, ny, nz, frame_w, frame_h
 
     def _check(self, ok, what):
         if not ok:
-            raise FireSimError(f"{what}: {last_error()}")
+            raise FireSimError(f"{what}: {last_error(self.lib)}")
 
     def close(self):
         if self.h:
@@ -315,38 +321,38 @@ class Scene:
 
 def batch_step(scenes, settings, render=None) -> None:
     """fireBatchStep: one queued step of every scene (settings[i] for scenes[i])."""
-    lib = load_library()
+    lib = scenes[0].lib if scenes else load_library()
     n = len(scenes)
     handles = (ctypes.c_void_p * n)(*[s.h for s in scenes])
     arr = (abi.FireSettings * n)(*settings)
     flags = None if render is None else (ctypes.c_int * n)(*[1 if r else 0 for r in render])
     if not lib.fireBatchStep(handles, arr, flags, n):
-        raise FireSimError(f"fireBatchStep: {last_error()}")
+        raise FireSimError(f"fireBatchStep: {last_error(lib)}")
 
 
 class Server:
     """fireServer*: requests arrive over time, are admitted within a device-memory
     budget and all admitted scenes advance one step per round."""
 
-    def __init__(self, budget_bytes: int, device: int = 0):
-        self.lib = load_library()
+    def __init__(self, budget_bytes: int, device: int = 0, precision: str = "f32"):
+        self.lib = load_library(precision)
         self.h = self.lib.fireServerCreate(device, budget_bytes)
         if not self.h:
-            raise FireSimError(f"fireServerCreate: {last_error()}")
+            raise FireSimError(f"fireServerCreate: {last_error(self.lib)}")
 
     def set_limits(self, max_active_voxels: int) -> None:
         """Admit only while the admitted scenes hold at most this many cells (0 = no limit)."""
         if not self.lib.fireServerSetLimits(self.h, max_active_voxels):
-            raise FireSimError(f"fireServerSetLimits: {last_error()}")
+            raise FireSimError(f"fireServerSetLimits: {last_error(self.lib)}")
 
     def submit(self, request) -> None:
         if not self.lib.fireServerSubmit(self.h, ctypes.byref(request)):
-            raise FireSimError(f"fireServerSubmit: {last_error()}")
+            raise FireSimError(f"fireServerSubmit: {last_error(self.lib)}")
 
     def run(self, max_seconds: float) -> dict:
         rep = abi.FireServeReport()
         if not self.lib.fireServerRun(self.h, max_seconds, ctypes.byref(rep)):
-            raise FireSimError(f"fireServerRun: {last_error()}")
+            raise FireSimError(f"fireServerRun: {last_error(self.lib)}")
         return rep.as_dict()
 
     def close(self):
