@@ -697,7 +697,10 @@ struct ResidentShape {
     static constexpr int EY = BY + 2, EZ = BZ + 2;
     static constexpr int PLANE = EZ * EY * EX;
     static constexpr int THREADS = KX * BY;
-    static constexpr size_t SHARED_BYTES = (2ull * PLANE + 2ull * BZ * THREADS) * sizeof(float);
+    // div plane pitch: one z plane apart is 16 banks apart, so a warp that
+    // reads two z rows of face cells (the y faces) does not conflict.
+    static constexpr int DPITCH = THREADS + 16;
+    static constexpr size_t SHARED_BYTES = (2ull * PLANE + 2ull * BZ * DPITCH) * sizeof(float);
     static_assert((2 * EX) % 32 == KX % 32 && EX >= KX + 2, "row pitch");
     static_assert(BY % (2 * RPW) == 0 && THREADS % 32 == 0, "warp-to-row mapping");
     static constexpr int HX = BY * BZ;
@@ -707,7 +710,7 @@ struct ResidentShape {
     static constexpr int PER_THREAD = (HALO + THREADS - 1) / THREADS;
     __device__ static int pidx(int c, int z, int y, int k) { return c * PLANE + ((z + 1) * EY + (y + 1)) * EX + (k + 1); }
     // div of the thread's own cells, laid out by thread: [colour][z][thread].
-    __device__ static int didx(int c, int z, int t) { return (c * BZ + z) * THREADS + t; }
+    __device__ static int didx(int c, int z, int t) { return (c * BZ + z) * DPITCH + t; }
 };
 
 // Global and shared index of halo cell i of colour c, or gi = -1 when the
@@ -746,17 +749,17 @@ __device__ __forceinline__ void residentHaloCell(int i, int c, int ox, int oy, i
 }
 
 // Face cells of one colour in a brick, updated after the halo has arrived:
-// both z faces (all k, y), both y faces (inner z), and in every inner (y, z)
-// row the one x-face cell of that colour (x = 0 when the row's offset is 0,
-// else x = BX - 1).  All other cells of the colour are the brick interior,
-// whose neighbours all lie in the brick.
+// both z faces (all k, y: each thread takes its own column at z = 0 and
+// z = BZ - 1), and from a list shared out over the threads, both y faces
+// (inner z) and in every inner (y, z) row the one x-face cell of that colour
+// (x = 0 when the row's offset is 0, else x = BX - 1).  All other cells of
+// the colour are the brick interior, whose neighbours all lie in the brick.
 template <int BX, int BY, int BZ>
 struct ResidentFaces {
     static constexpr int KX = BX / 2;
-    static constexpr int FZ = 2 * KX * BY;
     static constexpr int FY = 2 * KX * (BZ - 2);
     static constexpr int FX = (BY - 2) * (BZ - 2);
-    static constexpr int COUNT = FZ + FY + FX;
+    static constexpr int COUNT = FY + FX;  // the z faces are each thread's own column (z = 0, BZ - 1)
     static constexpr int PER_THREAD = (COUNT + KX * BY - 1) / (KX * BY);
 };
 
@@ -780,19 +783,15 @@ template <int BX, int BY, int BZ>
 __device__ __forceinline__ int residentFaceCell(int i, int c) {
     using F = ResidentFaces<BX, BY, BZ>;
     int k, y, z;
-    if (i < F::FZ) {
-        const int side = i / (F::KX * BY);
-        residentColumn<BX, BY, BZ>(i % (F::KX * BY), k, y);
-        z = side ? BZ - 1 : 0;
-    } else if (i < F::FZ + F::FY) {
-        const int j = i - F::FZ;
+    if (i < F::FY) {
+        const int j = i;
         const int side = j / (F::KX * (BZ - 2));
         const int r = j % (F::KX * (BZ - 2));
         k = r % F::KX;
         z = 1 + r / F::KX;
         y = side ? BY - 1 : 0;
     } else {
-        const int j = i - F::FZ - F::FY;
+        const int j = i - F::FY;
         y = 1 + j % (BY - 2);
         z = 1 + j / (BY - 2);
         k = ((c + y + z) & 1) ? F::KX - 1 : 0;
@@ -977,15 +976,11 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
             float* __restrict__ mineF = planes + c * S::PLANE;
             const float* __restrict__ otherF = planes + o * S::PLANE;
             const float* __restrict__ divF = divs;
-#pragma unroll
-            for (int j = 0; j < F::PER_THREAD; ++j) {
-                const int cell = face[c][j];
-                if (cell < 0) continue;
-                const int fk = cell & 0xff, fy = (cell >> 8) & 0xff, fz = cell >> 16;
+            auto faceUpdate = [&](int fk, int fy, int fz, int owner) {
                 const int s = (c + fy + fz) & 1;
                 const int fx = 2 * fk + s;
                 const int gx = ox + fx, fgy = oy + fy, gz = oz + fz;
-                if (gx >= g.nx || fgy >= g.ny || gz >= g.nz) continue;
+                if (gx >= g.nx || fgy >= g.ny || gz >= g.nz) return;
                 const float self = mineF[S::pidx(0, fz, fy, fk)];
                 const float pL = gx == 0 ? self : otherF[S::pidx(0, fz, fy, fk + s - 1)];
                 const float pR = gx == g.nx - 1 ? self : otherF[S::pidx(0, fz, fy, fk + s)];
@@ -993,13 +988,22 @@ __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restric
                 const float pU = fgy == g.ny - 1 ? self : otherF[S::pidx(0, fz, fy + 1, fk)];
                 const float pB = gz == 0 ? self : otherF[S::pidx(0, fz - 1, fy, fk)];
                 const float pF = gz == g.nz - 1 ? self : otherF[S::pidx(0, fz + 1, fy, fk)];
-                const float d = divF[S::didx(c, fz, residentOwner<BX, BY, BZ>(fk, fy))];
+                const float d = divF[S::didx(c, fz, owner)];
                 const float projected = (d + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
                 const float next = self + omega * (projected - self);
                 mineF[S::pidx(0, fz, fy, fk)] = next;
                 if (!last && !silent) {
                     storeExchange(sync.exchange + (gz * g.ny + fgy) * g.nx + gx, next, sync.epoch + static_cast<unsigned>(h + 1));
                 }
+            };
+            faceUpdate(k, y, 0, threadIdx.x);
+            faceUpdate(k, y, BZ - 1, threadIdx.x);
+#pragma unroll
+            for (int j = 0; j < F::PER_THREAD; ++j) {
+                const int cell = face[c][j];
+                if (cell < 0) continue;
+                const int fk = cell & 0xff, fy = (cell >> 8) & 0xff;
+                faceUpdate(fk, fy, cell >> 16, residentOwner<BX, BY, BZ>(fk, fy));
             }
             if (last) {
                 break;
