@@ -242,7 +242,7 @@ def run_reference(args, world: int, rank: int) -> None:
 def config_block(args) -> dict:
     return {"workload": f"reference frame pipeline (native-firesim physics, 10 scalars, MAC velocity), FP32, "
                         f"{args.grid}^3 grid, SOR {args.sor_iters} iterations omega {args.omega}, "
-                        f"{'FP16 storage, ' if args.precision == 'f16' else ''}"
+                        f"{args.precision.upper() + ' storage, ' if args.precision != 'f32' else ''}"
                         f"{args.frame}x{args.frame} HDR raymarch every {args.render_every} steps "
                         f"({args.samples} samples requested, clamped to 120)",
             "grid": [args.grid] * 3, "frame": [args.frame, args.frame], "sor_iterations": args.sor_iters,
@@ -394,8 +394,8 @@ def main() -> int:
     ap.add_argument("--reference-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="f32", choices=["f32", "f16"],
-                    help="storage of the transported fields: f32 (the reference's) or f16 (FP32 arithmetic)")
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
+                    help="storage of the transported fields: f32 (the reference's), f16 or bf16 (FP32 arithmetic)")
     ap.add_argument("--mode", default="single", choices=["single", "batched", "serve"],
                     help="single: the 128^3 scene (the headline line); batched: --scenes scenes per fireBatchStep; "
                          "serve: Poisson requests into the FireServer loop")
@@ -539,7 +539,7 @@ def main() -> int:
             "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": device_s * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if args.precision == "f32" else "f16-storage/f32-arithmetic",
+            "dtype": "f32" if args.precision == "f32" else f"{args.precision}-storage/f32-arithmetic",
             "data": "synthetic (seeded procedural fuel bed + validation-harness settings)",
             "config": config_block(args), "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "roofline": roofline, "stage_ms": per_step_ms, "step_latency": latency, "cpu_baseline": cpu,

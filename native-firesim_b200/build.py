@@ -20,9 +20,12 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OBJ = HERE / "_build"
 LIB = HERE / "libfiresim_b200.so"
-# The FP16-storage variant: the same sources with -DFIRE_STORAGE_F16.
-OBJ_F16 = HERE / "_build_f16"
-LIB_F16 = HERE / "libfiresim_b200_f16.so"
+# The reduced-storage variants: the same sources with -DFIRE_STORAGE_F16 / -DFIRE_STORAGE_BF16.
+VARIANTS = {
+    "f32": (HERE / "_build", HERE / "libfiresim_b200.so", []),
+    "f16": (HERE / "_build_f16", HERE / "libfiresim_b200_f16.so", ["-DFIRE_STORAGE_F16"]),
+    "bf16": (HERE / "_build_bf16", HERE / "libfiresim_b200_bf16.so", ["-DFIRE_STORAGE_BF16"]),
+}
 INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr"]
@@ -40,12 +43,12 @@ def headers() -> list[Path]:
     return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
 
 
-def _compile(src: Path, force: bool, verbose_ptxas: bool, f16: bool = False) -> tuple[Path, str]:
-    obj = (OBJ_F16 if f16 else OBJ) / (src.stem + ".o")
+def _compile(src: Path, force: bool, verbose_ptxas: bool, variant: str = "f32") -> tuple[Path, str]:
+    obj = VARIANTS[variant][0] / (src.stem + ".o")
     newest_dep = max([src.stat().st_mtime] + [h.stat().st_mtime for h in headers()])
     if not force and obj.exists() and obj.stat().st_mtime >= newest_dep and not verbose_ptxas:
         return obj, ""
-    cmd = [_nvcc(), *ARCH, *CUFLAGS, *(["-DFIRE_STORAGE_F16"] if f16 else []), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+    cmd = [_nvcc(), *ARCH, *CUFLAGS, *VARIANTS[variant][2], "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
     if verbose_ptxas:
         cmd[1:1] = ["-Xptxas", "-v"]
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -54,12 +57,12 @@ def _compile(src: Path, force: bool, verbose_ptxas: bool, f16: bool = False) -> 
     return obj, res.stderr
 
 
-def _build_variant(f16: bool, force: bool, verbose_ptxas: bool, quiet: bool) -> Path:
-    objdir, lib = (OBJ_F16, LIB_F16) if f16 else (OBJ, LIB)
+def _build_variant(variant: str, force: bool, verbose_ptxas: bool, quiet: bool) -> Path:
+    objdir, lib, _ = VARIANTS[variant]
     objdir.mkdir(parents=True, exist_ok=True)
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        results = list(ex.map(lambda s: _compile(s, force, verbose_ptxas, f16), srcs))
+        results = list(ex.map(lambda s: _compile(s, force, verbose_ptxas, variant), srcs))
     if verbose_ptxas:
         for _, log in results:
             print(log)
@@ -77,10 +80,11 @@ def _build_variant(f16: bool, force: bool, verbose_ptxas: bool, quiet: bool) -> 
 
 
 def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True, f16: bool = True) -> Path:
-    """Builds the FP32 library (returned) and, unless f16=False, the FP16-storage variant."""
-    lib = _build_variant(False, force, verbose_ptxas, quiet)
+    """Builds the FP32 library (returned) and, unless f16=False, the FP16- and BF16-storage variants."""
+    lib = _build_variant("f32", force, verbose_ptxas, quiet)
     if f16:
-        _build_variant(True, force, False, quiet)
+        _build_variant("f16", force, False, quiet)
+        _build_variant("bf16", force, False, quiet)
     return lib
 
 

@@ -15,6 +15,8 @@
 #include <stdint.h>
 #if defined(FIRE_STORAGE_F16)
 #include <cuda_fp16.h>
+#elif defined(FIRE_STORAGE_BF16)
+#include <cuda_bf16.h>
 #endif
 
 namespace firesim {
@@ -47,17 +49,34 @@ struct FrameParams {
 
 // Storage of the transported fields.  The default build stores the ten
 // scalars and the three face grids in FP32.  The FIRE_STORAGE_F16 build
-// (libfiresim_b200_f16.so) stores them as IEEE half, converted on every load
-// and rounded to nearest on every store; all arithmetic stays FP32, and
-// pressure, divergence, forcing, light and frames stay FP32.  ldv/stv are the
-// only accessors of these buffers, so in the FP32 build they are the plain
-// loads and stores they replace.
+// (libfiresim_b200_f16.so) stores them as IEEE half and the FIRE_STORAGE_BF16
+// build (libfiresim_b200_bf16.so) as bfloat16, converted on every load and
+// rounded to nearest on every store; all arithmetic stays FP32, and pressure,
+// divergence, forcing, light and frames stay FP32.  ldv/stv are the only
+// accessors of these buffers, so in the FP32 build they are the plain loads
+// and stores they replace.
+#if defined(FIRE_STORAGE_F16) || defined(FIRE_STORAGE_BF16)
 #if defined(FIRE_STORAGE_F16)
+using Half1 = __half;
+using Half2 = __half2;
+__device__ __forceinline__ float2 halfToFloat2(Half2 v) { return __half22float2(v); }
+__device__ __forceinline__ Half2 float2ToHalf(float a, float b) { return __floats2half2_rn(a, b); }
+__device__ __forceinline__ float halfToFloat(Half1 v) { return __half2float(v); }
+__device__ __forceinline__ Half1 floatToHalf(float v) { return __float2half_rn(v); }
+#else
+using Half1 = __nv_bfloat16;
+using Half2 = __nv_bfloat162;
+__device__ __forceinline__ float2 halfToFloat2(Half2 v) { return __bfloat1622float2(v); }
+__device__ __forceinline__ Half2 float2ToHalf(float a, float b) { return __floats2bfloat162_rn(a, b); }
+__device__ __forceinline__ float halfToFloat(Half1 v) { return __bfloat162float(v); }
+__device__ __forceinline__ Half1 floatToHalf(float v) { return __float2bfloat16_rn(v); }
+#endif
+#define FIRE_HALF_STORAGE 1
 struct __align__(8) Rec4 {
-    __half2 xy, zw;
+    Half2 xy, zw;
 };
-using Rec2 = __half2;
-using FaceT = __half;
+using Rec2 = Half2;
+using FaceT = Half1;
 constexpr bool kHalfStorage = true;
 #else
 using Rec4 = float4;
@@ -68,29 +87,35 @@ constexpr bool kHalfStorage = false;
 
 __device__ __forceinline__ float ldv(const float* p) { return __ldg(p); }
 __device__ __forceinline__ void stv(float* p, float v) { *p = v; }
-#if defined(FIRE_STORAGE_F16)
+#if defined(FIRE_HALF_STORAGE)
 __device__ __forceinline__ float4 ldv(const Rec4* p) {
     const uint2 raw = __ldg(reinterpret_cast<const uint2*>(p));
-    const float2 xy = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
-    const float2 zw = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+    const float2 xy = halfToFloat2(*reinterpret_cast<const Half2*>(&raw.x));
+    const float2 zw = halfToFloat2(*reinterpret_cast<const Half2*>(&raw.y));
     return make_float4(xy.x, xy.y, zw.x, zw.y);
 }
-__device__ __forceinline__ float2 ldv(const Rec2* p) { return __half22float2(__ldg(p)); }
-__device__ __forceinline__ float ldv(const __half* p) { return __half2float(__ldg(p)); }
+__device__ __forceinline__ float2 ldv(const Rec2* p) {
+    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(p));
+    return halfToFloat2(*reinterpret_cast<const Half2*>(&raw));
+}
+__device__ __forceinline__ float ldv(const Half1* p) {
+    const unsigned short raw = __ldg(reinterpret_cast<const unsigned short*>(p));
+    return halfToFloat(*reinterpret_cast<const Half1*>(&raw));
+}
 __device__ __forceinline__ void stv(Rec4* p, float4 v) {
     Rec4 r;
-    r.xy = __floats2half2_rn(v.x, v.y);
-    r.zw = __floats2half2_rn(v.z, v.w);
+    r.xy = float2ToHalf(v.x, v.y);
+    r.zw = float2ToHalf(v.z, v.w);
     *p = r;
 }
-__device__ __forceinline__ void stv(Rec2* p, float2 v) { *p = __floats2half2_rn(v.x, v.y); }
-__device__ __forceinline__ void stv(__half* p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ void stv(Rec2* p, float2 v) { *p = float2ToHalf(v.x, v.y); }
+__device__ __forceinline__ void stv(Half1* p, float v) { *p = floatToHalf(v); }
 __device__ __forceinline__ float4 ldv(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ float2 ldv(const float2* p) { return __ldg(p); }
 // Single components of a packed record.
-__device__ __forceinline__ float ldX(const Rec4* p) { return __half2float(__ldg(reinterpret_cast<const __half*>(p))); }
-__device__ __forceinline__ float ldW(const Rec4* p) { return __half2float(__ldg(reinterpret_cast<const __half*>(p) + 3)); }
-__device__ __forceinline__ float ldX(const Rec2* p) { return __half2float(__ldg(reinterpret_cast<const __half*>(p))); }
+__device__ __forceinline__ float ldX(const Rec4* p) { return ldv(reinterpret_cast<const Half1*>(p)); }
+__device__ __forceinline__ float ldW(const Rec4* p) { return ldv(reinterpret_cast<const Half1*>(p) + 3); }
+__device__ __forceinline__ float ldX(const Rec2* p) { return ldv(reinterpret_cast<const Half1*>(p)); }
 #else
 __device__ __forceinline__ float4 ldv(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ float2 ldv(const float2* p) { return __ldg(p); }

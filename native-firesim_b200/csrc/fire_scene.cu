@@ -956,10 +956,10 @@ float storedToFloat(const unsigned char* p, int bytes) {
         std::memcpy(&f, p, 4);
         return f;
     }
-#if defined(FIRE_STORAGE_F16)
-    __half h;
+#if defined(FIRE_HALF_STORAGE)
+    Half1 h;
     std::memcpy(&h, p, 2);
-    return __half2float(h);
+    return static_cast<float>(h);
 #else
     return 0.0f;
 #endif
@@ -970,8 +970,8 @@ void floatToStored(float f, unsigned char* p, int bytes) {
         std::memcpy(p, &f, 4);
         return;
     }
-#if defined(FIRE_STORAGE_F16)
-    const __half h = __float2half_rn(f);
+#if defined(FIRE_HALF_STORAGE)
+    const Half1 h(f);  // round to nearest
     std::memcpy(p, &h, 2);
 #endif
 }

@@ -19,8 +19,9 @@ from . import abi
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libfiresim_b200.so"
-# The same library built with FP16 storage of the transported fields (FP32 arithmetic).
+# The same library built with FP16 / BF16 storage of the transported fields (FP32 arithmetic).
 LIB_PATH_F16 = HERE / "libfiresim_b200_f16.so"
+LIB_PATH_BF16 = HERE / "libfiresim_b200_bf16.so"
 
 
 class FireSimError(RuntimeError):
@@ -32,12 +33,13 @@ _LIBS: dict = {}
 
 def load_library(precision: str = "f32") -> ctypes.CDLL:
     """Loads the in-tree library (build it with native-firesim_b200/build.py):
-    precision "f32" (the reference's storage) or "f16" (FP16 storage)."""
+    precision "f32" (the reference's storage), "f16" or "bf16" (half storage)."""
     if precision in _LIBS:
         return _LIBS[precision]
-    if precision not in ("f32", "f16"):
-        raise FireSimError(f"unknown precision {precision!r}: 'f32' or 'f16'")
-    path = LIB_PATH if precision == "f32" else LIB_PATH_F16
+    paths = {"f32": LIB_PATH, "f16": LIB_PATH_F16, "bf16": LIB_PATH_BF16}
+    if precision not in paths:
+        raise FireSimError(f"unknown precision {precision!r}: 'f32', 'f16' or 'bf16'")
+    path = paths[precision]
     if not path.exists():
         raise FireSimError(f"{path} is missing: run `python native-firesim_b200/build.py` first")
     L = ctypes.CDLL(str(path))

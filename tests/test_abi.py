@@ -35,7 +35,7 @@ def test_headers_declare_the_reference_abi():
     assert reference <= names, reference - names
 
 
-@pytest.mark.parametrize("precision", ["f32", "f16"])
+@pytest.mark.parametrize("precision", ["f32", "f16", "bf16"])
 def test_library_exports_every_declared_symbol(pkg, precision):
     """Both builds (FP32 and FP16 storage) export the whole declared ABI."""
     lib = pkg.load_library(precision)
@@ -78,7 +78,7 @@ def test_d3d11_entry_points_report_headless(pkg):
 def test_library_has_no_oracle_dependency():
     """The product neither links nor names the oracle."""
     import subprocess
-    for name in ("libfiresim_b200.so", "libfiresim_b200_f16.so"):
+    for name in ("libfiresim_b200.so", "libfiresim_b200_f16.so", "libfiresim_b200_bf16.so"):
         lib = ROOT / "native-firesim_b200" / name
         needed = subprocess.run(["readelf", "-d", str(lib)], capture_output=True, text=True).stdout
         assert "oracle" not in needed and "fire_ref" not in needed
