@@ -79,9 +79,27 @@ __global__ void forceProjectSetup(FaceT* uOut, FaceT* vOut, FaceT* wOut, float* 
                                   Velocity vel, FrameParams p);
 __global__ void velocityBoundary(FaceT* u, FaceT* v, FaceT* w, FrameParams p, int clampValues);
 __global__ void divergenceOf(float* divergence, float* pressureOrNull, Velocity vel, FrameParams p);
-__global__ void sorHalfSweep(float* pressure, const float* divergence, Grid g, int parity, float omega);
+// Colour-split layout of the non-resident solve: colour c, row (y, z), slot k
+// holds the cell x = 2k + ((c + y + z) & 1); H = (nx + 1) / 2 slots per row,
+// rows P = H rounded up to 4 floats apart (so a row starts on 16 bytes and a
+// half sweep moves float4s).  Slots k >= H, and k = H - 1 where its x is nx,
+// hold no cell and are never read.
+struct SplitGrid {
+    int nx, ny, nz, H, P;
+};
+inline SplitGrid splitGridOf(int nx, int ny, int nz) {
+    const int h = (nx + 1) / 2;
+    return SplitGrid{nx, ny, nz, h, (h + 3) & ~3};
+}
+__host__ __device__ inline int splitIdx(const SplitGrid& s, int c, int y, int z, int k) { return ((c * s.nz + z) * s.ny + y) * s.P + k; }
+constexpr int kSplitRows = 4;  // rows (y) per block of the split half sweep; a warp covers 128 slots of one row
+__global__ void sorSplitPack(float* split, float* splitDiv, const float* pressure, const float* divergence, SplitGrid s);
+__global__ void sorSplitUnpack(float* pressure, const float* split, SplitGrid s);
+__global__ void sorSplitHalfSweep(float* own, const float* other, const float* ownDiv, SplitGrid s, int c, float omega, const int* skip);
 __global__ void sorResidualPartials(const float* pressure, const float* divergence, Grid g, const SorGate* gate, double* partialSq,
                                     float* partialMax);
+__global__ void sorSplitResidualPartials(const float* split, const float* splitDiv, SplitGrid s, const SorGate* gate, double* partialSq,
+                                         float* partialMax);
 __global__ void sorResidualFinal(SorGate* gate, const double* partialSq, const float* partialMax, int partials, float tolerance,
                                  int chunkIterations);
 // The sorResident<BX, 16, 16> instantiation for brick width bx (32 or 16),

@@ -67,7 +67,7 @@ void Scene::release() {
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
                     shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_,
-                    rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_};
+                    rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_, split_, splitDiv_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
@@ -81,6 +81,8 @@ void Scene::release() {
     sorGate_ = nullptr;
     residualSq_ = nullptr;
     residualMax_ = nullptr;
+    split_ = nullptr;
+    splitDiv_ = nullptr;
     sorHostStatus_ = nullptr;
     curlLattice_ = nullptr;
     sourceLattice_ = nullptr;
@@ -411,8 +413,8 @@ bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
 
 // src/fire_cuda.cu:3280-3284 -- 2N half sweeps.  When the grid fits, one
 // cooperative launch keeps p and div in shared memory for all of them
-// (sorResident); otherwise the 2N launches are captured once per (N, omega)
-// into a CUDA graph so a step pays one graph launch.
+// (sorResident); otherwise they run on colour-split copies of p and div, as
+// one CUDA graph per solve.
 bool Scene::runSor(const FrameParams& p, std::string& err) {
     (void)p;
     if (pressureIterations == 0) return true;
@@ -456,21 +458,56 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
             return false;
         }
     }
-    if (sorExec_ == nullptr || sorIterations_ != pressureIterations || sorOmega_ != pressureOmega) {
+    // Grids too large for the resident solve: colour-split arrays and 2N
+    // launches (in gated chunks when a tolerance is set), captured once per
+    // (N, omega, tolerance, chunk) into a CUDA graph, so a step pays one launch.
+    const SplitGrid sg = splitGridOf(nx, ny, nz);
+    if (split_ == nullptr) {
+        const size_t slots = 2ull * sg.nz * sg.ny * sg.P;
+        if (!alloc(reinterpret_cast<void**>(&split_), slots * sizeof(float), "cudaMalloc SOR split pressure", err) ||
+            !alloc(reinterpret_cast<void**>(&splitDiv_), slots * sizeof(float), "cudaMalloc SOR split divergence", err) ||
+            !check("clear SOR split pressure", cudaMemsetAsync(split_, 0, slots * sizeof(float), stream), err) ||
+            !check("clear SOR split divergence", cudaMemsetAsync(splitDiv_, 0, slots * sizeof(float), stream), err)) {
+            return false;
+        }
+    }
+    const bool gated = pressureTolerance_ > 0.0;
+    const int chunk = gated ? std::max(1, std::min(pressureCheckEvery_, pressureIterations)) : pressureIterations;
+    const double tolKey = gated ? pressureTolerance_ : 0.0;
+    if (sorExec_ == nullptr || sorIterations_ != pressureIterations || sorOmega_ != pressureOmega || sorTolKey_ != tolKey ||
+        sorChunkKey_ != chunk) {
         if (sorExec_ != nullptr) {
             cudaGraphExecDestroy(sorExec_);
             sorExec_ = nullptr;
         }
-        const Grid g{nx, ny, nz};
-        const int half = (nx + 1) / 2;
-        const int bx = rowThreads(half);
-        const dim3 grid = cellGrid(bx, half, ny, nz);
+        const int bx = rowThreads(sg.H);
+        const dim3 both((sg.H + bx - 1) / bx, ny, 2 * nz);
+        const dim3 sweepBlock(32, kSplitRows);
+        const dim3 sweep((sg.H + 127) / 128, (ny + kSplitRows - 1) / kSplitRows, nz);
+        const int* skip = gated ? &sorGate_->converged : nullptr;
+        const size_t colour = static_cast<size_t>(sg.nz) * sg.ny * sg.P;
         cudaGraph_t graph = nullptr;
+        int count = 2;
         if (!check("SOR capture begin", cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), err)) return false;
-        for (int i = 0; i < pressureIterations; ++i) {
-            sorHalfSweep<<<grid, bx, 0, stream>>>(pressure_, divergence_, g, 0, pressureOmega);
-            sorHalfSweep<<<grid, bx, 0, stream>>>(pressure_, divergence_, g, 1, pressureOmega);
+        if (gated) cudaMemsetAsync(sorGate_, 0, sizeof(SorGate), stream);
+        sorSplitPack<<<both, bx, 0, stream>>>(split_, splitDiv_, pressure_, divergence_, sg);
+        for (int done = 0; done < pressureIterations; done += chunk) {
+            const int iterations = std::min(chunk, pressureIterations - done);
+            for (int i = 0; i < iterations; ++i) {
+                sorSplitHalfSweep<<<sweep, sweepBlock, 0, stream>>>(split_, split_ + colour, splitDiv_, sg, 0, pressureOmega, skip);
+                sorSplitHalfSweep<<<sweep, sweepBlock, 0, stream>>>(split_ + colour, split_, splitDiv_ + colour, sg, 1, pressureOmega,
+                                                                    skip);
+                count += 2;
+            }
+            if (gated) {
+                sorSplitResidualPartials<<<kResidualBlocks, kResidualThreads, 0, stream>>>(split_, splitDiv_, sg, sorGate_, residualSq_,
+                                                                                         residualMax_);
+                sorResidualFinal<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks,
+                                                       static_cast<float>(pressureTolerance_), iterations);
+                count += 2;
+            }
         }
+        sorSplitUnpack<<<both, bx, 0, stream>>>(pressure_, split_, sg);
         const cudaError_t launchErr = cudaGetLastError();
         const cudaError_t endErr = cudaStreamEndCapture(stream, &graph);
         if (!check("SOR capture launch", launchErr, err) || !check("SOR capture end", endErr, err)) {
@@ -482,9 +519,12 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
         if (!check("SOR graph instantiate", instErr, err)) return false;
         sorIterations_ = pressureIterations;
         sorOmega_ = pressureOmega;
+        sorTolKey_ = tolKey;
+        sorChunkKey_ = chunk;
+        sorGraphLaunches_ = count;
     }
-    launches_ += 2ull * static_cast<unsigned long long>(pressureIterations);
-    lastSolveGated_ = false;
+    launches_ += static_cast<unsigned long long>(sorGraphLaunches_);
+    lastSolveGated_ = gated;
     lastPressurePath_ = 1;
     return check("SOR graph launch", cudaGraphLaunch(sorExec_, stream), err);
 }

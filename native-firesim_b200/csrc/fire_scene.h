@@ -160,6 +160,11 @@ private:
     unsigned sorEpoch_ = 0;
     int sorSilentBrick_ = -1;
     unsigned long long sorWaitNs_ = 1000000000ull;
+    float* split_ = nullptr;      // colour-split p of the non-resident solve (allocated on first use)
+    float* splitDiv_ = nullptr;   // colour-split div
+    double sorTolKey_ = -1.0;
+    int sorChunkKey_ = -1;
+    int sorGraphLaunches_ = 0;
     int sorIterations_ = -1;
     float sorOmega_ = 0.0f;
 };

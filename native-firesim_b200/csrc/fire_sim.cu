@@ -7,7 +7,7 @@
 //   forceVelocityKernel           :1128-1183 -> forceContributions + face gathers (no atomics)
 //   velocityBoundaryKernel        :1261-1291 -> velocityBoundary / fused into forceProject
 //   divergenceKernel              :1185-1199 -> divergence / fused into forceProject
-//   sorPressureParityKernel       :1201-1227 -> sorHalfSweep
+//   sorPressureParityKernel       :1201-1227 -> sorResident / sorSplitHalfSweep
 //   subtractPressureKernel        :1229-1245 -> subtractWall (fused with the wall zeroing)
 //   velocityWallBoundaryKernel    :1293-1317
 #include "fire_kernels.h"
@@ -561,29 +561,141 @@ __global__ void __launch_bounds__(256) divergenceOf(float* __restrict__ divergen
     if (pressureOrNull != nullptr) pressureOrNull[idx] = 0.0f;
 }
 
-// src/fire_cuda.cu:1201-1227 -- one colour of in-place red-black SOR.  Thread
-// (i, y, z) owns cell x = 2i + ((parity ^ y ^ z) & 1); walls are Neumann
-// through the clamped neighbour index.
-__global__ void __launch_bounds__(256) sorHalfSweep(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g, int parity,
-                                                    float omega) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// ---------------------------------------------------------------------------
+// The solve for grids too large to stay in shared memory: p and div are copied
+// once per solve into colour-split arrays (colour c, row (y, z), slot k holds
+// x = 2k + ((c + y + z) & 1)), so every half sweep reads the other colour and
+// reads and writes its own colour in contiguous runs; the natural layout of the
+// reference's kernel reads both colours and writes every other float.  The
+// update is the reference's arithmetic in the reference's order
+// (src/fire_cuda.cu:1201-1227), so the result is the same bits.
+__global__ void __launch_bounds__(256) sorSplitPack(float* __restrict__ split, float* __restrict__ splitDiv, const float* __restrict__ pressure,
+                                                    const float* __restrict__ divergence, SplitGrid s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
+    const int z = blockIdx.z % s.nz;
+    const int c = blockIdx.z / s.nz;
+    const int x = 2 * k + ((c + y + z) & 1);
+    if (k >= s.H || x >= s.nx) return;
+    const int src = (z * s.ny + y) * s.nx + x;
+    split[splitIdx(s, c, y, z, k)] = __ldg(pressure + src);
+    splitDiv[splitIdx(s, c, y, z, k)] = __ldg(divergence + src);
+}
+
+__global__ void __launch_bounds__(256) sorSplitUnpack(float* __restrict__ pressure, const float* __restrict__ split, SplitGrid s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z % s.nz;
+    const int c = blockIdx.z / s.nz;
+    const int x = 2 * k + ((c + y + z) & 1);
+    if (k >= s.H || x >= s.nx) return;
+    pressure[(z * s.ny + y) * s.nx + x] = __ldg(split + splitIdx(s, c, y, z, k));
+}
+
+// One colour of a half sweep on the split arrays.  Thread (t, y, z) owns the
+// four slots 4t..4t+3 of colour c in row (y, z): its own cells, their div and
+// the four other-colour rows above, below, behind and in front are one float4
+// each, and the x-neighbours are the other colour's float4 of the same row
+// shifted by one slot (sx = 0: left = slot k - 1, right = slot k; sx = 1: left
+// = slot k, right = slot k + 1), whose missing end is one scalar.  own and
+// other are the two colour halves of one split array: disjoint, and other is
+// read-only for the whole launch.  Per cell the arithmetic is the reference's
+// in the reference's order (src/fire_cuda.cu:1201-1227).
+__global__ void __launch_bounds__(128) sorSplitHalfSweep(float* __restrict__ own, const float* __restrict__ other,
+                                                         const float* __restrict__ ownDiv, SplitGrid s, int c, float omega,
+                                                         const int* skip) {
+    if (skip != nullptr && *reinterpret_cast<const volatile int*>(skip) != 0) return;
+    const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
-    const int x = 2 * i + ((parity ^ y ^ z) & 1);
-    if (x >= g.nx) {
-        return;
+    if (k0 >= s.H || y >= s.ny) return;
+    const int sx = (c + y + z) & 1;
+    const int x0 = 2 * k0 + sx;
+    const int i = (z * s.ny + y) * s.P + k0;
+    const int plane = s.ny * s.P;
+    const float4 self = *reinterpret_cast<const float4*>(own + i);
+    const float4 mid = __ldg(reinterpret_cast<const float4*>(other + i));
+    const float4 dn = y == 0 ? self : __ldg(reinterpret_cast<const float4*>(other + i - s.P));
+    const float4 up = y == s.ny - 1 ? self : __ldg(reinterpret_cast<const float4*>(other + i + s.P));
+    const float4 bk = z == 0 ? self : __ldg(reinterpret_cast<const float4*>(other + i - plane));
+    const float4 ft = z == s.nz - 1 ? self : __ldg(reinterpret_cast<const float4*>(other + i + plane));
+    const float4 dv = __ldg(reinterpret_cast<const float4*>(ownDiv + i));
+    // The slot just outside the float4 on the side the shift needs, if it holds a cell.
+    float edge = 0.0f;
+    if (sx == 0 && k0 > 0) edge = __ldg(other + i - 1);
+    if (sx == 1 && 2 * (k0 + 4) < s.nx) edge = __ldg(other + i + 4);
+    const float sv[4] = {self.x, self.y, self.z, self.w};
+    const float mv[4] = {mid.x, mid.y, mid.z, mid.w};
+    const float dnv[4] = {dn.x, dn.y, dn.z, dn.w};
+    const float upv[4] = {up.x, up.y, up.z, up.w};
+    const float bkv[4] = {bk.x, bk.y, bk.z, bk.w};
+    const float ftv[4] = {ft.x, ft.y, ft.z, ft.w};
+    const float dvv[4] = {dv.x, dv.y, dv.z, dv.w};
+    float out[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int x = x0 + 2 * j;
+        const float me = sv[j];
+        const float left = sx == 0 ? (j == 0 ? edge : mv[j - 1]) : mv[j];
+        const float right = sx == 0 ? mv[j] : (j == 3 ? edge : mv[j + 1]);
+        const float pL = x == 0 ? me : left;
+        const float pR = x == s.nx - 1 ? me : right;
+        const float pD = y == 0 ? me : dnv[j];
+        const float pU = y == s.ny - 1 ? me : upv[j];
+        const float pB = z == 0 ? me : bkv[j];
+        const float pF = z == s.nz - 1 ? me : ftv[j];
+        const float projected = (dvv[j] + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
+        out[j] = x < s.nx ? me + omega * (projected - me) : me;
     }
-    const int idx = sAt(g, x, y, z);
-    const int row = idx - x;
-    const float pL = pressure[row + max(x - 1, 0)];
-    const float pR = pressure[row + min(x + 1, g.nx - 1)];
-    const float pD = pressure[sAt(g, x, max(y - 1, 0), z)];
-    const float pU = pressure[sAt(g, x, min(y + 1, g.ny - 1), z)];
-    const float pB = pressure[sAt(g, x, y, max(z - 1, 0))];
-    const float pF = pressure[sAt(g, x, y, min(z + 1, g.nz - 1))];
-    const float self = pressure[idx];
-    const float projected = (__ldg(divergence + idx) + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
-    pressure[idx] = self + omega * (projected - self);
+    *reinterpret_cast<float4*>(own + i) = make_float4(out[0], out[1], out[2], out[3]);
+}
+
+// Residual of the split arrays, per block over a fixed set of cells (as sorResidualPartials).
+__global__ void __launch_bounds__(kResidualThreads) sorSplitResidualPartials(const float* __restrict__ split,
+                                                                            const float* __restrict__ splitDiv, SplitGrid s,
+                                                                            const SorGate* gate, double* __restrict__ partialSq,
+                                                                            float* __restrict__ partialMax) {
+    if (gate->converged) return;
+    __shared__ double sq[kResidualThreads];
+    __shared__ float mx[kResidualThreads];
+    const long long slots = 2ll * s.nz * s.ny * s.P;
+    double acc = 0.0;
+    float m = 0.0f;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < slots;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int k = static_cast<int>(i % s.P);
+        const int y = static_cast<int>((i / s.P) % s.ny);
+        const int z = static_cast<int>((i / (static_cast<long long>(s.P) * s.ny)) % s.nz);
+        const int c = static_cast<int>(i / (static_cast<long long>(s.P) * s.ny * s.nz));
+        const int sx = (c + y + z) & 1;
+        const int x = 2 * k + sx;
+        if (x >= s.nx) continue;
+        const int o = 1 - c;
+        const float self = __ldg(split + i);
+        const float pL = x == 0 ? self : __ldg(split + splitIdx(s, o, y, z, k + sx - 1));
+        const float pR = x == s.nx - 1 ? self : __ldg(split + splitIdx(s, o, y, z, k + sx));
+        const float pD = y == 0 ? self : __ldg(split + splitIdx(s, o, y - 1, z, k));
+        const float pU = y == s.ny - 1 ? self : __ldg(split + splitIdx(s, o, y + 1, z, k));
+        const float pB = z == 0 ? self : __ldg(split + splitIdx(s, o, y, z - 1, k));
+        const float pF = z == s.nz - 1 ? self : __ldg(split + splitIdx(s, o, y, z + 1, k));
+        const float r = __fsub_rn(__ldg(splitDiv + i) + pL + pR + pD + pU + pB + pF, __fmul_rn(6.0f, self));
+        m = fmaxf(m, fabsf(r));
+        acc += static_cast<double>(r) * static_cast<double>(r);
+    }
+    sq[threadIdx.x] = acc;
+    mx[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kResidualThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sq[threadIdx.x] += sq[threadIdx.x + w];
+            mx[threadIdx.x] = fmaxf(mx[threadIdx.x], mx[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partialSq[blockIdx.x] = sq[0];
+        partialMax[blockIdx.x] = mx[0];
+    }
 }
 
 // src/fire_cuda.cu:1229-1245 + :1293-1317 -- u -= grad p on interior faces,
@@ -632,7 +744,7 @@ namespace firesim {
 // resident, so every poll is for a running CTA; each poll is still bounded in
 // time.  Walls are Neumann through the clamped neighbour (the cell itself), as
 // in sorPressureParityKernel.  Per-cell arithmetic is identical to
-// sorHalfSweep, so the result is bit-identical to the per-launch path.
+// sorSplitHalfSweep, so the result is bit-identical to the split path.
 namespace {
 
 __device__ __forceinline__ unsigned loadVolatile(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }

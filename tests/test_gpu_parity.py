@@ -214,7 +214,8 @@ def test_deterministic(product, abi):
 
 @pytest.mark.parametrize("dims", [(17, 21, 11), (64, 64, 64), (128, 128, 128), (40, 34, 70)])
 def test_sor_resident_equals_per_launch(dims, product, abi):
-    """The shared-memory-resident SOR (one cooperative launch) equals the per-half-sweep path bit for bit."""
+    """The shared-memory-resident SOR (one cooperative launch) equals the
+    colour-split path (one graph of per-half-sweep launches) bit for bit."""
     nx, ny, nz = dims
     rng = np.random.default_rng(nx * 7 + ny)
     p0 = rng.standard_normal((nz, ny, nx)).astype(np.float32)
@@ -333,10 +334,12 @@ def _residual(p, d):
     return float(np.abs(r).max()), float(np.sqrt(np.sum(r.astype(np.float64) ** 2)))
 
 
-def test_pressure_tolerance_gates_the_solve(product, abi):
+@pytest.mark.parametrize("pressure_path", [1, 2])
+def test_pressure_tolerance_gates_the_solve(pressure_path, product, abi):
     """The residual-gated solve stops at the first check with max |r| <= tolerance,
     and its result equals a fixed solve of the same iteration count; a tolerance
-    never reached runs every iteration and equals the fixed solve."""
+    never reached runs every iteration and equals the fixed solve.  Both solve
+    paths: resident (2) and colour-split (1)."""
     nx, ny, nz = 64, 48, 40
     rng = np.random.default_rng(5)
     p0 = np.zeros((nz, ny, nx), np.float32)
@@ -347,6 +350,7 @@ def test_pressure_tolerance_gates_the_solve(product, abi):
     def solve(iters, tol, every=10):
         sim = product.FireSim(32, 16, nx, ny, nz)
         sim.set_pressure_solver(iters, 1.8)
+        sim.set_pressure_path(pressure_path)
         sim.set_pressure_tolerance(tol, every)
         sim.set("pressure", p0)
         sim.set("divergence", d0)
@@ -356,7 +360,7 @@ def test_pressure_tolerance_gates_the_solve(product, abi):
         return out
 
     fixed, stats, path = solve(120, 0.0)
-    assert path == 2 and stats[0] == 120 and stats[1] == -1.0
+    assert path == pressure_path and stats[0] == 120 and stats[1] == -1.0
     never, stats_never, _ = solve(120, 1e-30)
     assert stats_never[0] == 120
     np.testing.assert_array_equal(never.view(np.uint32), fixed.view(np.uint32))
