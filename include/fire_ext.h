@@ -42,7 +42,10 @@ enum FireFieldId {
     FIRE_FIELD_SCENE_SHADOW = 16,
     FIRE_FIELD_HDR = 17,
     FIRE_FIELD_BGRA = 18,
-    FIRE_FIELD_DIVERGENCE_AFTER = 19
+    FIRE_FIELD_DIVERGENCE_AFTER = 19,
+    /* Config physics: transmittance to the point light, one float per cell of
+     * the half-resolution grid ((nx+1)/2 * (ny+1)/2 * (nz+1)/2). */
+    FIRE_FIELD_CONFIG_TRANSMITTANCE = 20
 };
 
 /* The passes of one frame, in order (the launch sequence of
@@ -93,9 +96,10 @@ FIRE_API bool fireCudaSetPressureSolver(int iterations, float omega);
 
 /* Execution path of the SOR solve (identical results): 0 = automatic (one
  * cooperative launch that keeps p and div in shared memory when every brick of
- * the grid can be co-resident, else one launch per half sweep), 1 = one launch
- * per half sweep, 2 = shared-memory-resident only (fails if the grid does not
- * fit). */
+ * the grid can be co-resident, else the colour-split solve), 1 = colour-split
+ * solve (p and div copied into per-colour arrays, one launch per half sweep,
+ * replayed as one CUDA graph), 2 = shared-memory-resident only (fails if the
+ * grid does not fit). */
 FIRE_API bool fireCudaSetPressurePath(int path);
 
 /* Scene/emitter contract.  Writes the emitter fields of *settings
@@ -119,21 +123,21 @@ FIRE_API bool fireCudaSetHashLattices(int enabled);
 
 /* Residual-gated pressure solve (SOR policy; the reference always runs a
  * fixed count, src/fire_cuda.cu:3280-3284).  With maxResidual > 0 the
- * shared-memory-resident solve runs in chunks of checkEvery iterations; after
+ * solve runs in chunks of checkEvery iterations; after
  * each chunk the residual r = div + (six neighbours, clamped at the walls) - 6p
  * is reduced in a fixed order (max |r| in FP32, L2 in FP64) and once
  * max |r| <= maxResidual the remaining chunks return at once, up to the
  * iteration count of fireCudaSetPressureSolver.  The host does not wait.
  * maxResidual = 0 restores the fixed count.  A gated solve that runs m
- * iterations gives the same bits as a fixed solve of m iterations.  The
- * per-launch path (fireCudaSetPressurePath(1)) ignores the tolerance. */
+ * iterations gives the same bits as a fixed solve of m iterations, on either
+ * path. */
 FIRE_API bool fireCudaSetPressureTolerance(double maxResidual, int checkEvery);
 /* Iterations run, max |r| and L2 residual of the latest gated solve (waits
  * for the scene's stream); after a fixed-count solve: the count and -1. */
 FIRE_API bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Residual);
 
-/* Path the latest SOR solve took: 0 = none yet (or no grid), 1 = one launch
- * per half sweep, 2 = shared-memory-resident. */
+/* Path the latest SOR solve took: 0 = none yet (or no grid), 1 = colour-split,
+ * 2 = shared-memory-resident. */
 FIRE_API int fireCudaGetPressurePathUsed(void);
 
 /* Failure detection of the shared-memory-resident SOR (no counterpart in the
@@ -202,6 +206,77 @@ FIRE_API bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float ti
                                           const float* u, const float* v, const float* w, float* uOut, float* vOut,
                                           float* wOut, float* divergence, float* pressure, void* stream);
 
+/* ---- Config physics ----------------------------------------------------
+ * A second physics of the same scene and kernels' projection, for workloads
+ * written as a plain T/F/S smoke-and-fire model rather than the reference's
+ * ten-scalar, sin-hash, fuel-bed model (which has no seeds, no disk emitters
+ * and no point light).  mode 0 (the default) keeps the reference's physics
+ * bit for bit and ignores every other field.  mode 1 ("config physics"):
+ *   - state: heat T, fuel F, soot S (the other seven scalars stay 0); MAC
+ *     faces in cells per step; cell (i,j,k) has its centre at (i+.5, j+.5, k+.5);
+ *   - advection: semi-Lagrangian, one Euler backtrace of a whole step
+ *     (X - velocity(X)), trilinear with clamped indices, faces and scalars;
+ *   - reaction: where T > ignitionHeat, burn = F * min(1, burnRate * dt):
+ *     F -= burn, T += heatRelease * burn, S += sootYield * burn; then T and S
+ *     decay by min(1, cooling * dt) and min(1, sootDecay * dt);
+ *   - emitters: the cells of row y = (int)centerY with (x - centerX)^2 +
+ *     (z - centerZ)^2 <= radius^2 take F = max(F, fuel * j), T = max(T, heat * j),
+ *     j = 1 - jitterScale * U, U uniform in [0,1) from SplitMix64 of (seed,
+ *     step, cell); their two v faces are set to upVelocity;
+ *   - forces (accelerations, times dt): buoyancy buoyancyHeat * (T -
+ *     ambientHeat) - buoyancySoot * S upward; vorticity confinement
+ *     vorticityEps * (N x omega) (Fedkiw, Stam and Jensen 2001; h = 1, central
+ *     differences with clamped neighbours); noiseAmplitude * curl(psi), psi
+ *     three seeded value-noise fields of period noisePeriod cells (cubic
+ *     Hermite interpolation, analytic gradient); wind (windX, windZ) on u and w;
+ *   - projection: the same divergence, red-black SOR and gradient subtraction
+ *     as mode 0 (walls closed, top open, Neumann pressure);
+ *   - render: transmittance to a point light at half grid resolution
+ *     (lightSamples per ray, clipped to the grid box), then primarySamples per
+ *     pixel from a pinhole camera: extinction * S + fuelExtinction * F absorbs,
+ *     in-scattering albedo * lightIntensity * transmittance, emission
+ *     emission * T with a fixed heat colour; HDR float4 (rgb, 1 - view
+ *     transmittance); the BGRA frame is the camera response of FireSettings.
+ * Times: dt is this struct's; FireSettings.dt still drives the clocks. */
+typedef struct FireEmitterDisk {
+    float centerX, centerY, centerZ; /* cell-index coordinates */
+    float radius;                    /* cells */
+    float fuel, heat;                /* injected amounts before jitter */
+    float upVelocity;                /* cells per step, written to the emitter cells' v faces */
+    float jitterScale;               /* 0..1 */
+    unsigned int seed;
+    unsigned int reserved;
+} FireEmitterDisk;
+
+#define FIRE_MAX_EMITTERS 4
+
+typedef struct FirePhysicsParams {
+    int mode;                        /* 0 reference physics, 1 config physics */
+    float dt;                        /* seconds per step */
+    float buoyancyHeat, buoyancySoot, ambientHeat;
+    float burnRate, ignitionHeat, heatRelease, sootYield; /* 1/s, -, -, - */
+    float cooling, sootDecay;        /* 1/s */
+    float vorticityEps;
+    float windX, windZ;              /* acceleration of u and w, cells/step per second */
+    float noiseAmplitude, noisePeriod;
+    unsigned int noiseSeed;
+    int emitterCount;                /* 0..FIRE_MAX_EMITTERS */
+    FireEmitterDisk emitters[FIRE_MAX_EMITTERS];
+    int primarySamples, lightSamples;
+    float lightX, lightY, lightZ, lightIntensity;
+    float extinction, fuelExtinction, emission, albedo;
+    float eyeX, eyeY, eyeZ, targetX, targetY, targetZ, fovYDegrees;
+} FirePhysicsParams;
+
+/* The defaults: mode 0; for mode 1 the reference's buoyancy constants (1.62
+ * heat, 0.095 soot, src/fire_cuda.cu:1176), no wind, noise or emitters, and a
+ * camera on the grid's -z side looking at its centre. */
+FIRE_API void fireCudaDefaultPhysicsParams(FirePhysicsParams* params, int nx, int ny, int nz);
+/* Validates (sample counts 1..4096, emitterCount 0..4, finite values, dt > 0)
+ * and applies from the next pass on.  Switching modes does not clear the fields. */
+FIRE_API bool fireCudaSetPhysicsParams(const FirePhysicsParams* params);
+FIRE_API bool fireCudaGetPhysicsParams(FirePhysicsParams* params);
+
 /* ---- Independent scenes, batched steps, serving ------------------------
  * No counterpart in the reference, whose scene is one process-wide singleton
  * (src/fire_cuda.cu:116-195).  A FireScene owns its fields, its stream and
@@ -218,6 +293,9 @@ FIRE_API void fireSceneDestroy(FireScene* scene);
 /* Device memory the scene holds, in bytes (for admission against a budget). */
 FIRE_API size_t fireSceneDeviceBytes(const FireScene* scene);
 FIRE_API bool fireSceneSetPressureSolver(FireScene* scene, int iterations, float omega);
+/* As fireCudaSetPressureTolerance / fireCudaSetPhysicsParams, for one scene. */
+FIRE_API bool fireSceneSetPressureTolerance(FireScene* scene, double maxResidual, int checkEvery);
+FIRE_API bool fireSceneSetPhysicsParams(FireScene* scene, const FirePhysicsParams* params);
 /* Caller-owned device HDR buffer the scene renders into (as fireCudaRegisterHdrBufferSlot). */
 FIRE_API bool fireSceneSetHdrBuffer(FireScene* scene, void* devicePtr, size_t pitchBytes, int format);
 /* Queues one step (render = 0) or one step and a render into the HDR buffer

@@ -12,7 +12,7 @@ FIELDS = {
     "heat": 0, "fuel": 1, "oxygen": 2, "soot": 3, "char": 4, "ash": 5, "pyrolysis": 6,
     "progress": 7, "turbulence_energy": 8, "soot_optics": 9, "pressure": 10, "divergence": 11,
     "u": 12, "v": 13, "w": 14, "scene_light": 15, "scene_shadow": 16, "hdr": 17, "bgra": 18,
-    "divergence_after": 19,
+    "divergence_after": 19, "config_transmittance": 20,
 }
 SCALAR_FIELDS = ["heat", "fuel", "oxygen", "soot", "char", "ash", "pyrolysis", "progress",
                  "turbulence_energy", "soot_optics"]
@@ -179,3 +179,106 @@ def validation_settings(frame: int, scene: int = 0, width: int = 960, height: in
     s.cameraPitch = 0.08
     s.cameraDistance = 2.62
     return s
+
+
+# ---- Config physics (FirePhysicsParams.mode 1, include/fire_ext.h) ----------
+
+MAX_EMITTERS = 4
+
+
+class FireEmitterDisk(ctypes.Structure):
+    """include/fire_ext.h FireEmitterDisk."""
+    _fields_ = [
+        ("centerX", ctypes.c_float), ("centerY", ctypes.c_float), ("centerZ", ctypes.c_float),
+        ("radius", ctypes.c_float), ("fuel", ctypes.c_float), ("heat", ctypes.c_float),
+        ("upVelocity", ctypes.c_float), ("jitterScale", ctypes.c_float), ("seed", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+_PHYSICS_FLOATS_A = ["dt", "buoyancyHeat", "buoyancySoot", "ambientHeat", "burnRate", "ignitionHeat",
+                     "heatRelease", "sootYield", "cooling", "sootDecay", "vorticityEps", "windX", "windZ",
+                     "noiseAmplitude", "noisePeriod"]
+_PHYSICS_FLOATS_B = ["lightX", "lightY", "lightZ", "lightIntensity", "extinction", "fuelExtinction",
+                     "emission", "albedo", "eyeX", "eyeY", "eyeZ", "targetX", "targetY", "targetZ", "fovYDegrees"]
+
+
+class FirePhysicsParams(ctypes.Structure):
+    """include/fire_ext.h FirePhysicsParams (fill it with default_physics first)."""
+    _fields_ = ([("mode", ctypes.c_int)] + [(n, ctypes.c_float) for n in _PHYSICS_FLOATS_A] +
+                [("noiseSeed", ctypes.c_uint32), ("emitterCount", ctypes.c_int),
+                 ("emitters", FireEmitterDisk * MAX_EMITTERS), ("primarySamples", ctypes.c_int),
+                 ("lightSamples", ctypes.c_int)] + [(n, ctypes.c_float) for n in _PHYSICS_FLOATS_B])
+
+    def as_dict(self) -> dict:
+        out = {n: getattr(self, n) for n, _ in self._fields_ if n != "emitters"}
+        out["emitters"] = [{k: getattr(self.emitters[e], k) for k, _ in FireEmitterDisk._fields_}
+                           for e in range(self.emitterCount)]
+        return out
+
+
+def default_physics(nx: int, ny: int, nz: int, lib=None) -> FirePhysicsParams:
+    """fireCudaDefaultPhysicsParams (host only, needs no GPU)."""
+    if lib is None:
+        from . import firesim  # noqa: PLC0415
+        lib = firesim.load_library()
+    p = FirePhysicsParams()
+    lib.fireCudaDefaultPhysicsParams(ctypes.byref(p), nx, ny, nz)
+    return p
+
+
+def _disk(cx, cy, cz, r, seed, fuel=1.0, heat=1.0, up=2.0, jitter=0.2) -> FireEmitterDisk:
+    return FireEmitterDisk(centerX=cx, centerY=cy, centerZ=cz, radius=r, fuel=fuel, heat=heat, upVelocity=up,
+                           jitterScale=jitter, seed=seed)
+
+
+def config_workload(name: str, lib=None) -> dict:
+    """The three single-scene workloads of the config physics, as FirePhysicsParams
+    plus the solver, render and run settings they are stated with.
+
+    c1: 64^3, disk emitter r 6 at (32, 4, 32), F = T = 1 with jitter 0.2 from
+        seed 1, upward 2 cells/step; dt 1/60, confinement 0.3, buoyancy 0.1
+        (soot) and 1.0 (heat), burn 0.5/s, soot yield 0.3; SOR 40 at omega 1.7;
+        100 steps; one 256^2 frame, 64 samples, 32 light samples, point light
+        at (32, 90, 32).
+    c2: 128^3, the same physics with the emitter scaled x2 (r 12 at (64, 8,
+        64)), wind 0.5 on x, curl of value noise (seed 7, amplitude 0.4, period
+        16); SOR 60 at omega 1.8; 200 steps; a 512^2 frame every 10 steps, 128
+        samples, 48 light samples, light at (64, 180, 64).
+    c3: 256^3, BF16 storage; emitters r 16 at (96, 6, 128) and r 10 at (170,
+        6, 110), seed 3; SOR until max |r| <= 1e-5 or 120 iterations at omega
+        1.85; 100 steps.
+    """
+    sizes = {"c1": 64, "c2": 128, "c3": 256}
+    if name not in sizes:
+        raise ValueError(f"unknown config workload {name!r}: c1, c2 or c3")
+    n = sizes[name]
+    p = default_physics(n, n, n, lib)
+    p.mode = 1
+    p.dt = 1.0 / 60.0
+    p.buoyancyHeat, p.buoyancySoot = 1.0, 0.1
+    p.burnRate, p.sootYield = 0.5, 0.3
+    p.vorticityEps = 0.3
+    w = dict(name=name, grid=(n, n, n), physics=p, tolerance=0.0, check_every=10, precision="f32")
+    if name == "c1":
+        p.emitterCount = 1
+        p.emitters[0] = _disk(32, 4, 32, 6, 1)
+        p.primarySamples, p.lightSamples = 64, 32
+        p.lightX, p.lightY, p.lightZ = 32, 90, 32
+        w.update(frame=(256, 256), sor=(40, 1.7), steps=100, render_every=100)
+    elif name == "c2":
+        p.emitterCount = 1
+        p.emitters[0] = _disk(64, 8, 64, 12, 1)
+        p.windX = 0.5
+        p.noiseSeed, p.noiseAmplitude, p.noisePeriod = 7, 0.4, 16.0
+        p.primarySamples, p.lightSamples = 128, 48
+        p.lightX, p.lightY, p.lightZ = 64, 180, 64
+        w.update(frame=(512, 512), sor=(60, 1.8), steps=200, render_every=10)
+    else:
+        p.emitterCount = 2
+        p.emitters[0] = _disk(96, 6, 128, 16, 3)
+        p.emitters[1] = _disk(170, 6, 110, 10, 3)
+        p.primarySamples, p.lightSamples = 128, 48
+        p.lightX, p.lightY, p.lightZ = 128, 360, 128
+        w.update(frame=(512, 512), sor=(120, 1.85), tolerance=1e-5, steps=100, render_every=100, precision="bf16")
+    return w

@@ -29,6 +29,9 @@ VARIANTS = {
 INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr"]
+# Per-file flags: the config-physics kernels round every product and sum as
+# written (no FMA contraction), so their CPU restatement can match them bit for bit.
+FILE_FLAGS = {"fire_config.cu": ["-fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -48,7 +51,8 @@ def _compile(src: Path, force: bool, verbose_ptxas: bool, variant: str = "f32") 
     newest_dep = max([src.stat().st_mtime] + [h.stat().st_mtime for h in headers()])
     if not force and obj.exists() and obj.stat().st_mtime >= newest_dep and not verbose_ptxas:
         return obj, ""
-    cmd = [_nvcc(), *ARCH, *CUFLAGS, *VARIANTS[variant][2], "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+    cmd = [_nvcc(), *ARCH, *CUFLAGS, *FILE_FLAGS.get(src.name, []), *VARIANTS[variant][2], "-I", str(INCLUDE), "-c", str(src), "-o",
+           str(obj)]
     if verbose_ptxas:
         cmd[1:1] = ["-Xptxas", "-v"]
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -214,6 +214,25 @@ bool fireCudaSetPressureTolerance(double maxResidual, int checkEvery) {
     return true;
 }
 
+void fireCudaDefaultPhysicsParams(FirePhysicsParams* params, int nx, int ny, int nz) {
+    if (params != nullptr) firesim::defaultPhysicsParams(*params, nx, ny, nz);
+}
+
+bool fireCudaSetPhysicsParams(const FirePhysicsParams* params) {
+    if (!requireScene()) return false;
+    if (params == nullptr) return fail("Physics parameter pointer was null.");
+    std::string err;
+    if (!g_scene->setPhysics(*params, err)) return fail(err);
+    return true;
+}
+
+bool fireCudaGetPhysicsParams(FirePhysicsParams* params) {
+    if (!requireScene()) return false;
+    if (params == nullptr) return fail("Physics parameter pointer was null.");
+    *params = g_scene->physics();
+    return true;
+}
+
 bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Residual) {
     if (!requireScene()) return false;
     if (iterations == nullptr || maxResidual == nullptr || l2Residual == nullptr) return fail("Pressure stats pointer was null.");

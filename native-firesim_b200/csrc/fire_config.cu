@@ -1,0 +1,379 @@
+// fire_config.cu -- kernels of the config physics (FirePhysicsParams.mode 1).
+//
+// A plain T/F/S smoke-and-fire model on the same MAC grid and projection as
+// the reference physics: semi-Lagrangian advection in cell units, first-order
+// burn, seeded disk emitters, vorticity confinement, curl of seeded value
+// noise, wind, and a point-light transmittance render.  The reference has
+// none of these (its model is the ten-scalar fuel bed of src/fire_cuda.cu);
+// the equations are stated in include/fire_ext.h.  The divergence, the SOR
+// solve and the gradient subtraction are the reference-physics kernels.
+//
+// This file is compiled with -fmad=false: every product and sum rounds as
+// written, so a CPU restatement that evaluates the same expressions in the
+// same order in IEEE float gives the same bits for the whole simulation step
+// (only +, -, *, /, sqrt, floor, min/max and integer hashing occur there).
+// The render uses expf and is compared within a tolerance.
+//
+// Memory: records are read and written through the storage accessors
+// (ldv/stv), so the FP16 and BF16 storage builds apply unchanged.  Only record
+// a = (heat, fuel, oxygen, soot) is advanced; b and c are not touched.
+#include "fire_kernels.h"
+
+namespace firesim {
+
+namespace {
+
+__device__ __forceinline__ int faceIndex(int x, int y, int z, int mx, int my) { return (z * my + y) * mx + x; }
+
+// Clamped trilinear sample of a grid of mx*my*mz values (x fastest) at index-space
+// position q: q clamped to [0, m-1] per axis, i0 = (int)q, i1 = min(i0 + 1, m - 1),
+// t = q - i0; lerp(a, b, t) = a + t * (b - a), along x, then y, then z.
+struct Corners {
+    int x0, x1, y0, y1, z0, z1;
+    float tx, ty, tz;
+};
+
+__device__ __forceinline__ void axisOf(float q, int m, int& i0, int& i1, float& t) {
+    q = fminf(fmaxf(q, 0.0f), static_cast<float>(m - 1));
+    i0 = static_cast<int>(q);
+    i1 = min(i0 + 1, m - 1);
+    t = q - static_cast<float>(i0);
+}
+
+__device__ __forceinline__ Corners cornersAt(float qx, float qy, float qz, int mx, int my, int mz) {
+    Corners c;
+    axisOf(qx, mx, c.x0, c.x1, c.tx);
+    axisOf(qy, my, c.y0, c.y1, c.ty);
+    axisOf(qz, mz, c.z0, c.z1, c.tz);
+    return c;
+}
+
+__device__ __forceinline__ float lerp1(float a, float b, float t) { return a + t * (b - a); }
+
+__device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
+    return make_float4(lerp1(a.x, b.x, t), lerp1(a.y, b.y, t), lerp1(a.z, b.z, t), lerp1(a.w, b.w, t));
+}
+
+template <typename P>
+__device__ __forceinline__ float trilinear1(const P* f, const Corners& c, int mx, int my) {
+    const float a00 = lerp1(ldv(f + faceIndex(c.x0, c.y0, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z0, mx, my)), c.tx);
+    const float a10 = lerp1(ldv(f + faceIndex(c.x0, c.y1, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z0, mx, my)), c.tx);
+    const float a01 = lerp1(ldv(f + faceIndex(c.x0, c.y0, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z1, mx, my)), c.tx);
+    const float a11 = lerp1(ldv(f + faceIndex(c.x0, c.y1, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z1, mx, my)), c.tx);
+    const float b0 = lerp1(a00, a10, c.ty);
+    const float b1 = lerp1(a01, a11, c.ty);
+    return lerp1(b0, b1, c.tz);
+}
+
+__device__ __forceinline__ float4 trilinearRec(const Rec4* f, const Corners& c, int mx, int my) {
+    const float4 a00 = lerp4(ldv(f + faceIndex(c.x0, c.y0, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z0, mx, my)), c.tx);
+    const float4 a10 = lerp4(ldv(f + faceIndex(c.x0, c.y1, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z0, mx, my)), c.tx);
+    const float4 a01 = lerp4(ldv(f + faceIndex(c.x0, c.y0, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z1, mx, my)), c.tx);
+    const float4 a11 = lerp4(ldv(f + faceIndex(c.x0, c.y1, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z1, mx, my)), c.tx);
+    const float4 b0 = lerp4(a00, a10, c.ty);
+    const float4 b1 = lerp4(a01, a11, c.ty);
+    return lerp4(b0, b1, c.tz);
+}
+
+// Velocity (cells per step) at a world position in cell units: u lives at
+// (i, j+.5, k+.5), v at (i+.5, j, k+.5), w at (i+.5, j+.5, k).
+__device__ __forceinline__ float3 velocityAt(const Velocity& vel, const ConfigParams& p, float x, float y, float z) {
+    const float u = trilinear1(vel.u, cornersAt(x, y - 0.5f, z - 0.5f, p.nx + 1, p.ny, p.nz), p.nx + 1, p.ny);
+    const float v = trilinear1(vel.v, cornersAt(x - 0.5f, y, z - 0.5f, p.nx, p.ny + 1, p.nz), p.nx, p.ny + 1);
+    const float w = trilinear1(vel.w, cornersAt(x - 0.5f, y - 0.5f, z, p.nx, p.ny, p.nz + 1), p.nx, p.ny);
+    return make_float3(u, v, w);
+}
+
+__device__ __forceinline__ float4 recordAt(const Rec4* a, const ConfigParams& p, float x, float y, float z) {
+    return trilinearRec(a, cornersAt(x - 0.5f, y - 0.5f, z - 0.5f, p.nx, p.ny, p.nz), p.nx, p.ny);
+}
+
+__device__ __forceinline__ bool inDisk(const ConfigEmitter& e, int x, int y, int z) {
+    if (y != e.row) return false;
+    const float dx = static_cast<float>(x) - e.cx;
+    const float dz = static_cast<float>(z) - e.cz;
+    return dx * dx + dz * dz <= e.r2;
+}
+
+// psi_c at position (x, y, z) (cell units) and its gradient: value noise on a
+// lattice of period 1/invPeriod cells, cubic Hermite weights s = f^2 (3 - 2f),
+// ds/df = 6 f (1 - f).
+__device__ __forceinline__ float3 noiseGradient(const ConfigParams& p, int comp, float x, float y, float z) {
+    const float qx = x * p.invPeriod, qy = y * p.invPeriod, qz = z * p.invPeriod;
+    const float fx0 = floorf(qx), fy0 = floorf(qy), fz0 = floorf(qz);
+    const int ix = static_cast<int>(fx0), iy = static_cast<int>(fy0), iz = static_cast<int>(fz0);
+    const float fx = qx - fx0, fy = qy - fy0, fz = qz - fz0;
+    const float sx = fx * fx * (3.0f - 2.0f * fx), sy = fy * fy * (3.0f - 2.0f * fy), sz = fz * fz * (3.0f - 2.0f * fz);
+    const float dsx = 6.0f * fx * (1.0f - fx), dsy = 6.0f * fy * (1.0f - fy), dsz = 6.0f * fz * (1.0f - fz);
+    const float c000 = latticeValue(p.noiseSeed, comp, ix, iy, iz), c100 = latticeValue(p.noiseSeed, comp, ix + 1, iy, iz);
+    const float c010 = latticeValue(p.noiseSeed, comp, ix, iy + 1, iz), c110 = latticeValue(p.noiseSeed, comp, ix + 1, iy + 1, iz);
+    const float c001 = latticeValue(p.noiseSeed, comp, ix, iy, iz + 1), c101 = latticeValue(p.noiseSeed, comp, ix + 1, iy, iz + 1);
+    const float c011 = latticeValue(p.noiseSeed, comp, ix, iy + 1, iz + 1), c111 = latticeValue(p.noiseSeed, comp, ix + 1, iy + 1, iz + 1);
+    const float a00 = lerp1(c000, c100, sx), a10 = lerp1(c010, c110, sx), a01 = lerp1(c001, c101, sx), a11 = lerp1(c011, c111, sx);
+    const float b0 = lerp1(a00, a10, sy), b1 = lerp1(a01, a11, sy);
+    const float e0 = lerp1(c100 - c000, c110 - c010, sy), e1 = lerp1(c101 - c001, c111 - c011, sy);
+    const float gx = dsx * lerp1(e0, e1, sz);
+    const float gy = dsy * lerp1(a10 - a00, a11 - a01, sz);
+    const float gz = dsz * (b1 - b0);
+    return make_float3(gx * p.invPeriod, gy * p.invPeriod, gz * p.invPeriod);
+}
+
+__device__ __forceinline__ float cellCentred(const FaceT* f, int lo, int hi) { return 0.5f * (ldv(f + lo) + ldv(f + hi)); }
+
+}  // namespace
+
+// Each thread owns u(x,y,z), v(x,y,z) and w(x,y,z) where they exist and
+// writes each as the face grid sampled at its one-step backtrace.
+__global__ void __launch_bounds__(128) cfgAdvectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                         Velocity vel, ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x > p.nx) return;
+    const float fx = static_cast<float>(x), fy = static_cast<float>(y), fz = static_cast<float>(z);
+    if (y < p.ny && z < p.nz) {
+        const float px = fx, py = fy + 0.5f, pz = fz + 0.5f;
+        const float3 d = velocityAt(vel, p, px, py, pz);
+        const float bx = px - d.x, by = py - d.y, bz = pz - d.z;
+        stv(uOut + faceIndex(x, y, z, p.nx + 1, p.ny),
+            trilinear1(vel.u, cornersAt(bx, by - 0.5f, bz - 0.5f, p.nx + 1, p.ny, p.nz), p.nx + 1, p.ny));
+    }
+    if (x < p.nx && z < p.nz) {
+        const float px = fx + 0.5f, py = fy, pz = fz + 0.5f;
+        const float3 d = velocityAt(vel, p, px, py, pz);
+        const float bx = px - d.x, by = py - d.y, bz = pz - d.z;
+        stv(vOut + faceIndex(x, y, z, p.nx, p.ny + 1), trilinear1(vel.v, cornersAt(bx - 0.5f, by, bz - 0.5f, p.nx, p.ny + 1, p.nz), p.nx, p.ny + 1));
+    }
+    if (x < p.nx && y < p.ny) {
+        const float px = fx + 0.5f, py = fy + 0.5f, pz = fz;
+        const float3 d = velocityAt(vel, p, px, py, pz);
+        const float bx = px - d.x, by = py - d.y, bz = pz - d.z;
+        stv(wOut + faceIndex(x, y, z, p.nx, p.ny), trilinear1(vel.w, cornersAt(bx - 0.5f, by - 0.5f, bz, p.nx, p.ny, p.nz + 1), p.nx, p.ny));
+    }
+}
+
+// Backtrace of record a from the cell centre, then burn, decay and emitters.
+__global__ void __launch_bounds__(128) cfgAdvectScalars(Rec4* __restrict__ aOut, const Rec4* __restrict__ aIn, Velocity vel, ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) return;
+    const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
+    const float3 d = velocityAt(vel, p, px, py, pz);
+    const float4 s = recordAt(aIn, p, px - d.x, py - d.y, pz - d.z);
+    float heat = s.x, fuel = s.y, soot = s.w;
+    if (heat > p.ignition) {
+        const float burn = fuel * p.burnFrac;
+        fuel = fuel - burn;
+        heat = heat + p.heatRelease * burn;
+        soot = soot + p.sootYield * burn;
+    }
+    heat = heat - heat * p.coolFrac;
+    soot = soot - soot * p.sootFrac;
+    const unsigned cell = static_cast<unsigned>((z * p.ny + y) * p.nx + x);
+    for (int e = 0; e < p.emitterCount; ++e) {
+        const ConfigEmitter& em = p.emitters[e];
+        if (!inDisk(em, x, y, z)) continue;
+        const float j = 1.0f - em.jitter * jitterUniform(em.seed, p.step, cell);
+        fuel = fmaxf(fuel, em.fuel * j);
+        heat = fmaxf(heat, em.heat * j);
+    }
+    stv(aOut + cell, make_float4(heat, fuel, 0.0f, soot));
+}
+
+// omega = curl of the cell-centred velocity (central differences, clamped
+// neighbours), and |omega|.
+__global__ void __launch_bounds__(128) cfgVorticity(float4* __restrict__ vort, Velocity vel, ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) return;
+    const int xm = max(x - 1, 0), xp = min(x + 1, p.nx - 1);
+    const int ym = max(y - 1, 0), yp = min(y + 1, p.ny - 1);
+    const int zm = max(z - 1, 0), zp = min(z + 1, p.nz - 1);
+    const int ux = p.nx + 1, vy = p.ny + 1;
+    auto ccx = [&](int i, int j, int k) { return cellCentred(vel.u, faceIndex(i, j, k, ux, p.ny), faceIndex(i + 1, j, k, ux, p.ny)); };
+    auto ccy = [&](int i, int j, int k) { return cellCentred(vel.v, faceIndex(i, j, k, p.nx, vy), faceIndex(i, j + 1, k, p.nx, vy)); };
+    auto ccz = [&](int i, int j, int k) { return cellCentred(vel.w, faceIndex(i, j, k, p.nx, p.ny), faceIndex(i, j, k + 1, p.nx, p.ny)); };
+    const float ox = 0.5f * (ccz(x, yp, z) - ccz(x, ym, z)) - 0.5f * (ccy(x, y, zp) - ccy(x, y, zm));
+    const float oy = 0.5f * (ccx(x, y, zp) - ccx(x, y, zm)) - 0.5f * (ccz(xp, y, z) - ccz(xm, y, z));
+    const float oz = 0.5f * (ccy(xp, y, z) - ccy(xm, y, z)) - 0.5f * (ccx(x, yp, z) - ccx(x, ym, z));
+    vort[(z * p.ny + y) * p.nx + x] = make_float4(ox, oy, oz, sqrtf(ox * ox + oy * oy + oz * oz));
+}
+
+// Cell-centred acceleration: buoyancy + confinement + curl noise.
+__global__ void __launch_bounds__(128) cfgCellForce(float4* __restrict__ force, const float4* __restrict__ vort, const Rec4* __restrict__ a,
+                                                    ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) return;
+    const int idx = (z * p.ny + y) * p.nx + x;
+    const float4 s = ldv(a + idx);
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    if (p.eps != 0.0f) {
+        const int xm = max(x - 1, 0), xp = min(x + 1, p.nx - 1);
+        const int ym = max(y - 1, 0), yp = min(y + 1, p.ny - 1);
+        const int zm = max(z - 1, 0), zp = min(z + 1, p.nz - 1);
+        const float4 o = vort[idx];
+        const float ex = 0.5f * (vort[(z * p.ny + y) * p.nx + xp].w - vort[(z * p.ny + y) * p.nx + xm].w);
+        const float ey = 0.5f * (vort[(z * p.ny + yp) * p.nx + x].w - vort[(z * p.ny + ym) * p.nx + x].w);
+        const float ez = 0.5f * (vort[(zp * p.ny + y) * p.nx + x].w - vort[(zm * p.ny + y) * p.nx + x].w);
+        const float len = sqrtf(ex * ex + ey * ey + ez * ez);
+        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+        if (len > 1e-20f) {
+            nx = ex / len;
+            ny = ey / len;
+            nz = ez / len;
+        }
+        cx = p.eps * (ny * o.z - nz * o.y);
+        cy = p.eps * (nz * o.x - nx * o.z);
+        cz = p.eps * (nx * o.y - ny * o.x);
+    }
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (p.noiseAmp != 0.0f) {
+        const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
+        const float3 g0 = noiseGradient(p, 0, px, py, pz);
+        const float3 g1 = noiseGradient(p, 1, px, py, pz);
+        const float3 g2 = noiseGradient(p, 2, px, py, pz);
+        fx = p.noiseAmp * (g2.y - g1.z);
+        fy = p.noiseAmp * (g0.z - g2.x);
+        fz = p.noiseAmp * (g1.x - g0.y);
+    }
+    const float buoyancy = p.buoyHeat * (s.x - p.ambient) - p.buoySoot * s.w;
+    force[idx] = make_float4(cx + fx, buoyancy + cy + fy, cz + fz, 0.0f);
+}
+
+// Faces += dt * (mean of the two adjacent cells' accelerations) + wind; the
+// emitter cells' v faces take upVelocity; walls (u at x = 0, nx; v at y = 0;
+// w at z = 0, nz) are zero; the top v faces keep the cell below's acceleration.
+__global__ void __launch_bounds__(128) cfgApplyForces(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                      Velocity vel, const float4* __restrict__ force, ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x > p.nx) return;
+    if (y < p.ny && z < p.nz) {
+        const int i = faceIndex(x, y, z, p.nx + 1, p.ny);
+        float u = 0.0f;
+        if (x > 0 && x < p.nx) {
+            const float fa = force[(z * p.ny + y) * p.nx + x - 1].x, fb = force[(z * p.ny + y) * p.nx + x].x;
+            u = ldv(vel.u + i) + (p.dt * (0.5f * (fa + fb)) + p.windDtX);
+        }
+        stv(uOut + i, u);
+    }
+    if (x < p.nx && z < p.nz) {
+        const int i = faceIndex(x, y, z, p.nx, p.ny + 1);
+        float v = 0.0f;
+        if (y > 0) {
+            const float fd = force[(z * p.ny + y - 1) * p.nx + x].y;
+            v = y < p.ny ? ldv(vel.v + i) + p.dt * (0.5f * (fd + force[(z * p.ny + y) * p.nx + x].y)) : ldv(vel.v + i) + p.dt * fd;
+            for (int e = 0; e < p.emitterCount; ++e) {
+                const ConfigEmitter& em = p.emitters[e];
+                if ((y < p.ny && inDisk(em, x, y, z)) || inDisk(em, x, y - 1, z)) v = em.up;
+            }
+        }
+        stv(vOut + i, v);
+    }
+    if (x < p.nx && y < p.ny) {
+        const int i = faceIndex(x, y, z, p.nx, p.ny);
+        float w = 0.0f;
+        if (z > 0 && z < p.nz) {
+            const float fb = force[((z - 1) * p.ny + y) * p.nx + x].z, ff = force[(z * p.ny + y) * p.nx + x].z;
+            w = ldv(vel.w + i) + (p.dt * (0.5f * (fb + ff)) + p.windDtZ);
+        }
+        stv(wOut + i, w);
+    }
+}
+
+// Transmittance toward the point light from the centre of each 2x2x2 block of
+// cells: lightSamples midpoint samples of extinction * S + fuelExtinction * F
+// along the segment, clipped where it leaves the grid box.
+__global__ void __launch_bounds__(128) cfgTransmittance(float* __restrict__ tr, const Rec4* __restrict__ a, ConfigParams p) {
+    const int lx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ly = blockIdx.y;
+    const int lz = blockIdx.z;
+    if (lx >= p.lx) return;
+    const float px = 2.0f * static_cast<float>(lx) + 1.0f, py = 2.0f * static_cast<float>(ly) + 1.0f, pz = 2.0f * static_cast<float>(lz) + 1.0f;
+    const float dx = p.light.x - px, dy = p.light.y - py, dz = p.light.z - pz;
+    const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+    float t = 1.0f;
+    if (dist > 1e-6f) {
+        const float rx = dx / dist, ry = dy / dist, rz = dz / dist;
+        float seg = dist;
+        if (rx > 0.0f) seg = fminf(seg, (static_cast<float>(p.nx) - px) / rx);
+        if (rx < 0.0f) seg = fminf(seg, (0.0f - px) / rx);
+        if (ry > 0.0f) seg = fminf(seg, (static_cast<float>(p.ny) - py) / ry);
+        if (ry < 0.0f) seg = fminf(seg, (0.0f - py) / ry);
+        if (rz > 0.0f) seg = fminf(seg, (static_cast<float>(p.nz) - pz) / rz);
+        if (rz < 0.0f) seg = fminf(seg, (0.0f - pz) / rz);
+        seg = fmaxf(seg, 0.0f);
+        const float ds = seg / static_cast<float>(p.lightSamples);
+        float tau = 0.0f;
+        for (int s = 0; s < p.lightSamples; ++s) {
+            const float at = (static_cast<float>(s) + 0.5f) * ds;
+            const float4 r = recordAt(a, p, px + rx * at, py + ry * at, pz + rz * at);
+            tau = tau + (p.extinction * r.w + p.fuelExtinction * r.y) * ds;
+        }
+        t = expf(-tau);
+    }
+    tr[(lz * p.ly + ly) * p.lx + lx] = t;
+}
+
+// One pixel: the camera ray's chord through the grid box in primarySamples
+// midpoint samples; absorption, in-scattering of the point light (its
+// transmittance volume) and emission; a dark background behind.
+__global__ void __launch_bounds__(128) cfgRaymarch(float4* __restrict__ hdr, const Rec4* __restrict__ a, const float* __restrict__ tr,
+                                                   ConfigParams p) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= p.frameW || py >= p.frameH) return;
+    const float sx = (2.0f * (static_cast<float>(px) + 0.5f) / static_cast<float>(p.frameW) - 1.0f) * p.tanHalf * p.aspect;
+    const float sy = (1.0f - 2.0f * (static_cast<float>(py) + 0.5f) / static_cast<float>(p.frameH)) * p.tanHalf;
+    float dx = p.forward.x + p.right.x * sx + p.up.x * sy;
+    float dy = p.forward.y + p.right.y * sx + p.up.y * sy;
+    float dz = p.forward.z + p.right.z * sx + p.up.z * sy;
+    const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+    dx = dx / len;
+    dy = dy / len;
+    dz = dz / len;
+    float t0 = 0.0f, t1 = 3.0e38f;
+    bool hit = true;
+    const float eye[3] = {p.eye.x, p.eye.y, p.eye.z};
+    const float dir[3] = {dx, dy, dz};
+    const float hiB[3] = {static_cast<float>(p.nx), static_cast<float>(p.ny), static_cast<float>(p.nz)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (dir[k] == 0.0f) {
+            if (eye[k] < 0.0f || eye[k] > hiB[k]) hit = false;
+        } else {
+            const float ta = (0.0f - eye[k]) / dir[k];
+            const float tb = (hiB[k] - eye[k]) / dir[k];
+            t0 = fmaxf(t0, fminf(ta, tb));
+            t1 = fminf(t1, fmaxf(ta, tb));
+        }
+    }
+    float r = 0.0f, g = 0.0f, b = 0.0f, view = 1.0f;
+    if (hit && t1 > t0) {
+        const float ds = (t1 - t0) / static_cast<float>(p.primarySamples);
+        for (int s = 0; s < p.primarySamples; ++s) {
+            const float at = t0 + (static_cast<float>(s) + 0.5f) * ds;
+            const float qx = p.eye.x + dx * at, qy = p.eye.y + dy * at, qz = p.eye.z + dz * at;
+            const float4 rec = recordAt(a, p, qx, qy, qz);
+            const float sigma = p.extinction * rec.w + p.fuelExtinction * rec.y;
+            const float alpha = 1.0f - expf(-(sigma * ds));
+            const float lt = trilinear1(tr, cornersAt(qx * 0.5f - 0.5f, qy * 0.5f - 0.5f, qz * 0.5f - 0.5f, p.lx, p.ly, p.lz), p.lx, p.ly);
+            const float scatter = p.albedo * p.lightIntensity * lt * alpha;
+            const float heat = fmaxf(rec.x, 0.0f);
+            const float h = heat / (heat + 1.0f);
+            const float e = p.emission * heat * ds;
+            r = r + view * (scatter + e);
+            g = g + view * (scatter + e * (0.35f + 0.45f * h));
+            b = b + view * (scatter + e * (0.08f + 0.50f * h * h));
+            view = view * (1.0f - alpha);
+        }
+    }
+    hdr[py * p.frameW + px] = make_float4(r + view * 0.015f, g + view * 0.016f, b + view * 0.020f, 1.0f - view);
+}
+
+}  // namespace firesim

@@ -137,4 +137,60 @@ __global__ void metricsPartials(MetricPartial* partials, ScalarFieldsIn s, const
                                 const float* divergenceBefore, const float* divergenceAfter, FrameParams p);
 __global__ void metricsFinal(MetricPartial* out, const MetricPartial* partials, int count);
 
+// ---------------------------------------------------------------------------
+// Config physics (FirePhysicsParams.mode 1, fire_config.cu).  Per-step
+// constants are formed on the host from FirePhysicsParams in float:
+// burnFrac = min(1, burnRate * dt), coolFrac = min(1, cooling * dt),
+// sootFrac = min(1, sootDecay * dt), windDtX/Z = dt * windX/Z,
+// invPeriod = 1 / noisePeriod, r2 = radius * radius, row = (int)centerY.
+struct ConfigEmitter {
+    float cx, cz, r2, fuel, heat, up, jitter;
+    int row;
+    unsigned seed;
+};
+struct ConfigParams {
+    int nx, ny, nz, lx, ly, lz, frameW, frameH;
+    unsigned long long step;
+    float dt, burnFrac, coolFrac, sootFrac, ignition, heatRelease, sootYield;
+    float buoyHeat, buoySoot, ambient, eps, windDtX, windDtZ;
+    float noiseAmp, invPeriod;
+    unsigned noiseSeed;
+    int emitterCount;
+    ConfigEmitter emitters[4];
+    int primarySamples, lightSamples;
+    float3 light;
+    float lightIntensity, extinction, fuelExtinction, emission, albedo;
+    float3 eye, forward, right, up;
+    float tanHalf, aspect;
+};
+
+// SplitMix64's output function (Steele, Lea and Flood, OOPSLA 2014).
+__host__ __device__ inline unsigned long long splitmix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// Emitter jitter: uniform in [0, 1) on a 2^-24 grid, one draw per (seed, step, cell).
+__host__ __device__ inline float jitterUniform(unsigned seed, unsigned long long step, unsigned cell) {
+    const unsigned long long k = (static_cast<unsigned long long>(seed) << 32) ^ (step * 0xD1B54A32D192ED03ull) ^ cell;
+    return static_cast<float>(splitmix64(k) >> 40) * (1.0f / 16777216.0f);
+}
+// Value-noise lattice value in [-1, 1) on a 2^-23 grid for component comp of the seeded field.
+__host__ __device__ inline float latticeValue(unsigned seed, int comp, int ix, int iy, int iz) {
+    const unsigned long long k = ((static_cast<unsigned long long>(seed) << 2) | static_cast<unsigned>(comp)) * 0xD1342543DE82EF95ull +
+                                 static_cast<unsigned long long>(static_cast<unsigned>(ix)) * 0x9E3779B97F4A7C15ull +
+                                 static_cast<unsigned long long>(static_cast<unsigned>(iy)) * 0xC2B2AE3D27D4EB4Full +
+                                 static_cast<unsigned long long>(static_cast<unsigned>(iz)) * 0x165667B19E3779F9ull;
+    return static_cast<float>(splitmix64(k) >> 40) * (1.0f / 8388608.0f) - 1.0f;
+}
+
+__global__ void cfgAdvectVelocity(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, ConfigParams p);
+__global__ void cfgAdvectScalars(Rec4* aOut, const Rec4* aIn, Velocity vel, ConfigParams p);
+__global__ void cfgVorticity(float4* vort, Velocity vel, ConfigParams p);
+__global__ void cfgCellForce(float4* force, const float4* vort, const Rec4* a, ConfigParams p);
+__global__ void cfgApplyForces(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, const float4* force, ConfigParams p);
+__global__ void cfgTransmittance(float* tr, const Rec4* a, ConfigParams p);
+__global__ void cfgRaymarch(float4* hdr, const Rec4* a, const float* tr, ConfigParams p);
+
 }  // namespace firesim

@@ -67,7 +67,8 @@ void Scene::release() {
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
                     shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_,
-                    rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_, split_, splitDiv_};
+                    rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_, split_, splitDiv_,
+                    cfgVort_, cfgLight_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
@@ -83,6 +84,8 @@ void Scene::release() {
     residualMax_ = nullptr;
     split_ = nullptr;
     splitDiv_ = nullptr;
+    cfgVort_ = nullptr;
+    cfgLight_ = nullptr;
     sorHostStatus_ = nullptr;
     curlLattice_ = nullptr;
     sourceLattice_ = nullptr;
@@ -120,6 +123,8 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
     nz = z;
     frameW = fw;
     frameH = fh;
+    defaultPhysicsParams(physics_, nx, ny, nz);
+    cfgStep_ = 0;
     // Light grid, src/fire_cuda.cu:2920-2922.
     lnx = clampI((nx + 3) / 4, 18, 48);
     lny = clampI((ny + 3) / 4, 20, 56);
@@ -656,6 +661,7 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
         err = "stage range out of order";
         return false;
     }
+    if (physics_.mode == 1) return runConfigStages(first, last, p, err);
     const int bx = rowThreads(nx);
     const int bxFace = rowThreads(nx + 1);
     const dim3 cells = cellGrid(bx, nx, ny, nz);
@@ -1021,8 +1027,11 @@ void floatToStored(float f, unsigned char* p, int bytes) {
 bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
     FaceT* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
     FieldView v;
-    if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_, bgra_,
-                   cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
+    if (field == FIRE_FIELD_CONFIG_TRANSMITTANCE) {
+        if (!ensureConfigBuffers(err)) return false;
+        v = {cfgLight_, static_cast<size_t>(cfgLx_) * cfgLy_ * cfgLz_, 1, 0, 1, 4};
+    } else if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_,
+                          bgra_, cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
         err = "unknown field id";
         return false;
     }
@@ -1048,8 +1057,11 @@ bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
 bool Scene::setField(int field, const void* host, size_t bytes, std::string& err) {
     FaceT* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
     FieldView v;
-    if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_, bgra_,
-                   cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
+    if (field == FIRE_FIELD_CONFIG_TRANSMITTANCE) {
+        if (!ensureConfigBuffers(err)) return false;
+        v = {cfgLight_, static_cast<size_t>(cfgLx_) * cfgLy_ * cfgLz_, 1, 0, 1, 4};
+    } else if (!fieldView(field, sa_[cur_], sb_[cur_], sc_[cur_], velNow, pressure_, divergence_, divergenceAfter_, light_, shadow_, hdr_,
+                          bgra_, cells_, nu_, nv_, nw_, lightCells_, pixels_, v)) {
         err = "unknown field id";
         return false;
     }
@@ -1162,6 +1174,268 @@ bool Scene::setResidentFault(int silentBrick, long long waitUs, std::string& err
     }
     sorSilentBrick_ = silentBrick < 0 ? -1 : silentBrick;
     sorWaitNs_ = static_cast<unsigned long long>(waitUs) * 1000ull;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Config physics (FirePhysicsParams.mode 1): parameters, buffers and stages.
+
+void defaultPhysicsParams(FirePhysicsParams& q, int nx, int ny, int nz) {
+    std::memset(&q, 0, sizeof(q));
+    q.mode = 0;
+    q.dt = 1.0f / 60.0f;
+    q.buoyancyHeat = 1.62f;   // src/fire_cuda.cu:1176
+    q.buoyancySoot = 0.095f;  // src/fire_cuda.cu:1176
+    q.ambientHeat = 0.0f;
+    q.burnRate = 0.5f;
+    q.ignitionHeat = 0.05f;
+    q.heatRelease = 1.0f;
+    q.sootYield = 0.3f;
+    q.cooling = 0.35f;
+    q.sootDecay = 0.05f;
+    q.vorticityEps = 0.0f;
+    q.noisePeriod = 16.0f;
+    q.noiseSeed = 7u;
+    q.primarySamples = 96;
+    q.lightSamples = 32;
+    q.lightX = 0.5f * static_cast<float>(nx);
+    q.lightY = 1.4f * static_cast<float>(ny);
+    q.lightZ = 0.5f * static_cast<float>(nz);
+    q.lightIntensity = 1.0f;
+    q.extinction = 0.9f;
+    q.fuelExtinction = 0.05f;
+    q.emission = 0.6f;
+    q.albedo = 0.7f;
+    q.eyeX = 0.5f * static_cast<float>(nx);
+    q.eyeY = 0.5f * static_cast<float>(ny);
+    q.eyeZ = -1.3f * static_cast<float>(std::max(nx, std::max(ny, nz)));
+    q.targetX = 0.5f * static_cast<float>(nx);
+    q.targetY = 0.5f * static_cast<float>(ny);
+    q.targetZ = 0.5f * static_cast<float>(nz);
+    q.fovYDegrees = 45.0f;
+}
+
+bool validatePhysicsParams(const FirePhysicsParams& q, std::string& err) {
+    if (q.mode != 0 && q.mode != 1) {
+        err = "physics mode must be 0 (reference) or 1 (config)";
+        return false;
+    }
+    const float vals[] = {q.dt, q.buoyancyHeat, q.buoyancySoot, q.ambientHeat, q.burnRate, q.ignitionHeat, q.heatRelease, q.sootYield,
+                          q.cooling, q.sootDecay, q.vorticityEps, q.windX, q.windZ, q.noiseAmplitude, q.noisePeriod, q.lightX,
+                          q.lightY, q.lightZ, q.lightIntensity, q.extinction, q.fuelExtinction, q.emission, q.albedo, q.eyeX,
+                          q.eyeY, q.eyeZ, q.targetX, q.targetY, q.targetZ, q.fovYDegrees};
+    for (float v : vals) {
+        if (!std::isfinite(v)) {
+            err = "physics parameters must be finite";
+            return false;
+        }
+    }
+    if (!(q.dt > 0.0f) || !(q.noisePeriod > 0.0f) || q.burnRate < 0.0f || q.cooling < 0.0f || q.sootDecay < 0.0f) {
+        err = "physics parameters: dt and noisePeriod must be > 0, rates >= 0";
+        return false;
+    }
+    if (q.primarySamples < 1 || q.primarySamples > 4096 || q.lightSamples < 1 || q.lightSamples > 4096) {
+        err = "physics parameters: sample counts must be in 1..4096";
+        return false;
+    }
+    if (!(q.fovYDegrees > 0.0f && q.fovYDegrees < 179.0f)) {
+        err = "physics parameters: fovYDegrees must be in (0, 179)";
+        return false;
+    }
+    if (q.emitterCount < 0 || q.emitterCount > FIRE_MAX_EMITTERS) {
+        err = "physics parameters: emitterCount must be in 0..4";
+        return false;
+    }
+    for (int e = 0; e < q.emitterCount; ++e) {
+        const FireEmitterDisk& d = q.emitters[e];
+        const float ev[] = {d.centerX, d.centerY, d.centerZ, d.radius, d.fuel, d.heat, d.upVelocity, d.jitterScale};
+        for (float v : ev) {
+            if (!std::isfinite(v)) {
+                err = "emitter parameters must be finite";
+                return false;
+            }
+        }
+        if (d.radius < 0.0f || d.jitterScale < 0.0f || d.jitterScale > 1.0f || std::fabs(d.centerY) > 1.0e6f) {
+            err = "emitter parameters: radius >= 0, jitterScale in [0, 1]";
+            return false;
+        }
+    }
+    const float fx = q.targetX - q.eyeX, fy = q.targetY - q.eyeY, fz = q.targetZ - q.eyeZ;
+    if (!(fx * fx + fy * fy + fz * fz > 0.0f)) {
+        err = "physics parameters: camera eye and target coincide";
+        return false;
+    }
+    return true;
+}
+
+bool Scene::setPhysics(const FirePhysicsParams& params, std::string& err) {
+    if (!validatePhysicsParams(params, err)) return false;
+    physics_ = params;
+    return true;
+}
+
+ConfigParams Scene::configParams() const {
+    const FirePhysicsParams& q = physics_;
+    ConfigParams c{};
+    c.nx = nx;
+    c.ny = ny;
+    c.nz = nz;
+    c.lx = (nx + 1) / 2;
+    c.ly = (ny + 1) / 2;
+    c.lz = (nz + 1) / 2;
+    c.frameW = frameW;
+    c.frameH = frameH;
+    c.step = cfgStep_;
+    c.dt = q.dt;
+    c.burnFrac = std::min(1.0f, q.burnRate * q.dt);
+    c.coolFrac = std::min(1.0f, q.cooling * q.dt);
+    c.sootFrac = std::min(1.0f, q.sootDecay * q.dt);
+    c.ignition = q.ignitionHeat;
+    c.heatRelease = q.heatRelease;
+    c.sootYield = q.sootYield;
+    c.buoyHeat = q.buoyancyHeat;
+    c.buoySoot = q.buoyancySoot;
+    c.ambient = q.ambientHeat;
+    c.eps = q.vorticityEps;
+    c.windDtX = q.dt * q.windX;
+    c.windDtZ = q.dt * q.windZ;
+    c.noiseAmp = q.noiseAmplitude;
+    c.invPeriod = 1.0f / q.noisePeriod;
+    c.noiseSeed = q.noiseSeed;
+    c.emitterCount = q.emitterCount;
+    for (int e = 0; e < q.emitterCount; ++e) {
+        const FireEmitterDisk& d = q.emitters[e];
+        c.emitters[e] = ConfigEmitter{d.centerX, d.centerZ, d.radius * d.radius, d.fuel, d.heat, d.upVelocity, d.jitterScale,
+                                      static_cast<int>(std::floor(d.centerY)), d.seed};
+    }
+    c.primarySamples = q.primarySamples;
+    c.lightSamples = q.lightSamples;
+    c.light = make_float3(q.lightX, q.lightY, q.lightZ);
+    c.lightIntensity = q.lightIntensity;
+    c.extinction = q.extinction;
+    c.fuelExtinction = q.fuelExtinction;
+    c.emission = q.emission;
+    c.albedo = q.albedo;
+    // Pinhole camera: forward to the target, right = forward x (0, 1, 0), up = right x forward.
+    float fx = q.targetX - q.eyeX, fy = q.targetY - q.eyeY, fz = q.targetZ - q.eyeZ;
+    const float fl = std::sqrt(fx * fx + fy * fy + fz * fz);
+    fx = fx / fl;
+    fy = fy / fl;
+    fz = fz / fl;
+    float rx = -fz, ry = 0.0f, rz = fx;
+    const float rl = std::sqrt(rx * rx + rz * rz);
+    if (rl > 0.0f) {
+        rx = rx / rl;
+        rz = rz / rl;
+    } else {
+        rx = 1.0f;
+        rz = 0.0f;
+    }
+    c.eye = make_float3(q.eyeX, q.eyeY, q.eyeZ);
+    c.forward = make_float3(fx, fy, fz);
+    c.right = make_float3(rx, ry, rz);
+    c.up = make_float3(ry * fz - rz * fy, rz * fx - rx * fz, rx * fy - ry * fx);
+    c.tanHalf = std::tan(q.fovYDegrees * 0.00872664626f);
+    c.aspect = static_cast<float>(frameW) / static_cast<float>(frameH);
+    return c;
+}
+
+bool Scene::ensureConfigBuffers(std::string& err) {
+    if (cfgVort_ != nullptr) return true;
+    cfgLx_ = (nx + 1) / 2;
+    cfgLy_ = (ny + 1) / 2;
+    cfgLz_ = (nz + 1) / 2;
+    const size_t lightCells = static_cast<size_t>(cfgLx_) * cfgLy_ * cfgLz_;
+    return alloc(reinterpret_cast<void**>(&cfgVort_), cells_ * sizeof(float4), "cudaMalloc config vorticity", err) &&
+           alloc(reinterpret_cast<void**>(&cfgLight_), lightCells * sizeof(float), "cudaMalloc config transmittance", err) &&
+           check("clear config vorticity", cudaMemsetAsync(cfgVort_, 0, cells_ * sizeof(float4), stream), err) &&
+           check("clear config transmittance", cudaMemsetAsync(cfgLight_, 0, lightCells * sizeof(float), stream), err);
+}
+
+// The config physics on the frame's stage ids: advect velocity, advect +
+// react + emit, forces (vorticity, cell accelerations, faces with the walls),
+// divergence, SOR, subtract, transmittance, raymarch, camera response,
+// metrics, reset.  VELOCITY_BOUNDARY, LIGHT_PROPAGATE, EMBERS and OVERLAY have
+// no counterpart here and do nothing.
+bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::string& err) {
+    if (!ensureConfigBuffers(err)) return false;
+    const int bx = rowThreads(nx);
+    const int bxFace = rowThreads(nx + 1);
+    const dim3 cells = cellGrid(bx, nx, ny, nz);
+    const dim3 faces = cellGrid(bxFace, nx + 1, ny + 1, nz + 1);
+    for (int s = first; s <= last; ++s) {
+        const ConfigParams c = configParams();
+        switch (s) {
+            case kAdvectVelocity:
+                cfgAdvectVelocity<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), c); ++launches_;
+                vcur_ = 1 - vcur_;
+                break;
+            case kAdvectReact:
+                cfgAdvectScalars<<<cells, bx, 0, stream>>>(sa_[1 - cur_], sa_[cur_], velocity(), c); ++launches_;
+                cur_ = 1 - cur_;
+                ++cfgStep_;
+                break;
+            case kForce:
+                if (c.eps != 0.0f) {
+                    cfgVorticity<<<cells, bx, 0, stream>>>(cfgVort_, velocity(), c); ++launches_;
+                }
+                cfgCellForce<<<cells, bx, 0, stream>>>(contrib_, cfgVort_, sa_[cur_], c); ++launches_;
+                cfgApplyForces<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), contrib_, c); ++launches_;
+                vcur_ = 1 - vcur_;
+                break;
+            case kDivergence:
+                divergenceOf<<<cells, bx, 0, stream>>>(divergence_, pressure_, velocity(), p); ++launches_;
+                break;
+            case kPressureSor:
+                if (!runSor(p, err)) return false;
+                break;
+            case kSubtract:
+                subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 1, last >= kWallBoundary ? 1 : 0); ++launches_;
+                if (last >= kWallBoundary) ++s;
+                break;
+            case kWallBoundary:
+                subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 0, 1); ++launches_;
+                break;
+            case kLightBuild: {
+                const int lbx = rowThreads(cfgLx_);
+                cfgTransmittance<<<dim3((cfgLx_ + lbx - 1) / lbx, cfgLy_, cfgLz_), lbx, 0, stream>>>(cfgLight_, sa_[cur_], c); ++launches_;
+                break;
+            }
+            case kRender:
+                cfgRaymarch<<<dim3((frameW + 15) / 16, (frameH + 7) / 8), dim3(16, 8), 0, stream>>>(hdr_, sa_[cur_], cfgLight_, c); ++launches_;
+                break;
+            case kTonemap:
+                tonemapOverlay<<<dim3((frameW + 15) / 16, (frameH + 15) / 16), dim3(16, 16), 0, stream>>>(bgra_, hdr_, p, 1, 0); ++launches_;
+                break;
+            case kMetrics:
+                if (!runMetrics(p, err)) return false;
+                break;
+            case kReset: {
+                bool ok = true;
+                for (int b = 0; b < 2 && ok; ++b) {
+                    ok = check("reset config scalars", cudaMemsetAsync(sa_[b], 0, cells_ * sizeof(Rec4), stream), err) &&
+                         check("reset config scalars", cudaMemsetAsync(sb_[b], 0, cells_ * sizeof(Rec4), stream), err) &&
+                         check("reset config scalars", cudaMemsetAsync(sc_[b], 0, cells_ * sizeof(Rec2), stream), err);
+                }
+                for (int f = 0; f < 3 && ok; ++f) {
+                    const size_t n = f == 0 ? nu_ : (f == 1 ? nv_ : nw_);
+                    ok = check("reset velocity", cudaMemsetAsync(vel_[f][0], 0, n * sizeof(FaceT), stream), err) &&
+                         check("reset velocity", cudaMemsetAsync(vel_[f][1], 0, n * sizeof(FaceT), stream), err);
+                }
+                ok = ok && check("reset pressure", cudaMemsetAsync(pressure_, 0, cells_ * sizeof(float), stream), err) &&
+                     check("reset divergence", cudaMemsetAsync(divergence_, 0, cells_ * sizeof(float), stream), err) &&
+                     check("reset divergence after", cudaMemsetAsync(divergenceAfter_, 0, cells_ * sizeof(float), stream), err) &&
+                     check("reset config transmittance",
+                           cudaMemsetAsync(cfgLight_, 0, static_cast<size_t>(cfgLx_) * cfgLy_ * cfgLz_ * sizeof(float), stream), err);
+                if (!ok) return false;
+                cfgStep_ = 0;
+                break;
+            }
+            default:
+                break;  // VELOCITY_BOUNDARY, LIGHT_PROPAGATE, EMBERS, OVERLAY
+        }
+        if (!check("config stage launch", cudaGetLastError(), err)) return false;
+    }
     return true;
 }
 

@@ -12,6 +12,7 @@
 #include <string>
 
 #include "../../include/fire_cuda.h"
+#include "../../include/fire_ext.h"
 #include "fire_kernels.h"
 
 namespace firesim {
@@ -30,6 +31,11 @@ struct MaterialKey {
     float burnerX0 = 0.0f, burnerZ0 = 0.0f;
     bool operator==(const MaterialKey& o) const;
 };
+
+// Defaults of FirePhysicsParams for a grid (fireCudaDefaultPhysicsParams).
+void defaultPhysicsParams(FirePhysicsParams& params, int nx, int ny, int nz);
+// Range and finiteness checks of fireCudaSetPhysicsParams.
+bool validatePhysicsParams(const FirePhysicsParams& params, std::string& err);
 
 class Scene {
 public:
@@ -71,6 +77,11 @@ public:
     bool pressureStats(int& iterations, float& maxResidual, double& l2Residual, std::string& err);
     // Hash lattices on (default) or off: off hashes every fbm corner in place (same bits, slower).
     void setHashLattices(bool enabled) { latticesEnabled_ = enabled; }
+    // Physics of the following passes (mode 0 reference, mode 1 config physics).
+    bool setPhysics(const FirePhysicsParams& params, std::string& err);
+    const FirePhysicsParams& physics() const { return physics_; }
+    // Steps of the config physics since the last reset (the emitter jitter's counter).
+    unsigned long long configStep() const { return cfgStep_; }
     bool synchronize(std::string& err);
     // After a host sync: fails once with "timed out" if a resident SOR wait ran out since the last check.
     bool checkSolverStatus(std::string& err);
@@ -167,6 +178,15 @@ private:
     int sorGraphLaunches_ = 0;
     int sorIterations_ = -1;
     float sorOmega_ = 0.0f;
+    // Config physics.
+    FirePhysicsParams physics_{};
+    float4* cfgVort_ = nullptr;   // vorticity (x, y, z, |omega|) per cell, allocated on first use
+    float* cfgLight_ = nullptr;   // transmittance to the point light, half resolution
+    int cfgLx_ = 0, cfgLy_ = 0, cfgLz_ = 0;
+    unsigned long long cfgStep_ = 0;
+    ConfigParams configParams() const;
+    bool ensureConfigBuffers(std::string& err);
+    bool runConfigStages(int first, int last, const FrameParams& p, std::string& err);
 };
 
 }  // namespace firesim

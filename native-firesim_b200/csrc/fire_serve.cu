@@ -94,6 +94,21 @@ extern "C" bool fireSceneSetPressureSolver(FireScene* scene, int iterations, flo
     return true;
 }
 
+extern "C" bool fireSceneSetPressureTolerance(FireScene* scene, double maxResidual, int checkEvery) {
+    if (scene == nullptr) return fail("Scene handle was null.");
+    std::string err;
+    if (!scene->scene->setPressureTolerance(maxResidual, checkEvery, err)) return fail(err);
+    return true;
+}
+
+extern "C" bool fireSceneSetPhysicsParams(FireScene* scene, const FirePhysicsParams* params) {
+    if (scene == nullptr) return fail("Scene handle was null.");
+    if (params == nullptr) return fail("Physics parameter pointer was null.");
+    std::string err;
+    if (!scene->scene->setPhysics(*params, err)) return fail(err);
+    return true;
+}
+
 extern "C" bool fireSceneSetHdrBuffer(FireScene* scene, void* devicePtr, size_t pitchBytes, int format) {
     if (scene == nullptr) return fail("Scene handle was null.");
     if (!useDevice(scene->device)) return false;

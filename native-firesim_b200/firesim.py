@@ -100,6 +100,11 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireCudaGetStream": (b, [ctypes.POINTER(ctypes.c_void_p)]),
         "fireCudaGetLaunchCount": (b, [ctypes.POINTER(ctypes.c_ulonglong)]),
         "fireCudaBuildInfo": (ctypes.c_char_p, []),
+        "fireCudaDefaultPhysicsParams": (None, [ctypes.POINTER(abi.FirePhysicsParams), ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "fireCudaSetPhysicsParams": (b, [ctypes.POINTER(abi.FirePhysicsParams)]),
+        "fireCudaGetPhysicsParams": (b, [ctypes.POINTER(abi.FirePhysicsParams)]),
+        "fireSceneSetPressureTolerance": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
+        "fireSceneSetPhysicsParams": (b, [ctypes.c_void_p, ctypes.POINTER(abi.FirePhysicsParams)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -187,7 +192,7 @@ class FireSim:
         self._check(self.lib.fireCudaSetPressureSolver(iterations, omega), "fireCudaSetPressureSolver")
 
     def set_pressure_path(self, path: int):
-        """0 automatic, 1 one launch per half sweep, 2 shared-memory-resident."""
+        """0 automatic, 1 colour-split (one launch per half sweep, as a graph), 2 shared-memory-resident."""
         self._check(self.lib.fireCudaSetPressurePath(path), "fireCudaSetPressurePath")
 
     def set_resident_sor_fault(self, silent_brick: int = -1, wait_us: int = 1_000_000):
@@ -204,12 +209,21 @@ class FireSim:
         self._check(self.lib.fireCudaGetPressureStats(ctypes.byref(it), ctypes.byref(mr), ctypes.byref(l2)), "fireCudaGetPressureStats")
         return it.value, mr.value, l2.value
 
+    def set_physics(self, params) -> None:
+        """FirePhysicsParams for the following passes (mode 1: config physics)."""
+        self._check(self.lib.fireCudaSetPhysicsParams(ctypes.byref(params)), "fireCudaSetPhysicsParams")
+
+    def physics(self):
+        p = abi.FirePhysicsParams()
+        self._check(self.lib.fireCudaGetPhysicsParams(ctypes.byref(p)), "fireCudaGetPhysicsParams")
+        return p
+
     def set_hash_lattices(self, enabled: bool):
         """Hash-lattice tables for the fbm fields on (default) or off (in-place hashing, same bits)."""
         self._check(self.lib.fireCudaSetHashLattices(1 if enabled else 0), "fireCudaSetHashLattices")
 
     def pressure_path_used(self) -> int:
-        """Path of the latest SOR solve: 0 none yet, 1 per-launch graph, 2 resident."""
+        """Path of the latest SOR solve: 0 none yet, 1 colour-split graph, 2 resident."""
         return int(self.lib.fireCudaGetPressurePathUsed())
 
     def shape_of(self, name: str):
@@ -219,6 +233,7 @@ class FireSim:
             "u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx),
             "scene_light": (lz, ly, lx, 4), "scene_shadow": (lz, ly, lx),
             "hdr": (self.frame_h, self.frame_w, 4), "bgra": (self.frame_h, self.frame_w),
+            "config_transmittance": ((nz + 1) // 2, (ny + 1) // 2, (nx + 1) // 2),
         }.get(name, (nz, ny, nx))
 
     def get(self, name: str) -> np.ndarray:
@@ -298,6 +313,12 @@ class Scene:
 
     def set_pressure_solver(self, iterations: int, omega: float):
         self._check(self.lib.fireSceneSetPressureSolver(self.h, iterations, omega), "fireSceneSetPressureSolver")
+
+    def set_pressure_tolerance(self, max_residual: float, check_every: int = 10):
+        self._check(self.lib.fireSceneSetPressureTolerance(self.h, max_residual, check_every), "fireSceneSetPressureTolerance")
+
+    def set_physics(self, params) -> None:
+        self._check(self.lib.fireSceneSetPhysicsParams(self.h, ctypes.byref(params)), "fireSceneSetPhysicsParams")
 
     def set_hdr_buffer(self, device_ptr: int, pitch_bytes: int, fmt: int = 0):
         self._check(self.lib.fireSceneSetHdrBuffer(self.h, device_ptr, pitch_bytes, fmt), "fireSceneSetHdrBuffer")

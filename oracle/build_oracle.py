@@ -17,8 +17,9 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_build"
 LIB = OUT / "libfire_oracle.so"
-SOURCES = [HERE / "fire_oracle.cpp"]
-HEADERS = [HERE / "fire_oracle.h", HERE.parent / "include" / "fire_cuda.h"]
+SOURCES = [HERE / "fire_oracle.cpp", HERE / "config_oracle.cpp"]
+HEADERS = [HERE / "fire_oracle.h", HERE / "config_oracle.h", HERE.parent / "include" / "fire_cuda.h",
+           HERE.parent / "include" / "fire_ext.h"]
 
 
 def build(verbose: bool = False) -> Path:

@@ -134,3 +134,92 @@ class OracleFire:
     def set_threads(n: int) -> None:
         if _LIB is not None:
             _LIB.oracle_set_threads(n)
+
+
+_CFG_READY = False
+
+
+def _cfg_lib(abi):
+    global _CFG_READY
+    L = lib(abi)
+    if not _CFG_READY:
+        P = ctypes.POINTER(abi.FirePhysicsParams)
+        L.cfg_oracle_create.restype = ctypes.c_void_p
+        L.cfg_oracle_create.argtypes = [ctypes.c_int] * 6
+        L.cfg_oracle_destroy.argtypes = [ctypes.c_void_p]
+        L.cfg_oracle_set_physics.argtypes = [ctypes.c_void_p, P]
+        L.cfg_oracle_set_pressure_solver.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
+        L.cfg_oracle_set_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
+        L.cfg_oracle_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
+        L.cfg_oracle_get_field_f64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
+        L.cfg_oracle_stages.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.cfg_oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cfg_oracle_step_count.restype = ctypes.c_ulonglong
+        L.cfg_oracle_step_count.argtypes = [ctypes.c_void_p]
+        L.cfg_oracle_last_error.restype = ctypes.c_char_p
+        _CFG_READY = True
+    return L
+
+
+class ConfigOracle:
+    """The config physics (FirePhysicsParams.mode 1) on the CPU, from an empty
+    scene. precision 'f32' (the product's rounding) or 'f64'."""
+
+    FIELDS = ("heat", "fuel", "soot", "pressure", "divergence", "u", "v", "w", "hdr", "config_transmittance")
+
+    def __init__(self, abi, frame_w: int, frame_h: int, nx: int, ny: int, nz: int, precision: str = "f32"):
+        self.abi = abi
+        self.lib = _cfg_lib(abi)
+        self.h = self.lib.cfg_oracle_create(0 if precision == "f32" else 1, frame_w, frame_h, nx, ny, nz)
+        if not self.h:
+            raise RuntimeError(self.lib.cfg_oracle_last_error().decode())
+        self.frame_w, self.frame_h = frame_w, frame_h
+        self.nx, self.ny, self.nz = nx, ny, nz
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.cfg_oracle_destroy(h)
+            self.h = None
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed: {self.lib.cfg_oracle_last_error().decode()}")
+
+    def shape_of(self, name: str):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        return {
+            "u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx),
+            "hdr": (self.frame_h, self.frame_w, 4),
+            "config_transmittance": ((nz + 1) // 2, (ny + 1) // 2, (nx + 1) // 2),
+        }.get(name, (nz, ny, nx))
+
+    def set_physics(self, params) -> None:
+        self._check(self.lib.cfg_oracle_set_physics(self.h, ctypes.byref(params)), "set_physics")
+
+    def set_pressure_solver(self, iterations: int, omega: float) -> None:
+        self.lib.cfg_oracle_set_pressure_solver(self.h, iterations, omega)
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape_of(name), dtype=np.float32)
+        self._check(self.lib.cfg_oracle_get_field(self.h, self.abi.FIELDS[name], out.ctypes.data, out.nbytes), f"get {name}")
+        return out
+
+    def get64(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape_of(name), dtype=np.float64)
+        self._check(self.lib.cfg_oracle_get_field_f64(self.h, self.abi.FIELDS[name], out.ctypes.data, out.size), f"get64 {name}")
+        return out
+
+    def set(self, name: str, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float32).reshape(self.shape_of(name))
+        self._check(self.lib.cfg_oracle_set_field(self.h, self.abi.FIELDS[name], a.ctypes.data, a.nbytes), f"set {name}")
+
+    def stages(self, first: str, last: str) -> None:
+        s = self.abi.STAGES
+        self._check(self.lib.cfg_oracle_stages(self.h, s[first], s[last]), f"stages {first}..{last}")
+
+    def step(self, render: bool = False) -> None:
+        self._check(self.lib.cfg_oracle_step(self.h, 1 if render else 0), "step")
+
+    def step_count(self) -> int:
+        return int(self.lib.cfg_oracle_step_count(self.h))
