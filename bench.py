@@ -379,6 +379,191 @@ def run_serve(args, pkg) -> None:
     print(json.dumps(line), flush=True)
 
 
+# Algorithmic bytes per cell of each config-physics stage (FP32 layout: record a
+# = heat, fuel, (unused), soot is 16 B; faces ~12 B; vorticity and force 16 B).
+CONFIG_STAGE_BYTES_PER_CELL = {
+    "advect_velocity": 24.0,                   # read + write the faces (gathers hit L1/L2)
+    "advect_react": 16.0 * 2 + 12.0,           # read + write record a, read the faces
+    "force": 12.0 + 16.0 + 16.0 * 3 + 12.0 * 2 + 16.0,  # vorticity w, cell force r/w, faces r/w
+    "divergence": 12.0 + 8.0,                  # read faces, write div and p
+    "pressure_sor": 6.0,                       # per half sweep
+    "subtract_walls": 4.0 + 24.0,
+}
+
+
+def config_stage_timings(sim, settings, iters: int = 3) -> dict:
+    import torch
+    ext = torch.cuda.ExternalStream(sim.stream())
+    ranges = {"advect_velocity": ("advect_velocity", "advect_velocity"), "advect_react": ("advect_react", "advect_react"),
+              "force": ("force", "velocity_boundary"), "divergence": ("divergence", "divergence"),
+              "pressure_sor": ("pressure_sor", "pressure_sor"), "subtract_walls": ("subtract", "wall_boundary"),
+              "light": ("light_build", "light_build"), "render": ("render", "render")}
+    out = {}
+    for name, (a, b) in ranges.items():
+        ms = []
+        for _ in range(iters):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(ext):
+                torch.cuda._sleep(400_000)
+            e0.record(ext)
+            sim.stages(a, b, settings, 0.0, wait=False)
+            e1.record(ext)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        sim.synchronize()
+        out[name] = min(ms)
+    return out
+
+
+def config_cpu_baseline(pkg, w, n_steps: int = 2) -> dict:
+    """The config-physics oracle (float, OpenMP, all host threads) on a bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as om  # noqa: PLC0415
+    abi = pkg.abi
+    n = w["grid"]
+    o = om.ConfigOracle(abi, w["frame"][0], w["frame"][1], *n)
+    o.set_physics(w["physics"])
+    o.set_pressure_solver(*w["sor"])
+    threads = os.cpu_count() or 1
+    om.OracleFire.set_threads(threads)
+    o.step()
+    t0 = time.perf_counter()
+    for _ in range(n_steps):
+        o.step()
+    t_sim = (time.perf_counter() - t0) / n_steps
+    t1 = time.perf_counter()
+    o.stages("light_build", "render")
+    t_render = time.perf_counter() - t1
+    per_step = t_sim + t_render / w["render_every"]
+    cells = int(np.prod(n))
+    return {"value": cells / per_step, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n_steps} config-physics steps of the {w['name']} workload after one warm-up step, plus one "
+                      f"{w['frame'][0]}^2 render amortised over {w['render_every']} steps (oracle/config_oracle.cpp, float)",
+            "seconds_per_step": per_step}
+
+
+def run_config(args, pkg, world: int, rank: int, local: int) -> None:
+    """One scene of the config physics (FirePhysicsParams mode 1) on workload c1, c2 or c3."""
+    import torch
+    abi = pkg.abi
+    w = abi.config_workload(args.workload)
+    precision = args.precision if args.precision_set else w["precision"]
+    n = w["grid"]
+    cells = int(np.prod(n))
+    fw, fh = w["frame"]
+    render_every = w["render_every"]
+    lib = pkg.load_library(precision)
+    if not lib.fireCudaSelectDevice(local):
+        raise RuntimeError(pkg.firesim.last_error(lib))
+    sim = pkg.FireSim(fw, fh, *n, precision=precision)
+    sim.set_physics(w["physics"])
+    sim.set_pressure_solver(*w["sor"])
+    if w["tolerance"] > 0:
+        sim.set_pressure_tolerance(w["tolerance"], w["check_every"])
+    sim.set_pressure_path({"auto": 0, "graph": 1, "resident": 2}[args.sor_path])
+    hdr = torch.zeros((fh, fw, 4), dtype=torch.float32, device="cuda")
+    sim.register_hdr_slot(0, hdr.data_ptr(), fw * 16, 0)
+    sim.set_hdr_slot(0)
+    ext = torch.cuda.ExternalStream(sim.stream())
+    settings = abi.FireSettings(width=fw, height=fh, dt=w["physics"].dt)
+    frame = 0
+
+    def one_step(host_bgra=None):
+        nonlocal frame
+        settings.reset = 1 if frame == 0 else 0
+        render = (frame % render_every) == render_every - 1
+        if host_bgra is not None and render:
+            if not lib.fireCudaStepAndRender(host_bgra.ctypes.data, settings):
+                raise RuntimeError(pkg.firesim.last_error(lib))
+        elif render:
+            sim.step_and_render_hdr(settings)
+        else:
+            sim.step(settings)
+        frame += 1
+
+    for _ in range(args.warmup):
+        one_step()
+    sim.synchronize()
+    sampler = ClockSampler(local)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = sim.launch_count()
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    marks[0].record(ext)
+    for i in range(args.steps):
+        one_step()
+        marks[i + 1].record(ext)
+    marks[-1].synchronize()
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clocks = sampler.stop()
+    launches = sim.launch_count() - launches0
+    step_ms = np.array([marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)])
+    device_s = dist_max(marks[0].elapsed_time(marks[-1]) / 1e3, world)
+    value = cells * args.steps * world / device_s
+    stats = sim.pressure_stats()
+
+    e2e = None
+    if not args.no_e2e:
+        host = np.zeros((fh, fw), dtype=np.uint32)
+        dist_barrier(world)
+        sim.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            one_step(host_bgra=host)
+        sim.synchronize()
+        wall = dist_max(time.perf_counter() - t0, world)
+        renders = sum(1 for f in range(frame - args.steps, frame) if f % render_every == render_every - 1)
+        e2e = {"value": cells * args.steps * world / wall, "unit": "voxel-steps/s",
+               "h2d_bytes_per_step": int(ctypes_sizeof_settings(abi)),
+               "d2h_bytes_per_step": int(renders * fw * fh * 4 / args.steps), "ms_per_step": wall * 1e3 / args.steps}
+
+    st = config_stage_timings(sim, settings)
+    per_step = {k: (v / render_every if k in ("light", "render") else v) for k, v in st.items()}
+    dominant = max((k for k in CONFIG_STAGE_BYTES_PER_CELL), key=per_step.get)
+    peaks, peak_src = measured_peaks()
+    iters = stats[0] if stats[1] >= 0 else w["sor"][0]
+    if dominant == "pressure_sor":
+        launches_per = 2 * iters
+        bytes_launch = CONFIG_STAGE_BYTES_PER_CELL["pressure_sor"] * cells
+        launch_ms = st["pressure_sor"] / launches_per
+    else:
+        bytes_launch = CONFIG_STAGE_BYTES_PER_CELL[dominant] * cells
+        launch_ms = st[dominant]
+    achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peak_src,
+                "bytes_per_launch": bytes_launch, "launch_ms": launch_ms}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = config_cpu_baseline(pkg, w)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        p = w["physics"]
+        line = {
+            "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": device_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if precision == "f32" else f"{precision}-storage/f32-arithmetic",
+            "data": "synthetic (seeded disk emitters, SplitMix64 jitter)",
+            "config": {"workload": f"config physics {w['name']}: {n[0]}^3, {p.emitterCount} disk emitter(s), SOR "
+                                   f"{w['sor'][0]} omega {w['sor'][1]}"
+                                   f"{' until max|r| <= %g' % w['tolerance'] if w['tolerance'] else ''}, "
+                                   f"{fw}x{fh} render every {render_every} steps ({p.primarySamples} samples, "
+                                   f"{p.lightSamples} light samples)",
+                       "grid": list(n), "physics": "config (FirePhysicsParams mode 1)", "sor_path": args.sor_path,
+                       "l2": "no flush", "parallelism": "replicas"},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "stage_ms": per_step,
+            "step_latency": {"unit": "ms", "p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                             "max": float(step_ms.max())},
+            "pressure_stats_last_step": {"iterations": stats[0], "max_residual": stats[1], "l2_residual": stats[2]},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,7 +579,11 @@ def main() -> int:
     ap.add_argument("--reference-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
+    ap.add_argument("--physics", default="reference", choices=["reference", "config"],
+                    help="reference: native-firesim's physics (the headline line); config: FirePhysicsParams mode 1")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"],
+                    help="config physics workload (abi.config_workload)")
+    ap.add_argument("--precision", default=None, choices=["f32", "f16", "bf16"],
                     help="storage of the transported fields: f32 (the reference's), f16 or bf16 (FP32 arithmetic)")
     ap.add_argument("--mode", default="single", choices=["single", "batched", "serve"],
                     help="single: the 128^3 scene (the headline line); batched: --scenes scenes per fireBatchStep; "
@@ -411,16 +600,29 @@ def main() -> int:
                     help="pressure SOR: per-launch half sweeps in a CUDA graph, one cooperative resident launch, or auto")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    args.precision_set = args.precision is not None
+    if args.precision is None:
+        args.precision = "f32"
 
     world, rank, local = dist_setup()
     if args.impl == "reference":
-        run_reference(args, world, rank)
+        if args.physics == "config":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "native-firesim has no config physics (disk "
+                                  "emitters, confinement, point light); its CPU restatement is this line's cpu_baseline"}),
+                      flush=True)
+        else:
+            run_reference(args, world, rank)
         dist_barrier(world)
         return 0
 
     import torch
     torch.cuda.set_device(local)
     pkg = load_package()
+    if args.physics == "config":
+        run_config(args, pkg, world, rank, local)
+        dist_barrier(world)
+        return 0
     if args.mode != "single":
         if rank == 0:
             if args.mode == "batched":

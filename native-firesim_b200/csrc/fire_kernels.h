@@ -60,7 +60,7 @@ struct SorGate {
     int pad;
     double l2Residual;   // sqrt(sum r^2), accumulated in FP64
 };
-constexpr int kResidualBlocks = 296;
+constexpr int kResidualBlocks = 592;  // 4 per SM; each warp takes whole rows
 constexpr int kResidualThreads = 256;
 constexpr unsigned kResidentMaxPolls = 1u << 24;
 constexpr int kMetricThreads = 128;

@@ -845,12 +845,15 @@ bool Scene::frame(uint32_t* hostBgra, const FireSettings& s, FireCudaFrameMetric
         if (!runStages(kAdvectVelocity, kAdvectVelocity, p, err) || !rec(kAfterVelocity)) return false;
         if (!runStages(kAdvectReact, kAdvectReact, p, err) || !rec(kAfterReaction)) return false;
         if (!runStages(kForce, kWallBoundary, p, err) || !rec(kAfterProjection) || !rec(kAfterSolve)) return false;
-        if (!runStages(kLightBuild, kLightPropagate, p, err) || !rec(kAfterLighting)) return false;
+        // The config physics builds its light (the point light's transmittance)
+        // only for a frame that is rendered.
+        if ((physics_.mode != 1 && !runStages(kLightBuild, kLightPropagate, p, err)) || !rec(kAfterLighting)) return false;
     }
     if (!render) {
         return true;
     }
     p.time = renderTime;
+    if (physics_.mode == 1 && !runStages(kLightBuild, kLightBuild, p, err)) return false;
     if (!runStages(kRender, kEmbers, p, err) || !rec(kAfterRaymarch)) return false;
     if (toHdrSlot) {
         const HdrSlot& slot = slots_[activeSlot_];

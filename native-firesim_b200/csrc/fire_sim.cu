@@ -592,19 +592,61 @@ __global__ void __launch_bounds__(256) sorSplitUnpack(float* __restrict__ pressu
     pressure[(z * s.ny + y) * s.nx + x] = __ldg(split + splitIdx(s, c, y, z, k));
 }
 
-// One colour of a half sweep on the split arrays.  Thread (t, y, z) owns the
-// four slots 4t..4t+3 of colour c in row (y, z): its own cells, their div and
-// the four other-colour rows above, below, behind and in front are one float4
-// each, and the x-neighbours are the other colour's float4 of the same row
-// shifted by one slot (sx = 0: left = slot k - 1, right = slot k; sx = 1: left
-// = slot k, right = slot k + 1), whose missing end is one scalar.  own and
-// other are the two colour halves of one split array: disjoint, and other is
-// read-only for the whole launch.  Per cell the arithmetic is the reference's
-// in the reference's order (src/fire_cuda.cu:1201-1227).
+// The four cells in slots k0..k0+3 of one colour-c row (y, z) of the split
+// arrays (own: this colour, other: the other colour, i: the row start + k0):
+// their values and the sums div + pL + pR + pD + pU + pB + pF, in the
+// reference's order (src/fire_cuda.cu:1201-1227), with Neumann walls (the cell
+// itself).  Own cells, their div and the four other-colour rows beside them
+// are one float4 each; the x-neighbours are the other colour's float4 of the
+// same row shifted by one slot (sx = 0: left = slot k - 1, right = slot k;
+// sx = 1: left = slot k, right = slot k + 1), whose missing end is one scalar.
+__device__ __forceinline__ void splitQuad(const float* __restrict__ own, const float* __restrict__ other, const float* __restrict__ div,
+                                          int i, int k0, int sx, int y, int z, const SplitGrid& s, float self[4], float sum[4]) {
+    const int plane = s.ny * s.P;
+    const float4 me = *reinterpret_cast<const float4*>(own + i);
+    const float4 mid = __ldg(reinterpret_cast<const float4*>(other + i));
+    const float4 dn = y == 0 ? me : __ldg(reinterpret_cast<const float4*>(other + i - s.P));
+    const float4 up = y == s.ny - 1 ? me : __ldg(reinterpret_cast<const float4*>(other + i + s.P));
+    const float4 bk = z == 0 ? me : __ldg(reinterpret_cast<const float4*>(other + i - plane));
+    const float4 ft = z == s.nz - 1 ? me : __ldg(reinterpret_cast<const float4*>(other + i + plane));
+    const float4 dv = __ldg(reinterpret_cast<const float4*>(div + i));
+    float edge = 0.0f;
+    if (sx == 0 && k0 > 0) edge = __ldg(other + i - 1);
+    if (sx == 1 && 2 * (k0 + 4) < s.nx) edge = __ldg(other + i + 4);
+    const float sv[4] = {me.x, me.y, me.z, me.w};
+    const float mv[4] = {mid.x, mid.y, mid.z, mid.w};
+    const float dnv[4] = {dn.x, dn.y, dn.z, dn.w};
+    const float upv[4] = {up.x, up.y, up.z, up.w};
+    const float bkv[4] = {bk.x, bk.y, bk.z, bk.w};
+    const float ftv[4] = {ft.x, ft.y, ft.z, ft.w};
+    const float dvv[4] = {dv.x, dv.y, dv.z, dv.w};
+    const int x0 = 2 * k0 + sx;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int x = x0 + 2 * j;
+        const float c = sv[j];
+        const float left = sx == 0 ? (j == 0 ? edge : mv[j - 1]) : mv[j];
+        const float right = sx == 0 ? mv[j] : (j == 3 ? edge : mv[j + 1]);
+        const float pL = x == 0 ? c : left;
+        const float pR = x == s.nx - 1 ? c : right;
+        const float pD = y == 0 ? c : dnv[j];
+        const float pU = y == s.ny - 1 ? c : upv[j];
+        const float pB = z == 0 ? c : bkv[j];
+        const float pF = z == s.nz - 1 ? c : ftv[j];
+        self[j] = c;
+        sum[j] = dvv[j] + pL + pR + pD + pU + pB + pF;
+    }
+}
+
+// One colour of a half sweep on the split arrays: thread (t, y, z) updates
+// the four slots 4t..4t+3 of colour c in row (y, z).  own and other are the
+// two colour halves of one split array: disjoint, and other is read-only for
+// the whole launch.
 __global__ void __launch_bounds__(128) sorSplitHalfSweep(float* __restrict__ own, const float* __restrict__ other,
                                                          const float* __restrict__ ownDiv, SplitGrid s, int c, float omega,
                                                          const int* skip) {
-    if (skip != nullptr && *reinterpret_cast<const volatile int*>(skip) != 0) return;
+    // The gate is written only between launches, so every SM may cache it.
+    if (skip != nullptr && __ldg(skip) != 0) return;
     const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
@@ -612,76 +654,52 @@ __global__ void __launch_bounds__(128) sorSplitHalfSweep(float* __restrict__ own
     const int sx = (c + y + z) & 1;
     const int x0 = 2 * k0 + sx;
     const int i = (z * s.ny + y) * s.P + k0;
-    const int plane = s.ny * s.P;
-    const float4 self = *reinterpret_cast<const float4*>(own + i);
-    const float4 mid = __ldg(reinterpret_cast<const float4*>(other + i));
-    const float4 dn = y == 0 ? self : __ldg(reinterpret_cast<const float4*>(other + i - s.P));
-    const float4 up = y == s.ny - 1 ? self : __ldg(reinterpret_cast<const float4*>(other + i + s.P));
-    const float4 bk = z == 0 ? self : __ldg(reinterpret_cast<const float4*>(other + i - plane));
-    const float4 ft = z == s.nz - 1 ? self : __ldg(reinterpret_cast<const float4*>(other + i + plane));
-    const float4 dv = __ldg(reinterpret_cast<const float4*>(ownDiv + i));
-    // The slot just outside the float4 on the side the shift needs, if it holds a cell.
-    float edge = 0.0f;
-    if (sx == 0 && k0 > 0) edge = __ldg(other + i - 1);
-    if (sx == 1 && 2 * (k0 + 4) < s.nx) edge = __ldg(other + i + 4);
-    const float sv[4] = {self.x, self.y, self.z, self.w};
-    const float mv[4] = {mid.x, mid.y, mid.z, mid.w};
-    const float dnv[4] = {dn.x, dn.y, dn.z, dn.w};
-    const float upv[4] = {up.x, up.y, up.z, up.w};
-    const float bkv[4] = {bk.x, bk.y, bk.z, bk.w};
-    const float ftv[4] = {ft.x, ft.y, ft.z, ft.w};
-    const float dvv[4] = {dv.x, dv.y, dv.z, dv.w};
-    float out[4];
+    float self[4], sum[4], out[4];
+    splitQuad(own, other, ownDiv, i, k0, sx, y, z, s, self, sum);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const int x = x0 + 2 * j;
-        const float me = sv[j];
-        const float left = sx == 0 ? (j == 0 ? edge : mv[j - 1]) : mv[j];
-        const float right = sx == 0 ? mv[j] : (j == 3 ? edge : mv[j + 1]);
-        const float pL = x == 0 ? me : left;
-        const float pR = x == s.nx - 1 ? me : right;
-        const float pD = y == 0 ? me : dnv[j];
-        const float pU = y == s.ny - 1 ? me : upv[j];
-        const float pB = z == 0 ? me : bkv[j];
-        const float pF = z == s.nz - 1 ? me : ftv[j];
-        const float projected = (dvv[j] + pL + pR + pD + pU + pB + pF) * (1.0f / 6.0f);
-        out[j] = x < s.nx ? me + omega * (projected - me) : me;
+        const float projected = sum[j] * (1.0f / 6.0f);
+        out[j] = x0 + 2 * j < s.nx ? self[j] + omega * (projected - self[j]) : self[j];
     }
     *reinterpret_cast<float4*>(own + i) = make_float4(out[0], out[1], out[2], out[3]);
 }
 
-// Residual of the split arrays, per block over a fixed set of cells (as sorResidualPartials).
+// Residual of the split arrays, as sorResidualPartials: each warp takes whole
+// rows (colour, y, z); lane l covers the slot groups 4l, 4l + 128, ... of a row.
 __global__ void __launch_bounds__(kResidualThreads) sorSplitResidualPartials(const float* __restrict__ split,
                                                                             const float* __restrict__ splitDiv, SplitGrid s,
                                                                             const SorGate* gate, double* __restrict__ partialSq,
                                                                             float* __restrict__ partialMax) {
     if (gate->converged) return;
-    __shared__ double sq[kResidualThreads];
-    __shared__ float mx[kResidualThreads];
-    const long long slots = 2ll * s.nz * s.ny * s.P;
+    const int lane = threadIdx.x & 31;
+    const int warps = kResidualThreads / 32;
+    const int rowsPerColour = s.ny * s.nz;
+    const int colour = s.nz * s.ny * s.P;
     double acc = 0.0;
     float m = 0.0f;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < slots;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int k = static_cast<int>(i % s.P);
-        const int y = static_cast<int>((i / s.P) % s.ny);
-        const int z = static_cast<int>((i / (static_cast<long long>(s.P) * s.ny)) % s.nz);
-        const int c = static_cast<int>(i / (static_cast<long long>(s.P) * s.ny * s.nz));
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < 2 * rowsPerColour; row += gridDim.x * warps) {
+        const int c = row / rowsPerColour;
+        const int yz = row - c * rowsPerColour;
+        const int y = yz % s.ny;
+        const int z = yz / s.ny;
         const int sx = (c + y + z) & 1;
-        const int x = 2 * k + sx;
-        if (x >= s.nx) continue;
-        const int o = 1 - c;
-        const float self = __ldg(split + i);
-        const float pL = x == 0 ? self : __ldg(split + splitIdx(s, o, y, z, k + sx - 1));
-        const float pR = x == s.nx - 1 ? self : __ldg(split + splitIdx(s, o, y, z, k + sx));
-        const float pD = y == 0 ? self : __ldg(split + splitIdx(s, o, y - 1, z, k));
-        const float pU = y == s.ny - 1 ? self : __ldg(split + splitIdx(s, o, y + 1, z, k));
-        const float pB = z == 0 ? self : __ldg(split + splitIdx(s, o, y, z - 1, k));
-        const float pF = z == s.nz - 1 ? self : __ldg(split + splitIdx(s, o, y, z + 1, k));
-        const float r = __fsub_rn(__ldg(splitDiv + i) + pL + pR + pD + pU + pB + pF, __fmul_rn(6.0f, self));
-        m = fmaxf(m, fabsf(r));
-        acc += static_cast<double>(r) * static_cast<double>(r);
+        const float* own = split + c * colour;
+        const float* other = split + (1 - c) * colour;
+        const float* dv = splitDiv + c * colour;
+        for (int k0 = 4 * lane; k0 < s.H; k0 += 128) {
+            float self[4], sum[4];
+            splitQuad(own, other, dv, yz * s.P + k0, k0, sx, y, z, s, self, sum);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (2 * (k0 + j) + sx >= s.nx || k0 + j >= s.H) continue;
+                const float r = __fsub_rn(sum[j], __fmul_rn(6.0f, self[j]));
+                m = fmaxf(m, fabsf(r));
+                acc += static_cast<double>(r) * static_cast<double>(r);
+            }
+        }
     }
+    __shared__ double sq[kResidualThreads];
+    __shared__ float mx[kResidualThreads];
     sq[threadIdx.x] = acc;
     mx[threadIdx.x] = m;
     __syncthreads();
@@ -1144,28 +1162,34 @@ __global__ void __launch_bounds__(kResidualThreads) sorResidualPartials(const fl
                                                                        const SorGate* gate, double* __restrict__ partialSq,
                                                                        float* __restrict__ partialMax) {
     if (gate->converged) return;
-    __shared__ double sq[kResidualThreads];
-    __shared__ float mx[kResidualThreads];
-    const long long cells = static_cast<long long>(g.nx) * g.ny * g.nz;
+    // Each warp takes whole rows (y, z); its lanes stride along x.  Every
+    // partial sums a fixed set of cells in a fixed order.
+    const int lane = threadIdx.x & 31;
+    const int warps = kResidualThreads / 32;
+    const int rows = g.ny * g.nz;
+    const int plane = g.nx * g.ny;
     double s = 0.0;
     float m = 0.0f;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < cells;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int x = static_cast<int>(i % g.nx);
-        const int y = static_cast<int>((i / g.nx) % g.ny);
-        const int z = static_cast<int>(i / (static_cast<long long>(g.nx) * g.ny));
-        const float self = __ldg(pressure + i);
-        const float pL = x > 0 ? __ldg(pressure + i - 1) : self;
-        const float pR = x < g.nx - 1 ? __ldg(pressure + i + 1) : self;
-        const float pD = y > 0 ? __ldg(pressure + i - g.nx) : self;
-        const float pU = y < g.ny - 1 ? __ldg(pressure + i + g.nx) : self;
-        const long long plane = static_cast<long long>(g.nx) * g.ny;
-        const float pB = z > 0 ? __ldg(pressure + i - plane) : self;
-        const float pF = z < g.nz - 1 ? __ldg(pressure + i + plane) : self;
-        const float r = __fsub_rn(__ldg(divergence + i) + pL + pR + pD + pU + pB + pF, __fmul_rn(6.0f, self));
-        m = fmaxf(m, fabsf(r));
-        s += static_cast<double>(r) * static_cast<double>(r);
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < rows; row += gridDim.x * warps) {
+        const int y = row % g.ny;
+        const int z = row / g.ny;
+        const float* pr = pressure + row * g.nx;
+        const float* dv = divergence + row * g.nx;
+        for (int x = lane; x < g.nx; x += 32) {
+            const float self = __ldg(pr + x);
+            const float pL = x > 0 ? __ldg(pr + x - 1) : self;
+            const float pR = x < g.nx - 1 ? __ldg(pr + x + 1) : self;
+            const float pD = y > 0 ? __ldg(pr + x - g.nx) : self;
+            const float pU = y < g.ny - 1 ? __ldg(pr + x + g.nx) : self;
+            const float pB = z > 0 ? __ldg(pr + x - plane) : self;
+            const float pF = z < g.nz - 1 ? __ldg(pr + x + plane) : self;
+            const float r = __fsub_rn(__ldg(dv + x) + pL + pR + pD + pU + pB + pF, __fmul_rn(6.0f, self));
+            m = fmaxf(m, fabsf(r));
+            s += static_cast<double>(r) * static_cast<double>(r);
+        }
     }
+    __shared__ double sq[kResidualThreads];
+    __shared__ float mx[kResidualThreads];
     sq[threadIdx.x] = s;
     mx[threadIdx.x] = m;
     __syncthreads();
@@ -1182,15 +1206,24 @@ __global__ void __launch_bounds__(kResidualThreads) sorResidualPartials(const fl
     }
 }
 
+// One warp: lane l sums partials l, l + 32, ... in order, then the lanes are
+// combined by a fixed butterfly; max |r| decides the gate.
 __global__ void sorResidualFinal(SorGate* gate, const double* __restrict__ partialSq, const float* __restrict__ partialMax, int partials,
                                  float tolerance, int chunkIterations) {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || gate->converged) return;
+    if (blockIdx.x != 0 || gate->converged) return;
+    const int lane = threadIdx.x;
     double s = 0.0;
     float m = 0.0f;
-    for (int b = 0; b < partials; ++b) {
+    for (int b = lane; b < partials; b += 32) {
         s += partialSq[b];
         m = fmaxf(m, partialMax[b]);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    if (lane != 0) return;
     gate->iterations += chunkIterations;
     gate->maxResidual = m;
     gate->l2Residual = sqrt(s);
