@@ -282,8 +282,11 @@ inline T trilinear(const T* f, int ex, int ey, int ez, int sx, int sy, T u, T v,
     auto at = [&](int x, int y, int z) { return f[(size_t(z) * sy + y) * sx + x]; };
     const T c000 = at(x0, y0, z0), c100 = at(x1, y0, z0), c010 = at(x0, y1, z0), c110 = at(x1, y1, z0);
     const T c001 = at(x0, y0, z1), c101 = at(x1, y0, z1), c011 = at(x0, y1, z1), c111 = at(x1, y1, z1);
-    return lerpf(lerpf(lerpf(c000, c100, tx), lerpf(c010, c110, tx), ty),
-                 lerpf(lerpf(c001, c101, tx), lerpf(c011, c111, tx), ty), tz);
+    // The reference's sm_100a build contracts each lerp a + (b - a) t into
+    // fma(b - a, t, a); with this form the velocity advection equals its
+    // output bit for bit (golden fixtures).
+    auto L = [](T a, T b, T t) { return std::fma(b - a, t, a); };
+    return L(L(L(c000, c100, tx), L(c010, c110, tx), ty), L(L(c001, c101, tx), L(c011, c111, tx), ty), tz);
 }
 
 template <class T> inline T sampleScalar(const T* f, const Params<T>& p, T u, T v, T w) {
@@ -509,7 +512,9 @@ template <class T> void stageReset(State<T>& s, const Params<T>& p) {
     std::fill(s.shadow.begin(), s.shadow.end(), F(0.0));
 }
 
-// src/fire_cuda.cu:880-932 -- semi-Lagrangian self-advection of the three face grids.
+// src/fire_cuda.cu:880-932 -- semi-Lagrangian self-advection of the three face
+// grids.  The backtrace f - vel * dt * 0.62 is one fused multiply-add in the
+// reference's build, fma(-(vel * dt), 0.62, f).
 template <class T> void stageAdvectVelocity(State<T>& s, const Params<T>& p) {
     std::vector<T> un(s.u.size()), vn(s.v.size()), wn(s.w.size());
     const T back = p.dt * T(kAdvectionScale);
@@ -526,8 +531,8 @@ template <class T> void stageAdvectVelocity(State<T>& s, const Params<T>& p) {
                 const T fu = T(static_cast<float>(x)) / T(static_cast<float>(p.nx));
                 const T fv = cellV(y, p), fw = cellW(z, p);
                 const V3<T> vel = sampleVelocity(s, p, fu, fv, fw);
-                un[o] = sampleU(s.u.data(), p, fu - vel.x * p.dt * T(kAdvectionScale),
-                                fv - vel.y * p.dt * T(kAdvectionScale), fw - vel.z * p.dt * T(kAdvectionScale)) *
+                un[o] = sampleU(s.u.data(), p, std::fma(-(vel.x * p.dt), T(kAdvectionScale), fu),
+                                std::fma(-(vel.y * p.dt), T(kAdvectionScale), fv), std::fma(-(vel.z * p.dt), T(kAdvectionScale), fw)) *
                         F(0.995);
             }
         }
@@ -545,8 +550,8 @@ template <class T> void stageAdvectVelocity(State<T>& s, const Params<T>& p) {
                 const T fv = T(static_cast<float>(y)) / T(static_cast<float>(p.ny));
                 const T fw = cellW(z, p);
                 const V3<T> vel = sampleVelocity(s, p, fu, fv, fw);
-                vn[o] = sampleV(s.v.data(), p, fu - vel.x * p.dt * T(kAdvectionScale),
-                                fv - vel.y * p.dt * T(kAdvectionScale), fw - vel.z * p.dt * T(kAdvectionScale)) *
+                vn[o] = sampleV(s.v.data(), p, std::fma(-(vel.x * p.dt), T(kAdvectionScale), fu),
+                                std::fma(-(vel.y * p.dt), T(kAdvectionScale), fv), std::fma(-(vel.z * p.dt), T(kAdvectionScale), fw)) *
                         F(0.996);
             }
         }
@@ -563,8 +568,8 @@ template <class T> void stageAdvectVelocity(State<T>& s, const Params<T>& p) {
                 const T fu = cellU(x, p), fv = cellV(y, p);
                 const T fw = T(static_cast<float>(z)) / T(static_cast<float>(p.nz));
                 const V3<T> vel = sampleVelocity(s, p, fu, fv, fw);
-                wn[o] = sampleW(s.w.data(), p, fu - vel.x * p.dt * T(kAdvectionScale),
-                                fv - vel.y * p.dt * T(kAdvectionScale), fw - vel.z * p.dt * T(kAdvectionScale)) *
+                wn[o] = sampleW(s.w.data(), p, std::fma(-(vel.x * p.dt), T(kAdvectionScale), fu),
+                                std::fma(-(vel.y * p.dt), T(kAdvectionScale), fv), std::fma(-(vel.z * p.dt), T(kAdvectionScale), fw)) *
                         F(0.995);
             }
         }
@@ -896,7 +901,10 @@ template <class T> void computeDivergence(const State<T>& s, const Params<T>& p,
 }
 
 // src/fire_cuda.cu:1201-1227 + loop :3280-3284 -- in-place red-black SOR,
-// Neumann walls through the clamped index map.
+// Neumann walls through the clamped index map.  The reference's sm_100a build
+// evaluates pressure + omega * (sum / 6 - pressure) as two fused multiply-adds,
+// fma(omega, fma(sum, 1/6, -p), p): every cell of a B200 half sweep matches
+// that form and none of the unfused ones, so the float oracle rounds it so.
 template <class T> void stagePressureSor(State<T>& s, const Params<T>& p) {
     T* pr = s.pressure.data();
     const T* div = s.divergence.data();
@@ -915,8 +923,8 @@ template <class T> void stagePressureSor(State<T>& s, const Params<T>& p) {
                         const T pU = pr[sIdx(p, x, y + 1, z)];
                         const T pB = pr[sIdx(p, x, y, z - 1)];
                         const T pF = pr[sIdx(p, x, y, z + 1)];
-                        const T projected = (div[idx] + pL + pR + pD + pU + pB + pF) * T(1.0f / 6.0f);
-                        pr[idx] = pr[idx] + omega * (projected - pr[idx]);
+                        const T sum = div[idx] + pL + pR + pD + pU + pB + pF;
+                        pr[idx] = std::fma(omega, std::fma(sum, T(1.0f / 6.0f), -pr[idx]), pr[idx]);
                     }
                 }
             }
