@@ -287,23 +287,41 @@ def scene_settings(abi, rng: SplitMix64, dims, frame_w: int, frame_h: int, radiu
     return s
 
 
+def config_scene_physics(abi, rng: SplitMix64, dims, seed: int, lib):
+    """A batched or served scene of the config physics: emitter centre uniform in
+    the middle half of the floor, radius U[4, 12] cells (at most a quarter of the
+    smaller floor edge), wind U[-0.5, 0.5] on x and on z, jitter seed `seed`."""
+    nx, ny, nz = dims
+    cx = rng.uniform(0.25, 0.75) * nx
+    cz = rng.uniform(0.25, 0.75) * nz
+    r = min(rng.uniform(4.0, 12.0), 0.25 * min(nx, nz))
+    return abi.config_scene(nx, ny, nz, cx, cz, r, rng.uniform(-0.5, 0.5), rng.uniform(-0.5, 0.5), seed, lib)
+
+
 def run_batched(args, pkg) -> None:
     """48 independent scenes of mixed sizes stepped together (fireBatchStep)."""
     import torch
     abi = pkg.abi
+    config = args.physics == "config"
+    precision = args.precision if args.precision_set or not config else "f16"
+    lib = pkg.load_library(precision)
     rng = SplitMix64(11)
     sizes = [(48, 48, 48), (64, 64, 64), (96, 96, 96), (128, 64, 64), (160, 96, 96)]
     dims = [sizes[rng.next() % len(sizes)] for _ in range(args.scenes)]
     scenes, settings, hdrs = [], [], []
-    for d in dims:
-        sc = pkg.Scene(256, 256, *d, precision=args.precision)
+    for i, d in enumerate(dims):
+        sc = pkg.Scene(256, 256, *d, precision=precision)
         sc.set_pressure_solver(40, 1.8)
         hdr = torch.zeros((256, 256, 4), dtype=torch.float32, device="cuda")
         sc.set_hdr_buffer(hdr.data_ptr(), 256 * 16, 0)
         scenes.append(sc)
         hdrs.append(hdr)
-        s = scene_settings(abi, rng, d, 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
-        s.raymarchSteps = 64
+        if config:
+            sc.set_physics(config_scene_physics(abi, rng, d, 1000 + i, lib))
+            s = abi.FireSettings(width=256, height=256, dt=1.0 / 60.0)
+        else:
+            s = scene_settings(abi, rng, d, 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
+            s.raymarchSteps = 64
         settings.append(s)
     voxels = sum(int(np.prod(d)) for d in dims)
 
@@ -325,10 +343,11 @@ def run_batched(args, pkg) -> None:
     wall = time.perf_counter() - t0
     line = {"metric": "voxel-steps/s", "mode": "batched", "value": voxels * args.steps / wall, "unit": "voxel-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_sub_step": wall * 1e3 / args.steps,
-            "higher_is_better": True, "dtype": args.precision, "data": "synthetic (SplitMix64 seed 11 draws)",
-            "config": {"workload": f"{args.scenes} independent scenes, sizes drawn from {sizes}, reference physics FP32, "
-                                   f"SOR 40 iterations omega 1.8, 256x256 render (64 samples) every {args.render_every} steps, "
-                                   "one fireBatchStep per sub-step, each scene on its own stream",
+            "higher_is_better": True, "dtype": precision, "data": "synthetic (SplitMix64 seed 11 draws)",
+            "config": {"workload": f"{args.scenes} independent scenes, sizes drawn from {sizes}, "
+                                   f"{'config physics (one disk emitter each, r U[4,12], wind U[-0.5,0.5]^2, seeds 1000+i)' if config else 'reference physics'}, "
+                                   f"{precision} storage, SOR 40 iterations omega 1.8, 256x256 render (64 samples) every "
+                                   f"{args.render_every} steps, one fireBatchStep per sub-step, each scene on its own stream",
                        "voxels_per_sub_step": voxels, "timing": "host wall clock around the sub-steps, synchronised on all scenes"}}
     print(json.dumps(line), flush=True)
     for sc in scenes:
@@ -338,8 +357,11 @@ def run_batched(args, pkg) -> None:
 def run_serve(args, pkg) -> None:
     """Poisson arrivals of scene requests into the FireServer loop."""
     abi = pkg.abi
+    config = args.physics == "config"
+    precision = args.precision if args.precision_set or not config else "bf16"
+    lib = pkg.load_library(precision)
     rng = SplitMix64(args.seed)
-    server = pkg.Server(budget_bytes=int(args.budget_gb * (1 << 30)), precision=args.precision)
+    server = pkg.Server(budget_bytes=int(args.budget_gb * (1 << 30)), precision=precision)
     server.set_limits(int(args.max_active_mvoxels * 1e6))
     t, n = 0.0, 0
     keep = []
@@ -356,15 +378,19 @@ def run_serve(args, pkg) -> None:
         r.renderEvery = 4
         r.sorIterations, r.sorOmega = 40, 1.8
         r.arrivalSeconds = t
-        r.settings = scene_settings(abi, rng, (edge, edge, edge), 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
-        r.settings.raymarchSteps = 64
+        if config:
+            r.settings = abi.FireSettings(width=256, height=256, dt=1.0 / 60.0)
+            r.physics = config_scene_physics(abi, rng, (edge, edge, edge), 5000 + n, lib)
+        else:
+            r.settings = scene_settings(abi, rng, (edge, edge, edge), 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
+            r.settings.raymarchSteps = 64
         server.submit(r)
         keep.append(r)
         n += 1
     rep = server.run(args.serve_seconds)
     server.close()
     line = {"metric": "voxel-steps/s", "mode": "serve", "value": rep["voxelSteps"] / max(rep["seconds"], 1e-9),
-            "unit": "voxel-steps/s", "n_gpus": 1, "higher_is_better": True, "dtype": args.precision, "data": "synthetic (SplitMix64 draws)",
+            "unit": "voxel-steps/s", "n_gpus": 1, "higher_is_better": True, "dtype": precision, "data": "synthetic (SplitMix64 draws)",
             "latency_ms": {"step_p50": rep["stepMsP50"], "step_p95": rep["stepMsP95"], "step_p99": rep["stepMsP99"],
                            "step_max": rep["stepMsMax"], "frame_p50": rep["frameMsP50"], "frame_p95": rep["frameMsP95"],
                            "frame_p99": rep["frameMsP99"], "queue_p50": rep["queueMsP50"], "queue_p99": rep["queueMsP99"]},
@@ -372,7 +398,8 @@ def run_serve(args, pkg) -> None:
             "device_bytes_peak": rep["deviceBytesPeak"], "seconds": rep["seconds"],
             "config": {"workload": f"Poisson arrivals at {args.rate}/s for {args.arrival_seconds} s; cubic edge log-normal "
                                    "(median 96, sigma 0.4) clamped to [32, 192], multiple of 16; steps U[30, 300]; "
-                                   "reference physics FP32, SOR 40; 256x256 render (64 samples) every 4 steps; "
+                                   f"{'config physics (per-request emitter, wind and seed)' if config else 'reference physics'}, "
+                                   f"{precision} storage, SOR 40; 256x256 render (64 samples) every 4 steps; "
                                    f"HBM budget {args.budget_gb} GB; at most {args.max_active_mvoxels} M active cells; "
                                    f"run bounded at {args.serve_seconds} s",
                        "latency": "device time between a scene's consecutive step completions, events on its stream"}}
@@ -619,7 +646,7 @@ def main() -> int:
     import torch
     torch.cuda.set_device(local)
     pkg = load_package()
-    if args.physics == "config":
+    if args.physics == "config" and args.mode == "single":
         run_config(args, pkg, world, rank, local)
         dist_barrier(world)
         return 0

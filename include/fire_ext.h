@@ -329,6 +329,8 @@ typedef struct FireServeRequest {
     FireSettings settings;      /* per-step settings (reset on the first step) */
     float* resultHeat;          /* optional host buffer (nx*ny*nz floats): final heat */
     float* resultHdr;           /* optional host buffer (frameW*frameH*4 floats): last frame */
+    FirePhysicsParams physics;  /* mode 1: the scene's config physics (validated at submit);
+                                   mode 0 (e.g. all zero): the reference's physics */
 } FireServeRequest;
 typedef struct FireServeReport {
     int submitted, completed, admittedPeak;

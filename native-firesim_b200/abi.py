@@ -113,31 +113,6 @@ CANONICAL = dict(cinematicMode=1, raymarchSteps=104, emberCount=176, exposure=0.
                  smokeDarkness=1.26, intensity=1.42, smoke=0.96, turbulence=1.34, renderDebugMode=0)
 
 
-class FireServeRequest(ctypes.Structure):
-    """include/fire_ext.h FireServeRequest."""
-    _fields_ = [
-        ("id", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
-        ("frameW", ctypes.c_int), ("frameH", ctypes.c_int), ("steps", ctypes.c_int), ("renderEvery", ctypes.c_int),
-        ("sorIterations", ctypes.c_int), ("sorOmega", ctypes.c_float), ("arrivalSeconds", ctypes.c_double),
-        ("settings", FireSettings), ("resultHeat", ctypes.c_void_p), ("resultHdr", ctypes.c_void_p),
-    ]
-
-
-class FireServeReport(ctypes.Structure):
-    """include/fire_ext.h FireServeReport."""
-    _fields_ = [
-        ("submitted", ctypes.c_int), ("completed", ctypes.c_int), ("admittedPeak", ctypes.c_int),
-        ("seconds", ctypes.c_double), ("voxelSteps", ctypes.c_double),
-        ("stepMsP50", ctypes.c_double), ("stepMsP95", ctypes.c_double), ("stepMsP99", ctypes.c_double),
-        ("stepMsMax", ctypes.c_double), ("frameMsP50", ctypes.c_double), ("frameMsP95", ctypes.c_double),
-        ("frameMsP99", ctypes.c_double), ("queueMsP50", ctypes.c_double), ("queueMsP99", ctypes.c_double),
-        ("deviceBytesPeak", ctypes.c_size_t),
-    ]
-
-    def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
-
-
 def validation_settings(frame: int, scene: int = 0, width: int = 960, height: int = 540,
                         pool_fire: bool = False, fire_scenes_dir=None) -> FireSettings:
     """FireSettings of frame `frame` of the reference's validation harness.
@@ -217,6 +192,32 @@ class FirePhysicsParams(ctypes.Structure):
         return out
 
 
+class FireServeRequest(ctypes.Structure):
+    """include/fire_ext.h FireServeRequest."""
+    _fields_ = [
+        ("id", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("frameW", ctypes.c_int), ("frameH", ctypes.c_int), ("steps", ctypes.c_int), ("renderEvery", ctypes.c_int),
+        ("sorIterations", ctypes.c_int), ("sorOmega", ctypes.c_float), ("arrivalSeconds", ctypes.c_double),
+        ("settings", FireSettings), ("resultHeat", ctypes.c_void_p), ("resultHdr", ctypes.c_void_p),
+        ("physics", FirePhysicsParams),
+    ]
+
+
+class FireServeReport(ctypes.Structure):
+    """include/fire_ext.h FireServeReport."""
+    _fields_ = [
+        ("submitted", ctypes.c_int), ("completed", ctypes.c_int), ("admittedPeak", ctypes.c_int),
+        ("seconds", ctypes.c_double), ("voxelSteps", ctypes.c_double),
+        ("stepMsP50", ctypes.c_double), ("stepMsP95", ctypes.c_double), ("stepMsP99", ctypes.c_double),
+        ("stepMsMax", ctypes.c_double), ("frameMsP50", ctypes.c_double), ("frameMsP95", ctypes.c_double),
+        ("frameMsP99", ctypes.c_double), ("queueMsP50", ctypes.c_double), ("queueMsP99", ctypes.c_double),
+        ("deviceBytesPeak", ctypes.c_size_t),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def default_physics(nx: int, ny: int, nz: int, lib=None) -> FirePhysicsParams:
     """fireCudaDefaultPhysicsParams (host only, needs no GPU)."""
     if lib is None:
@@ -230,6 +231,30 @@ def default_physics(nx: int, ny: int, nz: int, lib=None) -> FirePhysicsParams:
 def _disk(cx, cy, cz, r, seed, fuel=1.0, heat=1.0, up=2.0, jitter=0.2) -> FireEmitterDisk:
     return FireEmitterDisk(centerX=cx, centerY=cy, centerZ=cz, radius=r, fuel=fuel, heat=heat, upVelocity=up,
                            jitterScale=jitter, seed=seed)
+
+
+def _config_constants(p: FirePhysicsParams) -> FirePhysicsParams:
+    """The physics constants shared by every config workload."""
+    p.mode = 1
+    p.dt = 1.0 / 60.0
+    p.buoyancyHeat, p.buoyancySoot = 1.0, 0.1
+    p.burnRate, p.sootYield = 0.5, 0.3
+    p.vorticityEps = 0.3
+    return p
+
+
+def config_scene(nx: int, ny: int, nz: int, center_x: float, center_z: float, radius: float, wind_x: float,
+                 wind_z: float, seed: int, lib=None) -> FirePhysicsParams:
+    """One scene of the batched and served config workloads: the shared
+    constants, one disk emitter on row 2 (F = T = 1, upward 2 cells/step,
+    jitter 0.2 from `seed`), wind (wind_x, wind_z), 64 primary and 32 light
+    samples, the light above the grid's centre."""
+    p = _config_constants(default_physics(nx, ny, nz, lib))
+    p.emitterCount = 1
+    p.emitters[0] = _disk(center_x, 2, center_z, radius, seed)
+    p.windX, p.windZ = wind_x, wind_z
+    p.primarySamples, p.lightSamples = 64, 32
+    return p
 
 
 def config_workload(name: str, lib=None) -> dict:
@@ -253,12 +278,7 @@ def config_workload(name: str, lib=None) -> dict:
     if name not in sizes:
         raise ValueError(f"unknown config workload {name!r}: c1, c2 or c3")
     n = sizes[name]
-    p = default_physics(n, n, n, lib)
-    p.mode = 1
-    p.dt = 1.0 / 60.0
-    p.buoyancyHeat, p.buoyancySoot = 1.0, 0.1
-    p.burnRate, p.sootYield = 0.5, 0.3
-    p.vorticityEps = 0.3
+    p = _config_constants(default_physics(n, n, n, lib))
     w = dict(name=name, grid=(n, n, n), physics=p, tolerance=0.0, check_every=10, precision="f32")
     if name == "c1":
         p.emitterCount = 1

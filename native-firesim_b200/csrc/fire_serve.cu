@@ -251,6 +251,8 @@ extern "C" bool fireServerSubmit(FireServer* server, const FireServeRequest* req
     if (r.nx < 2 || r.ny < 2 || r.nz < 2 || r.frameW < 1 || r.frameH < 1 || r.steps < 1 || r.renderEvery < 0) {
         return fail("fireServerSubmit: invalid grid, frame, step count or render interval.");
     }
+    std::string err;
+    if (r.physics.mode != 0 && !firesim::validatePhysicsParams(r.physics, err)) return fail("fireServerSubmit: " + err);
     server->pending.push_back(r);
     return true;
 }
@@ -337,6 +339,13 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
             a->req = r;
             a->queued = 0;
             if (r.sorIterations > 0 && !a->scene->setPressureSolver(r.sorIterations, r.sorOmega, err)) {
+                ok = fail(err);
+                break;
+            }
+            // The request's physics; its first step resets the fields in that physics.
+            FirePhysicsParams physics = r.physics;
+            if (physics.mode == 0) firesim::defaultPhysicsParams(physics, r.nx, r.ny, r.nz);
+            if (!a->scene->setPhysics(physics, err)) {
                 ok = fail(err);
                 break;
             }

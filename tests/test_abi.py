@@ -85,3 +85,27 @@ def test_library_has_no_oracle_dependency():
     for src in (ROOT / "native-firesim_b200").rglob("*"):
         if src.suffix in (".cu", ".cuh", ".h", ".py", ".cpp"):
             assert "oracle" not in src.read_text().lower(), src
+
+
+@pytest.mark.parametrize("struct", ["FireSettings", "FireCudaFrameMetrics", "FireEmitterDisk", "FirePhysicsParams",
+                                    "FireServeRequest", "FireServeReport"])
+def test_struct_offsets_match_the_header(abi, struct, tmp_path):
+    """Every field of the ctypes mirror sits at the offset g++ gives it from include/*.h."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("g++ not found")
+    cls = getattr(abi, struct)
+    lines = [f'std::printf("size %zu\\n", sizeof({struct}));']
+    for name, _ in cls._fields_:
+        lines.append(f'std::printf("{name} %zu\\n", offsetof({struct}, {name}));')
+    src = tmp_path / "probe.cpp"
+    src.write_text('#include <cstddef>\n#include <cstdio>\n#include "fire_ext.h"\nint main() {\n' + "\n".join(lines) +
+                   "\nreturn 0;\n}\n")
+    exe = tmp_path / "probe"
+    subprocess.run([cxx, "-std=c++17", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines())
+    assert int(got["size"]) == ctypes.sizeof(cls)
+    for name, _ in cls._fields_:
+        assert int(got[name]) == getattr(cls, name).offset, name

@@ -170,3 +170,52 @@ def test_server_pool_and_voxel_limit(pkg, abi):
         alone = _alone(pkg, abi, (r.nx, r.ny, r.nz), r.steps, 4, settings=per_step)
         got = heats[i] if i < 8 else heat_again
         np.testing.assert_array_equal(got.view(np.uint32), alone["heat"].view(np.uint32), err_msg=f"request {i}")
+
+
+def test_server_config_physics_equals_alone(pkg, abi):
+    """Requests that carry config physics (one disk emitter each, their own
+    seeds and wind) mixed with reference-physics requests: each served result
+    equals the same scene stepped alone, and the pooled scenes switch physics
+    between requests."""
+    import torch
+    server = pkg.Server(budget_bytes=64 << 30)
+    reqs, heats = [], []
+    for i in range(5):
+        dims = SIZES[i % 2]
+        r = _request(abi, i, dims, steps=8, arrival=0.01 * i, scene=0)
+        if i % 2 == 0:
+            r.physics = abi.config_scene(*dims, dims[0] / 2 + i, dims[2] / 2, 4.0 + i, 0.3, -0.2, 100 + i)
+            r.settings = abi.FireSettings(width=64, height=48, dt=1.0 / 60.0)
+        heat = np.zeros(dims[::-1], dtype=np.float32)
+        r.resultHeat = heat.ctypes.data
+        reqs.append(r)
+        heats.append(heat)
+        server.submit(r)
+    rep = server.run(60.0)
+    server.close()
+    assert rep["completed"] == 5
+    for i, r in enumerate(reqs):
+        dims = SIZES[i % 2]
+        sc = pkg.Scene(64, 48, *dims)
+        hdr = torch.zeros((48, 64, 4), dtype=torch.float32, device="cuda")
+        sc.set_hdr_buffer(hdr.data_ptr(), 64 * 16, 0)
+        if r.physics.mode == 1:
+            sc.set_physics(r.physics)
+        for f in range(r.steps):
+            s = abi.FireSettings.from_buffer_copy(r.settings)
+            s.reset = 1 if f == 0 else 0
+            sc.step(s, render=f % 4 == 3)
+        alone = sc.get("heat")
+        sc.close()
+        np.testing.assert_array_equal(heats[i].view(np.uint32), alone.view(np.uint32), err_msg=f"request {i}")
+        assert heats[i].sum() > 0.0
+
+
+def test_server_rejects_invalid_physics(pkg, abi):
+    server = pkg.Server(budget_bytes=1 << 30)
+    r = _request(abi, 0, SIZES[0], steps=2, arrival=0.0, scene=0)
+    r.physics = abi.config_scene(*SIZES[0], 10.0, 10.0, 3.0, 0.0, 0.0, 1)
+    r.physics.lightSamples = 0
+    with pytest.raises(pkg.firesim.FireSimError, match="sample counts"):
+        server.submit(r)
+    server.close()
