@@ -136,8 +136,8 @@ FIRE_API bool fireCudaSetPressureTolerance(double maxResidual, int checkEvery);
  * for the scene's stream); after a fixed-count solve: the count and -1. */
 FIRE_API bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Residual);
 
-/* Path the latest SOR solve took: 0 = none yet (or no grid), 1 = colour-split,
- * 2 = shared-memory-resident. */
+/* Path the latest pressure solve took: 0 = none yet (or no grid),
+ * 1 = colour-split SOR, 2 = shared-memory-resident SOR, 3 = multigrid. */
 FIRE_API int fireCudaGetPressurePathUsed(void);
 
 /* Failure detection of the shared-memory-resident SOR (no counterpart in the
@@ -266,7 +266,17 @@ typedef struct FirePhysicsParams {
     float lightX, lightY, lightZ, lightIntensity;
     float extinction, fuelExtinction, emission, albedo;
     float eyeX, eyeY, eyeZ, targetX, targetY, targetZ, fovYDegrees;
+    int pressureTop;                 /* 0: Neumann (the reference's); 1: p = 0 above the top row
+                                        (needs the multigrid solver, fireCudaSetPressureMultigrid) */
 } FirePhysicsParams;
+
+/* Multigrid pressure solve (config physics with pressureTop = 1): up to
+ * maxCycles V-cycles per step, each with preSmooth / postSmooth red-black
+ * Gauss-Seidel sweeps per level (1..8); with fireCudaSetPressureTolerance
+ * set, the level-0 residual is checked after every cycle and the solve stops
+ * once max |r| <= tolerance (fireCudaGetPressureStats counts cycles).
+ * maxCycles = 0 restores the red-black SOR. */
+FIRE_API bool fireCudaSetPressureMultigrid(int maxCycles, int preSmooth, int postSmooth);
 
 /* The defaults: mode 0; for mode 1 the reference's buoyancy constants (1.62
  * heat, 0.095 soot, src/fire_cuda.cu:1176), no wind, noise or emitters, and a
@@ -296,6 +306,7 @@ FIRE_API bool fireSceneSetPressureSolver(FireScene* scene, int iterations, float
 /* As fireCudaSetPressureTolerance / fireCudaSetPhysicsParams, for one scene. */
 FIRE_API bool fireSceneSetPressureTolerance(FireScene* scene, double maxResidual, int checkEvery);
 FIRE_API bool fireSceneSetPhysicsParams(FireScene* scene, const FirePhysicsParams* params);
+FIRE_API bool fireSceneSetPressureMultigrid(FireScene* scene, int maxCycles, int preSmooth, int postSmooth);
 /* Caller-owned device HDR buffer the scene renders into (as fireCudaRegisterHdrBufferSlot). */
 FIRE_API bool fireSceneSetHdrBuffer(FireScene* scene, void* devicePtr, size_t pitchBytes, int format);
 /* Queues one step (render = 0) or one step and a render into the HDR buffer

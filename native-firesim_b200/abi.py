@@ -183,7 +183,8 @@ class FirePhysicsParams(ctypes.Structure):
     _fields_ = ([("mode", ctypes.c_int)] + [(n, ctypes.c_float) for n in _PHYSICS_FLOATS_A] +
                 [("noiseSeed", ctypes.c_uint32), ("emitterCount", ctypes.c_int),
                  ("emitters", FireEmitterDisk * MAX_EMITTERS), ("primarySamples", ctypes.c_int),
-                 ("lightSamples", ctypes.c_int)] + [(n, ctypes.c_float) for n in _PHYSICS_FLOATS_B])
+                 ("lightSamples", ctypes.c_int)] + [(n, ctypes.c_float) for n in _PHYSICS_FLOATS_B] +
+                [("pressureTop", ctypes.c_int)])
 
     def as_dict(self) -> dict:
         out = {n: getattr(self, n) for n, _ in self._fields_ if n != "emitters"}

@@ -29,9 +29,10 @@ VARIANTS = {
 INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr"]
-# Per-file flags: the config-physics kernels round every product and sum as
-# written (no FMA contraction), so their CPU restatement can match them bit for bit.
-FILE_FLAGS = {"fire_config.cu": ["-fmad=false"]}
+# Per-file flags: the config-physics and multigrid kernels round every product
+# and sum as written (no FMA contraction), so their CPU restatement can match
+# them bit for bit.
+FILE_FLAGS = {"fire_config.cu": ["-fmad=false"], "fire_mg.cu": ["-fmad=false"]}
 
 
 def _nvcc() -> str:

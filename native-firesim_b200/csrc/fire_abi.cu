@@ -226,6 +226,13 @@ bool fireCudaSetPhysicsParams(const FirePhysicsParams* params) {
     return true;
 }
 
+bool fireCudaSetPressureMultigrid(int maxCycles, int preSmooth, int postSmooth) {
+    if (!requireScene()) return false;
+    std::string err;
+    if (!g_scene->setPressureMultigrid(maxCycles, preSmooth, postSmooth, err)) return fail(err);
+    return true;
+}
+
 bool fireCudaGetPhysicsParams(FirePhysicsParams* params) {
     if (!requireScene()) return false;
     if (params == nullptr) return fail("Physics parameter pointer was null.");

@@ -193,4 +193,21 @@ __global__ void cfgApplyForces(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity v
 __global__ void cfgTransmittance(float* tr, const Rec4* a, ConfigParams p);
 __global__ void cfgRaymarch(float4* hdr, const Rec4* a, const float* tr, ConfigParams p);
 
+// ---------------------------------------------------------------------------
+// Multigrid pressure solve of the config physics (fire_mg.cu).
+// A level: extents, axis weights 1/h^2 (fine spacing 1), 2 (wx + wy + wz) and
+// its reciprocal, and which axes were halved from the level above.
+struct MgLevel {
+    int nx, ny, nz;
+    float wx, wy, wz, diag, invDiag;
+    int cx, cy, cz;
+};
+__global__ void mgSmooth(float* p, const float* rhs, MgLevel L, int colour, const int* skip);
+__global__ void mgRestrict(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);
+__global__ void mgProlong(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip);
+__global__ void mgCoarsest(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
+__global__ void mgResidualPartials(const float* p, const float* rhs, MgLevel L, const SorGate* gate, double* partialSq, float* partialMax);
+__global__ void cfgTopFaces(FaceT* v, const float* p, int nx, int ny, int nz);
+constexpr int kMgCoarsestSweeps = 32;
+
 }  // namespace firesim

@@ -1,0 +1,178 @@
+// fire_mg.cu -- geometric multigrid for the pressure equation of the config
+// physics with a Dirichlet top (p = 0 on the top face).
+//
+// Level equation: sum over axes a of w_a (2p - p_a- - p_a+) = rhs, with
+// Neumann walls and floor (a missing neighbour is the cell itself) and an
+// antisymmetric ghost above the top row (-p), which keeps the boundary on the
+// top face at every level.  Level 0 is the grid with w = (1, 1, 1) and rhs =
+// the projection's divergence array (-div u).  Level l + 1 halves every axis
+// whose extent is even and at least 4 (semi-coarsening keeps odd extents) and
+// divides that axis's weight by 4 (the doubled spacing squared).  A V-cycle:
+// pre-smoothing (red-black Gauss-Seidel), the residual averaged onto the
+// coarse cells, the coarse correction from zero, its cell-centred
+// interpolation (3/4, 1/4 along each halved axis, neighbours clamped) added
+// back, post-smoothing; the coarsest level is relaxed by one block.  After
+// each cycle the level-0 residual is reduced into the solve's gate
+// (sorResidualFinal); once max |r| is within the tolerance every later kernel
+// of the solve returns at once.
+//
+// Compiled with -fmad=false: every operation rounds as written, so a CPU
+// restatement in the same order gives the same bits.
+#include "fire_kernels.h"
+
+namespace firesim {
+
+namespace {
+
+__device__ __forceinline__ int mgAt(const MgLevel& L, int x, int y, int z) { return (z * L.ny + y) * L.nx + x; }
+
+__device__ __forceinline__ bool skipped(const int* skip) { return skip != nullptr && __ldg(skip) != 0; }
+
+// rhs + wx (pL + pR) + wy (pD + pU) + wz (pB + pF) for cell (x, y, z) with the boundary rules.
+__device__ __forceinline__ float weightedSum(const float* p, const float* rhs, const MgLevel& L, int x, int y, int z, float self) {
+    const int i = mgAt(L, x, y, z);
+    const float pL = x > 0 ? p[i - 1] : self;
+    const float pR = x < L.nx - 1 ? p[i + 1] : self;
+    const float pD = y > 0 ? p[i - L.nx] : self;
+    const float pU = y < L.ny - 1 ? p[i + L.nx] : 0.0f - self;
+    const float pB = z > 0 ? p[i - L.nx * L.ny] : self;
+    const float pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
+    return rhs[i] + L.wx * (pL + pR) + L.wy * (pD + pU) + L.wz * (pB + pF);
+}
+
+__device__ __forceinline__ float residualAt(const float* p, const float* rhs, const MgLevel& L, int x, int y, int z) {
+    const float self = p[mgAt(L, x, y, z)];
+    return weightedSum(p, rhs, L, x, y, z, self) - L.diag * self;
+}
+
+}  // namespace
+
+// One colour of red-black Gauss-Seidel: cells with (x + y + z) % 2 == colour.
+__global__ void __launch_bounds__(128) mgSmooth(float* __restrict__ p, const float* __restrict__ rhs, MgLevel L, int colour,
+                                                const int* skip) {
+    if (skipped(skip)) return;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((colour + y + z) & 1);
+    if (x >= L.nx) return;
+    const int i = mgAt(L, x, y, z);
+    p[i] = weightedSum(p, rhs, L, x, y, z, p[i]) * L.invDiag;
+}
+
+// Coarse rhs = the mean residual of the covered fine cells (averaged along x,
+// then y, then z over the halved axes), coarse p = 0.
+__global__ void __launch_bounds__(128) mgRestrict(float* __restrict__ rhsC, float* __restrict__ pC, const float* __restrict__ p,
+                                                  const float* __restrict__ rhs, MgLevel F, MgLevel C, const int* skip) {
+    if (skipped(skip)) return;
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y;
+    const int Z = blockIdx.z;
+    if (X >= C.nx) return;
+    const int x0 = C.cx ? 2 * X : X, y0 = C.cy ? 2 * Y : Y, z0 = C.cz ? 2 * Z : Z;
+    float az[2];
+    for (int dz = 0; dz <= C.cz; ++dz) {
+        float ay[2];
+        for (int dy = 0; dy <= C.cy; ++dy) {
+            const float r0 = residualAt(p, rhs, F, x0, y0 + dy, z0 + dz);
+            ay[dy] = C.cx ? 0.5f * (r0 + residualAt(p, rhs, F, x0 + 1, y0 + dy, z0 + dz)) : r0;
+        }
+        az[dz] = C.cy ? 0.5f * (ay[0] + ay[1]) : ay[0];
+    }
+    const int c = mgAt(C, X, Y, Z);
+    rhsC[c] = C.cz ? 0.5f * (az[0] + az[1]) : az[0];
+    pC[c] = 0.0f;
+}
+
+// p += the coarse correction interpolated along the halved axes (weights 3/4
+// and 1/4, neighbour clamped; weights 1 and 0 along kept axes), x, then y, then z.
+__global__ void __launch_bounds__(128) mgProlong(float* __restrict__ p, const float* __restrict__ pC, MgLevel F, MgLevel C,
+                                                 const int* skip) {
+    if (skipped(skip)) return;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= F.nx) return;
+    const int X0 = C.cx ? x >> 1 : x, Y0 = C.cy ? y >> 1 : y, Z0 = C.cz ? z >> 1 : z;
+    const int X1 = !C.cx ? X0 : ((x & 1) ? min(X0 + 1, C.nx - 1) : max(X0 - 1, 0));
+    const int Y1 = !C.cy ? Y0 : ((y & 1) ? min(Y0 + 1, C.ny - 1) : max(Y0 - 1, 0));
+    const int Z1 = !C.cz ? Z0 : ((z & 1) ? min(Z0 + 1, C.nz - 1) : max(Z0 - 1, 0));
+    const float ux = C.cx ? 0.75f : 1.0f, vx = C.cx ? 0.25f : 0.0f;
+    const float uy = C.cy ? 0.75f : 1.0f, vy = C.cy ? 0.25f : 0.0f;
+    const float uz = C.cz ? 0.75f : 1.0f, vz = C.cz ? 0.25f : 0.0f;
+    const float a0 = ux * pC[mgAt(C, X0, Y0, Z0)] + vx * pC[mgAt(C, X1, Y0, Z0)];
+    const float a1 = ux * pC[mgAt(C, X0, Y1, Z0)] + vx * pC[mgAt(C, X1, Y1, Z0)];
+    const float a2 = ux * pC[mgAt(C, X0, Y0, Z1)] + vx * pC[mgAt(C, X1, Y0, Z1)];
+    const float a3 = ux * pC[mgAt(C, X0, Y1, Z1)] + vx * pC[mgAt(C, X1, Y1, Z1)];
+    const float b0 = uy * a0 + vy * a1, b1 = uy * a2 + vy * a3;
+    const int i = mgAt(F, x, y, z);
+    p[i] = p[i] + (uz * b0 + vz * b1);
+}
+
+// The coarsest level: `sweeps` red-black Gauss-Seidel iterations by one block.
+__global__ void __launch_bounds__(256) mgCoarsest(float* __restrict__ p, const float* __restrict__ rhs, MgLevel L, int sweeps,
+                                                  const int* skip) {
+    if (skipped(skip)) return;
+    const int cells = L.nx * L.ny * L.nz;
+    for (int s = 0; s < sweeps; ++s) {
+        for (int colour = 0; colour < 2; ++colour) {
+            for (int i = threadIdx.x; i < cells; i += blockDim.x) {
+                const int x = i % L.nx;
+                const int y = (i / L.nx) % L.ny;
+                const int z = i / (L.nx * L.ny);
+                if (((x + y + z) & 1) != colour) continue;
+                p[i] = weightedSum(p, rhs, L, x, y, z, p[i]) * L.invDiag;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Level-0 residual r = (weighted neighbour sum) - 6p with the Dirichlet top,
+// per block over whole rows (as sorResidualPartials).
+__global__ void __launch_bounds__(kResidualThreads) mgResidualPartials(const float* __restrict__ p, const float* __restrict__ rhs, MgLevel L,
+                                                                       const SorGate* gate, double* __restrict__ partialSq,
+                                                                       float* __restrict__ partialMax) {
+    if (gate->converged) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = kResidualThreads / 32;
+    double s = 0.0;
+    float m = 0.0f;
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < L.ny * L.nz; row += gridDim.x * warps) {
+        const int y = row % L.ny;
+        const int z = row / L.ny;
+        for (int x = lane; x < L.nx; x += 32) {
+            const float r = residualAt(p, rhs, L, x, y, z);
+            m = fmaxf(m, fabsf(r));
+            s += static_cast<double>(r) * static_cast<double>(r);
+        }
+    }
+    __shared__ double sq[kResidualThreads];
+    __shared__ float mx[kResidualThreads];
+    sq[threadIdx.x] = s;
+    mx[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kResidualThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sq[threadIdx.x] += sq[threadIdx.x + w];
+            mx[threadIdx.x] = fmaxf(mx[threadIdx.x], mx[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partialSq[blockIdx.x] = sq[0];
+        partialMax[blockIdx.x] = mx[0];
+    }
+}
+
+// The top faces under a Dirichlet top: v(x, ny, z) -= (ghost - p) with the
+// antisymmetric ghost -p of the top cell.
+__global__ void __launch_bounds__(128) cfgTopFaces(FaceT* __restrict__ v, const float* __restrict__ p, int nx, int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y;
+    if (x >= nx) return;
+    const int face = (z * (ny + 1) + ny) * nx + x;
+    const float top = p[(z * ny + ny - 1) * nx + x];
+    stv(v + face, ldv(v + face) - ((0.0f - top) - top));
+}
+
+}  // namespace firesim

@@ -64,6 +64,16 @@ void Scene::release() {
         cudaGraphExecDestroy(sorExec_);
         sorExec_ = nullptr;
     }
+    if (mgExec_ != nullptr) {
+        cudaGraphExecDestroy(mgExec_);
+        mgExec_ = nullptr;
+    }
+    for (float* b : mgP_) cudaFree(b);
+    for (float* b : mgRhs_) cudaFree(b);
+    mgP_.clear();
+    mgRhs_.clear();
+    mgLevels_.clear();
+    mgKeyCycles_ = -1;
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
                     shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_,
@@ -422,6 +432,18 @@ bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
 // one CUDA graph per solve.
 bool Scene::runSor(const FrameParams& p, std::string& err) {
     (void)p;
+    const bool dirichletTop = physics_.mode == 1 && physics_.pressureTop == 1;
+    if (mgCycles_ > 0 || dirichletTop) {
+        if (!dirichletTop) {
+            err = "multigrid pressure solve needs the config physics with a Dirichlet top (FirePhysicsParams.pressureTop = 1)";
+            return false;
+        }
+        if (mgCycles_ == 0) {
+            err = "a Dirichlet top needs the multigrid pressure solve (fireCudaSetPressureMultigrid)";
+            return false;
+        }
+        return runMultigrid(err);
+    }
     if (pressureIterations == 0) return true;
     if (pressurePath_ != 1) {
         ResidentBrick r;
@@ -532,6 +554,122 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
     lastSolveGated_ = gated;
     lastPressurePath_ = 1;
     return check("SOR graph launch", cudaGraphLaunch(sorExec_, stream), err);
+}
+
+bool Scene::setPressureMultigrid(int maxCycles, int preSmooth, int postSmooth, std::string& err) {
+    if (maxCycles < 0 || maxCycles > 1000 || preSmooth < 1 || preSmooth > 8 || postSmooth < 1 || postSmooth > 8) {
+        err = "multigrid: maxCycles must be in 0..1000 and the smoothing sweeps in 1..8";
+        return false;
+    }
+    mgCycles_ = maxCycles;
+    mgPre_ = preSmooth;
+    mgPost_ = postSmooth;
+    return true;
+}
+
+// V-cycles of the multigrid solve (fire_mg.cu), captured once per (cycles,
+// smoothing, tolerance) into a CUDA graph; with a tolerance every cycle ends
+// with the level-0 residual check of the solve's gate.
+bool Scene::runMultigrid(std::string& err) {
+    if (mgLevels_.empty()) {
+        auto withWeights = [](MgLevel L) {
+            L.diag = 2.0f * (L.wx + L.wy + L.wz);
+            L.invDiag = 1.0f / L.diag;
+            return L;
+        };
+        MgLevel L = withWeights(MgLevel{nx, ny, nz, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0, 0, 0});
+        mgLevels_.push_back(L);
+        while (mgLevels_.size() < 10) {
+            const int cx = L.nx % 2 == 0 && L.nx >= 4, cy = L.ny % 2 == 0 && L.ny >= 4, cz = L.nz % 2 == 0 && L.nz >= 4;
+            if (!cx && !cy && !cz) break;
+            L = withWeights(MgLevel{cx ? L.nx / 2 : L.nx, cy ? L.ny / 2 : L.ny, cz ? L.nz / 2 : L.nz, cx ? L.wx * 0.25f : L.wx,
+                                    cy ? L.wy * 0.25f : L.wy, cz ? L.wz * 0.25f : L.wz, 0.0f, 0.0f, cx, cy, cz});
+            const size_t n = static_cast<size_t>(L.nx) * L.ny * L.nz;
+            float* pl = nullptr;
+            float* rl = nullptr;
+            if (!alloc(reinterpret_cast<void**>(&pl), n * sizeof(float), "cudaMalloc multigrid level", err)) return false;
+            mgP_.push_back(pl);
+            if (!alloc(reinterpret_cast<void**>(&rl), n * sizeof(float), "cudaMalloc multigrid level", err)) return false;
+            mgRhs_.push_back(rl);
+            if (!check("clear multigrid level", cudaMemsetAsync(pl, 0, n * sizeof(float), stream), err) ||
+                !check("clear multigrid level", cudaMemsetAsync(rl, 0, n * sizeof(float), stream), err)) {
+                return false;
+            }
+            mgLevels_.push_back(L);
+        }
+    }
+    const bool gated = pressureTolerance_ > 0.0;
+    const double tolKey = gated ? pressureTolerance_ : 0.0;
+    if (mgExec_ == nullptr || mgKeyCycles_ != mgCycles_ || mgKeyPre_ != mgPre_ || mgKeyPost_ != mgPost_ || mgKeyTol_ != tolKey) {
+        if (mgExec_ != nullptr) {
+            cudaGraphExecDestroy(mgExec_);
+            mgExec_ = nullptr;
+        }
+        const int levels = static_cast<int>(mgLevels_.size());
+        auto P = [&](int l) { return l == 0 ? pressure_ : mgP_[l - 1]; };
+        auto R = [&](int l) { return l == 0 ? divergence_ : mgRhs_[l - 1]; };
+        const int* skip = gated ? &sorGate_->converged : nullptr;
+        int count = 0;
+        auto smooth = [&](int l, int sweeps) {
+            const MgLevel& L = mgLevels_[l];
+            const int half = (L.nx + 1) / 2;
+            const int bx = rowThreads(half);
+            const dim3 g((half + bx - 1) / bx, L.ny, L.nz);
+            for (int k = 0; k < sweeps; ++k) {
+                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 0, skip);
+                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 1, skip);
+                count += 2;
+            }
+        };
+        cudaGraph_t graph = nullptr;
+        if (!check("multigrid capture begin", cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), err)) return false;
+        if (gated) cudaMemsetAsync(sorGate_, 0, sizeof(SorGate), stream);
+        for (int c = 0; c < mgCycles_; ++c) {
+            for (int l = 0; l + 1 < levels; ++l) {
+                smooth(l, mgPre_);
+                const MgLevel& F = mgLevels_[l];
+                const MgLevel& C = mgLevels_[l + 1];
+                const int bx = rowThreads(C.nx);
+                mgRestrict<<<dim3((C.nx + bx - 1) / bx, C.ny, C.nz), bx, 0, stream>>>(R(l + 1), P(l + 1), P(l), R(l), F, C, skip);
+                ++count;
+            }
+            mgCoarsest<<<1, 256, 0, stream>>>(P(levels - 1), R(levels - 1), mgLevels_[levels - 1], kMgCoarsestSweeps, skip);
+            ++count;
+            for (int l = levels - 2; l >= 0; --l) {
+                const MgLevel& F = mgLevels_[l];
+                const MgLevel& C = mgLevels_[l + 1];
+                const int bx = rowThreads(F.nx);
+                mgProlong<<<dim3((F.nx + bx - 1) / bx, F.ny, F.nz), bx, 0, stream>>>(P(l), P(l + 1), F, C, skip);
+                ++count;
+                smooth(l, mgPost_);
+            }
+            if (gated) {
+                mgResidualPartials<<<kResidualBlocks, kResidualThreads, 0, stream>>>(pressure_, divergence_, mgLevels_[0], sorGate_,
+                                                                                   residualSq_, residualMax_);
+                sorResidualFinal<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks,
+                                                       static_cast<float>(pressureTolerance_), 1);
+                count += 2;
+            }
+        }
+        const cudaError_t launchErr = cudaGetLastError();
+        const cudaError_t endErr = cudaStreamEndCapture(stream, &graph);
+        if (!check("multigrid capture launch", launchErr, err) || !check("multigrid capture end", endErr, err)) {
+            if (graph) cudaGraphDestroy(graph);
+            return false;
+        }
+        const cudaError_t instErr = cudaGraphInstantiate(&mgExec_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (!check("multigrid graph instantiate", instErr, err)) return false;
+        mgKeyCycles_ = mgCycles_;
+        mgKeyPre_ = mgPre_;
+        mgKeyPost_ = mgPost_;
+        mgKeyTol_ = tolKey;
+        mgGraphLaunches_ = count;
+    }
+    launches_ += static_cast<unsigned long long>(mgGraphLaunches_);
+    lastSolveGated_ = gated;
+    lastPressurePath_ = 3;
+    return check("multigrid graph launch", cudaGraphLaunch(mgExec_, stream), err);
 }
 
 bool Scene::runMetrics(const FrameParams& p, std::string& err) {
@@ -1223,6 +1361,10 @@ bool validatePhysicsParams(const FirePhysicsParams& q, std::string& err) {
         err = "physics mode must be 0 (reference) or 1 (config)";
         return false;
     }
+    if (q.pressureTop != 0 && q.pressureTop != 1) {
+        err = "physics parameters: pressureTop must be 0 (Neumann) or 1 (Dirichlet)";
+        return false;
+    }
     const float vals[] = {q.dt, q.buoyancyHeat, q.buoyancySoot, q.ambientHeat, q.burnRate, q.ignitionHeat, q.heatRelease, q.sootYield,
                           q.cooling, q.sootDecay, q.vorticityEps, q.windX, q.windZ, q.noiseAmplitude, q.noisePeriod, q.lightX,
                           q.lightY, q.lightZ, q.lightIntensity, q.extinction, q.fuelExtinction, q.emission, q.albedo, q.eyeX,
@@ -1394,6 +1536,9 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                 break;
             case kSubtract:
                 subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 1, last >= kWallBoundary ? 1 : 0); ++launches_;
+                if (physics_.pressureTop == 1) {
+                    cfgTopFaces<<<dim3((nx + bx - 1) / bx, nz), bx, 0, stream>>>(vel_[1][vcur_], pressure_, nx, ny, nz); ++launches_;
+                }
                 if (last >= kWallBoundary) ++s;
                 break;
             case kWallBoundary:

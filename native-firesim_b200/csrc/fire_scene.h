@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/fire_cuda.h"
 #include "../../include/fire_ext.h"
@@ -77,6 +78,8 @@ public:
     bool pressureStats(int& iterations, float& maxResidual, double& l2Residual, std::string& err);
     // Hash lattices on (default) or off: off hashes every fbm corner in place (same bits, slower).
     void setHashLattices(bool enabled) { latticesEnabled_ = enabled; }
+    // Multigrid pressure solve (config physics with a Dirichlet top); maxCycles 0 = red-black SOR.
+    bool setPressureMultigrid(int maxCycles, int preSmooth, int postSmooth, std::string& err);
     // Physics of the following passes (mode 0 reference, mode 1 config physics).
     bool setPhysics(const FirePhysicsParams& params, std::string& err);
     const FirePhysicsParams& physics() const { return physics_; }
@@ -185,6 +188,14 @@ private:
     int cfgLx_ = 0, cfgLy_ = 0, cfgLz_ = 0;
     unsigned long long cfgStep_ = 0;
     ConfigParams configParams() const;
+    // Multigrid levels (level 0 is pressure_/divergence_), their buffers and the captured V-cycles.
+    int mgCycles_ = 0, mgPre_ = 2, mgPost_ = 2;
+    std::vector<MgLevel> mgLevels_;
+    std::vector<float*> mgP_, mgRhs_;
+    cudaGraphExec_t mgExec_ = nullptr;
+    int mgKeyCycles_ = -1, mgKeyPre_ = -1, mgKeyPost_ = -1, mgGraphLaunches_ = 0;
+    double mgKeyTol_ = -1.0;
+    bool runMultigrid(std::string& err);
     bool ensureConfigBuffers(std::string& err);
     bool runConfigStages(int first, int last, const FrameParams& p, std::string& err);
 };

@@ -109,6 +109,13 @@ extern "C" bool fireSceneSetPhysicsParams(FireScene* scene, const FirePhysicsPar
     return true;
 }
 
+extern "C" bool fireSceneSetPressureMultigrid(FireScene* scene, int maxCycles, int preSmooth, int postSmooth) {
+    if (scene == nullptr) return fail("Scene handle was null.");
+    std::string err;
+    if (!scene->scene->setPressureMultigrid(maxCycles, preSmooth, postSmooth, err)) return fail(err);
+    return true;
+}
+
 extern "C" bool fireSceneSetHdrBuffer(FireScene* scene, void* devicePtr, size_t pitchBytes, int format) {
     if (scene == nullptr) return fail("Scene handle was null.");
     if (!useDevice(scene->device)) return false;

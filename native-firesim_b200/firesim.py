@@ -105,6 +105,8 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireCudaGetPhysicsParams": (b, [ctypes.POINTER(abi.FirePhysicsParams)]),
         "fireSceneSetPressureTolerance": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
         "fireSceneSetPhysicsParams": (b, [ctypes.c_void_p, ctypes.POINTER(abi.FirePhysicsParams)]),
+        "fireCudaSetPressureMultigrid": (b, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "fireSceneSetPressureMultigrid": (b, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -213,6 +215,10 @@ class FireSim:
         """FirePhysicsParams for the following passes (mode 1: config physics)."""
         self._check(self.lib.fireCudaSetPhysicsParams(ctypes.byref(params)), "fireCudaSetPhysicsParams")
 
+    def set_pressure_multigrid(self, max_cycles: int, pre_smooth: int = 2, post_smooth: int = 2) -> None:
+        """Multigrid V-cycles for the config physics with a Dirichlet top (0 cycles: red-black SOR)."""
+        self._check(self.lib.fireCudaSetPressureMultigrid(max_cycles, pre_smooth, post_smooth), "fireCudaSetPressureMultigrid")
+
     def physics(self):
         p = abi.FirePhysicsParams()
         self._check(self.lib.fireCudaGetPhysicsParams(ctypes.byref(p)), "fireCudaGetPhysicsParams")
@@ -223,7 +229,7 @@ class FireSim:
         self._check(self.lib.fireCudaSetHashLattices(1 if enabled else 0), "fireCudaSetHashLattices")
 
     def pressure_path_used(self) -> int:
-        """Path of the latest SOR solve: 0 none yet, 1 colour-split graph, 2 resident."""
+        """Path of the latest pressure solve: 0 none yet, 1 colour-split SOR, 2 resident SOR, 3 multigrid."""
         return int(self.lib.fireCudaGetPressurePathUsed())
 
     def shape_of(self, name: str):
@@ -319,6 +325,10 @@ class Scene:
 
     def set_physics(self, params) -> None:
         self._check(self.lib.fireSceneSetPhysicsParams(self.h, ctypes.byref(params)), "fireSceneSetPhysicsParams")
+
+    def set_pressure_multigrid(self, max_cycles: int, pre_smooth: int = 2, post_smooth: int = 2) -> None:
+        self._check(self.lib.fireSceneSetPressureMultigrid(self.h, max_cycles, pre_smooth, post_smooth),
+                    "fireSceneSetPressureMultigrid")
 
     def set_hdr_buffer(self, device_ptr: int, pitch_bytes: int, fmt: int = 0):
         self._check(self.lib.fireSceneSetHdrBuffer(self.h, device_ptr, pitch_bytes, fmt), "fireSceneSetHdrBuffer")

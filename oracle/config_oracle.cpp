@@ -82,6 +82,11 @@ struct Scene {
     int iterations = 40;
     float omega = 1.52f;
     uint64_t step = 0;
+    // Multigrid (Dirichlet top): cycles per solve, smoothing sweeps, tolerance on max |r| (0 = none).
+    int mgCycles = 0, mgPre = 2, mgPost = 2;
+    float mgTolerance = 0.0f;
+    int mgCyclesRun = 0;
+    float mgMaxResidual = -1.0f;
 
     int cells() const { return nx * ny * nz; }
     int sI(int x, int y, int z) const { return (z * ny + y) * nx + x; }
@@ -474,6 +479,146 @@ template <class T> void subtract(Scene<T>& s) {
 }
 
 // src/fire_cuda.cu:1293-1317 -- closed walls: u at x = 0, nx; v at y = 0; w at z = 0, nz.
+// ---- Multigrid for the Dirichlet top (the product's fire_mg.cu) ----------
+// Level equation: sum over axes of w_a (2p - p_a- - p_a+) = rhs; walls and
+// floor Neumann (the cell itself), the antisymmetric ghost -p above the top
+// row.  Level 0: w = (1, 1, 1).  The next level halves every axis whose extent
+// is even and at least 4 and divides its weight by 4; at most 10 levels.
+template <class T>
+struct Lvl {
+    int nx, ny, nz;
+    T wx, wy, wz, diag, invDiag;
+    int cx, cy, cz;
+    int at(int x, int y, int z) const { return (z * ny + y) * nx + x; }
+};
+
+template <class T> Lvl<T> withWeights(Lvl<T> L) {
+    L.diag = T(2) * (L.wx + L.wy + L.wz);
+    L.invDiag = T(1) / L.diag;
+    return L;
+}
+
+template <class T> T wsum(const std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z, T self) {
+    const int i = L.at(x, y, z);
+    const T pL = x > 0 ? p[i - 1] : self;
+    const T pR = x < L.nx - 1 ? p[i + 1] : self;
+    const T pD = y > 0 ? p[i - L.nx] : self;
+    const T pU = y < L.ny - 1 ? p[i + L.nx] : T(0) - self;
+    const T pB = z > 0 ? p[i - L.nx * L.ny] : self;
+    const T pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
+    return rhs[i] + L.wx * (pL + pR) + L.wy * (pD + pU) + L.wz * (pB + pF);
+}
+
+template <class T> T resAt(const std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z) {
+    const T self = p[L.at(x, y, z)];
+    return wsum(p, rhs, L, x, y, z, self) - L.diag * self;
+}
+
+template <class T> void mgSmooth(std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L, int sweeps) {
+    for (int k = 0; k < sweeps; ++k) {
+        for (int colour = 0; colour < 2; ++colour) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int z = 0; z < L.nz; ++z) {
+                for (int y = 0; y < L.ny; ++y) {
+                    for (int x = (colour + y + z) & 1; x < L.nx; x += 2) {
+                        const int i = L.at(x, y, z);
+                        p[i] = wsum(p, rhs, L, x, y, z, p[i]) * L.invDiag;
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <class T> T residualMax(const std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L) {
+    T m = T(0);
+    for (int z = 0; z < L.nz; ++z)
+        for (int y = 0; y < L.ny; ++y)
+            for (int x = 0; x < L.nx; ++x) m = std::fmax(m, std::fabs(resAt(p, rhs, L, x, y, z)));
+    return m;
+}
+
+template <class T> void multigrid(Scene<T>& s) {
+    std::vector<Lvl<T>> lv{withWeights(Lvl<T>{s.nx, s.ny, s.nz, T(1), T(1), T(1), T(0), T(0), 0, 0, 0})};
+    while (lv.size() < 10) {
+        const Lvl<T> b = lv.back();
+        const int cx = b.nx % 2 == 0 && b.nx >= 4, cy = b.ny % 2 == 0 && b.ny >= 4, cz = b.nz % 2 == 0 && b.nz >= 4;
+        if (!cx && !cy && !cz) break;
+        lv.push_back(withWeights(Lvl<T>{cx ? b.nx / 2 : b.nx, cy ? b.ny / 2 : b.ny, cz ? b.nz / 2 : b.nz,
+                                        cx ? b.wx * T(0.25f) : b.wx, cy ? b.wy * T(0.25f) : b.wy, cz ? b.wz * T(0.25f) : b.wz,
+                                        T(0), T(0), cx, cy, cz}));
+    }
+    const int n = int(lv.size());
+    std::vector<std::vector<T>> P(n), R(n);
+    for (int l = 1; l < n; ++l) {
+        P[l].assign(size_t(lv[l].nx) * lv[l].ny * lv[l].nz, T(0));
+        R[l].assign(P[l].size(), T(0));
+    }
+    std::vector<T>& p0 = s.pressure;
+    const std::vector<T>& r0 = s.divergence;
+    auto Pl = [&](int l) -> std::vector<T>& { return l == 0 ? p0 : P[l]; };
+    auto Rl = [&](int l) -> const std::vector<T>& { return l == 0 ? r0 : R[l]; };
+    const T half = T(0.5f);
+    s.mgCyclesRun = 0;
+    s.mgMaxResidual = -1.0f;
+    for (int c = 0; c < s.mgCycles; ++c) {
+        for (int l = 0; l + 1 < n; ++l) {
+            mgSmooth(Pl(l), Rl(l), lv[l], s.mgPre);
+            const Lvl<T>& F = lv[l];
+            const Lvl<T>& C = lv[l + 1];
+            const std::vector<T>& pf = Pl(l);
+            const std::vector<T>& rf = Rl(l);
+            for (int Z = 0; Z < C.nz; ++Z)
+                for (int Y = 0; Y < C.ny; ++Y)
+                    for (int X = 0; X < C.nx; ++X) {
+                        const int x0 = C.cx ? 2 * X : X, y0 = C.cy ? 2 * Y : Y, z0 = C.cz ? 2 * Z : Z;
+                        T az[2];
+                        for (int dz = 0; dz <= C.cz; ++dz) {
+                            T ay[2];
+                            for (int dy = 0; dy <= C.cy; ++dy) {
+                                const T a = resAt(pf, rf, F, x0, y0 + dy, z0 + dz);
+                                ay[dy] = C.cx ? half * (a + resAt(pf, rf, F, x0 + 1, y0 + dy, z0 + dz)) : a;
+                            }
+                            az[dz] = C.cy ? half * (ay[0] + ay[1]) : ay[0];
+                        }
+                        R[l + 1][C.at(X, Y, Z)] = C.cz ? half * (az[0] + az[1]) : az[0];
+                        P[l + 1][C.at(X, Y, Z)] = T(0);
+                    }
+        }
+        mgSmooth(Pl(n - 1), Rl(n - 1), lv[n - 1], 32);
+        for (int l = n - 2; l >= 0; --l) {
+            const Lvl<T>& F = lv[l];
+            const Lvl<T>& C = lv[l + 1];
+            std::vector<T>& pf = Pl(l);
+            const std::vector<T>& pc = P[l + 1];
+            const T ux = C.cx ? T(0.75f) : T(1), vx = C.cx ? T(0.25f) : T(0);
+            const T uy = C.cy ? T(0.75f) : T(1), vy = C.cy ? T(0.25f) : T(0);
+            const T uz = C.cz ? T(0.75f) : T(1), vz = C.cz ? T(0.25f) : T(0);
+            for (int z = 0; z < F.nz; ++z)
+                for (int y = 0; y < F.ny; ++y)
+                    for (int x = 0; x < F.nx; ++x) {
+                        const int X0 = C.cx ? x >> 1 : x, Y0 = C.cy ? y >> 1 : y, Z0 = C.cz ? z >> 1 : z;
+                        const int X1 = !C.cx ? X0 : ((x & 1) ? std::min(X0 + 1, C.nx - 1) : std::max(X0 - 1, 0));
+                        const int Y1 = !C.cy ? Y0 : ((y & 1) ? std::min(Y0 + 1, C.ny - 1) : std::max(Y0 - 1, 0));
+                        const int Z1 = !C.cz ? Z0 : ((z & 1) ? std::min(Z0 + 1, C.nz - 1) : std::max(Z0 - 1, 0));
+                        const T a0 = ux * pc[C.at(X0, Y0, Z0)] + vx * pc[C.at(X1, Y0, Z0)];
+                        const T a1 = ux * pc[C.at(X0, Y1, Z0)] + vx * pc[C.at(X1, Y1, Z0)];
+                        const T a2 = ux * pc[C.at(X0, Y0, Z1)] + vx * pc[C.at(X1, Y0, Z1)];
+                        const T a3 = ux * pc[C.at(X0, Y1, Z1)] + vx * pc[C.at(X1, Y1, Z1)];
+                        const T b0 = uy * a0 + vy * a1, b1 = uy * a2 + vy * a3;
+                        const int i = F.at(x, y, z);
+                        pf[i] = pf[i] + (uz * b0 + vz * b1);
+                    }
+            mgSmooth(pf, Rl(l), F, s.mgPost);
+        }
+        ++s.mgCyclesRun;
+        if (s.mgTolerance > 0.0f) {
+            s.mgMaxResidual = float(residualMax(p0, r0, lv[0]));
+            if (s.mgMaxResidual <= s.mgTolerance) break;
+        }
+    }
+}
+
 template <class T> void walls(Scene<T>& s) {
     for (int z = 0; z < s.nz; ++z) {
         for (int y = 0; y < s.ny; ++y) {
@@ -599,9 +744,24 @@ template <class T> int runStages(Scene<T>& s, int first, int last) {
             case FIRE_STAGE_ADVECT_REACT: advectScalars(s, d); break;
             case FIRE_STAGE_FORCE: forces(s, d); break;
             case FIRE_STAGE_DIVERGENCE: divergence(s); break;
-            case FIRE_STAGE_PRESSURE_SOR: sor(s); break;
+            case FIRE_STAGE_PRESSURE_SOR:
+                if (s.phys.pressureTop == 1) {
+                    multigrid(s);
+                } else {
+                    sor(s);
+                }
+                break;
             case FIRE_STAGE_SUBTRACT:
                 subtract(s);
+                if (s.phys.pressureTop == 1) {
+                    // The top faces: v(x, ny, z) -= (ghost - p) with the antisymmetric ghost -p.
+                    for (int z = 0; z < s.nz; ++z)
+                        for (int x = 0; x < s.nx; ++x) {
+                            T& v = s.v[size_t(s.vI(x, s.ny, z))];
+                            const T top = s.pressure[size_t(s.sI(x, s.ny - 1, z))];
+                            v = v - ((T(0) - top) - top);
+                        }
+                }
                 if (last >= FIRE_STAGE_WALL_BOUNDARY) {
                     walls(s);
                     ++st;
@@ -701,6 +861,14 @@ int cfg_oracle_set_physics(void* o, const FirePhysicsParams* params) {
 }
 
 void cfg_oracle_set_pressure_solver(void* o, int iterations, float omega) { CFG_DISPATCH(o, (s.iterations = iterations, s.omega = omega)); }
+
+void cfg_oracle_set_multigrid(void* o, int maxCycles, int preSmooth, int postSmooth, float tolerance) {
+    CFG_DISPATCH(o, (s.mgCycles = maxCycles, s.mgPre = preSmooth, s.mgPost = postSmooth, s.mgTolerance = tolerance));
+}
+
+void cfg_oracle_multigrid_stats(void* o, int* cycles, float* maxResidual) {
+    CFG_DISPATCH(o, (*cycles = s.mgCyclesRun, *maxResidual = s.mgMaxResidual));
+}
 
 int cfg_oracle_set_field(void* o, int field, const void* host, long long bytes) {
     int rc = 0;

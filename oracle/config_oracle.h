@@ -27,6 +27,10 @@ void* cfg_oracle_create(int precision, int frameW, int frameH, int nx, int ny, i
 void cfg_oracle_destroy(void* o);
 int cfg_oracle_set_physics(void* o, const FirePhysicsParams* params);
 void cfg_oracle_set_pressure_solver(void* o, int iterations, float omega);
+// Multigrid solve of the Dirichlet top (FirePhysicsParams.pressureTop = 1): up
+// to maxCycles V-cycles, stopping once max |r| <= tolerance (0: all cycles).
+void cfg_oracle_set_multigrid(void* o, int maxCycles, int preSmooth, int postSmooth, float tolerance);
+void cfg_oracle_multigrid_stats(void* o, int* cycles, float* maxResidual);
 // Fields: HEAT, FUEL, SOOT, PRESSURE, DIVERGENCE, U, V, W, HDR, CONFIG_TRANSMITTANCE (float32).
 int cfg_oracle_set_field(void* o, int field, const void* host, long long bytes);
 int cfg_oracle_get_field(void* o, int field, void* host, long long bytes);

@@ -149,6 +149,8 @@ def _cfg_lib(abi):
         L.cfg_oracle_destroy.argtypes = [ctypes.c_void_p]
         L.cfg_oracle_set_physics.argtypes = [ctypes.c_void_p, P]
         L.cfg_oracle_set_pressure_solver.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
+        L.cfg_oracle_set_multigrid.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
+        L.cfg_oracle_multigrid_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
         L.cfg_oracle_set_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
         L.cfg_oracle_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
         L.cfg_oracle_get_field_f64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
@@ -199,6 +201,14 @@ class ConfigOracle:
 
     def set_pressure_solver(self, iterations: int, omega: float) -> None:
         self.lib.cfg_oracle_set_pressure_solver(self.h, iterations, omega)
+
+    def set_multigrid(self, max_cycles: int, pre_smooth: int = 2, post_smooth: int = 2, tolerance: float = 0.0) -> None:
+        self.lib.cfg_oracle_set_multigrid(self.h, max_cycles, pre_smooth, post_smooth, tolerance)
+
+    def multigrid_stats(self):
+        c, m = ctypes.c_int(), ctypes.c_float()
+        self.lib.cfg_oracle_multigrid_stats(self.h, ctypes.byref(c), ctypes.byref(m))
+        return c.value, m.value
 
     def get(self, name: str) -> np.ndarray:
         out = np.empty(self.shape_of(name), dtype=np.float32)

@@ -183,3 +183,70 @@ def test_float_oracle_tracks_the_double_oracle(abi, oracle_mod):
         rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
         assert rel < 1e-4, (n, rel)
     assert outs[1]["heat"].sum() > 10.0
+
+
+def _mg_oracle(abi, oracle_mod, dims, cycles, tol, seed=2):
+    o = oracle_mod.ConfigOracle(abi, 16, 16, *dims)
+    p = abi.default_physics(*dims)
+    p.mode, p.pressureTop = 1, 1
+    o.set_physics(p)
+    d = (0.3 * np.random.default_rng(seed).standard_normal(dims[::-1])).astype(np.float32)
+    o.set("divergence", d)
+    o.set("pressure", np.zeros(dims[::-1], np.float32))
+    o.set_multigrid(cycles, 2, 2, tol)
+    return o, d
+
+
+def _residual_dirichlet_top(p, d):
+    """d + (neighbours: the cell itself at walls and floor, -p above the top row) - 6p, in float64."""
+    p = p.astype(np.float64)
+    pad = np.pad(p, 1, mode="edge")
+    pad[1:-1, -1, 1:-1] = -p[:, -1, :]
+    nb = (pad[1:-1, 1:-1, :-2] + pad[1:-1, 1:-1, 2:] + pad[1:-1, :-2, 1:-1] + pad[1:-1, 2:, 1:-1] + pad[:-2, 1:-1, 1:-1] +
+          pad[2:, 1:-1, 1:-1])
+    return d + nb - 6.0 * p
+
+
+@pytest.mark.parametrize("dims,max_cycles", [((32, 32, 32), 8), ((64, 48, 40), 8), ((48, 24, 40), 8)])
+def test_multigrid_converges(abi, oracle_mod, dims, max_cycles):
+    """Semi-coarsening V-cycles with the Dirichlet top reach max |r| <= 1e-5 in a
+    few cycles (about a factor 6 per cycle), and the reported residual is the
+    residual of the returned pressure."""
+    o, d = _mg_oracle(abi, oracle_mod, dims, 40, 1e-5)
+    o.stages("pressure_sor", "pressure_sor")
+    cycles, max_r = o.multigrid_stats()
+    assert cycles <= max_cycles and max_r <= 1e-5, (cycles, max_r)
+    # The float residual near 1e-5 carries the rounding of its O(|p|) terms (a few 1e-7 each).
+    r = _residual_dirichlet_top(o.get("pressure"), d)
+    assert np.abs(r).max() == pytest.approx(max_r, abs=2e-6)
+
+
+def test_multigrid_odd_extents_stay_stable(abi, oracle_mod):
+    """Odd extents are not coarsened: the solve degrades to the smoother but
+    still decreases the residual monotonically over cycles."""
+    prev = None
+    for cycles in (2, 6, 12):
+        o, d = _mg_oracle(abi, oracle_mod, (33, 17, 21), cycles, 0.0)
+        o.stages("pressure_sor", "pressure_sor")
+        m = float(np.abs(_residual_dirichlet_top(o.get("pressure"), d)).max())
+        assert prev is None or m < prev
+        prev = m
+
+
+def test_config_projection_meets_the_divergence_bound(abi, oracle_mod):
+    """Config physics with the Dirichlet top and the multigrid solve at max |r|
+    <= 1e-5: after every projection of 6 steps the velocity's divergence
+    (every cell, top faces included) is below 1e-4."""
+    dims = (32, 32, 32)
+    w = abi.config_workload("c1")
+    p = w["physics"]
+    p.emitters[0].centerX, p.emitters[0].centerZ, p.emitters[0].radius = 16, 16, 4
+    p.pressureTop = 1
+    o = oracle_mod.ConfigOracle(abi, 16, 16, *dims)
+    o.set_physics(p)
+    o.set_multigrid(30, 2, 2, 1e-5)
+    for _ in range(6):
+        o.step()
+        div = _divergence(o.get("u"), o.get("v"), o.get("w"))
+        assert np.abs(div).max() <= 1e-4, np.abs(div).max()
+    assert o.get("heat").sum() > 1.0

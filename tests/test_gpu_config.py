@@ -237,3 +237,80 @@ def test_config_gated_solve_on_both_paths(product, abi):
     assert out[0][0][0] == out[1][0][0]
     for n in out[0][1]:
         _bits_equal(f"gated/{n}", out[0][1][n], out[1][1][n])
+
+
+@pytest.mark.parametrize("dims,cycles,tol", [((32, 32, 32), 12, 1e-5), ((64, 48, 40), 12, 1e-5), ((33, 17, 21), 5, 0.0),
+                                             ((128, 128, 128), 10, 1e-5)])
+def test_multigrid_equals_the_oracle_bitwise(dims, cycles, tol, product, abi, oracle_mod):
+    """The multigrid solve (Dirichlet top) from a random right-hand side: the
+    same pressure bits and the same number of V-cycles as the oracle, gated
+    and fixed."""
+    p = abi.default_physics(*dims)
+    p.mode, p.pressureTop = 1, 1
+    d = (0.3 * np.random.default_rng(4).standard_normal(dims[::-1])).astype(np.float32)
+    sim = product.FireSim(32, 16, *dims)
+    sim.set_physics(p)
+    sim.set_pressure_multigrid(cycles, 2, 2)
+    sim.set_pressure_tolerance(tol, 1)
+    sim.set("divergence", d)
+    sim.set("pressure", np.zeros_like(d))
+    sim.stages("pressure_sor", "pressure_sor", abi.FireSettings(), 0.0)
+    assert sim.pressure_path_used() == 3
+    o = oracle_mod.ConfigOracle(abi, 32, 16, *dims)
+    o.set_physics(p)
+    o.set_multigrid(cycles, 2, 2, tol)
+    o.set("divergence", d)
+    o.set("pressure", np.zeros_like(d))
+    o.stages("pressure_sor", "pressure_sor")
+    _bits_equal(f"mg{dims}", sim.get("pressure"), o.get("pressure"))
+    if tol > 0:
+        stats, (oc, om) = sim.pressure_stats(), o.multigrid_stats()
+        assert stats[0] == oc and stats[1] == om and om <= tol, (stats, oc, om)
+    sim.close()
+
+
+def test_config_dirichlet_trajectory_meets_the_divergence_bound(product, abi, oracle_mod):
+    """Config physics with the Dirichlet top and the multigrid solve (max |r| <=
+    1e-5): 15 steps equal the oracle bit for bit, and after every projection
+    the divergence of the velocity (every cell, top faces included) is below
+    1e-4."""
+    dims = (48, 40, 44)
+    p = _physics(abi, dims)
+    p.pressureTop = 1
+    sim = product.FireSim(32, 16, *dims)
+    sim.set_physics(p)
+    sim.set_pressure_multigrid(30, 2, 2)
+    sim.set_pressure_tolerance(1e-5, 1)
+    sim.reset()
+    o = oracle_mod.ConfigOracle(abi, 32, 16, *dims)
+    o.set_physics(p)
+    o.set_multigrid(30, 2, 2, 1e-5)
+    s = abi.FireSettings()
+    for step in range(15):
+        sim.stages("advect_velocity", "wall_boundary", s, 0.0)
+        o.step()
+        u, v, w = sim.get("u"), sim.get("v"), sim.get("w")
+        div = (u[:, :, 1:] - u[:, :, :-1]) + (v[:, 1:, :] - v[:, :-1, :]) + (w[1:] - w[:-1])
+        assert np.abs(div).max() <= 1e-4, (step, np.abs(div).max())
+    for n in STATE:
+        _bits_equal(f"dirichlet/{n}", sim.get(n), o.get(n))
+    sim.close()
+
+
+def test_solver_and_top_must_match(product, abi):
+    dims = (16, 16, 16)
+    sim = product.FireSim(32, 16, *dims)
+    s = abi.FireSettings()
+    p = abi.default_physics(*dims)
+    p.mode, p.pressureTop = 1, 1
+    sim.set_physics(p)
+    with pytest.raises(product.firesim.FireSimError, match="needs the multigrid"):
+        sim.stages("pressure_sor", "pressure_sor", s, 0.0)
+    p.pressureTop = 0
+    sim.set_physics(p)
+    sim.set_pressure_multigrid(4)
+    with pytest.raises(product.firesim.FireSimError, match="Dirichlet top"):
+        sim.stages("pressure_sor", "pressure_sor", s, 0.0)
+    with pytest.raises(product.firesim.FireSimError, match="multigrid"):
+        sim.set_pressure_multigrid(4, 0, 2)
+    sim.close()
