@@ -469,6 +469,23 @@ def config_cpu_baseline(pkg, w, n_steps: int = 2) -> dict:
             "seconds_per_step": per_step}
 
 
+# Level-0 half sweeps of one V-cycle: 2 pre- and 2 post-smoothing sweeps of two colours.
+MG_LEVEL0_HALF_SWEEPS = 8
+
+
+def divergence_after(pkg, lib, sim, settings, fw: int, fh: int) -> dict:
+    """|div u| after the projection of one more measured step (FireCudaFrameMetrics, FP64)."""
+    import ctypes
+    abi = pkg.abi
+    m = abi.FireCudaFrameMetrics()
+    host = np.zeros((fh, fw), dtype=np.uint32)
+    settings.reset = 0
+    if not lib.fireCudaStepAndRenderMeasured(host.ctypes.data, ctypes.byref(settings), ctypes.byref(m)):
+        raise RuntimeError(pkg.firesim.last_error(lib))
+    return {"max": m.divergenceAfterMax, "l2": m.divergenceAfterL2, "before_max": m.divergenceBeforeMax,
+            "note": "one measured step after the timed regions; max over cells, every face included"}
+
+
 def run_config(args, pkg, world: int, rank: int, local: int) -> None:
     """One scene of the config physics (FirePhysicsParams mode 1) on workload c1, c2 or c3."""
     import torch
@@ -483,10 +500,20 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
     if not lib.fireCudaSelectDevice(local):
         raise RuntimeError(pkg.firesim.last_error(lib))
     sim = pkg.FireSim(fw, fh, *n, precision=precision)
-    sim.set_physics(w["physics"])
-    sim.set_pressure_solver(*w["sor"])
-    if w["tolerance"] > 0:
-        sim.set_pressure_tolerance(w["tolerance"], w["check_every"])
+    physics = w["physics"]
+    if args.solver == "mg":
+        # p = 0 on the top face and multigrid V-cycles until max |r| <= half the
+        # divergence target (|div u| after the projection equals |r| up to the
+        # rounding of the face update).
+        physics.pressureTop = 1
+        sim.set_physics(physics)
+        sim.set_pressure_multigrid(args.mg_cycles, 2, 2)
+        sim.set_pressure_tolerance(0.5 * args.div_target, 1)
+    else:
+        sim.set_physics(physics)
+        sim.set_pressure_solver(*w["sor"])
+        if w["tolerance"] > 0:
+            sim.set_pressure_tolerance(w["tolerance"], w["check_every"])
     sim.set_pressure_path({"auto": 0, "graph": 1, "resident": 2}[args.sor_path])
     hdr = torch.zeros((fh, fw, 4), dtype=torch.float32, device="cuda")
     sim.register_hdr_slot(0, hdr.data_ptr(), fw * 16, 0)
@@ -546,12 +573,17 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
                "h2d_bytes_per_step": int(ctypes_sizeof_settings(abi)),
                "d2h_bytes_per_step": int(renders * fw * fh * 4 / args.steps), "ms_per_step": wall * 1e3 / args.steps}
 
+    divergence = divergence_after(pkg, lib, sim, settings, fw, fh)
     st = config_stage_timings(sim, settings)
     per_step = {k: (v / render_every if k in ("light", "render") else v) for k, v in st.items()}
     dominant = max((k for k in CONFIG_STAGE_BYTES_PER_CELL), key=per_step.get)
     peaks, peak_src = measured_peaks()
     iters = stats[0] if stats[1] >= 0 else w["sor"][0]
-    if dominant == "pressure_sor":
+    if dominant == "pressure_sor" and args.solver == "mg":
+        # One "launch" here is the whole solve: its level-0 half sweeps at 6 B/cell each.
+        bytes_launch = CONFIG_STAGE_BYTES_PER_CELL["pressure_sor"] * cells * MG_LEVEL0_HALF_SWEEPS * iters
+        launch_ms = st["pressure_sor"]
+    elif dominant == "pressure_sor":
         launches_per = 2 * iters
         bytes_launch = CONFIG_STAGE_BYTES_PER_CELL["pressure_sor"] * cells
         launch_ms = st["pressure_sor"] / launches_per
@@ -574,9 +606,12 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if precision == "f32" else f"{precision}-storage/f32-arithmetic",
             "data": "synthetic (seeded disk emitters, SplitMix64 jitter)",
-            "config": {"workload": f"config physics {w['name']}: {n[0]}^3, {p.emitterCount} disk emitter(s), SOR "
-                                   f"{w['sor'][0]} omega {w['sor'][1]}"
-                                   f"{' until max|r| <= %g' % w['tolerance'] if w['tolerance'] else ''}, "
+            "config": {"workload": f"config physics {w['name']}: {n[0]}^3, {p.emitterCount} disk emitter(s), "
+                                   + (f"p = 0 on the top face, multigrid V-cycles until max|r| <= {0.5 * args.div_target:g} "
+                                      f"(|div u| <= {args.div_target:g}), at most {args.mg_cycles}"
+                                      if args.solver == "mg" else
+                                      f"SOR {w['sor'][0]} omega {w['sor'][1]}"
+                                      f"{' until max|r| <= %g' % w['tolerance'] if w['tolerance'] else ''}") + ", "
                                    f"{fw}x{fh} render every {render_every} steps ({p.primarySamples} samples, "
                                    f"{p.lightSamples} light samples)",
                        "grid": list(n), "physics": "config (FirePhysicsParams mode 1)", "sor_path": args.sor_path,
@@ -584,7 +619,9 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "stage_ms": per_step,
             "step_latency": {"unit": "ms", "p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                              "max": float(step_ms.max())},
-            "pressure_stats_last_step": {"iterations": stats[0], "max_residual": stats[1], "l2_residual": stats[2]},
+            "pressure_stats_last_step": {"iterations": stats[0], "max_residual": stats[1], "l2_residual": stats[2],
+                                         "solver": args.solver},
+            "divergence_after": divergence,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -610,6 +647,11 @@ def main() -> int:
                     help="reference: native-firesim's physics (the headline line); config: FirePhysicsParams mode 1")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"],
                     help="config physics workload (abi.config_workload)")
+    ap.add_argument("--solver", default="sor", choices=["sor", "mg"],
+                    help="config physics: the workload's red-black SOR, or p = 0 on the top face with multigrid "
+                         "V-cycles until |div u| <= --div-target")
+    ap.add_argument("--div-target", type=float, default=1e-4)
+    ap.add_argument("--mg-cycles", type=int, default=30)
     ap.add_argument("--precision", default=None, choices=["f32", "f16", "bf16"],
                     help="storage of the transported fields: f32 (the reference's), f16 or bf16 (FP32 arithmetic)")
     ap.add_argument("--mode", default="single", choices=["single", "batched", "serve"],
@@ -758,6 +800,7 @@ def main() -> int:
     peaks, peak_src = measured_peaks()
     roofline = roofline_block(dominant, st, args, cells, peaks, peak_src, sim.pressure_path_used())
 
+    divergence = divergence_after(pkg, lib, sim, workload_settings(abi, frame, args), args.frame, args.frame)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(pkg, args)
@@ -771,7 +814,8 @@ def main() -> int:
             "dtype": "f32" if args.precision == "f32" else f"{args.precision}-storage/f32-arithmetic",
             "data": "synthetic (seeded procedural fuel bed + validation-harness settings)",
             "config": config_block(args), "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-            "roofline": roofline, "stage_ms": per_step_ms, "step_latency": latency, "cpu_baseline": cpu,
+            "roofline": roofline, "stage_ms": per_step_ms, "step_latency": latency, "divergence_after": divergence,
+            "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     sim.close()

@@ -208,6 +208,9 @@ __global__ void mgProlong(float* p, const float* pC, MgLevel F, MgLevel C, const
 __global__ void mgCoarsest(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
 __global__ void mgResidualPartials(const float* p, const float* rhs, MgLevel L, const SorGate* gate, double* partialSq, float* partialMax);
 __global__ void cfgTopFaces(FaceT* v, const float* p, int nx, int ny, int nz);
+__global__ void mgCycleEnd(SorGate* gate, const double* partialSq, const float* partialMax, int partials, float tolerance, int gated,
+                           int maxCycles, cudaGraphConditionalHandle loop);
 constexpr int kMgCoarsestSweeps = 32;
+constexpr int kMgHardCycleCap = 1000;  // fireCudaSetPressureMultigrid accepts at most this many cycles
 
 }  // namespace firesim

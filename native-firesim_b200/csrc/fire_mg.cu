@@ -164,6 +164,42 @@ __global__ void __launch_bounds__(kResidualThreads) mgResidualPartials(const flo
     }
 }
 
+// End of one V-cycle inside the solve's conditional WHILE node: one warp
+// reduces the level-0 residual partials (when gated, as sorResidualFinal),
+// counts the cycle and sets the loop condition, which is cleared once the
+// residual is within the tolerance or maxCycles cycles have run.  The count
+// always advances, so the loop ends after at most maxCycles bodies.
+__global__ void mgCycleEnd(SorGate* gate, const double* __restrict__ partialSq, const float* __restrict__ partialMax, int partials,
+                           float tolerance, int gated, int maxCycles, cudaGraphConditionalHandle loop) {
+    const int lane = threadIdx.x;
+    if (gated) {
+        double s = 0.0;
+        float m = 0.0f;
+        for (int b = lane; b < partials; b += 32) {
+            s += partialSq[b];
+            m = fmaxf(m, partialMax[b]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        }
+        if (lane == 0) {
+            gate->maxResidual = m;
+            gate->l2Residual = sqrt(s);
+            if (m <= tolerance) gate->converged = 1;
+        }
+    }
+    if (lane != 0) return;
+    if (!gated) {
+        gate->maxResidual = -1.0f;
+        gate->l2Residual = -1.0;
+    }
+    gate->iterations += 1;
+    const bool more = gate->converged == 0 && gate->iterations < maxCycles && gate->iterations < kMgHardCycleCap;
+    cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
+
 // The top faces under a Dirichlet top: v(x, ny, z) -= (ghost - p) with the
 // antisymmetric ghost -p of the top cell.
 __global__ void __launch_bounds__(128) cfgTopFaces(FaceT* __restrict__ v, const float* __restrict__ p, int nx, int ny, int nz) {

@@ -567,9 +567,11 @@ bool Scene::setPressureMultigrid(int maxCycles, int preSmooth, int postSmooth, s
     return true;
 }
 
-// V-cycles of the multigrid solve (fire_mg.cu), captured once per (cycles,
-// smoothing, tolerance) into a CUDA graph; with a tolerance every cycle ends
-// with the level-0 residual check of the solve's gate.
+// The multigrid solve (fire_mg.cu) as one CUDA graph per (cycles, smoothing,
+// tolerance): a memset of the gate, then a conditional WHILE node whose body
+// is one V-cycle, the level-0 residual partials (with a tolerance) and
+// mgCycleEnd, which clears the loop condition when the solve has converged or
+// run maxCycles cycles -- a converged solve launches nothing more.
 bool Scene::runMultigrid(std::string& err) {
     if (mgLevels_.empty()) {
         auto withWeights = [](MgLevel L) {
@@ -608,7 +610,6 @@ bool Scene::runMultigrid(std::string& err) {
         const int levels = static_cast<int>(mgLevels_.size());
         auto P = [&](int l) { return l == 0 ? pressure_ : mgP_[l - 1]; };
         auto R = [&](int l) { return l == 0 ? divergence_ : mgRhs_[l - 1]; };
-        const int* skip = gated ? &sorGate_->converged : nullptr;
         int count = 0;
         auto smooth = [&](int l, int sweeps) {
             const MgLevel& L = mgLevels_[l];
@@ -616,47 +617,71 @@ bool Scene::runMultigrid(std::string& err) {
             const int bx = rowThreads(half);
             const dim3 g((half + bx - 1) / bx, L.ny, L.nz);
             for (int k = 0; k < sweeps; ++k) {
-                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 0, skip);
-                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 1, skip);
+                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 0, nullptr);
+                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 1, nullptr);
                 count += 2;
             }
         };
         cudaGraph_t graph = nullptr;
-        if (!check("multigrid capture begin", cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), err)) return false;
-        if (gated) cudaMemsetAsync(sorGate_, 0, sizeof(SorGate), stream);
-        for (int c = 0; c < mgCycles_; ++c) {
-            for (int l = 0; l + 1 < levels; ++l) {
-                smooth(l, mgPre_);
-                const MgLevel& F = mgLevels_[l];
-                const MgLevel& C = mgLevels_[l + 1];
-                const int bx = rowThreads(C.nx);
-                mgRestrict<<<dim3((C.nx + bx - 1) / bx, C.ny, C.nz), bx, 0, stream>>>(R(l + 1), P(l + 1), P(l), R(l), F, C, skip);
-                ++count;
-            }
-            mgCoarsest<<<1, 256, 0, stream>>>(P(levels - 1), R(levels - 1), mgLevels_[levels - 1], kMgCoarsestSweeps, skip);
+        if (!check("multigrid graph create", cudaGraphCreate(&graph, 0), err)) return false;
+        auto failGraph = [&](const char* label, cudaError_t e) {
+            cudaGraphDestroy(graph);
+            return check(label, e, err);
+        };
+        cudaGraphNode_t reset = nullptr;
+        cudaMemsetParams ms{};
+        ms.dst = sorGate_;
+        ms.value = 0;
+        ms.elementSize = 4;
+        ms.width = sizeof(SorGate) / 4;
+        ms.height = 1;
+        cudaError_t e = cudaGraphAddMemsetNode(&reset, graph, nullptr, 0, &ms);
+        if (e != cudaSuccess) return failGraph("multigrid gate reset node", e);
+        cudaGraphConditionalHandle loop{};
+        e = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return failGraph("multigrid loop handle", e);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t condNode = nullptr;
+        e = cudaGraphAddNode(&condNode, graph, &reset, 1, &cp);
+        if (e != cudaSuccess) return failGraph("multigrid loop node", e);
+        cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(stream, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return failGraph("multigrid body capture begin", e);
+        for (int l = 0; l + 1 < levels; ++l) {
+            smooth(l, mgPre_);
+            const MgLevel& F = mgLevels_[l];
+            const MgLevel& C = mgLevels_[l + 1];
+            const int bx = rowThreads(C.nx);
+            mgRestrict<<<dim3((C.nx + bx - 1) / bx, C.ny, C.nz), bx, 0, stream>>>(R(l + 1), P(l + 1), P(l), R(l), F, C, nullptr);
             ++count;
-            for (int l = levels - 2; l >= 0; --l) {
-                const MgLevel& F = mgLevels_[l];
-                const MgLevel& C = mgLevels_[l + 1];
-                const int bx = rowThreads(F.nx);
-                mgProlong<<<dim3((F.nx + bx - 1) / bx, F.ny, F.nz), bx, 0, stream>>>(P(l), P(l + 1), F, C, skip);
-                ++count;
-                smooth(l, mgPost_);
-            }
-            if (gated) {
-                mgResidualPartials<<<kResidualBlocks, kResidualThreads, 0, stream>>>(pressure_, divergence_, mgLevels_[0], sorGate_,
-                                                                                   residualSq_, residualMax_);
-                sorResidualFinal<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks,
-                                                       static_cast<float>(pressureTolerance_), 1);
-                count += 2;
-            }
         }
+        mgCoarsest<<<1, 256, 0, stream>>>(P(levels - 1), R(levels - 1), mgLevels_[levels - 1], kMgCoarsestSweeps, nullptr);
+        ++count;
+        for (int l = levels - 2; l >= 0; --l) {
+            const MgLevel& F = mgLevels_[l];
+            const MgLevel& C = mgLevels_[l + 1];
+            const int bx = rowThreads(F.nx);
+            mgProlong<<<dim3((F.nx + bx - 1) / bx, F.ny, F.nz), bx, 0, stream>>>(P(l), P(l + 1), F, C, nullptr);
+            ++count;
+            smooth(l, mgPost_);
+        }
+        if (gated) {
+            mgResidualPartials<<<kResidualBlocks, kResidualThreads, 0, stream>>>(pressure_, divergence_, mgLevels_[0], sorGate_,
+                                                                               residualSq_, residualMax_);
+            ++count;
+        }
+        mgCycleEnd<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks, static_cast<float>(pressureTolerance_),
+                                         gated ? 1 : 0, mgCycles_, loop);
+        ++count;
         const cudaError_t launchErr = cudaGetLastError();
-        const cudaError_t endErr = cudaStreamEndCapture(stream, &graph);
-        if (!check("multigrid capture launch", launchErr, err) || !check("multigrid capture end", endErr, err)) {
-            if (graph) cudaGraphDestroy(graph);
-            return false;
-        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t endErr = cudaStreamEndCapture(stream, &captured);
+        if (launchErr != cudaSuccess) return failGraph("multigrid body launch", launchErr);
+        if (endErr != cudaSuccess) return failGraph("multigrid body capture end", endErr);
         const cudaError_t instErr = cudaGraphInstantiate(&mgExec_, graph, 0);
         cudaGraphDestroy(graph);
         if (!check("multigrid graph instantiate", instErr, err)) return false;
@@ -664,10 +689,11 @@ bool Scene::runMultigrid(std::string& err) {
         mgKeyPre_ = mgPre_;
         mgKeyPost_ = mgPost_;
         mgKeyTol_ = tolKey;
-        mgGraphLaunches_ = count;
+        mgGraphLaunches_ = count;  // per V-cycle
     }
+    // The launch count cannot know how many cycles will run; it counts one V-cycle's kernels.
     launches_ += static_cast<unsigned long long>(mgGraphLaunches_);
-    lastSolveGated_ = gated;
+    lastSolveGated_ = true;
     lastPressurePath_ = 3;
     return check("multigrid graph launch", cudaGraphLaunch(mgExec_, stream), err);
 }
