@@ -418,27 +418,30 @@ CONFIG_STAGE_BYTES_PER_CELL = {
 }
 
 
-def config_stage_timings(sim, settings, iters: int = 3) -> dict:
+def config_stage_timings(sim, settings, steps: int = 3) -> dict:
+    """Device time of each stage inside real steps: `steps` whole steps (render
+    included), each queued stage by stage with events between consecutive
+    stages on the scene stream; the minimum per stage over the steps."""
     import torch
     ext = torch.cuda.ExternalStream(sim.stream())
-    ranges = {"advect_velocity": ("advect_velocity", "advect_velocity"), "advect_react": ("advect_react", "advect_react"),
-              "force": ("force", "velocity_boundary"), "divergence": ("divergence", "divergence"),
-              "pressure_sor": ("pressure_sor", "pressure_sor"), "subtract_walls": ("subtract", "wall_boundary"),
-              "light": ("light_build", "light_build"), "render": ("render", "render")}
-    out = {}
-    for name, (a, b) in ranges.items():
-        ms = []
-        for _ in range(iters):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(ext):
-                torch.cuda._sleep(400_000)
-            e0.record(ext)
+    ranges = [("advect_velocity", "advect_velocity", "advect_velocity"), ("advect_react", "advect_react", "advect_react"),
+              ("force", "force", "velocity_boundary"), ("divergence", "divergence", "divergence"),
+              ("pressure_sor", "pressure_sor", "pressure_sor"), ("subtract_walls", "subtract", "wall_boundary"),
+              ("light", "light_build", "light_build"), ("render", "render", "render")]
+    out = {name: float("inf") for name, _, _ in ranges}
+    for _ in range(steps):
+        # The spin (about 1 ms) holds the stream until every stage of the step is queued.
+        with torch.cuda.stream(ext):
+            torch.cuda._sleep(2_000_000)
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(ranges) + 1)]
+        marks[0].record(ext)
+        for k, (name, a, b) in enumerate(ranges):
             sim.stages(a, b, settings, 0.0, wait=False)
-            e1.record(ext)
-            e1.synchronize()
-            ms.append(e0.elapsed_time(e1))
-        sim.synchronize()
-        out[name] = min(ms)
+            marks[k + 1].record(ext)
+        marks[-1].synchronize()
+        for k, (name, _, _) in enumerate(ranges):
+            out[name] = min(out[name], marks[k].elapsed_time(marks[k + 1]))
+    sim.synchronize()
     return out
 
 

@@ -201,12 +201,20 @@ struct MgLevel {
     int nx, ny, nz;
     float wx, wy, wz, diag, invDiag;
     int cx, cy, cz;
+    int wide;  // 1: the level's pressure is double (level 0)
 };
-__global__ void mgSmooth(float* p, const float* rhs, MgLevel L, int colour, const int* skip);
-__global__ void mgRestrict(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);
-__global__ void mgProlong(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip);
-__global__ void mgCoarsest(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
-__global__ void mgResidualPartials(const float* p, const float* rhs, MgLevel L, const SorGate* gate, double* partialSq, float* partialMax);
+// F: float pressure (the coarser levels); D: double pressure (level 0).
+__global__ void mgSmoothF(float* p, const float* rhs, MgLevel L, int colour, const int* skip);
+__global__ void mgSmoothD(double* p, const float* rhs, MgLevel L, int colour, const int* skip);
+__global__ void mgRestrictF(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);
+__global__ void mgRestrictD(float* rhsC, float* pC, const double* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);
+__global__ void mgProlongF(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip);
+__global__ void mgProlongD(double* p, const float* pC, MgLevel F, MgLevel C, const int* skip);
+__global__ void mgCoarsestF(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
+__global__ void mgCoarsestD(double* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
+__global__ void mgResidualPartialsD(const double* p, const float* rhs, MgLevel L, const SorGate* gate, double* partialSq, float* partialMax);
+__global__ void mgStoreFloat(float* dst, const double* src, int n);
+__global__ void cfgSubtractWide(FaceT* u, FaceT* v, FaceT* w, const double* p, int nx, int ny, int nz, int doWalls);
 __global__ void cfgTopFaces(FaceT* v, const float* p, int nx, int ny, int nz);
 __global__ void mgCycleEnd(SorGate* gate, const double* partialSq, const float* partialMax, int partials, float tolerance, int gated,
                            int maxCycles, cudaGraphConditionalHandle loop);

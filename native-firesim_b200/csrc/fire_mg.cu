@@ -16,6 +16,13 @@
 // (sorResidualFinal); once max |r| is within the tolerance every later kernel
 // of the solve returns at once.
 //
+// Level 0 holds p in double (its smoothing, residuals and prolongation run in
+// double; rhs stays float): in float, the rounding of p itself floors the
+// residual near 6 ulp(|p|), ~1e-4 for |p| ~ 140, and with it |div u| after
+// the projection.  The coarser levels carry small corrections in float.  The
+// solve ends by writing the float pressure field; under a Dirichlet top the
+// gradient subtraction reads the double pressure (cfgSubtractWide).
+//
 // Compiled with -fmad=false: every operation rounds as written, so a CPU
 // restatement in the same order gives the same bits.
 #include "fire_kernels.h"
@@ -28,65 +35,77 @@ __device__ __forceinline__ int mgAt(const MgLevel& L, int x, int y, int z) { ret
 
 __device__ __forceinline__ bool skipped(const int* skip) { return skip != nullptr && __ldg(skip) != 0; }
 
-// rhs + wx (pL + pR) + wy (pD + pU) + wz (pB + pF) for cell (x, y, z) with the boundary rules.
-__device__ __forceinline__ float weightedSum(const float* p, const float* rhs, const MgLevel& L, int x, int y, int z, float self) {
+// rhs + wx (pL + pR) + wy (pD + pU) + wz (pB + pF) for cell (x, y, z) with the
+// boundary rules, in the level's pressure type P (double on level 0).
+template <typename P>
+__device__ __forceinline__ P weightedSum(const P* p, const float* rhs, const MgLevel& L, int x, int y, int z, P self) {
     const int i = mgAt(L, x, y, z);
-    const float pL = x > 0 ? p[i - 1] : self;
-    const float pR = x < L.nx - 1 ? p[i + 1] : self;
-    const float pD = y > 0 ? p[i - L.nx] : self;
-    const float pU = y < L.ny - 1 ? p[i + L.nx] : 0.0f - self;
-    const float pB = z > 0 ? p[i - L.nx * L.ny] : self;
-    const float pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
-    return rhs[i] + L.wx * (pL + pR) + L.wy * (pD + pU) + L.wz * (pB + pF);
+    const P pL = x > 0 ? p[i - 1] : self;
+    const P pR = x < L.nx - 1 ? p[i + 1] : self;
+    const P pD = y > 0 ? p[i - L.nx] : self;
+    const P pU = y < L.ny - 1 ? p[i + L.nx] : static_cast<P>(0) - self;
+    const P pB = z > 0 ? p[i - L.nx * L.ny] : self;
+    const P pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
+    return static_cast<P>(rhs[i]) + static_cast<P>(L.wx) * (pL + pR) + static_cast<P>(L.wy) * (pD + pU) +
+           static_cast<P>(L.wz) * (pB + pF);
 }
 
-__device__ __forceinline__ float residualAt(const float* p, const float* rhs, const MgLevel& L, int x, int y, int z) {
-    const float self = p[mgAt(L, x, y, z)];
-    return weightedSum(p, rhs, L, x, y, z, self) - L.diag * self;
+template <typename P>
+__device__ __forceinline__ P residualAt(const P* p, const float* rhs, const MgLevel& L, int x, int y, int z) {
+    const P self = p[mgAt(L, x, y, z)];
+    return weightedSum(p, rhs, L, x, y, z, self) - static_cast<P>(L.diag) * self;
+}
+
+template <typename P>
+__device__ __forceinline__ void smoothCell(P* p, const float* rhs, const MgLevel& L, int x, int y, int z) {
+    const int i = mgAt(L, x, y, z);
+    p[i] = weightedSum(p, rhs, L, x, y, z, p[i]) * static_cast<P>(L.invDiag);
 }
 
 }  // namespace
 
 // One colour of red-black Gauss-Seidel: cells with (x + y + z) % 2 == colour.
-__global__ void __launch_bounds__(128) mgSmooth(float* __restrict__ p, const float* __restrict__ rhs, MgLevel L, int colour,
-                                                const int* skip) {
+template <typename P>
+__device__ __forceinline__ void mgSmoothBody(P* __restrict__ p, const float* __restrict__ rhs, const MgLevel& L, int colour, const int* skip) {
     if (skipped(skip)) return;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
     const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((colour + y + z) & 1);
     if (x >= L.nx) return;
-    const int i = mgAt(L, x, y, z);
-    p[i] = weightedSum(p, rhs, L, x, y, z, p[i]) * L.invDiag;
+    smoothCell(p, rhs, L, x, y, z);
 }
 
 // Coarse rhs = the mean residual of the covered fine cells (averaged along x,
-// then y, then z over the halved axes), coarse p = 0.
-__global__ void __launch_bounds__(128) mgRestrict(float* __restrict__ rhsC, float* __restrict__ pC, const float* __restrict__ p,
-                                                  const float* __restrict__ rhs, MgLevel F, MgLevel C, const int* skip) {
+// then y, then z over the halved axes, in the fine level's type), coarse p = 0.
+template <typename P>
+__device__ __forceinline__ void mgRestrictBody(float* __restrict__ rhsC, float* __restrict__ pC, const P* __restrict__ p,
+                                               const float* __restrict__ rhs, const MgLevel& F, const MgLevel& C, const int* skip) {
     if (skipped(skip)) return;
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y;
     const int Z = blockIdx.z;
     if (X >= C.nx) return;
     const int x0 = C.cx ? 2 * X : X, y0 = C.cy ? 2 * Y : Y, z0 = C.cz ? 2 * Z : Z;
-    float az[2];
+    const P half = static_cast<P>(0.5f);
+    P az[2];
     for (int dz = 0; dz <= C.cz; ++dz) {
-        float ay[2];
+        P ay[2];
         for (int dy = 0; dy <= C.cy; ++dy) {
-            const float r0 = residualAt(p, rhs, F, x0, y0 + dy, z0 + dz);
-            ay[dy] = C.cx ? 0.5f * (r0 + residualAt(p, rhs, F, x0 + 1, y0 + dy, z0 + dz)) : r0;
+            const P r0 = residualAt(p, rhs, F, x0, y0 + dy, z0 + dz);
+            ay[dy] = C.cx ? half * (r0 + residualAt(p, rhs, F, x0 + 1, y0 + dy, z0 + dz)) : r0;
         }
-        az[dz] = C.cy ? 0.5f * (ay[0] + ay[1]) : ay[0];
+        az[dz] = C.cy ? half * (ay[0] + ay[1]) : ay[0];
     }
     const int c = mgAt(C, X, Y, Z);
-    rhsC[c] = C.cz ? 0.5f * (az[0] + az[1]) : az[0];
+    rhsC[c] = static_cast<float>(C.cz ? half * (az[0] + az[1]) : az[0]);
     pC[c] = 0.0f;
 }
 
 // p += the coarse correction interpolated along the halved axes (weights 3/4
 // and 1/4, neighbour clamped; weights 1 and 0 along kept axes), x, then y, then z.
-__global__ void __launch_bounds__(128) mgProlong(float* __restrict__ p, const float* __restrict__ pC, MgLevel F, MgLevel C,
-                                                 const int* skip) {
+template <typename P>
+__device__ __forceinline__ void mgProlongBody(P* __restrict__ p, const float* __restrict__ pC, const MgLevel& F, const MgLevel& C,
+                                              const int* skip) {
     if (skipped(skip)) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -105,12 +124,13 @@ __global__ void __launch_bounds__(128) mgProlong(float* __restrict__ p, const fl
     const float a3 = ux * pC[mgAt(C, X0, Y1, Z1)] + vx * pC[mgAt(C, X1, Y1, Z1)];
     const float b0 = uy * a0 + vy * a1, b1 = uy * a2 + vy * a3;
     const int i = mgAt(F, x, y, z);
-    p[i] = p[i] + (uz * b0 + vz * b1);
+    p[i] = p[i] + static_cast<P>(uz * b0 + vz * b1);
 }
 
 // The coarsest level: `sweeps` red-black Gauss-Seidel iterations by one block.
-__global__ void __launch_bounds__(256) mgCoarsest(float* __restrict__ p, const float* __restrict__ rhs, MgLevel L, int sweeps,
-                                                  const int* skip) {
+template <typename P>
+__device__ __forceinline__ void mgCoarsestBody(P* __restrict__ p, const float* __restrict__ rhs, const MgLevel& L, int sweeps,
+                                               const int* skip) {
     if (skipped(skip)) return;
     const int cells = L.nx * L.ny * L.nz;
     for (int s = 0; s < sweeps; ++s) {
@@ -120,7 +140,7 @@ __global__ void __launch_bounds__(256) mgCoarsest(float* __restrict__ p, const f
                 const int y = (i / L.nx) % L.ny;
                 const int z = i / (L.nx * L.ny);
                 if (((x + y + z) & 1) != colour) continue;
-                p[i] = weightedSum(p, rhs, L, x, y, z, p[i]) * L.invDiag;
+                smoothCell(p, rhs, L, x, y, z);
             }
             __syncthreads();
         }
@@ -129,9 +149,9 @@ __global__ void __launch_bounds__(256) mgCoarsest(float* __restrict__ p, const f
 
 // Level-0 residual r = (weighted neighbour sum) - 6p with the Dirichlet top,
 // per block over whole rows (as sorResidualPartials).
-__global__ void __launch_bounds__(kResidualThreads) mgResidualPartials(const float* __restrict__ p, const float* __restrict__ rhs, MgLevel L,
-                                                                       const SorGate* gate, double* __restrict__ partialSq,
-                                                                       float* __restrict__ partialMax) {
+template <typename P>
+__device__ __forceinline__ void mgResidualPartialsBody(const P* __restrict__ p, const float* __restrict__ rhs, const MgLevel& L,
+                                                       const SorGate* gate, double* __restrict__ partialSq, float* __restrict__ partialMax) {
     if (gate->converged) return;
     const int lane = threadIdx.x & 31;
     const int warps = kResidualThreads / 32;
@@ -141,9 +161,9 @@ __global__ void __launch_bounds__(kResidualThreads) mgResidualPartials(const flo
         const int y = row % L.ny;
         const int z = row / L.ny;
         for (int x = lane; x < L.nx; x += 32) {
-            const float r = residualAt(p, rhs, L, x, y, z);
-            m = fmaxf(m, fabsf(r));
-            s += static_cast<double>(r) * static_cast<double>(r);
+            const double r = static_cast<double>(residualAt(p, rhs, L, x, y, z));
+            m = fmaxf(m, static_cast<float>(fabs(r)));
+            s += r * r;
         }
     }
     __shared__ double sq[kResidualThreads];
@@ -161,6 +181,74 @@ __global__ void __launch_bounds__(kResidualThreads) mgResidualPartials(const flo
     if (threadIdx.x == 0) {
         partialSq[blockIdx.x] = sq[0];
         partialMax[blockIdx.x] = mx[0];
+    }
+}
+
+// The kernels, one per pressure type (F: float, the coarser levels; D: double, level 0).
+__global__ void __launch_bounds__(128) mgSmoothF(float* p, const float* rhs, MgLevel L, int colour, const int* skip) {
+    mgSmoothBody(p, rhs, L, colour, skip);
+}
+__global__ void __launch_bounds__(128) mgSmoothD(double* p, const float* rhs, MgLevel L, int colour, const int* skip) {
+    mgSmoothBody(p, rhs, L, colour, skip);
+}
+__global__ void __launch_bounds__(128) mgRestrictF(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C,
+                                                   const int* skip) {
+    mgRestrictBody(rhsC, pC, p, rhs, F, C, skip);
+}
+__global__ void __launch_bounds__(128) mgRestrictD(float* rhsC, float* pC, const double* p, const float* rhs, MgLevel F, MgLevel C,
+                                                   const int* skip) {
+    mgRestrictBody(rhsC, pC, p, rhs, F, C, skip);
+}
+__global__ void __launch_bounds__(128) mgProlongF(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip) {
+    mgProlongBody(p, pC, F, C, skip);
+}
+__global__ void __launch_bounds__(128) mgProlongD(double* p, const float* pC, MgLevel F, MgLevel C, const int* skip) {
+    mgProlongBody(p, pC, F, C, skip);
+}
+__global__ void __launch_bounds__(256) mgCoarsestF(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip) {
+    mgCoarsestBody(p, rhs, L, sweeps, skip);
+}
+__global__ void __launch_bounds__(256) mgCoarsestD(double* p, const float* rhs, MgLevel L, int sweeps, const int* skip) {
+    mgCoarsestBody(p, rhs, L, sweeps, skip);
+}
+__global__ void __launch_bounds__(kResidualThreads) mgResidualPartialsD(const double* p, const float* rhs, MgLevel L, const SorGate* gate,
+                                                                        double* partialSq, float* partialMax) {
+    mgResidualPartialsBody(p, rhs, L, gate, partialSq, partialMax);
+}
+
+// The float pressure field from the double level-0 pressure of the solve.
+__global__ void __launch_bounds__(256) mgStoreFloat(float* __restrict__ dst, const double* __restrict__ src, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = static_cast<float>(src[i]);
+}
+
+// The gradient subtraction under a Dirichlet top from the double pressure:
+// each face's difference is formed in double and rounded once before the
+// float update; the top faces use the antisymmetric ghost -p; with doWalls
+// the closed walls are zeroed as in subtractWall.
+__global__ void __launch_bounds__(128) cfgSubtractWide(FaceT* __restrict__ u, FaceT* __restrict__ v, FaceT* __restrict__ w,
+                                                       const double* __restrict__ p, int nx, int ny, int nz, int doWalls) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx) return;
+    const int i = (z * ny + y) * nx + x;
+    const double pc = p[i];
+    const int ui = (z * ny + y) * (nx + 1) + x;
+    const int vi = (z * (ny + 1) + y) * nx + x;
+    const int wi = (z * ny + y) * nx + x;
+    if (x > 0) stv(u + ui, ldv(u + ui) - static_cast<float>(pc - p[i - 1]));
+    if (y > 0) stv(v + vi, ldv(v + vi) - static_cast<float>(pc - p[i - nx]));
+    if (z > 0) stv(w + wi, ldv(w + wi) - static_cast<float>(pc - p[i - nx * ny]));
+    if (y == ny - 1) {
+        const int top = (z * (ny + 1) + ny) * nx + x;
+        stv(v + top, ldv(v + top) - static_cast<float>((0.0 - pc) - pc));
+    }
+    if (doWalls) {
+        if (x == 0) stv(u + ui, 0.0f);
+        if (x == nx - 1) stv(u + ui + 1, 0.0f);
+        if (y == 0) stv(v + vi, 0.0f);
+        if (z == 0) stv(w + wi, 0.0f);
+        if (z == nz - 1) stv(w + (nz * ny + y) * nx + x, 0.0f);
     }
 }
 

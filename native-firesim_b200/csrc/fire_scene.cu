@@ -68,6 +68,9 @@ void Scene::release() {
         cudaGraphExecDestroy(mgExec_);
         mgExec_ = nullptr;
     }
+    if (mgP0_ != nullptr) cudaFree(mgP0_);
+    mgP0_ = nullptr;
+    mgP0Valid_ = false;
     for (float* b : mgP_) cudaFree(b);
     for (float* b : mgRhs_) cudaFree(b);
     mgP_.clear();
@@ -579,13 +582,14 @@ bool Scene::runMultigrid(std::string& err) {
             L.invDiag = 1.0f / L.diag;
             return L;
         };
-        MgLevel L = withWeights(MgLevel{nx, ny, nz, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0, 0, 0});
+        MgLevel L = withWeights(MgLevel{nx, ny, nz, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0, 0, 0, 1});
         mgLevels_.push_back(L);
+        if (!alloc(reinterpret_cast<void**>(&mgP0_), cells_ * sizeof(double), "cudaMalloc multigrid level-0 pressure", err)) return false;
         while (mgLevels_.size() < 10) {
             const int cx = L.nx % 2 == 0 && L.nx >= 4, cy = L.ny % 2 == 0 && L.ny >= 4, cz = L.nz % 2 == 0 && L.nz >= 4;
             if (!cx && !cy && !cz) break;
             L = withWeights(MgLevel{cx ? L.nx / 2 : L.nx, cy ? L.ny / 2 : L.ny, cz ? L.nz / 2 : L.nz, cx ? L.wx * 0.25f : L.wx,
-                                    cy ? L.wy * 0.25f : L.wy, cz ? L.wz * 0.25f : L.wz, 0.0f, 0.0f, cx, cy, cz});
+                                    cy ? L.wy * 0.25f : L.wy, cz ? L.wz * 0.25f : L.wz, 0.0f, 0.0f, cx, cy, cz, 0});
             const size_t n = static_cast<size_t>(L.nx) * L.ny * L.nz;
             float* pl = nullptr;
             float* rl = nullptr;
@@ -608,7 +612,8 @@ bool Scene::runMultigrid(std::string& err) {
             mgExec_ = nullptr;
         }
         const int levels = static_cast<int>(mgLevels_.size());
-        auto P = [&](int l) { return l == 0 ? pressure_ : mgP_[l - 1]; };
+        // Level 0's pressure is the double mgP0_; the coarser levels' are float.
+        auto P = [&](int l) { return mgP_[l - 1]; };
         auto R = [&](int l) { return l == 0 ? divergence_ : mgRhs_[l - 1]; };
         int count = 0;
         auto smooth = [&](int l, int sweeps) {
@@ -617,9 +622,14 @@ bool Scene::runMultigrid(std::string& err) {
             const int bx = rowThreads(half);
             const dim3 g((half + bx - 1) / bx, L.ny, L.nz);
             for (int k = 0; k < sweeps; ++k) {
-                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 0, nullptr);
-                mgSmooth<<<g, bx, 0, stream>>>(P(l), R(l), L, 1, nullptr);
-                count += 2;
+                for (int colour = 0; colour < 2; ++colour) {
+                    if (l == 0) {
+                        mgSmoothD<<<g, bx, 0, stream>>>(mgP0_, R(0), L, colour, nullptr);
+                    } else {
+                        mgSmoothF<<<g, bx, 0, stream>>>(P(l), R(l), L, colour, nullptr);
+                    }
+                    ++count;
+                }
             }
         };
         cudaGraph_t graph = nullptr;
@@ -646,7 +656,16 @@ bool Scene::runMultigrid(std::string& err) {
         cp.conditional.type = cudaGraphCondTypeWhile;
         cp.conditional.size = 1;
         cudaGraphNode_t condNode = nullptr;
-        e = cudaGraphAddNode(&condNode, graph, &reset, 1, &cp);
+        cudaGraphNode_t zeroP0 = nullptr;
+        cudaMemsetParams mz{};
+        mz.dst = mgP0_;
+        mz.value = 0;
+        mz.elementSize = 4;
+        mz.width = cells_ * 2;
+        mz.height = 1;
+        e = cudaGraphAddMemsetNode(&zeroP0, graph, &reset, 1, &mz);
+        if (e != cudaSuccess) return failGraph("multigrid level-0 reset node", e);
+        e = cudaGraphAddNode(&condNode, graph, &zeroP0, 1, &cp);
         if (e != cudaSuccess) return failGraph("multigrid loop node", e);
         cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(stream, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
@@ -656,32 +675,54 @@ bool Scene::runMultigrid(std::string& err) {
             const MgLevel& F = mgLevels_[l];
             const MgLevel& C = mgLevels_[l + 1];
             const int bx = rowThreads(C.nx);
-            mgRestrict<<<dim3((C.nx + bx - 1) / bx, C.ny, C.nz), bx, 0, stream>>>(R(l + 1), P(l + 1), P(l), R(l), F, C, nullptr);
+            const dim3 rg((C.nx + bx - 1) / bx, C.ny, C.nz);
+            if (l == 0) {
+                mgRestrictD<<<rg, bx, 0, stream>>>(R(1), P(1), mgP0_, R(0), F, C, nullptr);
+            } else {
+                mgRestrictF<<<rg, bx, 0, stream>>>(R(l + 1), P(l + 1), P(l), R(l), F, C, nullptr);
+            }
             ++count;
         }
-        mgCoarsest<<<1, 256, 0, stream>>>(P(levels - 1), R(levels - 1), mgLevels_[levels - 1], kMgCoarsestSweeps, nullptr);
+        if (levels == 1) {
+            mgCoarsestD<<<1, 256, 0, stream>>>(mgP0_, R(0), mgLevels_[0], kMgCoarsestSweeps, nullptr);
+        } else {
+            mgCoarsestF<<<1, 256, 0, stream>>>(P(levels - 1), R(levels - 1), mgLevels_[levels - 1], kMgCoarsestSweeps, nullptr);
+        }
         ++count;
         for (int l = levels - 2; l >= 0; --l) {
             const MgLevel& F = mgLevels_[l];
             const MgLevel& C = mgLevels_[l + 1];
             const int bx = rowThreads(F.nx);
-            mgProlong<<<dim3((F.nx + bx - 1) / bx, F.ny, F.nz), bx, 0, stream>>>(P(l), P(l + 1), F, C, nullptr);
+            const dim3 pg((F.nx + bx - 1) / bx, F.ny, F.nz);
+            if (l == 0) {
+                mgProlongD<<<pg, bx, 0, stream>>>(mgP0_, P(1), F, C, nullptr);
+            } else {
+                mgProlongF<<<pg, bx, 0, stream>>>(P(l), P(l + 1), F, C, nullptr);
+            }
             ++count;
             smooth(l, mgPost_);
         }
         if (gated) {
-            mgResidualPartials<<<kResidualBlocks, kResidualThreads, 0, stream>>>(pressure_, divergence_, mgLevels_[0], sorGate_,
-                                                                               residualSq_, residualMax_);
+            mgResidualPartialsD<<<kResidualBlocks, kResidualThreads, 0, stream>>>(mgP0_, divergence_, mgLevels_[0], sorGate_,
+                                                                                       residualSq_, residualMax_);
             ++count;
         }
         mgCycleEnd<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks, static_cast<float>(pressureTolerance_),
                                          gated ? 1 : 0, mgCycles_, loop);
         ++count;
-        const cudaError_t launchErr = cudaGetLastError();
+        cudaError_t launchErr = cudaGetLastError();
         cudaGraph_t captured = nullptr;
-        const cudaError_t endErr = cudaStreamEndCapture(stream, &captured);
+        cudaError_t endErr = cudaStreamEndCapture(stream, &captured);
         if (launchErr != cudaSuccess) return failGraph("multigrid body launch", launchErr);
         if (endErr != cudaSuccess) return failGraph("multigrid body capture end", endErr);
+        // After the loop: the float pressure field from the double level-0 pressure.
+        e = cudaStreamBeginCaptureToGraph(stream, graph, &condNode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return failGraph("multigrid store capture begin", e);
+        mgStoreFloat<<<kResidualBlocks, 256, 0, stream>>>(pressure_, mgP0_, static_cast<int>(cells_));
+        launchErr = cudaGetLastError();
+        endErr = cudaStreamEndCapture(stream, &captured);
+        if (launchErr != cudaSuccess) return failGraph("multigrid store launch", launchErr);
+        if (endErr != cudaSuccess) return failGraph("multigrid store capture end", endErr);
         const cudaError_t instErr = cudaGraphInstantiate(&mgExec_, graph, 0);
         cudaGraphDestroy(graph);
         if (!check("multigrid graph instantiate", instErr, err)) return false;
@@ -692,9 +733,10 @@ bool Scene::runMultigrid(std::string& err) {
         mgGraphLaunches_ = count;  // per V-cycle
     }
     // The launch count cannot know how many cycles will run; it counts one V-cycle's kernels.
-    launches_ += static_cast<unsigned long long>(mgGraphLaunches_);
+    launches_ += static_cast<unsigned long long>(mgGraphLaunches_) + 1;
     lastSolveGated_ = true;
     lastPressurePath_ = 3;
+    mgP0Valid_ = true;
     return check("multigrid graph launch", cudaGraphLaunch(mgExec_, stream), err);
 }
 
@@ -1222,6 +1264,7 @@ bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
 }
 
 bool Scene::setField(int field, const void* host, size_t bytes, std::string& err) {
+    if (field == FIRE_FIELD_PRESSURE) mgP0Valid_ = false;  // the field, not an older solve, is the pressure now
     FaceT* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
     FieldView v;
     if (field == FIRE_FIELD_CONFIG_TRANSMITTANCE) {
@@ -1561,9 +1604,15 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                 if (!runSor(p, err)) return false;
                 break;
             case kSubtract:
-                subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 1, last >= kWallBoundary ? 1 : 0); ++launches_;
-                if (physics_.pressureTop == 1) {
-                    cfgTopFaces<<<dim3((nx + bx - 1) / bx, nz), bx, 0, stream>>>(vel_[1][vcur_], pressure_, nx, ny, nz); ++launches_;
+                if (physics_.pressureTop == 1 && mgP0Valid_) {
+                    // The Dirichlet top's solve left its pressure in double: subtract from that.
+                    cfgSubtractWide<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], mgP0_, nx, ny, nz,
+                                                            last >= kWallBoundary ? 1 : 0); ++launches_;
+                } else {
+                    subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 1, last >= kWallBoundary ? 1 : 0); ++launches_;
+                    if (physics_.pressureTop == 1) {
+                        cfgTopFaces<<<dim3((nx + bx - 1) / bx, nz), bx, 0, stream>>>(vel_[1][vcur_], pressure_, nx, ny, nz); ++launches_;
+                    }
                 }
                 if (last >= kWallBoundary) ++s;
                 break;
@@ -1603,6 +1652,7 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                            cudaMemsetAsync(cfgLight_, 0, static_cast<size_t>(cfgLx_) * cfgLy_ * cfgLz_ * sizeof(float), stream), err);
                 if (!ok) return false;
                 cfgStep_ = 0;
+                mgP0Valid_ = false;
                 break;
             }
             default:

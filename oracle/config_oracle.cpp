@@ -76,6 +76,7 @@ template <class T>
 struct Scene {
     int nx, ny, nz, lx, ly, lz, W, H;
     std::vector<T> heat, fuel, soot, u, v, w, pressure, divergence, transmittance, hdr;
+    std::vector<double> p64;  // the multigrid's level-0 pressure (Dirichlet top), in double
     std::vector<T> vort;   // 4 per cell
     std::vector<T> force;  // 3 per cell
     FirePhysicsParams phys;
@@ -107,6 +108,7 @@ struct Scene {
         transmittance.assign(size_t(lx) * ly * lz, T(0));
         hdr.assign(size_t(W) * H * 4, T(0));
         vort.assign(n * 4, T(0));
+        p64.clear();
         force.assign(n * 3, T(0));
         step = 0;
     }
@@ -489,6 +491,7 @@ struct Lvl {
     int nx, ny, nz;
     T wx, wy, wz, diag, invDiag;
     int cx, cy, cz;
+    int wide;  // level 0: smoothing and residuals evaluated in double, p stored in T
     int at(int x, int y, int z) const { return (z * ny + y) * nx + x; }
 };
 
@@ -498,23 +501,25 @@ template <class T> Lvl<T> withWeights(Lvl<T> L) {
     return L;
 }
 
-template <class T> T wsum(const std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z, T self) {
+// The level operations in the level's pressure type P (double on level 0,
+// T on the coarser levels), as the product's fire_mg.cu.
+template <class P, class T> P wsum(const std::vector<P>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z, P self) {
     const int i = L.at(x, y, z);
-    const T pL = x > 0 ? p[i - 1] : self;
-    const T pR = x < L.nx - 1 ? p[i + 1] : self;
-    const T pD = y > 0 ? p[i - L.nx] : self;
-    const T pU = y < L.ny - 1 ? p[i + L.nx] : T(0) - self;
-    const T pB = z > 0 ? p[i - L.nx * L.ny] : self;
-    const T pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
-    return rhs[i] + L.wx * (pL + pR) + L.wy * (pD + pU) + L.wz * (pB + pF);
+    const P pL = x > 0 ? p[i - 1] : self;
+    const P pR = x < L.nx - 1 ? p[i + 1] : self;
+    const P pD = y > 0 ? p[i - L.nx] : self;
+    const P pU = y < L.ny - 1 ? p[i + L.nx] : P(0) - self;
+    const P pB = z > 0 ? p[i - L.nx * L.ny] : self;
+    const P pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
+    return P(rhs[i]) + P(L.wx) * (pL + pR) + P(L.wy) * (pD + pU) + P(L.wz) * (pB + pF);
 }
 
-template <class T> T resAt(const std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z) {
-    const T self = p[L.at(x, y, z)];
-    return wsum(p, rhs, L, x, y, z, self) - L.diag * self;
+template <class P, class T> P resAt(const std::vector<P>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z) {
+    const P self = p[L.at(x, y, z)];
+    return wsum(p, rhs, L, x, y, z, self) - P(L.diag) * self;
 }
 
-template <class T> void mgSmooth(std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L, int sweeps) {
+template <class P, class T> void mgSmooth(std::vector<P>& p, const std::vector<T>& rhs, const Lvl<T>& L, int sweeps) {
     for (int k = 0; k < sweeps; ++k) {
         for (int colour = 0; colour < 2; ++colour) {
 #pragma omp parallel for collapse(2) schedule(static)
@@ -522,7 +527,7 @@ template <class T> void mgSmooth(std::vector<T>& p, const std::vector<T>& rhs, c
                 for (int y = 0; y < L.ny; ++y) {
                     for (int x = (colour + y + z) & 1; x < L.nx; x += 2) {
                         const int i = L.at(x, y, z);
-                        p[i] = wsum(p, rhs, L, x, y, z, p[i]) * L.invDiag;
+                        p[i] = wsum(p, rhs, L, x, y, z, p[i]) * P(L.invDiag);
                     }
                 }
             }
@@ -530,23 +535,63 @@ template <class T> void mgSmooth(std::vector<T>& p, const std::vector<T>& rhs, c
     }
 }
 
-template <class T> T residualMax(const std::vector<T>& p, const std::vector<T>& rhs, const Lvl<T>& L) {
-    T m = T(0);
+// max |r| as the GPU reduces it: |r| in the level's type, rounded to float.
+template <class P, class T> float residualMax(const std::vector<P>& p, const std::vector<T>& rhs, const Lvl<T>& L) {
+    float m = 0.0f;
     for (int z = 0; z < L.nz; ++z)
         for (int y = 0; y < L.ny; ++y)
-            for (int x = 0; x < L.nx; ++x) m = std::fmax(m, std::fabs(resAt(p, rhs, L, x, y, z)));
+            for (int x = 0; x < L.nx; ++x) m = std::fmax(m, float(std::fabs(double(resAt(p, rhs, L, x, y, z)))));
     return m;
 }
 
+// Coarse rhs at (X, Y, Z): the mean residual of the covered fine cells in the fine level's type.
+template <class P, class T>
+T restrictMean(const std::vector<P>& pf, const std::vector<T>& rf, const Lvl<T>& F, const Lvl<T>& C, int X, int Y, int Z) {
+    const int x0 = C.cx ? 2 * X : X, y0 = C.cy ? 2 * Y : Y, z0 = C.cz ? 2 * Z : Z;
+    const P half = P(0.5f);
+    P az[2] = {P(0), P(0)};
+    for (int dz = 0; dz <= C.cz; ++dz) {
+        P ay[2] = {P(0), P(0)};
+        for (int dy = 0; dy <= C.cy; ++dy) {
+            const P a = resAt(pf, rf, F, x0, y0 + dy, z0 + dz);
+            ay[dy] = C.cx ? half * (a + resAt(pf, rf, F, x0 + 1, y0 + dy, z0 + dz)) : a;
+        }
+        az[dz] = C.cy ? half * (ay[0] + ay[1]) : ay[0];
+    }
+    return T(C.cz ? half * (az[0] + az[1]) : az[0]);
+}
+
+// p += the coarse correction (evaluated in T) interpolated along the halved axes.
+template <class P, class T> void prolong(std::vector<P>& pf, const std::vector<T>& pc, const Lvl<T>& F, const Lvl<T>& C) {
+    const T ux = C.cx ? T(0.75f) : T(1), vx = C.cx ? T(0.25f) : T(0);
+    const T uy = C.cy ? T(0.75f) : T(1), vy = C.cy ? T(0.25f) : T(0);
+    const T uz = C.cz ? T(0.75f) : T(1), vz = C.cz ? T(0.25f) : T(0);
+    for (int z = 0; z < F.nz; ++z)
+        for (int y = 0; y < F.ny; ++y)
+            for (int x = 0; x < F.nx; ++x) {
+                const int X0 = C.cx ? x >> 1 : x, Y0 = C.cy ? y >> 1 : y, Z0 = C.cz ? z >> 1 : z;
+                const int X1 = !C.cx ? X0 : ((x & 1) ? std::min(X0 + 1, C.nx - 1) : std::max(X0 - 1, 0));
+                const int Y1 = !C.cy ? Y0 : ((y & 1) ? std::min(Y0 + 1, C.ny - 1) : std::max(Y0 - 1, 0));
+                const int Z1 = !C.cz ? Z0 : ((z & 1) ? std::min(Z0 + 1, C.nz - 1) : std::max(Z0 - 1, 0));
+                const T a0 = ux * pc[C.at(X0, Y0, Z0)] + vx * pc[C.at(X1, Y0, Z0)];
+                const T a1 = ux * pc[C.at(X0, Y1, Z0)] + vx * pc[C.at(X1, Y1, Z0)];
+                const T a2 = ux * pc[C.at(X0, Y0, Z1)] + vx * pc[C.at(X1, Y0, Z1)];
+                const T a3 = ux * pc[C.at(X0, Y1, Z1)] + vx * pc[C.at(X1, Y1, Z1)];
+                const T b0 = uy * a0 + vy * a1, b1 = uy * a2 + vy * a3;
+                const int i = F.at(x, y, z);
+                pf[i] = pf[i] + P(uz * b0 + vz * b1);
+            }
+}
+
 template <class T> void multigrid(Scene<T>& s) {
-    std::vector<Lvl<T>> lv{withWeights(Lvl<T>{s.nx, s.ny, s.nz, T(1), T(1), T(1), T(0), T(0), 0, 0, 0})};
+    std::vector<Lvl<T>> lv{withWeights(Lvl<T>{s.nx, s.ny, s.nz, T(1), T(1), T(1), T(0), T(0), 0, 0, 0, 1})};
     while (lv.size() < 10) {
         const Lvl<T> b = lv.back();
         const int cx = b.nx % 2 == 0 && b.nx >= 4, cy = b.ny % 2 == 0 && b.ny >= 4, cz = b.nz % 2 == 0 && b.nz >= 4;
         if (!cx && !cy && !cz) break;
         lv.push_back(withWeights(Lvl<T>{cx ? b.nx / 2 : b.nx, cy ? b.ny / 2 : b.ny, cz ? b.nz / 2 : b.nz,
                                         cx ? b.wx * T(0.25f) : b.wx, cy ? b.wy * T(0.25f) : b.wy, cz ? b.wz * T(0.25f) : b.wz,
-                                        T(0), T(0), cx, cy, cz}));
+                                        T(0), T(0), cx, cy, cz, 0}));
     }
     const int n = int(lv.size());
     std::vector<std::vector<T>> P(n), R(n);
@@ -554,69 +599,65 @@ template <class T> void multigrid(Scene<T>& s) {
         P[l].assign(size_t(lv[l].nx) * lv[l].ny * lv[l].nz, T(0));
         R[l].assign(P[l].size(), T(0));
     }
-    std::vector<T>& p0 = s.pressure;
+    // Level 0: the pressure in double, from zero; rhs the divergence array.
+    std::vector<double>& p0 = s.p64;
+    p0.assign(size_t(s.cells()), 0.0);
     const std::vector<T>& r0 = s.divergence;
-    auto Pl = [&](int l) -> std::vector<T>& { return l == 0 ? p0 : P[l]; };
-    auto Rl = [&](int l) -> const std::vector<T>& { return l == 0 ? r0 : R[l]; };
-    const T half = T(0.5f);
     s.mgCyclesRun = 0;
     s.mgMaxResidual = -1.0f;
     for (int c = 0; c < s.mgCycles; ++c) {
         for (int l = 0; l + 1 < n; ++l) {
-            mgSmooth(Pl(l), Rl(l), lv[l], s.mgPre);
             const Lvl<T>& F = lv[l];
             const Lvl<T>& C = lv[l + 1];
-            const std::vector<T>& pf = Pl(l);
-            const std::vector<T>& rf = Rl(l);
+            if (l == 0) {
+                mgSmooth(p0, r0, F, s.mgPre);
+            } else {
+                mgSmooth(P[l], R[l], F, s.mgPre);
+            }
             for (int Z = 0; Z < C.nz; ++Z)
                 for (int Y = 0; Y < C.ny; ++Y)
                     for (int X = 0; X < C.nx; ++X) {
-                        const int x0 = C.cx ? 2 * X : X, y0 = C.cy ? 2 * Y : Y, z0 = C.cz ? 2 * Z : Z;
-                        T az[2];
-                        for (int dz = 0; dz <= C.cz; ++dz) {
-                            T ay[2];
-                            for (int dy = 0; dy <= C.cy; ++dy) {
-                                const T a = resAt(pf, rf, F, x0, y0 + dy, z0 + dz);
-                                ay[dy] = C.cx ? half * (a + resAt(pf, rf, F, x0 + 1, y0 + dy, z0 + dz)) : a;
-                            }
-                            az[dz] = C.cy ? half * (ay[0] + ay[1]) : ay[0];
-                        }
-                        R[l + 1][C.at(X, Y, Z)] = C.cz ? half * (az[0] + az[1]) : az[0];
+                        R[l + 1][C.at(X, Y, Z)] = l == 0 ? restrictMean(p0, r0, F, C, X, Y, Z) : restrictMean(P[l], R[l], F, C, X, Y, Z);
                         P[l + 1][C.at(X, Y, Z)] = T(0);
                     }
         }
-        mgSmooth(Pl(n - 1), Rl(n - 1), lv[n - 1], 32);
+        if (n == 1) {
+            mgSmooth(p0, r0, lv[0], 32);
+        } else {
+            mgSmooth(P[n - 1], R[n - 1], lv[n - 1], 32);
+        }
         for (int l = n - 2; l >= 0; --l) {
-            const Lvl<T>& F = lv[l];
-            const Lvl<T>& C = lv[l + 1];
-            std::vector<T>& pf = Pl(l);
-            const std::vector<T>& pc = P[l + 1];
-            const T ux = C.cx ? T(0.75f) : T(1), vx = C.cx ? T(0.25f) : T(0);
-            const T uy = C.cy ? T(0.75f) : T(1), vy = C.cy ? T(0.25f) : T(0);
-            const T uz = C.cz ? T(0.75f) : T(1), vz = C.cz ? T(0.25f) : T(0);
-            for (int z = 0; z < F.nz; ++z)
-                for (int y = 0; y < F.ny; ++y)
-                    for (int x = 0; x < F.nx; ++x) {
-                        const int X0 = C.cx ? x >> 1 : x, Y0 = C.cy ? y >> 1 : y, Z0 = C.cz ? z >> 1 : z;
-                        const int X1 = !C.cx ? X0 : ((x & 1) ? std::min(X0 + 1, C.nx - 1) : std::max(X0 - 1, 0));
-                        const int Y1 = !C.cy ? Y0 : ((y & 1) ? std::min(Y0 + 1, C.ny - 1) : std::max(Y0 - 1, 0));
-                        const int Z1 = !C.cz ? Z0 : ((z & 1) ? std::min(Z0 + 1, C.nz - 1) : std::max(Z0 - 1, 0));
-                        const T a0 = ux * pc[C.at(X0, Y0, Z0)] + vx * pc[C.at(X1, Y0, Z0)];
-                        const T a1 = ux * pc[C.at(X0, Y1, Z0)] + vx * pc[C.at(X1, Y1, Z0)];
-                        const T a2 = ux * pc[C.at(X0, Y0, Z1)] + vx * pc[C.at(X1, Y0, Z1)];
-                        const T a3 = ux * pc[C.at(X0, Y1, Z1)] + vx * pc[C.at(X1, Y1, Z1)];
-                        const T b0 = uy * a0 + vy * a1, b1 = uy * a2 + vy * a3;
-                        const int i = F.at(x, y, z);
-                        pf[i] = pf[i] + (uz * b0 + vz * b1);
-                    }
-            mgSmooth(pf, Rl(l), F, s.mgPost);
+            if (l == 0) {
+                prolong(p0, P[1], lv[0], lv[1]);
+                mgSmooth(p0, r0, lv[0], s.mgPost);
+            } else {
+                prolong(P[l], P[l + 1], lv[l], lv[l + 1]);
+                mgSmooth(P[l], R[l], lv[l], s.mgPost);
+            }
         }
         ++s.mgCyclesRun;
         if (s.mgTolerance > 0.0f) {
-            s.mgMaxResidual = float(residualMax(p0, r0, lv[0]));
+            s.mgMaxResidual = residualMax(p0, r0, lv[0]);
             if (s.mgMaxResidual <= s.mgTolerance) break;
         }
     }
+    for (size_t i = 0; i < p0.size(); ++i) s.pressure[i] = T(p0[i]);
+}
+
+// The gradient subtraction from the multigrid's double pressure (Dirichlet
+// top): each face difference in double, rounded once to T; top faces with the
+// antisymmetric ghost -p.
+template <class T> void subtractWide(Scene<T>& s) {
+    const std::vector<double>& pr = s.p64;
+    for (int z = 0; z < s.nz; ++z)
+        for (int y = 0; y < s.ny; ++y)
+            for (int x = 0; x < s.nx; ++x) {
+                const double pc = pr[size_t(s.sI(x, y, z))];
+                if (x > 0) s.u[size_t(s.uI(x, y, z))] -= T(pc - pr[size_t(s.sI(x - 1, y, z))]);
+                if (y > 0) s.v[size_t(s.vI(x, y, z))] -= T(pc - pr[size_t(s.sI(x, y - 1, z))]);
+                if (z > 0) s.w[size_t(s.wI(x, y, z))] -= T(pc - pr[size_t(s.sI(x, y, z - 1))]);
+                if (y == s.ny - 1) s.v[size_t(s.vI(x, s.ny, z))] -= T((0.0 - pc) - pc);
+            }
 }
 
 template <class T> void walls(Scene<T>& s) {
@@ -752,15 +793,19 @@ template <class T> int runStages(Scene<T>& s, int first, int last) {
                 }
                 break;
             case FIRE_STAGE_SUBTRACT:
-                subtract(s);
-                if (s.phys.pressureTop == 1) {
-                    // The top faces: v(x, ny, z) -= (ghost - p) with the antisymmetric ghost -p.
-                    for (int z = 0; z < s.nz; ++z)
-                        for (int x = 0; x < s.nx; ++x) {
-                            T& v = s.v[size_t(s.vI(x, s.ny, z))];
-                            const T top = s.pressure[size_t(s.sI(x, s.ny - 1, z))];
-                            v = v - ((T(0) - top) - top);
-                        }
+                if (s.phys.pressureTop == 1 && s.p64.size() == size_t(s.cells())) {
+                    subtractWide(s);
+                } else {
+                    subtract(s);
+                    if (s.phys.pressureTop == 1) {
+                        // No multigrid pressure: the top faces from the float field, ghost -p.
+                        for (int z = 0; z < s.nz; ++z)
+                            for (int x = 0; x < s.nx; ++x) {
+                                T& v = s.v[size_t(s.vI(x, s.ny, z))];
+                                const T top = s.pressure[size_t(s.sI(x, s.ny - 1, z))];
+                                v = v - ((T(0) - top) - top);
+                            }
+                    }
                 }
                 if (last >= FIRE_STAGE_WALL_BOUNDARY) {
                     walls(s);
@@ -881,6 +926,7 @@ int cfg_oracle_set_field(void* o, int field, const void* host, long long bytes) 
         } else {
             const float* in = static_cast<const float*>(host);
             for (size_t i = 0; i < f->size(); ++i) (*f)[i] = in[i];
+            if (field == FIRE_FIELD_PRESSURE) s.p64.clear();
         }
     });
     return rc;
