@@ -445,8 +445,9 @@ def config_stage_timings(sim, settings, steps: int = 3) -> dict:
     return out
 
 
-def config_cpu_baseline(pkg, w, n_steps: int = 2) -> dict:
-    """The config-physics oracle (float, OpenMP, all host threads) on a bounded sample."""
+def config_cpu_baseline(pkg, w, n_steps: int = 2, args=None) -> dict:
+    """The config-physics oracle (float, OpenMP, all host threads) on a bounded
+    sample, with the same pressure solver as the GPU line."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as om  # noqa: PLC0415
     abi = pkg.abi
@@ -454,6 +455,8 @@ def config_cpu_baseline(pkg, w, n_steps: int = 2) -> dict:
     o = om.ConfigOracle(abi, w["frame"][0], w["frame"][1], *n)
     o.set_physics(w["physics"])
     o.set_pressure_solver(*w["sor"])
+    if args is not None and args.solver == "mg":
+        o.set_multigrid(args.mg_cycles, 2, 2, 0.5 * args.div_target)
     threads = os.cpu_count() or 1
     om.OracleFire.set_threads(threads)
     o.step()
@@ -468,7 +471,8 @@ def config_cpu_baseline(pkg, w, n_steps: int = 2) -> dict:
     cells = int(np.prod(n))
     return {"value": cells / per_step, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
             "sample": f"{n_steps} config-physics steps of the {w['name']} workload after one warm-up step, plus one "
-                      f"{w['frame'][0]}^2 render amortised over {w['render_every']} steps (oracle/config_oracle.cpp, float)",
+                      f"{w['frame'][0]}^2 render amortised over {w['render_every']} steps (oracle/config_oracle.cpp, float"
+                      f"{', multigrid' if args is not None and args.solver == 'mg' else ''})",
             "seconds_per_step": per_step}
 
 
@@ -614,7 +618,7 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
                 "bytes_per_launch": bytes_launch, "launch_ms": launch_ms}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = config_cpu_baseline(pkg, w)
+        cb = config_cpu_baseline(pkg, w, args=args)
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         p = w["physics"]
