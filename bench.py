@@ -857,8 +857,11 @@ def ctypes_sizeof_settings(abi) -> int:
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the
-# dominant kernel, from one ncu capture of this workload (128^3, SOR 60).
-NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): 30157312 + 1525760}
+# dominant kernel, from one ncu capture of each workload: the resident solve at
+# 128^3 (one launch, SOR 60) and one colour-split half sweep at 256^3
+# (profiles/sor_split_256cubed_halfsweep.md: 4.72 TB/s x 23.42 us).
+NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): 30157312 + 1525760,
+                     ("pressure_sor", "split", 256, 60): 110542400}
 
 
 def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str, sor_path: int) -> dict:
@@ -867,14 +870,14 @@ def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_
     The pressure solve's algorithmic bytes are those of the global-memory
     formulation, 12 B per cell per iteration (read p, write p, read div).  The
     resident path runs the whole solve as one launch, so its launch carries
-    all N iterations; the per-launch path has one launch per half sweep."""
+    all N iterations; the colour-split path has one launch per half sweep."""
     traffic = None
     if dominant == "pressure_sor":
         resident = sor_path == 2
         launches = 1 if resident else 2 * args.sor_iters
         per_launch_ms = st["pressure_sor"] / launches
         bytes_per_launch = 12.0 * args.sor_iters * cells / launches
-        traffic = NCU_TRAFFIC_BYTES.get(("pressure_sor", "resident" if resident else "graph", args.grid, args.sor_iters))
+        traffic = NCU_TRAFFIC_BYTES.get(("pressure_sor", "resident" if resident else "split", args.grid, args.sor_iters))
     elif dominant in STAGE_BYTES_PER_CELL and STAGE_BYTES_PER_CELL[dominant] > 0:
         per_launch_ms = st[dominant]
         bytes_per_launch = STAGE_BYTES_PER_CELL[dominant] * cells

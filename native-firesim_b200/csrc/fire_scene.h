@@ -65,7 +65,7 @@ public:
     bool setActiveSlot(int slot, std::string& err);
     void clearSlots();
     bool setPressureSolver(int iterations, float omega, std::string& err);
-    // 0 = automatic (shared-memory-resident when the grid fits co-resident), 1 = one launch per half sweep, 2 = resident only.
+    // 0 = automatic (shared-memory-resident when the grid fits co-resident), 1 = colour-split, 2 = resident only.
     bool setPressurePath(int path, std::string& err);
     int lastPressurePath() const { return lastPressurePath_; }
     // Fault injection for the resident SOR's bounded waits: brick `silentBrick`
