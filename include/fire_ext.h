@@ -274,7 +274,9 @@ typedef struct FirePhysicsParams {
  * maxCycles V-cycles per step, each with preSmooth / postSmooth red-black
  * Gauss-Seidel sweeps per level (1..8); with fireCudaSetPressureTolerance
  * set, the level-0 residual is checked after every cycle and the solve stops
- * once max |r| <= tolerance (fireCudaGetPressureStats counts cycles).
+ * once max |r| <= tolerance (fireCudaGetPressureStats counts cycles).  Level 0
+ * holds the pressure in double, and each solve starts from the previous one's
+ * (from zero after a reset or a write of FIRE_FIELD_PRESSURE).
  * maxCycles = 0 restores the red-black SOR. */
 FIRE_API bool fireCudaSetPressureMultigrid(int maxCycles, int preSmooth, int postSmooth);
 

@@ -570,8 +570,9 @@ bool Scene::setPressureMultigrid(int maxCycles, int preSmooth, int postSmooth, s
     return true;
 }
 
-// The multigrid solve (fire_mg.cu) as one CUDA graph per (cycles, smoothing,
-// tolerance): a memset of the gate, then a conditional WHILE node whose body
+// The multigrid solve (fire_mg.cu), warm-started from the previous solve's
+// level-0 pressure, as one CUDA graph per (cycles, smoothing, tolerance): a
+// memset of the gate, then a conditional WHILE node whose body
 // is one V-cycle, the level-0 residual partials (with a tolerance) and
 // mgCycleEnd, which clears the loop condition when the solve has converged or
 // run maxCycles cycles -- a converged solve launches nothing more.
@@ -656,16 +657,7 @@ bool Scene::runMultigrid(std::string& err) {
         cp.conditional.type = cudaGraphCondTypeWhile;
         cp.conditional.size = 1;
         cudaGraphNode_t condNode = nullptr;
-        cudaGraphNode_t zeroP0 = nullptr;
-        cudaMemsetParams mz{};
-        mz.dst = mgP0_;
-        mz.value = 0;
-        mz.elementSize = 4;
-        mz.width = cells_ * 2;
-        mz.height = 1;
-        e = cudaGraphAddMemsetNode(&zeroP0, graph, &reset, 1, &mz);
-        if (e != cudaSuccess) return failGraph("multigrid level-0 reset node", e);
-        e = cudaGraphAddNode(&condNode, graph, &zeroP0, 1, &cp);
+        e = cudaGraphAddNode(&condNode, graph, &reset, 1, &cp);
         if (e != cudaSuccess) return failGraph("multigrid loop node", e);
         cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(stream, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
@@ -731,6 +723,11 @@ bool Scene::runMultigrid(std::string& err) {
         mgKeyPost_ = mgPost_;
         mgKeyTol_ = tolKey;
         mgGraphLaunches_ = count;  // per V-cycle
+    }
+    // Warm start: the solve starts from the previous solve's double pressure;
+    // after a reset or a write of the pressure field, from zero.
+    if (!mgP0Valid_ && !check("clear multigrid level-0 pressure", cudaMemsetAsync(mgP0_, 0, cells_ * sizeof(double), stream), err)) {
+        return false;
     }
     // The launch count cannot know how many cycles will run; it counts one V-cycle's kernels.
     launches_ += static_cast<unsigned long long>(mgGraphLaunches_) + 1;

@@ -193,7 +193,7 @@ private:
     std::vector<MgLevel> mgLevels_;
     std::vector<float*> mgP_, mgRhs_;  // levels >= 1
     double* mgP0_ = nullptr;           // level-0 pressure in double (the float field is written from it)
-    bool mgP0Valid_ = false;           // mgP0_ holds the latest solve's pressure
+    bool mgP0Valid_ = false;           // mgP0_ holds the latest solve's pressure (the next solve starts from it)
     cudaGraphExec_t mgExec_ = nullptr;
     int mgKeyCycles_ = -1, mgKeyPre_ = -1, mgKeyPost_ = -1, mgGraphLaunches_ = 0;
     double mgKeyTol_ = -1.0;

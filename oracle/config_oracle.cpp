@@ -599,9 +599,10 @@ template <class T> void multigrid(Scene<T>& s) {
         P[l].assign(size_t(lv[l].nx) * lv[l].ny * lv[l].nz, T(0));
         R[l].assign(P[l].size(), T(0));
     }
-    // Level 0: the pressure in double, from zero; rhs the divergence array.
+    // Level 0: the pressure in double, warm-started from the previous solve (from zero
+    // after a reset or a write of the pressure field); rhs the divergence array.
     std::vector<double>& p0 = s.p64;
-    p0.assign(size_t(s.cells()), 0.0);
+    if (p0.size() != size_t(s.cells())) p0.assign(size_t(s.cells()), 0.0);
     const std::vector<T>& r0 = s.divergence;
     s.mgCyclesRun = 0;
     s.mgMaxResidual = -1.0f;
