@@ -332,6 +332,33 @@ bool fireCudaGetLaunchCount(unsigned long long* count) {
 
 const char* fireCudaBuildInfo(void) { return "firesim-b200 sm_100a"; }
 
+// The reference declares its seventeen entry points with C++ linkage in the
+// global namespace (src/fire_cuda.h:102-118), so a caller built against that
+// header links against their mangled names.  A const FireSettings& passes as
+// a pointer, so each mangled name is an alias of the C entry point above:
+// such a caller links against this library without being recompiled.
+#define FIRE_CXX_ALIAS(mangled, target) __attribute__((alias(#target), visibility("default")))
+FIRE_API bool _Z18fireCudaInitializeiiii(int, int, int, int) FIRE_CXX_ALIAS(_, fireCudaInitialize);
+FIRE_API bool _Z21fireCudaStepAndRenderPjRK12FireSettings(uint32_t*, const FireSettings&) FIRE_CXX_ALIAS(_, fireCudaStepAndRender);
+FIRE_API bool _Z29fireCudaStepAndRenderMeasuredPjRK12FireSettingsP20FireCudaFrameMetrics(uint32_t*, const FireSettings&, FireCudaFrameMetrics*)
+    FIRE_CXX_ALIAS(_, fireCudaStepAndRenderMeasured);
+FIRE_API bool _Z28fireCudaSelectDeviceForD3D11Pv(void*) FIRE_CXX_ALIAS(_, fireCudaSelectDeviceForD3D11);
+FIRE_API bool _Z28fireCudaRegisterD3D11TexturePv(void*) FIRE_CXX_ALIAS(_, fireCudaRegisterD3D11Texture);
+FIRE_API bool _Z32fireCudaRegisterD3D11TextureSlotiPv(int, void*) FIRE_CXX_ALIAS(_, fireCudaRegisterD3D11TextureSlot);
+FIRE_API bool _Z27fireCudaSetD3D11TextureSloti(int) FIRE_CXX_ALIAS(_, fireCudaSetD3D11TextureSlot);
+FIRE_API bool _Z17fireCudaStepD3D11RK12FireSettings(const FireSettings&) FIRE_CXX_ALIAS(_, fireCudaStepD3D11);
+FIRE_API bool _Z26fireCudaStepAndRenderD3D11RK12FireSettings(const FireSettings&) FIRE_CXX_ALIAS(_, fireCudaStepAndRenderD3D11);
+FIRE_API bool _Z34fireCudaStepAndRenderD3D11MeasuredRK12FireSettingsP20FireCudaFrameMetrics(const FireSettings&, FireCudaFrameMetrics*)
+    FIRE_CXX_ALIAS(_, fireCudaStepAndRenderD3D11Measured);
+FIRE_API bool _Z19fireCudaRenderD3D11RK12FireSettings(const FireSettings&) FIRE_CXX_ALIAS(_, fireCudaRenderD3D11);
+FIRE_API void _Z30fireCudaUnregisterD3D11Texturev(void) FIRE_CXX_ALIAS(_, fireCudaUnregisterD3D11Texture);
+FIRE_API bool _Z19fireCudaSynchronizev(void) FIRE_CXX_ALIAS(_, fireCudaSynchronize);
+FIRE_API bool _Z13fireCudaResetv(void) FIRE_CXX_ALIAS(_, fireCudaReset);
+FIRE_API bool _Z22fireCudaGetDiagnosticsP19FireCudaDiagnostics(FireCudaDiagnostics*) FIRE_CXX_ALIAS(_, fireCudaGetDiagnostics);
+FIRE_API void _Z16fireCudaShutdownv(void) FIRE_CXX_ALIAS(_, fireCudaShutdown);
+FIRE_API const char* _Z17fireCudaLastErrorv(void) FIRE_CXX_ALIAS(_, fireCudaLastError);
+#undef FIRE_CXX_ALIAS
+
 }  // extern "C"
 
 namespace firesim {

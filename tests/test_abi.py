@@ -109,3 +109,65 @@ def test_struct_offsets_match_the_header(abi, struct, tmp_path):
     assert int(got["size"]) == ctypes.sizeof(cls)
     for name, _ in cls._fields_:
         assert int(got[name]) == getattr(cls, name).offset, name
+
+
+def test_callers_of_the_reference_header_link_unchanged(tmp_path):
+    """A C++ caller compiled against declarations with the reference header's
+    C++ linkage (src/fire_cuda.h:102-118) links against libfiresim_b200.so
+    through the exported mangled aliases and gets the reference's messages."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("g++ not found")
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+struct FireSettings { unsigned char bytes[176]; };
+struct FireCudaFrameMetrics; struct FireCudaDiagnostics;
+bool fireCudaInitialize(int, int, int, int);
+bool fireCudaStepAndRender(std::uint32_t*, const FireSettings&);
+bool fireCudaStepAndRenderMeasured(std::uint32_t*, const FireSettings&, FireCudaFrameMetrics*);
+bool fireCudaSelectDeviceForD3D11(void*);
+bool fireCudaRegisterD3D11Texture(void*);
+bool fireCudaRegisterD3D11TextureSlot(int, void*);
+bool fireCudaSetD3D11TextureSlot(int);
+bool fireCudaStepD3D11(const FireSettings&);
+bool fireCudaStepAndRenderD3D11(const FireSettings&);
+bool fireCudaStepAndRenderD3D11Measured(const FireSettings&, FireCudaFrameMetrics*);
+bool fireCudaRenderD3D11(const FireSettings&);
+void fireCudaUnregisterD3D11Texture();
+bool fireCudaSynchronize();
+bool fireCudaReset();
+bool fireCudaGetDiagnostics(FireCudaDiagnostics*);
+void fireCudaShutdown();
+const char* fireCudaLastError();
+int main() {
+    void* all[] = {(void*)&fireCudaInitialize, (void*)&fireCudaStepAndRenderMeasured, (void*)&fireCudaRegisterD3D11TextureSlot,
+                   (void*)&fireCudaSetD3D11TextureSlot, (void*)&fireCudaStepD3D11, (void*)&fireCudaStepAndRenderD3D11,
+                   (void*)&fireCudaStepAndRenderD3D11Measured, (void*)&fireCudaRenderD3D11, (void*)&fireCudaUnregisterD3D11Texture,
+                   (void*)&fireCudaSynchronize, (void*)&fireCudaGetDiagnostics};
+    for (void* f : all) if (f == nullptr) return 2;
+    fireCudaShutdown();
+    FireSettings s{};
+    std::uint32_t px[4] = {};
+    if (fireCudaStepAndRender(px, s)) return 3;
+    std::printf("%s\n", fireCudaLastError());
+    if (fireCudaReset()) return 4;
+    if (fireCudaSelectDeviceForD3D11(nullptr)) return 5;
+    std::printf("%s\n", fireCudaLastError());
+    if (fireCudaRegisterD3D11Texture(nullptr)) return 6;
+    return 0;
+}
+''')
+    lib_dir = ROOT / "native-firesim_b200"
+    exe = tmp_path / "caller"
+    subprocess.run([cxx, "-std=c++17", str(src), "-o", str(exe), f"-L{lib_dir}", "-lfiresim_b200",
+                    f"-Wl,-rpath,{lib_dir}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    lines = out.stdout.splitlines()
+    assert lines[0] == "CUDA renderer is not initialized."
+    assert "D3D11 unavailable on headless build" in lines[1]
