@@ -75,13 +75,60 @@ __device__ __forceinline__ float4 trilinearRec(const Rec4* f, const Corners& c, 
     return lerp4(b0, b1, c.tz);
 }
 
-// Velocity (cells per step) at a world position in cell units: u lives at
-// (i, j+.5, k+.5), v at (i+.5, j, k+.5), w at (i+.5, j+.5, k).
-__device__ __forceinline__ float3 velocityAt(const Velocity& vel, const ConfigParams& p, float x, float y, float z) {
-    const float u = trilinear1(vel.u, cornersAt(x, y - 0.5f, z - 0.5f, p.nx + 1, p.ny, p.nz), p.nx + 1, p.ny);
-    const float v = trilinear1(vel.v, cornersAt(x - 0.5f, y, z - 0.5f, p.nx, p.ny + 1, p.nz), p.nx, p.ny + 1);
-    const float w = trilinear1(vel.w, cornersAt(x - 0.5f, y - 0.5f, z, p.nx, p.ny, p.nz + 1), p.nx, p.ny);
-    return make_float3(u, v, w);
+// Velocity (cells per step) at the faces and cell centres the advection
+// traces back from.  u lives at (i, j+.5, k+.5), v at (i+.5, j, k+.5), w at
+// (i+.5, j+.5, k); the velocity at a point is the clamped trilinear sample of
+// each face grid (x, then y, then z).  At these points one or two of each
+// sample's weights are 0, and lerp(a, b, 0) = a, so those axes are skipped and
+// the remaining lerps are taken in the same order: for finite velocities the
+// values equal the full trilinear samples, except possibly in the sign of a
+// zero, which the callers (position - velocity, position >= 0) cannot see.
+__device__ __forceinline__ float faceAt(const FaceT* f, int x, int y, int z, int mx, int my) { return ldv(f + faceIndex(x, y, z, mx, my)); }
+
+// At the u face (x, y + .5, z + .5).
+__device__ __forceinline__ float3 velocityAtUFace(const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
+    int x0, x1;
+    float tx;
+    axisOf(static_cast<float>(x) - 0.5f, p.nx, x0, x1, tx);
+    const int yv = y + 1, zw = z + 1;  // v at y and y + 1 (weight 1/2), w at z and z + 1 (weight 1/2)
+    const float v = lerp1(lerp1(faceAt(vel.v, x0, y, z, p.nx, p.ny + 1), faceAt(vel.v, x1, y, z, p.nx, p.ny + 1), tx),
+                          lerp1(faceAt(vel.v, x0, yv, z, p.nx, p.ny + 1), faceAt(vel.v, x1, yv, z, p.nx, p.ny + 1), tx), 0.5f);
+    const float w = lerp1(lerp1(faceAt(vel.w, x0, y, z, p.nx, p.ny), faceAt(vel.w, x1, y, z, p.nx, p.ny), tx),
+                          lerp1(faceAt(vel.w, x0, y, zw, p.nx, p.ny), faceAt(vel.w, x1, y, zw, p.nx, p.ny), tx), 0.5f);
+    return make_float3(faceAt(vel.u, x, y, z, p.nx + 1, p.ny), v, w);
+}
+
+// At the v face (x + .5, y, z + .5).
+__device__ __forceinline__ float3 velocityAtVFace(const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
+    int y0, y1;
+    float ty;
+    axisOf(static_cast<float>(y) - 0.5f, p.ny, y0, y1, ty);
+    const int xu = x + 1, zw = z + 1;
+    const float u = lerp1(lerp1(faceAt(vel.u, x, y0, z, p.nx + 1, p.ny), faceAt(vel.u, xu, y0, z, p.nx + 1, p.ny), 0.5f),
+                          lerp1(faceAt(vel.u, x, y1, z, p.nx + 1, p.ny), faceAt(vel.u, xu, y1, z, p.nx + 1, p.ny), 0.5f), ty);
+    const float w = lerp1(lerp1(faceAt(vel.w, x, y0, z, p.nx, p.ny), faceAt(vel.w, x, y1, z, p.nx, p.ny), ty),
+                          lerp1(faceAt(vel.w, x, y0, zw, p.nx, p.ny), faceAt(vel.w, x, y1, zw, p.nx, p.ny), ty), 0.5f);
+    return make_float3(u, faceAt(vel.v, x, y, z, p.nx, p.ny + 1), w);
+}
+
+// At the w face (x + .5, y + .5, z).
+__device__ __forceinline__ float3 velocityAtWFace(const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
+    int z0, z1;
+    float tz;
+    axisOf(static_cast<float>(z) - 0.5f, p.nz, z0, z1, tz);
+    const int xu = x + 1, yv = y + 1;
+    const float u = lerp1(lerp1(faceAt(vel.u, x, y, z0, p.nx + 1, p.ny), faceAt(vel.u, xu, y, z0, p.nx + 1, p.ny), 0.5f),
+                          lerp1(faceAt(vel.u, x, y, z1, p.nx + 1, p.ny), faceAt(vel.u, xu, y, z1, p.nx + 1, p.ny), 0.5f), tz);
+    const float v = lerp1(lerp1(faceAt(vel.v, x, y, z0, p.nx, p.ny + 1), faceAt(vel.v, x, yv, z0, p.nx, p.ny + 1), 0.5f),
+                          lerp1(faceAt(vel.v, x, y, z1, p.nx, p.ny + 1), faceAt(vel.v, x, yv, z1, p.nx, p.ny + 1), 0.5f), tz);
+    return make_float3(u, v, faceAt(vel.w, x, y, z, p.nx, p.ny));
+}
+
+// At the cell centre (x + .5, y + .5, z + .5): the mean of the two faces along each axis.
+__device__ __forceinline__ float3 velocityAtCentre(const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
+    return make_float3(lerp1(faceAt(vel.u, x, y, z, p.nx + 1, p.ny), faceAt(vel.u, x + 1, y, z, p.nx + 1, p.ny), 0.5f),
+                       lerp1(faceAt(vel.v, x, y, z, p.nx, p.ny + 1), faceAt(vel.v, x, y + 1, z, p.nx, p.ny + 1), 0.5f),
+                       lerp1(faceAt(vel.w, x, y, z, p.nx, p.ny), faceAt(vel.w, x, y, z + 1, p.nx, p.ny), 0.5f));
 }
 
 __device__ __forceinline__ float4 recordAt(const Rec4* a, const ConfigParams& p, float x, float y, float z) {
@@ -133,20 +180,20 @@ __global__ void __launch_bounds__(128) cfgAdvectVelocity(FaceT* __restrict__ uOu
     const float fx = static_cast<float>(x), fy = static_cast<float>(y), fz = static_cast<float>(z);
     if (y < p.ny && z < p.nz) {
         const float px = fx, py = fy + 0.5f, pz = fz + 0.5f;
-        const float3 d = velocityAt(vel, p, px, py, pz);
+        const float3 d = velocityAtUFace(vel, p, x, y, z);
         const float bx = px - d.x, by = py - d.y, bz = pz - d.z;
         stv(uOut + faceIndex(x, y, z, p.nx + 1, p.ny),
             trilinear1(vel.u, cornersAt(bx, by - 0.5f, bz - 0.5f, p.nx + 1, p.ny, p.nz), p.nx + 1, p.ny));
     }
     if (x < p.nx && z < p.nz) {
         const float px = fx + 0.5f, py = fy, pz = fz + 0.5f;
-        const float3 d = velocityAt(vel, p, px, py, pz);
+        const float3 d = velocityAtVFace(vel, p, x, y, z);
         const float bx = px - d.x, by = py - d.y, bz = pz - d.z;
         stv(vOut + faceIndex(x, y, z, p.nx, p.ny + 1), trilinear1(vel.v, cornersAt(bx - 0.5f, by, bz - 0.5f, p.nx, p.ny + 1, p.nz), p.nx, p.ny + 1));
     }
     if (x < p.nx && y < p.ny) {
         const float px = fx + 0.5f, py = fy + 0.5f, pz = fz;
-        const float3 d = velocityAt(vel, p, px, py, pz);
+        const float3 d = velocityAtWFace(vel, p, x, y, z);
         const float bx = px - d.x, by = py - d.y, bz = pz - d.z;
         stv(wOut + faceIndex(x, y, z, p.nx, p.ny), trilinear1(vel.w, cornersAt(bx - 0.5f, by - 0.5f, bz, p.nx, p.ny, p.nz + 1), p.nx, p.ny));
     }
@@ -159,7 +206,7 @@ __global__ void __launch_bounds__(128) cfgAdvectScalars(Rec4* __restrict__ aOut,
     const int z = blockIdx.z;
     if (x >= p.nx) return;
     const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
-    const float3 d = velocityAt(vel, p, px, py, pz);
+    const float3 d = velocityAtCentre(vel, p, x, y, z);
     const float4 s = recordAt(aIn, p, px - d.x, py - d.y, pz - d.z);
     float heat = s.x, fuel = s.y, soot = s.w;
     if (heat > p.ignition) {
@@ -201,9 +248,25 @@ __global__ void __launch_bounds__(128) cfgVorticity(float4* __restrict__ vort, V
     vort[(z * p.ny + y) * p.nx + x] = make_float4(ox, oy, oz, sqrtf(ox * ox + oy * oy + oz * oz));
 }
 
-// Cell-centred acceleration: buoyancy + confinement + curl noise.
+// The curl-noise acceleration amplitude * curl(psi) at every cell centre.  It
+// depends only on the noise parameters and the grid, so the scene builds it
+// once per parameter set and cfgCellForce reads it.
+__global__ void __launch_bounds__(128) cfgNoiseField(float4* __restrict__ noise, ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= p.nx) return;
+    const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
+    const float3 g0 = noiseGradient(p, 0, px, py, pz);
+    const float3 g1 = noiseGradient(p, 1, px, py, pz);
+    const float3 g2 = noiseGradient(p, 2, px, py, pz);
+    noise[(z * p.ny + y) * p.nx + x] = make_float4(p.noiseAmp * (g2.y - g1.z), p.noiseAmp * (g0.z - g2.x), p.noiseAmp * (g1.x - g0.y), 0.0f);
+}
+
+// Cell-centred acceleration: buoyancy + confinement + curl noise (read from
+// the field cfgNoiseField built; null when the amplitude is 0).
 __global__ void __launch_bounds__(128) cfgCellForce(float4* __restrict__ force, const float4* __restrict__ vort, const Rec4* __restrict__ a,
-                                                    ConfigParams p) {
+                                                    const float4* __restrict__ noise, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
@@ -232,13 +295,10 @@ __global__ void __launch_bounds__(128) cfgCellForce(float4* __restrict__ force, 
     }
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     if (p.noiseAmp != 0.0f) {
-        const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
-        const float3 g0 = noiseGradient(p, 0, px, py, pz);
-        const float3 g1 = noiseGradient(p, 1, px, py, pz);
-        const float3 g2 = noiseGradient(p, 2, px, py, pz);
-        fx = p.noiseAmp * (g2.y - g1.z);
-        fy = p.noiseAmp * (g0.z - g2.x);
-        fz = p.noiseAmp * (g1.x - g0.y);
+        const float4 n = __ldg(noise + idx);
+        fx = n.x;
+        fy = n.y;
+        fz = n.z;
     }
     const float buoyancy = p.buoyHeat * (s.x - p.ambient) - p.buoySoot * s.w;
     force[idx] = make_float4(cx + fx, buoyancy + cy + fy, cz + fz, 0.0f);

@@ -188,7 +188,8 @@ __host__ __device__ inline float latticeValue(unsigned seed, int comp, int ix, i
 __global__ void cfgAdvectVelocity(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, ConfigParams p);
 __global__ void cfgAdvectScalars(Rec4* aOut, const Rec4* aIn, Velocity vel, ConfigParams p);
 __global__ void cfgVorticity(float4* vort, Velocity vel, ConfigParams p);
-__global__ void cfgCellForce(float4* force, const float4* vort, const Rec4* a, ConfigParams p);
+__global__ void cfgNoiseField(float4* noise, ConfigParams p);
+__global__ void cfgCellForce(float4* force, const float4* vort, const Rec4* a, const float4* noise, ConfigParams p);
 __global__ void cfgApplyForces(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, const float4* force, ConfigParams p);
 __global__ void cfgTransmittance(float* tr, const Rec4* a, ConfigParams p);
 __global__ void cfgRaymarch(float4* hdr, const Rec4* a, const float* tr, ConfigParams p);

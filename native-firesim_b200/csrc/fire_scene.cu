@@ -81,7 +81,7 @@ void Scene::release() {
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
                     shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_,
                     rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_, split_, splitDiv_,
-                    cfgVort_, cfgLight_};
+                    cfgVort_, cfgLight_, cfgNoise_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
     }
@@ -99,6 +99,8 @@ void Scene::release() {
     splitDiv_ = nullptr;
     cfgVort_ = nullptr;
     cfgLight_ = nullptr;
+    cfgNoise_ = nullptr;
+    cfgNoiseValid_ = false;
     sorHostStatus_ = nullptr;
     curlLattice_ = nullptr;
     sourceLattice_ = nullptr;
@@ -1590,7 +1592,21 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                 if (c.eps != 0.0f) {
                     cfgVorticity<<<cells, bx, 0, stream>>>(cfgVort_, velocity(), c); ++launches_;
                 }
-                cfgCellForce<<<cells, bx, 0, stream>>>(contrib_, cfgVort_, sa_[cur_], c); ++launches_;
+                if (c.noiseAmp != 0.0f) {
+                    // The curl-noise field depends only on its parameters: build it when they change.
+                    const float key[3] = {c.noiseAmp, c.invPeriod, static_cast<float>(c.noiseSeed)};
+                    if (!cfgNoiseValid_ || std::memcmp(key, cfgNoiseKey_, sizeof(key)) != 0 || cfgNoiseSeed_ != c.noiseSeed) {
+                        if (cfgNoise_ == nullptr &&
+                            !alloc(reinterpret_cast<void**>(&cfgNoise_), cells_ * sizeof(float4), "cudaMalloc config noise field", err)) {
+                            return false;
+                        }
+                        cfgNoiseField<<<cells, bx, 0, stream>>>(cfgNoise_, c); ++launches_;
+                        std::memcpy(cfgNoiseKey_, key, sizeof(key));
+                        cfgNoiseSeed_ = c.noiseSeed;
+                        cfgNoiseValid_ = true;
+                    }
+                }
+                cfgCellForce<<<cells, bx, 0, stream>>>(contrib_, cfgVort_, sa_[cur_], cfgNoise_, c); ++launches_;
                 cfgApplyForces<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), contrib_, c); ++launches_;
                 vcur_ = 1 - vcur_;
                 break;

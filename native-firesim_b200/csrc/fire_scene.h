@@ -185,6 +185,10 @@ private:
     FirePhysicsParams physics_{};
     float4* cfgVort_ = nullptr;   // vorticity (x, y, z, |omega|) per cell, allocated on first use
     float* cfgLight_ = nullptr;   // transmittance to the point light, half resolution
+    float4* cfgNoise_ = nullptr;  // curl-noise acceleration per cell, rebuilt when its parameters change
+    bool cfgNoiseValid_ = false;
+    float cfgNoiseKey_[3] = {0.0f, 0.0f, 0.0f};
+    unsigned cfgNoiseSeed_ = 0;
     int cfgLx_ = 0, cfgLy_ = 0, cfgLz_ = 0;
     unsigned long long cfgStep_ = 0;
     ConfigParams configParams() const;
