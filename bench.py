@@ -128,11 +128,13 @@ def dist_setup():
 
 
 def dist_max(x: float, world: int) -> float:
+    """The maximum of x over the ranks (a device tensor under NCCL, a host tensor under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
