@@ -205,6 +205,10 @@ struct MgLevel {
     int wide;  // 1: the level's pressure is double (level 0)
 };
 // F: float pressure (the coarser levels); D: double pressure (level 0).
+// Smoothing and prolongation take blocks of kMgRowBlockThreads: 32, 64 or 128
+// threads along a row and as many rows (y) as fill the block, so that the
+// grid has few, large blocks.
+constexpr int kMgRowBlockThreads = 256;
 __global__ void mgSmoothF(float* p, const float* rhs, MgLevel L, int colour, const int* skip);
 __global__ void mgSmoothD(double* p, const float* rhs, MgLevel L, int colour, const int* skip);
 __global__ void mgRestrictF(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);

@@ -35,8 +35,14 @@ __device__ __forceinline__ int mgAt(const MgLevel& L, int x, int y, int z) { ret
 
 __device__ __forceinline__ bool skipped(const int* skip) { return skip != nullptr && __ldg(skip) != 0; }
 
-// rhs + wx (pL + pR) + wy (pD + pU) + wz (pB + pF) for cell (x, y, z) with the
-// boundary rules, in the level's pressure type P (double on level 0).
+// rhs + wx (pL + pR) + wy (pD + pU) + wz (pB + pF), in the level's pressure
+// type P (double on level 0), in this order.
+template <typename P>
+__device__ __forceinline__ P combine(float rhs, P pL, P pR, P pD, P pU, P pB, P pF, const MgLevel& L) {
+    return static_cast<P>(rhs) + static_cast<P>(L.wx) * (pL + pR) + static_cast<P>(L.wy) * (pD + pU) + static_cast<P>(L.wz) * (pB + pF);
+}
+
+// The weighted sum for cell (x, y, z) with the boundary rules.
 template <typename P>
 __device__ __forceinline__ P weightedSum(const P* p, const float* rhs, const MgLevel& L, int x, int y, int z, P self) {
     const int i = mgAt(L, x, y, z);
@@ -46,8 +52,7 @@ __device__ __forceinline__ P weightedSum(const P* p, const float* rhs, const MgL
     const P pU = y < L.ny - 1 ? p[i + L.nx] : static_cast<P>(0) - self;
     const P pB = z > 0 ? p[i - L.nx * L.ny] : self;
     const P pF = z < L.nz - 1 ? p[i + L.nx * L.ny] : self;
-    return static_cast<P>(rhs[i]) + static_cast<P>(L.wx) * (pL + pR) + static_cast<P>(L.wy) * (pD + pU) +
-           static_cast<P>(L.wz) * (pB + pF);
+    return combine(rhs[i], pL, pR, pD, pU, pB, pF, L);
 }
 
 template <typename P>
@@ -68,8 +73,9 @@ __device__ __forceinline__ void smoothCell(P* p, const float* rhs, const MgLevel
 template <typename P>
 __device__ __forceinline__ void mgSmoothBody(P* __restrict__ p, const float* __restrict__ rhs, const MgLevel& L, int colour, const int* skip) {
     if (skipped(skip)) return;
-    const int y = blockIdx.y;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
+    if (y >= L.ny) return;
     const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((colour + y + z) & 1);
     if (x >= L.nx) return;
     smoothCell(p, rhs, L, x, y, z);
@@ -108,9 +114,9 @@ __device__ __forceinline__ void mgProlongBody(P* __restrict__ p, const float* __
                                               const int* skip) {
     if (skipped(skip)) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
-    if (x >= F.nx) return;
+    if (x >= F.nx || y >= F.ny) return;
     const int X0 = C.cx ? x >> 1 : x, Y0 = C.cy ? y >> 1 : y, Z0 = C.cz ? z >> 1 : z;
     const int X1 = !C.cx ? X0 : ((x & 1) ? min(X0 + 1, C.nx - 1) : max(X0 - 1, 0));
     const int Y1 = !C.cy ? Y0 : ((y & 1) ? min(Y0 + 1, C.ny - 1) : max(Y0 - 1, 0));
@@ -127,12 +133,53 @@ __device__ __forceinline__ void mgProlongBody(P* __restrict__ p, const float* __
     p[i] = p[i] + static_cast<P>(uz * b0 + vz * b1);
 }
 
-// The coarsest level: `sweeps` red-black Gauss-Seidel iterations by one block.
+// `sweeps` red-black Gauss-Seidel iterations over cells first, first + stride,
+// ... (at most four of them) of a level, whose coordinates are worked out once;
+// each colour ends with a barrier of the warp (warpOnly) or of the block.
+template <typename P>
+__device__ __forceinline__ void smoothCells(P* __restrict__ p, const float* __restrict__ rhs, const MgLevel& L, int sweeps, int first,
+                                            int stride, bool warpOnly) {
+    const int cells = L.nx * L.ny * L.nz;
+    int xs[4], ys[4], zs[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int i = first + k * stride;
+        xs[k] = i < cells ? i % L.nx : -1;
+        ys[k] = (i / L.nx) % L.ny;
+        zs[k] = i / (L.nx * L.ny);
+    }
+    for (int s = 0; s < sweeps; ++s) {
+        for (int colour = 0; colour < 2; ++colour) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (xs[k] >= 0 && ((xs[k] + ys[k] + zs[k]) & 1) == colour) smoothCell(p, rhs, L, xs[k], ys[k], zs[k]);
+            }
+            if (warpOnly) {
+                __syncwarp();
+            } else {
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// The coarsest level: `sweeps` red-black Gauss-Seidel iterations by one
+// block.  A level of at most 128 cells is relaxed by the first warp alone,
+// with warp barriers between the colours; one of at most four cells per
+// thread works out each thread's cells once.
 template <typename P>
 __device__ __forceinline__ void mgCoarsestBody(P* __restrict__ p, const float* __restrict__ rhs, const MgLevel& L, int sweeps,
                                                const int* skip) {
     if (skipped(skip)) return;
     const int cells = L.nx * L.ny * L.nz;
+    if (cells <= 4 * 32) {
+        if (threadIdx.x < 32) smoothCells(p, rhs, L, sweeps, static_cast<int>(threadIdx.x), 32, true);
+        return;
+    }
+    if (cells <= 4 * static_cast<int>(blockDim.x)) {
+        smoothCells(p, rhs, L, sweeps, static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x), false);
+        return;
+    }
     for (int s = 0; s < sweeps; ++s) {
         for (int colour = 0; colour < 2; ++colour) {
             for (int i = threadIdx.x; i < cells; i += blockDim.x) {
@@ -185,10 +232,10 @@ __device__ __forceinline__ void mgResidualPartialsBody(const P* __restrict__ p, 
 }
 
 // The kernels, one per pressure type (F: float, the coarser levels; D: double, level 0).
-__global__ void __launch_bounds__(128) mgSmoothF(float* p, const float* rhs, MgLevel L, int colour, const int* skip) {
+__global__ void __launch_bounds__(kMgRowBlockThreads) mgSmoothF(float* p, const float* rhs, MgLevel L, int colour, const int* skip) {
     mgSmoothBody(p, rhs, L, colour, skip);
 }
-__global__ void __launch_bounds__(128) mgSmoothD(double* p, const float* rhs, MgLevel L, int colour, const int* skip) {
+__global__ void __launch_bounds__(kMgRowBlockThreads) mgSmoothD(double* p, const float* rhs, MgLevel L, int colour, const int* skip) {
     mgSmoothBody(p, rhs, L, colour, skip);
 }
 __global__ void __launch_bounds__(128) mgRestrictF(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C,
@@ -199,10 +246,10 @@ __global__ void __launch_bounds__(128) mgRestrictD(float* rhsC, float* pC, const
                                                    const int* skip) {
     mgRestrictBody(rhsC, pC, p, rhs, F, C, skip);
 }
-__global__ void __launch_bounds__(128) mgProlongF(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip) {
+__global__ void __launch_bounds__(kMgRowBlockThreads) mgProlongF(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip) {
     mgProlongBody(p, pC, F, C, skip);
 }
-__global__ void __launch_bounds__(128) mgProlongD(double* p, const float* pC, MgLevel F, MgLevel C, const int* skip) {
+__global__ void __launch_bounds__(kMgRowBlockThreads) mgProlongD(double* p, const float* pC, MgLevel F, MgLevel C, const int* skip) {
     mgProlongBody(p, pC, F, C, skip);
 }
 __global__ void __launch_bounds__(256) mgCoarsestF(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip) {

@@ -619,11 +619,12 @@ bool Scene::runMultigrid(std::string& err) {
         auto P = [&](int l) { return mgP_[l - 1]; };
         auto R = [&](int l) { return l == 0 ? divergence_ : mgRhs_[l - 1]; };
         int count = 0;
+        auto rowBlock = [](int rowThreadCount, int ny) { return dim3(rowThreadCount, std::min(kMgRowBlockThreads / rowThreadCount, ny), 1); };
         auto smooth = [&](int l, int sweeps) {
             const MgLevel& L = mgLevels_[l];
             const int half = (L.nx + 1) / 2;
-            const int bx = rowThreads(half);
-            const dim3 g((half + bx - 1) / bx, L.ny, L.nz);
+            const dim3 bx = rowBlock(rowThreads(half), L.ny);
+            const dim3 g((half + bx.x - 1) / bx.x, (L.ny + bx.y - 1) / bx.y, L.nz);
             for (int k = 0; k < sweeps; ++k) {
                 for (int colour = 0; colour < 2; ++colour) {
                     if (l == 0) {
@@ -686,8 +687,8 @@ bool Scene::runMultigrid(std::string& err) {
         for (int l = levels - 2; l >= 0; --l) {
             const MgLevel& F = mgLevels_[l];
             const MgLevel& C = mgLevels_[l + 1];
-            const int bx = rowThreads(F.nx);
-            const dim3 pg((F.nx + bx - 1) / bx, F.ny, F.nz);
+            const dim3 bx = rowBlock(rowThreads(F.nx), F.ny);
+            const dim3 pg((F.nx + bx.x - 1) / bx.x, (F.ny + bx.y - 1) / bx.y, F.nz);
             if (l == 0) {
                 mgProlongD<<<pg, bx, 0, stream>>>(mgP0_, P(1), F, C, nullptr);
             } else {
