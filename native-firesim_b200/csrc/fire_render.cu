@@ -310,6 +310,10 @@ namespace {
 
 // src/fire_cuda.cu:1953-2244 -- one primary ray through the packed field
 // records; writes RGB and alpha = 1 to pixel (x, y) of the internal HDR frame.
+// SC >= 0: the scene id, fixed at compile time (the caller launches this
+// instantiation only for that scene and a debug mode other than 6); SC < 0:
+// read from p.  Fixing it drops the other scenes' branches from the sample loop.
+template <int SC>
 __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int y, const ScalarFieldsIn& s, const Velocity& vel,
                                            const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
                                            const RenderLattices& lat) {
@@ -327,7 +331,8 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
     float trans = 1.0f;
     float flameGlow = 0.0f, smokeOcclusion = 0.0f, debugFlame = 0.0f, debugOpticalDepth = 0.0f;
     float debugTemperature = 0.0f, debugFuel = 0.0f, debugVelocity = 0.0f;
-    const int sc = p.sceneId;
+    const int sc = SC >= 0 ? SC : p.sceneId;
+    const bool velocityDebug = SC < 0 && p.renderDebugMode == 6;
 
     if (intersectBox(p.eye, rd, make_float3(-1.05f, 0.02f, -0.82f), make_float3(1.05f, 2.05f, 0.82f), &boxNear, &boxFar)) {
         const int raySteps = min(max(p.raymarchSteps, 24), kMaxRaymarchSteps);
@@ -368,7 +373,7 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
             const float4 sceneLight = sampleSceneLight(lightF, L, wu, wv, ww);
             const float sceneShadow = sampleSceneShadow(shadowF, L, wu, wv, ww);
             float3 velocity = make_float3(0.0f, 0.0f, 0.0f);
-            if (p.renderDebugMode == 6) {
+            if (velocityDebug) {
                 velocity = sampleVelocity(vel, g, wu, wv, ww);
             }
             const float activeField = (heat + fuel * 0.42f + soot * 0.34f + progress * 0.32f + pyrolysis * 0.18f) * domainFade;
@@ -376,7 +381,7 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
                 continue;
             }
             debugFuel = fmaxf(debugFuel, domainFade * saturate(fuel * 0.18f + charMass * 0.22f + pyrolysis * 0.30f));
-            if (p.renderDebugMode == 6) {
+            if (velocityDebug) {
                 debugVelocity = fmaxf(debugVelocity, saturate(sqrtf(dot3(velocity, velocity)) * 0.22f));
             }
             const float cellX = 1.0f / static_cast<float>(p.nx);
@@ -599,9 +604,10 @@ __global__ void __launch_bounds__(256) hashLattice3Build(RenderLattices lat) {
 // warp repeatedly takes the next 8x4-pixel tile from a counter, in an order
 // that starts at the centre of the frame (where the fire box projects) and
 // ends at the corners, until no tile is left.
-__global__ void __launch_bounds__(128, 5) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
-                                                   const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
-                                                   RayTiles tiles, RenderLattices lat) {
+template <int SC>
+__device__ __forceinline__ void raymarchBody(float4* __restrict__ out, const ScalarFieldsIn& s, const Velocity& vel,
+                                             const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
+                                             const RayTiles& tiles, const RenderLattices& lat) {
     const int lane = threadIdx.x & 31;
     for (;;) {
         int t = 0;
@@ -616,9 +622,32 @@ __global__ void __launch_bounds__(128, 5) raymarch(float4* __restrict__ out, Sca
         const int x = (tile % tiles.tilesX) * kRayTileW + (lane % kRayTileW);
         const int y = (tile / tiles.tilesX) * kRayTileH + (lane / kRayTileW);
         if (x < p.frameW && y < p.frameH) {
-            shadePixel(out, x, y, s, vel, lightF, shadowF, p, lat);
+            shadePixel<SC>(out, x, y, s, vel, lightF, shadowF, p, lat);
         }
     }
+}
+
+// Any scene and debug mode.
+__global__ void __launch_bounds__(128, 5) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+                                                   const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
+                                                   RayTiles tiles, RenderLattices lat) {
+    raymarchBody<-1>(out, s, vel, lightF, shadowF, p, tiles, lat);
+}
+// Scenes 0, 1, 2 with debug modes other than 6.
+__global__ void __launch_bounds__(128, 5) raymarchScene0(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+                                                         const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
+                                                         RayTiles tiles, RenderLattices lat) {
+    raymarchBody<0>(out, s, vel, lightF, shadowF, p, tiles, lat);
+}
+__global__ void __launch_bounds__(128, 5) raymarchScene1(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+                                                         const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
+                                                         RayTiles tiles, RenderLattices lat) {
+    raymarchBody<1>(out, s, vel, lightF, shadowF, p, tiles, lat);
+}
+__global__ void __launch_bounds__(128, 5) raymarchScene2(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+                                                         const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
+                                                         RayTiles tiles, RenderLattices lat) {
+    raymarchBody<2>(out, s, vel, lightF, shadowF, p, tiles, lat);
 }
 
 // ---------------------------------------------------------------------------

@@ -195,9 +195,13 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
         ok = alloc(reinterpret_cast<void**>(&rayTileOrder_), order.size() * sizeof(int), "cudaMalloc ray tiles", err) &&
              alloc(reinterpret_cast<void**>(&rayTileCounter_), sizeof(int), "cudaMalloc ray tile counter", err) &&
              check("upload ray tiles", cudaMemcpy(rayTileOrder_, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice), err) &&
-             check("SM count", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), err) &&
-             check("raymarch occupancy", cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, raymarch, 128, 0), err);
-        rayBlocks_ = std::max(1, sms * std::max(1, perSm));
+             check("SM count", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), err);
+        const void* kernels[4] = {reinterpret_cast<const void*>(raymarch), reinterpret_cast<const void*>(raymarchScene0),
+                                  reinterpret_cast<const void*>(raymarchScene1), reinterpret_cast<const void*>(raymarchScene2)};
+        for (int k = 0; ok && k < 4; ++k) {
+            ok = check("raymarch occupancy", cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernels[k], 128, 0), err);
+            rayBlocks_[k] = std::max(1, sms * std::max(1, perSm));
+        }
     }
     ok = ok && alloc(reinterpret_cast<void**>(&sorGate_), sizeof(SorGate), "cudaMalloc SOR gate", err) &&
          check("clear SOR gate", cudaMemsetAsync(sorGate_, 0, sizeof(SorGate), stream), err) &&
@@ -950,8 +954,12 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                 renderLattices(p, lat);
                 hashLattice3Build<<<dim3(512, 4), 256, 0, stream>>>(lat); ++launches_;
                 if (!check("clear ray tile counter", cudaMemsetAsync(rayTileCounter_, 0, sizeof(int), stream), err)) return false;
-                raymarch<<<rayBlocks_, 128, 0, stream>>>(hdr_, scalarsIn(), velocity(), light_, shadow_, p,
-                                                         RayTiles{rayTileCounter_, rayTileOrder_, rayTilesX_, rayTileCount_}, lat); ++launches_;
+                // Scenes 0-2 outside the velocity debug view take the
+                // instantiation with the scene id fixed.
+                const int k = p.renderDebugMode != 6 && p.sceneId >= 0 && p.sceneId <= 2 ? 1 + p.sceneId : 0;
+                const RayTiles tiles{rayTileCounter_, rayTileOrder_, rayTilesX_, rayTileCount_};
+                auto kernel = k == 1 ? raymarchScene0 : (k == 2 ? raymarchScene1 : (k == 3 ? raymarchScene2 : raymarch));
+                kernel<<<rayBlocks_[k], 128, 0, stream>>>(hdr_, scalarsIn(), velocity(), light_, shadow_, p, tiles, lat); ++launches_;
             }
                 s = kEmbers;
                 break;

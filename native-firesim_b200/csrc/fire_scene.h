@@ -161,7 +161,8 @@ private:
     // Raymarch work list: tile order (centre first) and the tile counter.
     int* rayTileOrder_ = nullptr;
     int* rayTileCounter_ = nullptr;
-    int rayTilesX_ = 0, rayTileCount_ = 0, rayBlocks_ = 0;
+    int rayTilesX_ = 0, rayTileCount_ = 0;
+    int rayBlocks_[4] = {0, 0, 0, 0};  // persistent grid of raymarch, raymarchScene0..2
     double pressureTolerance_ = 0.0;
     int pressureCheckEvery_ = 10;
     bool lastSolveGated_ = false;
