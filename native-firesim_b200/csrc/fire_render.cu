@@ -603,7 +603,10 @@ __global__ void __launch_bounds__(256) hashLattice3Build(RenderLattices lat) {
 // static grid leaves most SMs idle while the last blocks finish.  Here every
 // warp repeatedly takes the next 8x4-pixel tile from a counter, in an order
 // that starts at the centre of the frame (where the fire box projects) and
-// ends at the corners, until no tile is left.
+// ends at the corners, until no tile is left.  The kernels ask for 4 blocks of
+// 128 threads per SM: 128 registers and no spills.  At 5 blocks (96
+// registers, spills) a 512^2 frame of a developed 128^3 fire took 1.42 ms
+// instead of 1.27 ms; at 3 or 2 blocks it was no faster.
 template <int SC>
 __device__ __forceinline__ void raymarchBody(float4* __restrict__ out, const ScalarFieldsIn& s, const Velocity& vel,
                                              const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
@@ -628,23 +631,23 @@ __device__ __forceinline__ void raymarchBody(float4* __restrict__ out, const Sca
 }
 
 // Any scene and debug mode.
-__global__ void __launch_bounds__(128, 5) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+__global__ void __launch_bounds__(128, 4) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                    const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
                                                    RayTiles tiles, RenderLattices lat) {
     raymarchBody<-1>(out, s, vel, lightF, shadowF, p, tiles, lat);
 }
 // Scenes 0, 1, 2 with debug modes other than 6.
-__global__ void __launch_bounds__(128, 5) raymarchScene0(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+__global__ void __launch_bounds__(128, 4) raymarchScene0(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
                                                          RayTiles tiles, RenderLattices lat) {
     raymarchBody<0>(out, s, vel, lightF, shadowF, p, tiles, lat);
 }
-__global__ void __launch_bounds__(128, 5) raymarchScene1(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+__global__ void __launch_bounds__(128, 4) raymarchScene1(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
                                                          RayTiles tiles, RenderLattices lat) {
     raymarchBody<1>(out, s, vel, lightF, shadowF, p, tiles, lat);
 }
-__global__ void __launch_bounds__(128, 5) raymarchScene2(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
+__global__ void __launch_bounds__(128, 4) raymarchScene2(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
                                                          RayTiles tiles, RenderLattices lat) {
     raymarchBody<2>(out, s, vel, lightF, shadowF, p, tiles, lat);
