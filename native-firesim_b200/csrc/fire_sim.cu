@@ -988,19 +988,22 @@ __device__ __forceinline__ void residentInteriorAny(bool full, float* planes, co
 }  // namespace
 
 // One half sweep h (colour c) of a brick runs as
-//   interior cells, first half of z
+//   interior cells, first three quarters of z
 //   issue the loads of the neighbours' face cells (colour 1 - c) of half
 //     sweep h - 1 from the tagged exchange words
-//   interior cells, second half of z      (hides the loads' latency)
+//   interior cells, last quarter of z     (hides the loads' latency)
 //   words whose tag is not yet h: poll until it is; values -> halo; barrier
 //   face cells, each also published as a tagged word; barrier
 // so the exchange overlaps the interior update and costs one L2 round trip.
+// Issuing the loads after three quarters of the interior rather than half
+// leaves the neighbours' stores longer to land: a 40-iteration 128^3 solve
+// took 250 instead of 256 us (after a quarter: 260 us).
 template <int BX, int BY, int BZ>
 __global__ void __launch_bounds__((BX / 2) * BY, 2) sorResident(float* __restrict__ pressure, const float* __restrict__ divergence, Grid g,
                                                                ResidentBrick r, ResidentSync sync, int iterations, float omega) {
     using S = ResidentShape<BX, BY, BZ>;
     using F = ResidentFaces<BX, BY, BZ>;
-    constexpr int ZMID = BZ / 2;
+    constexpr int ZMID = 3 * BZ / 4;
     if (sync.skip != nullptr && *reinterpret_cast<const volatile int*>(sync.skip) != 0) {
         return;  // an earlier chunk of this solve converged (the same word for every block)
     }
