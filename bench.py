@@ -458,7 +458,7 @@ def config_cpu_baseline(pkg, w, n_steps: int = 2, args=None) -> dict:
     o.set_physics(w["physics"])
     o.set_pressure_solver(*w["sor"])
     if args is not None and args.solver == "mg":
-        o.set_multigrid(args.mg_cycles, 2, 2, 0.5 * args.div_target)
+        o.set_multigrid(args.mg_cycles, args.mg_pre, args.mg_post, 0.5 * args.div_target)
     threads = os.cpu_count() or 1
     om.OracleFire.set_threads(threads)
     o.step()
@@ -478,8 +478,6 @@ def config_cpu_baseline(pkg, w, n_steps: int = 2, args=None) -> dict:
             "seconds_per_step": per_step}
 
 
-# Level-0 half sweeps of one V-cycle: 2 pre- and 2 post-smoothing sweeps of two colours.
-MG_LEVEL0_HALF_SWEEPS = 8
 
 
 _PINNED = []  # keeps the page-locked tensors behind pinned_frame's arrays alive
@@ -527,7 +525,7 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
         # rounding of the face update).
         physics.pressureTop = 1
         sim.set_physics(physics)
-        sim.set_pressure_multigrid(args.mg_cycles, 2, 2)
+        sim.set_pressure_multigrid(args.mg_cycles, args.mg_pre, args.mg_post)
         sim.set_pressure_tolerance(0.5 * args.div_target, 1)
     else:
         sim.set_physics(physics)
@@ -605,7 +603,9 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
     iters = stats[0] if stats[1] >= 0 else w["sor"][0]
     if dominant == "pressure_sor" and args.solver == "mg":
         # One "launch" here is the whole solve: its level-0 half sweeps at 6 B/cell each.
-        bytes_launch = CONFIG_STAGE_BYTES_PER_CELL["pressure_sor"] * cells * MG_LEVEL0_HALF_SWEEPS * iters
+        # Level-0 half sweeps of one V-cycle: pre- and post-smoothing sweeps of two colours.
+        level0_half_sweeps = 2 * (args.mg_pre + args.mg_post)
+        bytes_launch = CONFIG_STAGE_BYTES_PER_CELL["pressure_sor"] * cells * level0_half_sweeps * iters
         launch_ms = st["pressure_sor"]
     elif dominant == "pressure_sor":
         launches_per = 2 * iters
@@ -632,7 +632,8 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
             "data": "synthetic (seeded disk emitters, SplitMix64 jitter)",
             "config": {"workload": f"config physics {w['name']}: {n[0]}^3, {p.emitterCount} disk emitter(s), "
                                    + (f"p = 0 on the top face, multigrid V-cycles until max|r| <= {0.5 * args.div_target:g} "
-                                      f"(|div u| <= {args.div_target:g}), at most {args.mg_cycles}"
+                                      f"(|div u| <= {args.div_target:g}), at most {args.mg_cycles}, "
+                                      f"V({args.mg_pre},{args.mg_post})"
                                       if args.solver == "mg" else
                                       f"SOR {w['sor'][0]} omega {w['sor'][1]}"
                                       f"{' until max|r| <= %g' % w['tolerance'] if w['tolerance'] else ''}") + ", "
@@ -676,6 +677,8 @@ def main() -> int:
                          "V-cycles until |div u| <= --div-target")
     ap.add_argument("--div-target", type=float, default=1e-4)
     ap.add_argument("--mg-cycles", type=int, default=30)
+    ap.add_argument("--mg-pre", type=int, default=2, help="pre-smoothing sweeps per multigrid level")
+    ap.add_argument("--mg-post", type=int, default=2, help="post-smoothing sweeps per multigrid level")
     ap.add_argument("--precision", default=None, choices=["f32", "f16", "bf16"],
                     help="storage of the transported fields: f32 (the reference's), f16 or bf16 (FP32 arithmetic)")
     ap.add_argument("--mode", default="single", choices=["single", "batched", "serve"],
