@@ -65,4 +65,5 @@ def test_reference_arm_prints_one_line_from_rank_zero(tmp_path):
     assert len(lines) == 1, out.stdout
     line = json.loads(lines[0])
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["steps"] == 1 and line["warmup"] == 3
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
