@@ -127,7 +127,7 @@ struct RayTiles {
 __global__ void hashLattice3Build(RenderLattices lat);
 __global__ void raymarch(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p, RayTiles tiles,
                          RenderLattices lat);
-// The same for one scene id (0, 1, 2) fixed at compile time, debug modes other than 6.
+// The same for one scene id (0, 1, 2) fixed at compile time, without a debug view.
 __global__ void raymarchScene0(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p,
                                RayTiles tiles, RenderLattices lat);
 __global__ void raymarchScene1(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p,

@@ -311,8 +311,9 @@ namespace {
 // src/fire_cuda.cu:1953-2244 -- one primary ray through the packed field
 // records; writes RGB and alpha = 1 to pixel (x, y) of the internal HDR frame.
 // SC >= 0: the scene id, fixed at compile time (the caller launches this
-// instantiation only for that scene and a debug mode other than 6); SC < 0:
-// read from p.  Fixing it drops the other scenes' branches from the sample loop.
+// instantiation only for that scene with no debug view); SC < 0: read from p,
+// with the debug views.  Fixing it drops the other scenes' branches and the
+// debug views' per-sample maxima from the sample loop.
 template <int SC>
 __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int y, const ScalarFieldsIn& s, const Velocity& vel,
                                            const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
@@ -332,7 +333,8 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
     float flameGlow = 0.0f, smokeOcclusion = 0.0f, debugFlame = 0.0f, debugOpticalDepth = 0.0f;
     float debugTemperature = 0.0f, debugFuel = 0.0f, debugVelocity = 0.0f;
     const int sc = SC >= 0 ? SC : p.sceneId;
-    const bool velocityDebug = SC < 0 && p.renderDebugMode == 6;
+    constexpr bool debugViews = SC < 0;
+    const bool velocityDebug = debugViews && p.renderDebugMode == 6;
 
     if (intersectBox(p.eye, rd, make_float3(-1.05f, 0.02f, -0.82f), make_float3(1.05f, 2.05f, 0.82f), &boxNear, &boxFar)) {
         const int raySteps = min(max(p.raymarchSteps, 24), kMaxRaymarchSteps);
@@ -380,7 +382,9 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
             if (activeField <= 0.0025f) {
                 continue;
             }
-            debugFuel = fmaxf(debugFuel, domainFade * saturate(fuel * 0.18f + charMass * 0.22f + pyrolysis * 0.30f));
+            if (debugViews) {
+                debugFuel = fmaxf(debugFuel, domainFade * saturate(fuel * 0.18f + charMass * 0.22f + pyrolysis * 0.30f));
+            }
             if (velocityDebug) {
                 debugVelocity = fmaxf(debugVelocity, saturate(sqrtf(dot3(velocity, velocity)) * 0.22f));
             }
@@ -536,9 +540,11 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
             const float3 smokeScatterLight = lerp3(neutralScatterLight, localIrradiance, nearFlameWarmLeak);
             const float coalGlow = smoothstepf(0.004f, 0.18f, charMass) * smoothstepf(0.54f, 0.02f, fv) * (0.070f + pyrolysis * 0.12f + heat * 0.009f);
 
-            debugFlame = fmaxf(debugFlame, saturate(flameDensity * radiantPower * 0.26f));
-            debugOpticalDepth = saturate(debugOpticalDepth + sootExtinction * stepT);
-            debugTemperature = fmaxf(debugTemperature, saturate((tempK - 520.0f) / 1900.0f));
+            if (debugViews) {
+                debugFlame = fmaxf(debugFlame, saturate(flameDensity * radiantPower * 0.26f));
+                debugOpticalDepth = saturate(debugOpticalDepth + sootExtinction * stepT);
+                debugTemperature = fmaxf(debugTemperature, saturate((tempK - 520.0f) / 1900.0f));
+            }
             accum = add3(accum, mul3(flameEmission, trans));
             accum = add3(accum, mul3(make_float3(1.0f, 0.24f, 0.035f), trans * coalGlow * stepT));
             accum = add3(accum, mul3(smokeColor, trans * scatterGain * smokeOnlyMask));
@@ -549,7 +555,7 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
         }
     }
 
-    if (p.renderDebugMode != 0) {
+    if (debugViews && p.renderDebugMode != 0) {
         float3 dc = make_float3(0.0f, 0.0f, 0.0f);
         if (p.renderDebugMode == 1) {
             dc = debugHeatColor(debugFlame);
@@ -636,7 +642,7 @@ __global__ void __launch_bounds__(128, 4) raymarch(float4* __restrict__ out, Sca
                                                    RayTiles tiles, RenderLattices lat) {
     raymarchBody<-1>(out, s, vel, lightF, shadowF, p, tiles, lat);
 }
-// Scenes 0, 1, 2 with debug modes other than 6.
+// Scenes 0, 1, 2 without a debug view (renderDebugMode 0).
 __global__ void __launch_bounds__(128, 4) raymarchScene0(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
                                                          RayTiles tiles, RenderLattices lat) {

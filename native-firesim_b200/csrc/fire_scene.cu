@@ -954,9 +954,9 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                 renderLattices(p, lat);
                 hashLattice3Build<<<dim3(512, 4), 256, 0, stream>>>(lat); ++launches_;
                 if (!check("clear ray tile counter", cudaMemsetAsync(rayTileCounter_, 0, sizeof(int), stream), err)) return false;
-                // Scenes 0-2 outside the velocity debug view take the
-                // instantiation with the scene id fixed.
-                const int k = p.renderDebugMode != 6 && p.sceneId >= 0 && p.sceneId <= 2 ? 1 + p.sceneId : 0;
+                // Scenes 0-2 without a debug view take the instantiation with
+                // the scene id fixed; the generic kernel draws the debug views.
+                const int k = p.renderDebugMode == 0 && p.sceneId >= 0 && p.sceneId <= 2 ? 1 + p.sceneId : 0;
                 const RayTiles tiles{rayTileCounter_, rayTileOrder_, rayTilesX_, rayTileCount_};
                 auto kernel = k == 1 ? raymarchScene0 : (k == 2 ? raymarchScene1 : (k == 3 ? raymarchScene2 : raymarch));
                 kernel<<<rayBlocks_[k], 128, 0, stream>>>(hdr_, scalarsIn(), velocity(), light_, shadow_, p, tiles, lat); ++launches_;
