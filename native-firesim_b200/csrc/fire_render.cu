@@ -356,6 +356,9 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
         const float t0 = fmaxf(0.0f, boxNear);
         const float t1 = fminf(boxFar, t0 + 3.05f);
         const float stepT = (t1 - t0) / static_cast<float>(raySteps);
+        const float cellX = 1.0f / static_cast<float>(p.nx);
+        const float cellY = 1.0f / static_cast<float>(p.ny);
+        const float cellZ = 1.0f / static_cast<float>(p.nz);
         const float rayJitter = hash21((static_cast<float>(x) + 0.5f) * 0.754877f, (static_cast<float>(y) + 0.5f) * 0.569840f);
         for (int i = 0; i < raySteps && trans > 0.018f; ++i) {
             const float t = t0 + (static_cast<float>(i) + rayJitter) * stepT;
@@ -403,9 +406,6 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
             if (velocityDebug) {
                 debugVelocity = fmaxf(debugVelocity, saturate(sqrtf(dot3(velocity, velocity)) * 0.22f));
             }
-            const float cellX = 1.0f / static_cast<float>(p.nx);
-            const float cellY = 1.0f / static_cast<float>(p.ny);
-            const float cellZ = 1.0f / static_cast<float>(p.nz);
             const float gradHeatX = sampleHeat(s, g, wu + cellX, wv, ww) - sampleHeat(s, g, wu - cellX, wv, ww);
             const float gradHeatY = sampleHeat(s, g, wu, wv + cellY, ww) - sampleHeat(s, g, wu, wv - cellY, ww);
             const float gradHeatZ = sampleHeat(s, g, wu, wv, ww + cellZ) - sampleHeat(s, g, wu, wv, ww - cellZ);
