@@ -67,3 +67,14 @@ def test_reference_arm_prints_one_line_from_rank_zero(tmp_path):
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["steps"] == 1 and line["warmup"] == 3
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_reference_arm_for_config_workloads_is_unavailable(tmp_path):
+    """native-firesim has no config physics, so its arm prints an `unavailable`
+    line (one, from rank 0) and exits 0."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--physics", "config", "--workload", "c2"],
+                         env=env, capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference" and "config physics" in lines[0]["unavailable"]
