@@ -305,8 +305,9 @@ def config_scene_physics(abi, rng: SplitMix64, dims, seed: int, lib):
     return abi.config_scene(nx, ny, nz, cx, cz, r, rng.uniform(-0.5, 0.5), rng.uniform(-0.5, 0.5), seed, lib)
 
 
-def run_batched(args, pkg) -> None:
-    """48 independent scenes of mixed sizes stepped together (fireBatchStep)."""
+def run_batched(args, pkg, emit: bool = True) -> dict:
+    """48 independent scenes of mixed sizes stepped together: one FireBatch for
+    the config physics with the multigrid projection, else fireBatchStep."""
     import torch
     abi = pkg.abi
     config = args.physics == "config"
@@ -324,44 +325,78 @@ def run_batched(args, pkg) -> None:
         scenes.append(sc)
         hdrs.append(hdr)
         if config:
-            sc.set_physics(config_scene_physics(abi, rng, d, 1000 + i, lib))
+            phys = config_scene_physics(abi, rng, d, 1000 + i, lib)
+            if args.solver == "mg":
+                phys.pressureTop = 1
+            sc.set_physics(phys)
+            if args.solver == "mg":
+                sc.set_pressure_multigrid(args.mg_cycles, args.mg_pre, args.mg_post)
+                sc.set_pressure_tolerance(0.5 * args.div_target, 1)
             s = abi.FireSettings(width=256, height=256, dt=1.0 / 60.0)
         else:
             s = scene_settings(abi, rng, d, 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
             s.raymarchSteps = 64
         settings.append(s)
     voxels = sum(int(np.prod(d)) for d in dims)
+    # The config physics with the multigrid projection runs as one FireBatch
+    # (one launch per stage over every scene); otherwise fireBatchStep queues
+    # each scene's own launches on its own stream.
+    batch = pkg.Batch(scenes) if config and args.solver == "mg" else None
 
     def sub_step(i):
         for s in settings:
             s.reset = 1 if i == 0 else 0
-        pkg.batch_step(scenes, settings, render=[(i % args.render_every) == args.render_every - 1] * len(scenes))
+        render = [(i % args.render_every) == args.render_every - 1] * len(scenes)
+        if batch is not None:
+            batch.run(settings, render=render)
+        else:
+            pkg.batch_step(scenes, settings, render=render)
+
+    def sync_all():
+        if batch is not None:
+            batch.synchronize()
+        for sc in scenes:
+            sc.synchronize()
 
     for i in range(args.warmup):
         sub_step(i)
-    for sc in scenes:
-        sc.synchronize()
+    sync_all()
     torch.cuda.synchronize()
+    launches0 = batch.launch_count() if batch is not None else None
     t0 = time.perf_counter()
     for i in range(args.warmup, args.warmup + args.steps):
         sub_step(i)
-    for sc in scenes:
-        sc.synchronize()
+    sync_all()
     wall = time.perf_counter() - t0
+    stats = [sc.pressure_stats() for sc in scenes] if config and args.solver == "mg" else []
     line = {"metric": "voxel-steps/s", "mode": "batched", "value": voxels * args.steps / wall, "unit": "voxel-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_sub_step": wall * 1e3 / args.steps,
             "higher_is_better": True, "dtype": precision, "data": "synthetic (SplitMix64 seed 11 draws)",
             "config": {"workload": f"{args.scenes} independent scenes, sizes drawn from {sizes}, "
                                    f"{'config physics (one disk emitter each, r U[4,12], wind U[-0.5,0.5]^2, seeds 1000+i)' if config else 'reference physics'}, "
-                                   f"{precision} storage, SOR 40 iterations omega 1.8, 256x256 render (64 samples) every "
+                                   f"{precision} storage, "
+                                   + (f"p = 0 on the top face, multigrid until max|r| <= {0.5 * args.div_target:g}, "
+                                      if config and args.solver == "mg" else "SOR 40 iterations omega 1.8, ")
+                                   + "256x256 render (64 samples) every "
                                    f"{args.render_every} steps, one fireBatchStep per sub-step, each scene on its own stream",
-                       "voxels_per_sub_step": voxels, "timing": "host wall clock around the sub-steps, synchronised on all scenes"}}
-    print(json.dumps(line), flush=True)
+                       "voxels_per_sub_step": voxels, "timing": "host wall clock around the sub-steps, synchronised on all scenes",
+                       "launch": "FireBatch: one launch per stage over all scenes" if batch is not None else
+                                 "fireBatchStep: each scene's launches on its own stream"}}
+    if batch is not None:
+        line["gpu_launches"] = batch.launch_count() - launches0
+    if stats:
+        line["multigrid_last_sub_step"] = {"cycles_max": max(st[0] for st in stats), "cycles_mean": float(np.mean([st[0] for st in stats])),
+                                           "max_residual": max(st[1] for st in stats)}
+    if emit:
+        print(json.dumps(line), flush=True)
+    if batch is not None:
+        batch.close()
     for sc in scenes:
         sc.close()
+    return line
 
 
-def run_serve(args, pkg) -> None:
+def run_serve(args, pkg, emit: bool = True) -> dict:
     """Poisson arrivals of scene requests into the FireServer loop."""
     abi = pkg.abi
     config = args.physics == "config"
@@ -388,6 +423,10 @@ def run_serve(args, pkg) -> None:
         if config:
             r.settings = abi.FireSettings(width=256, height=256, dt=1.0 / 60.0)
             r.physics = config_scene_physics(abi, rng, (edge, edge, edge), 5000 + n, lib)
+            if args.solver == "mg":
+                r.physics.pressureTop = 1
+                r.multigridCycles, r.multigridPre, r.multigridPost = args.mg_cycles, args.mg_pre, args.mg_post
+                r.pressureTolerance = 0.5 * args.div_target
         else:
             r.settings = scene_settings(abi, rng, (edge, edge, edge), 256, 256, (4.0, 12.0), rng.uniform(-0.5, 0.5))
             r.settings.raymarchSteps = 64
@@ -406,11 +445,16 @@ def run_serve(args, pkg) -> None:
             "config": {"workload": f"Poisson arrivals at {args.rate}/s for {args.arrival_seconds} s; cubic edge log-normal "
                                    "(median 96, sigma 0.4) clamped to [32, 192], multiple of 16; steps U[30, 300]; "
                                    f"{'config physics (per-request emitter, wind and seed)' if config else 'reference physics'}, "
-                                   f"{precision} storage, SOR 40; 256x256 render (64 samples) every 4 steps; "
+                                   f"{precision} storage, "
+                                   + (f"p = 0 on the top face, multigrid until max|r| <= {0.5 * args.div_target:g}; "
+                                      if config and args.solver == "mg" else "SOR 40; ")
+                                   + "256x256 render (64 samples) every 4 steps; "
                                    f"HBM budget {args.budget_gb} GB; at most {args.max_active_mvoxels} M active cells; "
                                    f"run bounded at {args.serve_seconds} s",
-                       "latency": "device time between a scene's consecutive step completions, events on its stream"}}
-    print(json.dumps(line), flush=True)
+                       "latency": "device time between a scene's consecutive step completions (events)"}}
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 # Algorithmic bytes per cell of each config-physics stage (FP32 layout: record a
@@ -509,7 +553,7 @@ def divergence_after(pkg, lib, sim, settings, fw: int, fh: int) -> dict:
             "note": "one measured step after the timed regions; max over cells, every face included"}
 
 
-def run_config(args, pkg, world: int, rank: int, local: int) -> None:
+def run_config(args, pkg, world: int, rank: int, local: int, emit: bool = True) -> dict | None:
     """One scene of the config physics (FirePhysicsParams mode 1) on workload c1, c2 or c3."""
     import torch
     abi = pkg.abi
@@ -654,8 +698,52 @@ def run_config(args, pkg, world: int, rank: int, local: int) -> None:
             "divergence_after": divergence,
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     sim.close()
+    return line if rank == 0 else None
+
+
+def headline_block(args, pkg, world: int, rank: int, local: int) -> dict | None:
+    """The comparison at |div u| <= --div-target (p = 0 on the top face,
+    multigrid until max |r| <= half of it), measured in the same run: the
+    plain 128^3 FP32 single scene (workload c2's physics and render cadence),
+    the batched mix (48 scenes of mixed sizes, FP16 storage, one FireBatch),
+    and a bounded served run (Poisson arrivals, BF16 storage), with the ratios
+    of the batched and served rates to the plain one."""
+    import copy
+    base = copy.copy(args)
+    base.physics, base.solver, base.precision_set = "config", "mg", True
+    plain_args = copy.copy(base)
+    plain_args.workload, plain_args.precision = "c2", "f32"
+    plain_args.steps, plain_args.warmup = args.headline_steps, 10
+    plain_args.no_cpu_baseline, plain_args.no_e2e = True, False
+    plain = run_config(plain_args, pkg, world, rank, local, emit=False)
+    if rank != 0:
+        return None
+    batched_args = copy.copy(base)
+    batched_args.mode, batched_args.precision, batched_args.scenes = "batched", "f16", 48
+    batched_args.steps, batched_args.warmup, batched_args.render_every = args.headline_batched_steps, 10, 10
+    batched = run_batched(batched_args, pkg, emit=False)
+    served_args = copy.copy(base)
+    served_args.mode, served_args.precision = "serve", "bf16"
+    served_args.arrival_seconds, served_args.serve_seconds = args.headline_arrival_seconds, args.headline_serve_seconds
+    served = run_serve(served_args, pkg, emit=False)
+    pv = plain["value"]
+    return {
+        "condition": f"|div u| <= {args.div_target:g}: p = 0 on the top face, multigrid until max|r| <= {0.5 * args.div_target:g}",
+        "plain": {"value": pv, "e2e": plain["e2e"]["value"] if plain.get("e2e") else None, "unit": "voxel-steps/s",
+                  "workload": plain["config"]["workload"], "dtype": plain["dtype"], "ms_per_step": plain["ms_per_step"],
+                  "divergence_after_max": plain["divergence_after"]["max"],
+                  "multigrid_cycles_last_step": plain["pressure_stats_last_step"]["iterations"]},
+        "batched": {"value": batched["value"], "unit": "voxel-steps/s", "dtype": batched["dtype"],
+                    "ms_per_sub_step": batched["ms_per_sub_step"], "voxels_per_sub_step": batched["config"]["voxels_per_sub_step"],
+                    "gpu_launches": batched.get("gpu_launches"), "multigrid": batched.get("multigrid_last_sub_step"),
+                    "workload": batched["config"]["workload"], "ratio_to_plain": batched["value"] / pv},
+        "served": {"value": served["value"], "unit": "voxel-steps/s", "dtype": served["dtype"], "latency_ms": served["latency_ms"],
+                   "requests": served["requests"], "seconds": served["seconds"], "workload": served["config"]["workload"],
+                   "ratio_to_plain": served["value"] / pv},
+    }
 
 
 def main() -> int:
@@ -698,6 +786,12 @@ def main() -> int:
     ap.add_argument("--max-active-mvoxels", type=float, default=24.0,
                     help="serve: admit while the admitted scenes hold at most this many million cells (0 = no limit)")
     ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--no-headline", action="store_true",
+                    help="single mode: skip the headline block (plain, batched and served at |div u| <= --div-target)")
+    ap.add_argument("--headline-steps", type=int, default=100)
+    ap.add_argument("--headline-batched-steps", type=int, default=20)
+    ap.add_argument("--headline-arrival-seconds", type=float, default=5.0)
+    ap.add_argument("--headline-serve-seconds", type=float, default=15.0)
     ap.add_argument("--sor-path", default="auto", choices=["auto", "graph", "resident"],
                     help="pressure SOR: per-launch half sweeps in a CUDA graph, one cooperative resident launch, or auto")
     args = ap.parse_args()
@@ -718,6 +812,9 @@ def main() -> int:
         dist_barrier(world)
         return 0
 
+    # The GPU arms warm up for at least one whole render interval, so the first
+    # timed frame does not pay the first render's one-time costs.
+    args.warmup = max(args.warmup, args.render_every)
     import torch
     torch.cuda.set_device(local)
     pkg = load_package()
@@ -838,6 +935,8 @@ def main() -> int:
     roofline = roofline_block(dominant, st, args, cells, peaks, peak_src, sim.pressure_path_used())
 
     divergence = divergence_after(pkg, lib, sim, workload_settings(abi, frame, args), args.frame, args.frame)
+    sim.close()
+    headline = None if args.no_headline else headline_block(args, pkg, world, rank, local)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(pkg, args)
@@ -852,10 +951,9 @@ def main() -> int:
             "data": "synthetic (seeded procedural fuel bed + validation-harness settings)",
             "config": config_block(args), "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "roofline": roofline, "stage_ms": per_step_ms, "step_latency": latency, "divergence_after": divergence,
-            "cpu_baseline": cpu,
+            "cpu_baseline": cpu, "headline": headline,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -149,6 +149,15 @@ FIRE_API int fireCudaGetPressurePathUsed(void);
  * announces its half sweeps.  Pass (-1, 1000000) to restore the defaults. */
 FIRE_API bool fireCudaSetResidentSorFault(int silentBrick, long long waitUs);
 
+/* Host-side fault injection of device allocations (no counterpart in the
+ * reference): -1 turns it off; n >= 0 lets n more of the library's scene
+ * allocations succeed, after which every one fails as cudaMalloc does when
+ * device memory runs out ("out of memory (injected)").  Nothing reaches the
+ * GPU: the failing call is never made.  Initialisation that hits it fails
+ * and frees what it had allocated, as the reference's init does
+ * (src/fire_cuda.cu:2981). */
+FIRE_API bool fireCudaSetAllocationFault(long long succeedBeforeFailing);
+
 /* nx, ny, nz, lightNx, lightNy, lightNz, frameWidth, frameHeight. */
 FIRE_API bool fireCudaGetGridInfo(int* dims8);
 
@@ -187,12 +196,27 @@ FIRE_API bool fireCudaGetLaunchCount(unsigned long long* count);
  * captured into a CUDA graph (cudaMalloc cannot be captured), plugins whose
  * host forbids allocations after start-up.
  *
- * Inputs: the cell records in this library's packed layout (recordsA: float4
- * heat, fuel, oxygen, soot; recordsB: float4 char, ash, pyrolysis, progress;
- * recordsC: float2 turbulenceEnergy, sootOptics; nx*ny*nz each, x fastest) and
+ * Inputs: the cell records in this library's packed layout (recordsA: 4-vector
+ * heat, fuel, oxygen, soot; recordsB: 4-vector char, ash, pyrolysis, progress;
+ * recordsC: 2-vector turbulenceEnergy, sootOptics; nx*ny*nz each, x fastest) and
  * the MAC faces u, v, w.  Outputs: uOut, vOut, wOut, divergence (nx*ny*nz) and
  * pressure (set to 0).  All device pointers; work is queued on `stream`
  * (0 = legacy default stream) and the call returns without synchronising.
+ *
+ * Element type: records and faces (inputs and uOut/vOut/wOut) are in the
+ * storage type of the library that is loaded: float in libfiresim_b200.so,
+ * IEEE half in libfiresim_b200_f16.so, bfloat16 in libfiresim_b200_bf16.so
+ * (the pointer types below are float only for the FP32 build's sake);
+ * divergence and pressure are float in every build.
+ *
+ * Physics: this is the reference physics' force pass (FirePhysicsParams mode
+ * 0) only.  It takes no physics parameters and ignores any mode set with
+ * fireCudaSetPhysicsParams; the config physics' FORCE..DIVERGENCE stages are
+ * different kernels.
+ *
+ * Errors: if a CUDA error from the caller's earlier work is already pending,
+ * nothing is launched and the call fails without clearing it.  ny and nz are
+ * at most 65535.
  *
  * Limit: at most 1,048,576 cells (nx*ny*nz); larger grids are rejected.  The
  * per-cell increments live in one fixed 16 MiB array that every GPU loading
@@ -318,11 +342,36 @@ FIRE_API bool fireSceneSynchronize(FireScene* scene);
 FIRE_API bool fireSceneGetStream(FireScene* scene, void** stream);
 /* Waits for the scene, then copies one field (FIRE_FIELD_*), as fireCudaGetField. */
 FIRE_API bool fireSceneGetField(FireScene* scene, int field, void* host, size_t bytes);
+/* As fireCudaGetPressureStats, for one scene (waits for the scene's stream). */
+FIRE_API bool fireSceneGetPressureStats(FireScene* scene, int* iterations, float* maxResidual, double* l2Residual);
 
 /* One sub-step of n scenes: queues fireSceneStep(scenes[i], &settings[i],
  * render ? render[i] : 0) for every scene, each on its own stream, so the
  * scenes' kernels run side by side on the GPU. */
 FIRE_API bool fireBatchStep(FireScene* const* scenes, const FireSettings* settings, const int* render, int n);
+
+/* A batch of scenes of the config physics stepped as one: per sub-step one
+ * upload of the scenes' step descriptors, one launch per stage whose blocks
+ * cover every scene, and the pressure solve of every scene in one persistent
+ * multigrid launch.  No counterpart in the reference (one process-wide scene).
+ * Every scene must use the config physics with p = 0 on the top face
+ * (FirePhysicsParams mode 1, pressureTop 1) and the multigrid solve, with the
+ * same cycles, smoothing sweeps and tolerance; sizes may differ; at most 128
+ * scenes.  Each scene's result is the same bits as stepping it alone.  While
+ * a scene belongs to a batch, its own calls (fireSceneGetField, ...) run on
+ * the batch's stream; fireBatchDestroy gives each scene its stream back.
+ * Destroy the batch before its scenes. */
+typedef struct FireBatch FireBatch;
+FIRE_API FireBatch* fireBatchCreate(FireScene* const* scenes, int n);
+FIRE_API void fireBatchDestroy(FireBatch* batch);
+/* One sub-step of every scene: settings[i] for scene i (its reset flag and dt
+ * clamp as in fireSceneStep); render[i] != 0 (render may be NULL) also
+ * renders scene i's frame into its HDR buffer.  Queued; returns at once. */
+FIRE_API bool fireBatchRun(FireBatch* batch, const FireSettings* settings, const int* render);
+FIRE_API bool fireBatchSynchronize(FireBatch* batch);
+FIRE_API bool fireBatchGetStream(FireBatch* batch, void** stream);
+/* Kernels (and the solve's one persistent launch) queued by the batch so far. */
+FIRE_API bool fireBatchGetLaunchCount(FireBatch* batch, unsigned long long* count);
 
 /* A serving loop over FireScenes: requests arrive over time, are admitted
  * while the device memory of the admitted scenes stays within a budget, and
@@ -344,6 +393,10 @@ typedef struct FireServeRequest {
     float* resultHdr;           /* optional host buffer (frameW*frameH*4 floats): last frame */
     FirePhysicsParams physics;  /* mode 1: the scene's config physics (validated at submit);
                                    mode 0 (e.g. all zero): the reference's physics */
+    int multigridCycles;        /* > 0 (config physics with pressureTop 1 only): the pressure is
+                                   solved by multigrid V-cycles, at most this many per step */
+    int multigridPre, multigridPost;  /* smoothing sweeps per level (0 = 2) */
+    double pressureTolerance;   /* > 0: stop the solve once max |r| <= this (checked per cycle) */
 } FireServeRequest;
 typedef struct FireServeReport {
     int submitted, completed, admittedPeak;
@@ -372,8 +425,17 @@ FIRE_API bool fireServerSubmit(FireServer* server, const FireServeRequest* reque
 /* Runs rounds until every submitted request has completed or `maxSeconds`
  * of wall time have passed.  Step latency is the device time between the
  * completions of a scene's consecutive steps (its first step: from its
- * admission), measured with events on the scene's stream; it contains the
- * time the scene shares the GPU with the others. */
+ * admission), measured with events; it contains the time the scene shares
+ * the GPU with the others.
+ *
+ * When every submitted request uses the config physics with the multigrid
+ * projection (physics.mode 1, pressureTop 1, multigridCycles > 0), each round
+ * steps all admitted scenes as one batch (one launch per stage over all of
+ * them, as FireBatch), and the scenes are created before the clock starts:
+ * per grid shape as many as the active-cell limit lets run at once, within
+ * the budget.  The loop then allocates no device memory; a request whose
+ * shape has no free scene waits for one.  At most 128 scenes are admitted at
+ * once.  Otherwise each admitted scene takes its own steps on its own stream. */
 FIRE_API bool fireServerRun(FireServer* server, double maxSeconds, FireServeReport* report);
 
 /* Name of the build and its compute capability target, for diagnostics. */

@@ -200,7 +200,8 @@ class FireServeRequest(ctypes.Structure):
         ("frameW", ctypes.c_int), ("frameH", ctypes.c_int), ("steps", ctypes.c_int), ("renderEvery", ctypes.c_int),
         ("sorIterations", ctypes.c_int), ("sorOmega", ctypes.c_float), ("arrivalSeconds", ctypes.c_double),
         ("settings", FireSettings), ("resultHeat", ctypes.c_void_p), ("resultHdr", ctypes.c_void_p),
-        ("physics", FirePhysicsParams),
+        ("physics", FirePhysicsParams), ("multigridCycles", ctypes.c_int), ("multigridPre", ctypes.c_int),
+        ("multigridPost", ctypes.c_int), ("pressureTolerance", ctypes.c_double),
     ]
 
 

@@ -74,6 +74,12 @@ bool fireCudaInitializeGrid(int frameWidth, int frameHeight, int nx, int ny, int
     return initialize(frameWidth, frameHeight, nx, ny, nz);
 }
 
+bool fireCudaSetAllocationFault(long long succeedBeforeFailing) {
+    if (succeedBeforeFailing < -1) return fail("fireCudaSetAllocationFault: the count must be -1 (off) or >= 0.");
+    firesim::setAllocationFault(succeedBeforeFailing);
+    return true;
+}
+
 bool fireCudaStepAndRender(uint32_t* bgraPixels, const FireSettings& settings) {
     return frame(bgraPixels, &settings, nullptr, false, true, true);
 }

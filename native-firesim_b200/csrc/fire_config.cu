@@ -171,12 +171,8 @@ __device__ __forceinline__ float cellCentred(const FaceT* f, int lo, int hi) { r
 
 // Each thread owns u(x,y,z), v(x,y,z) and w(x,y,z) where they exist and
 // writes each as the face grid sampled at its one-step backtrace.
-__global__ void __launch_bounds__(128) cfgAdvectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
-                                                         Velocity vel, ConfigParams p) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
-    if (x > p.nx) return;
+__device__ __forceinline__ void cfgAdvectVelocityAt(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                         const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
     const float fx = static_cast<float>(x), fy = static_cast<float>(y), fz = static_cast<float>(z);
     if (y < p.ny && z < p.nz) {
         const float px = fx, py = fy + 0.5f, pz = fz + 0.5f;
@@ -199,12 +195,17 @@ __global__ void __launch_bounds__(128) cfgAdvectVelocity(FaceT* __restrict__ uOu
     }
 }
 
-// Backtrace of record a from the cell centre, then burn, decay and emitters.
-__global__ void __launch_bounds__(128) cfgAdvectScalars(Rec4* __restrict__ aOut, const Rec4* __restrict__ aIn, Velocity vel, ConfigParams p) {
+__global__ void __launch_bounds__(128) cfgAdvectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                         Velocity vel, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
-    if (x >= p.nx) return;
+    if (x > p.nx) return;
+    cfgAdvectVelocityAt(uOut, vOut, wOut, vel, p, x, y, z);
+}
+
+// Backtrace of record a from the cell centre, then burn, decay and emitters.
+__device__ __forceinline__ void cfgAdvectScalarsAt(Rec4* __restrict__ aOut, const Rec4* __restrict__ aIn, const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
     const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
     const float3 d = velocityAtCentre(vel, p, x, y, z);
     const float4 s = recordAt(aIn, p, px - d.x, py - d.y, pz - d.z);
@@ -228,13 +229,17 @@ __global__ void __launch_bounds__(128) cfgAdvectScalars(Rec4* __restrict__ aOut,
     stv(aOut + cell, make_float4(heat, fuel, 0.0f, soot));
 }
 
-// omega = curl of the cell-centred velocity (central differences, clamped
-// neighbours), and |omega|.
-__global__ void __launch_bounds__(128) cfgVorticity(float4* __restrict__ vort, Velocity vel, ConfigParams p) {
+__global__ void __launch_bounds__(128) cfgAdvectScalars(Rec4* __restrict__ aOut, const Rec4* __restrict__ aIn, Velocity vel, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
     if (x >= p.nx) return;
+    cfgAdvectScalarsAt(aOut, aIn, vel, p, x, y, z);
+}
+
+// omega = curl of the cell-centred velocity (central differences, clamped
+// neighbours), and |omega|.
+__device__ __forceinline__ void cfgVorticityAt(float4* __restrict__ vort, const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
     const int xm = max(x - 1, 0), xp = min(x + 1, p.nx - 1);
     const int ym = max(y - 1, 0), yp = min(y + 1, p.ny - 1);
     const int zm = max(z - 1, 0), zp = min(z + 1, p.nz - 1);
@@ -248,14 +253,18 @@ __global__ void __launch_bounds__(128) cfgVorticity(float4* __restrict__ vort, V
     vort[(z * p.ny + y) * p.nx + x] = make_float4(ox, oy, oz, sqrtf(ox * ox + oy * oy + oz * oz));
 }
 
-// The curl-noise acceleration amplitude * curl(psi) at every cell centre.  It
-// depends only on the noise parameters and the grid, so the scene builds it
-// once per parameter set and cfgCellForce reads it.
-__global__ void __launch_bounds__(128) cfgNoiseField(float4* __restrict__ noise, ConfigParams p) {
+__global__ void __launch_bounds__(128) cfgVorticity(float4* __restrict__ vort, Velocity vel, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
     if (x >= p.nx) return;
+    cfgVorticityAt(vort, vel, p, x, y, z);
+}
+
+// The curl-noise acceleration amplitude * curl(psi) at every cell centre.  It
+// depends only on the noise parameters and the grid, so the scene builds it
+// once per parameter set and cfgCellForce reads it.
+__device__ __forceinline__ void cfgNoiseFieldAt(float4* __restrict__ noise, const ConfigParams& p, int x, int y, int z) {
     const float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f, pz = static_cast<float>(z) + 0.5f;
     const float3 g0 = noiseGradient(p, 0, px, py, pz);
     const float3 g1 = noiseGradient(p, 1, px, py, pz);
@@ -263,14 +272,18 @@ __global__ void __launch_bounds__(128) cfgNoiseField(float4* __restrict__ noise,
     noise[(z * p.ny + y) * p.nx + x] = make_float4(p.noiseAmp * (g2.y - g1.z), p.noiseAmp * (g0.z - g2.x), p.noiseAmp * (g1.x - g0.y), 0.0f);
 }
 
-// Cell-centred acceleration: buoyancy + confinement + curl noise (read from
-// the field cfgNoiseField built; null when the amplitude is 0).
-__global__ void __launch_bounds__(128) cfgCellForce(float4* __restrict__ force, const float4* __restrict__ vort, const Rec4* __restrict__ a,
-                                                    const float4* __restrict__ noise, ConfigParams p) {
+__global__ void __launch_bounds__(128) cfgNoiseField(float4* __restrict__ noise, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
     if (x >= p.nx) return;
+    cfgNoiseFieldAt(noise, p, x, y, z);
+}
+
+// Cell-centred acceleration: buoyancy + confinement + curl noise (read from
+// the field cfgNoiseField built; null when the amplitude is 0).
+__device__ __forceinline__ void cfgCellForceAt(float4* __restrict__ force, const float4* __restrict__ vort, const Rec4* __restrict__ a,
+                                                    const float4* __restrict__ noise, const ConfigParams& p, int x, int y, int z) {
     const int idx = (z * p.ny + y) * p.nx + x;
     const float4 s = ldv(a + idx);
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
@@ -304,15 +317,20 @@ __global__ void __launch_bounds__(128) cfgCellForce(float4* __restrict__ force, 
     force[idx] = make_float4(cx + fx, buoyancy + cy + fy, cz + fz, 0.0f);
 }
 
-// Faces += dt * (mean of the two adjacent cells' accelerations) + wind; the
-// emitter cells' v faces take upVelocity; walls (u at x = 0, nx; v at y = 0;
-// w at z = 0, nz) are zero; the top v faces keep the cell below's acceleration.
-__global__ void __launch_bounds__(128) cfgApplyForces(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
-                                                      Velocity vel, const float4* __restrict__ force, ConfigParams p) {
+__global__ void __launch_bounds__(128) cfgCellForce(float4* __restrict__ force, const float4* __restrict__ vort, const Rec4* __restrict__ a,
+                                                    const float4* __restrict__ noise, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
-    if (x > p.nx) return;
+    if (x >= p.nx) return;
+    cfgCellForceAt(force, vort, a, noise, p, x, y, z);
+}
+
+// Faces += dt * (mean of the two adjacent cells' accelerations) + wind; the
+// emitter cells' v faces take upVelocity; walls (u at x = 0, nx; v at y = 0;
+// w at z = 0, nz) are zero; the top v faces keep the cell below's acceleration.
+__device__ __forceinline__ void cfgApplyForcesAt(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                      const Velocity& vel, const float4* __restrict__ force, const ConfigParams& p, int x, int y, int z) {
     if (y < p.ny && z < p.nz) {
         const int i = faceIndex(x, y, z, p.nx + 1, p.ny);
         float u = 0.0f;
@@ -346,14 +364,19 @@ __global__ void __launch_bounds__(128) cfgApplyForces(FaceT* __restrict__ uOut, 
     }
 }
 
+__global__ void __launch_bounds__(128) cfgApplyForces(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                      Velocity vel, const float4* __restrict__ force, ConfigParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x > p.nx) return;
+    cfgApplyForcesAt(uOut, vOut, wOut, vel, force, p, x, y, z);
+}
+
 // Transmittance toward the point light from the centre of each 2x2x2 block of
 // cells: lightSamples midpoint samples of extinction * S + fuelExtinction * F
 // along the segment, clipped where it leaves the grid box.
-__global__ void __launch_bounds__(128) cfgTransmittance(float* __restrict__ tr, const Rec4* __restrict__ a, ConfigParams p) {
-    const int lx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ly = blockIdx.y;
-    const int lz = blockIdx.z;
-    if (lx >= p.lx) return;
+__device__ __forceinline__ void cfgTransmittanceAt(float* __restrict__ tr, const Rec4* __restrict__ a, const ConfigParams& p, int lx, int ly, int lz) {
     const float px = 2.0f * static_cast<float>(lx) + 1.0f, py = 2.0f * static_cast<float>(ly) + 1.0f, pz = 2.0f * static_cast<float>(lz) + 1.0f;
     const float dx = p.light.x - px, dy = p.light.y - py, dz = p.light.z - pz;
     const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -380,14 +403,19 @@ __global__ void __launch_bounds__(128) cfgTransmittance(float* __restrict__ tr, 
     tr[(lz * p.ly + ly) * p.lx + lx] = t;
 }
 
+__global__ void __launch_bounds__(128) cfgTransmittance(float* __restrict__ tr, const Rec4* __restrict__ a, ConfigParams p) {
+    const int lx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ly = blockIdx.y;
+    const int lz = blockIdx.z;
+    if (lx >= p.lx) return;
+    cfgTransmittanceAt(tr, a, p, lx, ly, lz);
+}
+
 // One pixel: the camera ray's chord through the grid box in primarySamples
 // midpoint samples; absorption, in-scattering of the point light (its
 // transmittance volume) and emission; a dark background behind.
-__global__ void __launch_bounds__(128) cfgRaymarch(float4* __restrict__ hdr, const Rec4* __restrict__ a, const float* __restrict__ tr,
-                                                   ConfigParams p) {
-    const int px = blockIdx.x * blockDim.x + threadIdx.x;
-    const int py = blockIdx.y * blockDim.y + threadIdx.y;
-    if (px >= p.frameW || py >= p.frameH) return;
+__device__ __forceinline__ void cfgRaymarchAt(float4* __restrict__ hdr, const Rec4* __restrict__ a, const float* __restrict__ tr,
+                                                   const ConfigParams& p, int px, int py) {
     const float sx = (2.0f * (static_cast<float>(px) + 0.5f) / static_cast<float>(p.frameW) - 1.0f) * p.tanHalf * p.aspect;
     const float sy = (1.0f - 2.0f * (static_cast<float>(py) + 0.5f) / static_cast<float>(p.frameH)) * p.tanHalf;
     float dx = p.forward.x + p.right.x * sx + p.up.x * sy;
@@ -434,6 +462,199 @@ __global__ void __launch_bounds__(128) cfgRaymarch(float4* __restrict__ hdr, con
         }
     }
     hdr[py * p.frameW + px] = make_float4(r + view * 0.015f, g + view * 0.016f, b + view * 0.020f, 1.0f - view);
+}
+
+__global__ void __launch_bounds__(128) cfgRaymarch(float4* __restrict__ hdr, const Rec4* __restrict__ a, const float* __restrict__ tr,
+                                                   ConfigParams p) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= p.frameW || py >= p.frameH) return;
+    cfgRaymarchAt(hdr, a, tr, p, px, py);
+}
+
+// ---- the incremental projection of the multigrid solve (fire_mg.cu) ----
+
+// The incremental projection's first half (see the file comment), out of
+// place: per cell, the faces it owns (u at x, v at y, w at z, and the last
+// face of each axis for the last cell) are written to the other velocity
+// buffer, the interior ones and the top ones minus the previous pressure's
+// gradient, rounded to storage, the wall ones as they are; rhs = -div of the
+// cell's six updated faces (those it does not own recomputed the same way).
+__device__ __forceinline__ void cfgPrepareIncrementAt(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                      const Velocity& vel, const float* __restrict__ pressure, float* __restrict__ rhs,
+                                                      int nx, int ny, int nz, int x, int y, int z) {
+    const int i = (z * ny + y) * nx + x;
+    const int ui = (z * ny + y) * (nx + 1) + x;
+    const int vi = (z * (ny + 1) + y) * nx + x;
+    const int wi = (z * ny + y) * nx + x;
+    const float pc = pressure[i];
+    const float u0 = x > 0 ? storageRound(ldv(vel.u + ui) - (pc - pressure[i - 1])) : ldv(vel.u + ui);
+    const float u1 = x + 1 < nx ? storageRound(ldv(vel.u + ui + 1) - (pressure[i + 1] - pc)) : ldv(vel.u + ui + 1);
+    const float v0 = y > 0 ? storageRound(ldv(vel.v + vi) - (pc - pressure[i - nx])) : ldv(vel.v + vi);
+    const float v1 = y + 1 < ny ? storageRound(ldv(vel.v + vi + nx) - (pressure[i + nx] - pc))
+                                : storageRound(ldv(vel.v + vi + nx) - ((0.0f - pc) - pc));
+    const float w0 = z > 0 ? storageRound(ldv(vel.w + wi) - (pc - pressure[i - nx * ny])) : ldv(vel.w + wi);
+    const float w1 = z + 1 < nz ? storageRound(ldv(vel.w + wi + nx * ny) - (pressure[i + nx * ny] - pc)) : ldv(vel.w + wi + nx * ny);
+    const float div = u1 - u0 + v1 - v0 + w1 - w0;
+    rhs[i] = -div;
+    stv(uOut + ui, u0);
+    stv(vOut + vi, v0);
+    stv(wOut + wi, w0);
+    if (x == nx - 1) stv(uOut + ui + 1, u1);
+    if (y == ny - 1) stv(vOut + vi + nx, v1);
+    if (z == nz - 1) stv(wOut + wi + nx * ny, w1);
+}
+
+// The incremental projection's second half: u -= grad delta on the interior
+// faces and the top faces (ghost -delta); with doWalls the closed walls are
+// zeroed as in subtractWall.
+__device__ __forceinline__ void cfgSubtractIncrementAt(FaceT* __restrict__ u, FaceT* __restrict__ v, FaceT* __restrict__ w,
+                                                       const float* __restrict__ delta, int nx, int ny, int nz, int doWalls, int x, int y,
+                                                       int z) {
+    const int i = (z * ny + y) * nx + x;
+    const float dc = delta[i];
+    const int ui = (z * ny + y) * (nx + 1) + x;
+    const int vi = (z * (ny + 1) + y) * nx + x;
+    const int wi = (z * ny + y) * nx + x;
+    if (x > 0) stv(u + ui, ldv(u + ui) - (dc - delta[i - 1]));
+    if (y > 0) stv(v + vi, ldv(v + vi) - (dc - delta[i - nx]));
+    if (z > 0) stv(w + wi, ldv(w + wi) - (dc - delta[i - nx * ny]));
+    if (y == ny - 1) {
+        const int top = (z * (ny + 1) + ny) * nx + x;
+        stv(v + top, ldv(v + top) - ((0.0f - dc) - dc));
+    }
+    if (doWalls) {
+        if (x == 0) stv(u + ui, 0.0f);
+        if (x == nx - 1) stv(u + ui + 1, 0.0f);
+        if (y == 0) stv(v + vi, 0.0f);
+        if (z == 0) stv(w + wi, 0.0f);
+        if (z == nz - 1) stv(w + (nz * ny + y) * nx + x, 0.0f);
+    }
+}
+
+__global__ void __launch_bounds__(128) cfgPrepareIncrement(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                           Velocity vel, const float* __restrict__ pressure, float* __restrict__ rhs,
+                                                           int nx, int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nx) return;
+    cfgPrepareIncrementAt(uOut, vOut, wOut, vel, pressure, rhs, nx, ny, nz, x, blockIdx.y, blockIdx.z);
+}
+
+__global__ void __launch_bounds__(128) cfgSubtractIncrement(FaceT* __restrict__ u, FaceT* __restrict__ v, FaceT* __restrict__ w,
+                                                            const float* __restrict__ delta, int nx, int ny, int nz, int doWalls) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nx) return;
+    cfgSubtractIncrementAt(u, v, w, delta, nx, ny, nz, doWalls, x, blockIdx.y, blockIdx.z);
+}
+
+// ---- batched stages (BatchScene, BatchPlan in fire_kernels.h) ----------
+
+namespace {
+
+// The scene of this block: the last s with start[s] <= blockIdx.x.
+__device__ __forceinline__ int batchSceneOf(const int* start, int n) {
+    const int b = static_cast<int>(blockIdx.x);
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(start + mid) <= b) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// This thread's scene and element of index space `space`; false past the end.
+__device__ __forceinline__ bool batchElement(const BatchScene* scenes, const BatchPlan* plan, int space, int& s, int& i) {
+    const int n = plan->scenes;
+    s = batchSceneOf(plan->start[space], n);
+    i = (static_cast<int>(blockIdx.x) - __ldg(plan->start[space] + s)) * kBatchThreads + static_cast<int>(threadIdx.x);
+    return i < scenes[s].count[space];
+}
+
+__device__ __forceinline__ Velocity velocityOf(FaceT* const (&f)[3]) { return Velocity{f[0], f[1], f[2]}; }
+
+}  // namespace
+
+__global__ void __launch_bounds__(kBatchThreads) batchAdvectVelocity(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchFaces, s, i)) return;
+    const BatchScene& B = scenes[s];
+    const int mx = B.c.nx + 1, my = B.c.ny + 1;
+    cfgAdvectVelocityAt(B.adv[0], B.adv[1], B.adv[2], B.vel, B.c, i % mx, (i / mx) % my, i / (mx * my));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchAdvectScalars(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
+    const BatchScene& B = scenes[s];
+    cfgAdvectScalarsAt(B.aOut, B.aIn, velocityOf(B.adv), B.c, i % B.c.nx, (i / B.c.nx) % B.c.ny, i / (B.c.nx * B.c.ny));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchVorticity(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
+    const BatchScene& B = scenes[s];
+    if (B.c.eps == 0.0f) return;
+    cfgVorticityAt(B.vort, velocityOf(B.adv), B.c, i % B.c.nx, (i / B.c.nx) % B.c.ny, i / (B.c.nx * B.c.ny));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchCellForce(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
+    const BatchScene& B = scenes[s];
+    cfgCellForceAt(B.force, B.vort, B.aOut, B.noise, B.c, i % B.c.nx, (i / B.c.nx) % B.c.ny, i / (B.c.nx * B.c.ny));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchApplyForces(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchFaces, s, i)) return;
+    const BatchScene& B = scenes[s];
+    const int mx = B.c.nx + 1, my = B.c.ny + 1;
+    cfgApplyForcesAt(B.forced[0], B.forced[1], B.forced[2], velocityOf(B.adv), B.force, B.c, i % mx, (i / mx) % my, i / (mx * my));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchPrepareIncrement(const BatchScene* __restrict__ scenes,
+                                                                      const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
+    const BatchScene& B = scenes[s];
+    const int nx = B.c.nx, ny = B.c.ny, nz = B.c.nz;
+    cfgPrepareIncrementAt(B.proj[0], B.proj[1], B.proj[2], velocityOf(B.forced), B.pressure, B.divergence, nx, ny, nz, i % nx,
+                          (i / nx) % ny, i / (nx * ny));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchSubtractIncrement(const BatchScene* __restrict__ scenes,
+                                                                       const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
+    const BatchScene& B = scenes[s];
+    const int nx = B.c.nx, ny = B.c.ny, nz = B.c.nz;
+    cfgSubtractIncrementAt(B.proj[0], B.proj[1], B.proj[2], B.delta, nx, ny, nz, 1, i % nx, (i / nx) % ny, i / (nx * ny));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchTransmittance(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchLight, s, i)) return;
+    const BatchScene& B = scenes[s];
+    cfgTransmittanceAt(B.transmittance, B.aOut, B.c, i % B.c.lx, (i / B.c.lx) % B.c.ly, i / (B.c.lx * B.c.ly));
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchRaymarch(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchPixels, s, i)) return;
+    const BatchScene& B = scenes[s];
+    cfgRaymarchAt(B.hdr, B.aOut, B.transmittance, B.c, i % B.c.frameW, i / B.c.frameW);
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batchPackHdr(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
+    int s, i;
+    if (!batchElement(scenes, plan, kBatchPixels, s, i)) return;
+    const BatchScene& B = scenes[s];
+    if (B.slot == nullptr) return;
+    packHdrPixel(B.slot, B.slotPitch, B.slotFormat, B.hdr[i], i % B.c.frameW, i / B.c.frameW);
 }
 
 }  // namespace firesim

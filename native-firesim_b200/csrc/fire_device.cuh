@@ -11,11 +11,10 @@
 // bit.  A one-ulp change there would scramble the noise pattern.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
-#if defined(FIRE_STORAGE_F16)
-#include <cuda_fp16.h>
-#elif defined(FIRE_STORAGE_BF16)
+#if defined(FIRE_STORAGE_BF16)
 #include <cuda_bf16.h>
 #endif
 
@@ -87,6 +86,30 @@ constexpr bool kHalfStorage = false;
 
 __device__ __forceinline__ float ldv(const float* p) { return __ldg(p); }
 __device__ __forceinline__ void stv(float* p, float v) { *p = v; }
+// One pixel of the HDR frame into a caller-owned buffer (the headless form of
+// packFp16SurfaceKernel, src/fire_cuda.cu:2303-2321): float4 RGBA32F, or
+// RGBA16F with negative values clamped to 0 as the reference's halfBits does;
+// alpha is 1.
+__device__ __forceinline__ void packHdrPixel(void* dst, size_t pitchBytes, int halfFormat, float4 r, int x, int y) {
+    char* row = static_cast<char*>(dst) + static_cast<size_t>(y) * pitchBytes;
+    if (halfFormat) {
+        const __half2 rg = __floats2half2_rn(fmaxf(0.0f, r.x), fmaxf(0.0f, r.y));
+        const __half2 ba = __floats2half2_rn(fmaxf(0.0f, r.z), 1.0f);
+        reinterpret_cast<__half2*>(row)[2 * x] = rg;
+        reinterpret_cast<__half2*>(row)[2 * x + 1] = ba;
+    } else {
+        reinterpret_cast<float4*>(row)[x] = make_float4(r.x, r.y, r.z, 1.0f);
+    }
+}
+
+// The value a face or scalar store of v leaves in this build's storage.
+__device__ __forceinline__ float storageRound(float v) {
+#if defined(FIRE_STORAGE_F16) || defined(FIRE_STORAGE_BF16)
+    return halfToFloat(floatToHalf(v));
+#else
+    return v;
+#endif
+}
 #if defined(FIRE_HALF_STORAGE)
 __device__ __forceinline__ float4 ldv(const Rec4* p) {
     const uint2 raw = __ldg(reinterpret_cast<const uint2*>(p));

@@ -202,35 +202,107 @@ __global__ void cfgTransmittance(float* tr, const Rec4* a, ConfigParams p);
 __global__ void cfgRaymarch(float4* hdr, const Rec4* a, const float* tr, ConfigParams p);
 
 // ---------------------------------------------------------------------------
-// Multigrid pressure solve of the config physics (fire_mg.cu).
+// Multigrid pressure solve of the config physics (fire_mg.cu): the
+// incremental projection (cfgPrepareIncrement, mgSolve, cfgSubtractIncrement)
+// for one scene or a batch of scenes in one persistent launch.
 // A level: extents, axis weights 1/h^2 (fine spacing 1), 2 (wx + wy + wz) and
 // its reciprocal, and which axes were halved from the level above.
 struct MgLevel {
     int nx, ny, nz;
     float wx, wy, wz, diag, invDiag;
     int cx, cy, cz;
-    int wide;  // 1: the level's pressure is double (level 0)
 };
-// F: float pressure (the coarser levels); D: double pressure (level 0).
-// Smoothing and prolongation take blocks of kMgRowBlockThreads: 32, 64 or 128
-// threads along a row and as many rows (y) as fill the block, so that the
-// grid has few, large blocks.
-constexpr int kMgRowBlockThreads = 256;
-__global__ void mgSmoothF(float* p, const float* rhs, MgLevel L, int colour, const int* skip);
-__global__ void mgSmoothD(double* p, const float* rhs, MgLevel L, int colour, const int* skip);
-__global__ void mgRestrictF(float* rhsC, float* pC, const float* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);
-__global__ void mgRestrictD(float* rhsC, float* pC, const double* p, const float* rhs, MgLevel F, MgLevel C, const int* skip);
-__global__ void mgProlongF(float* p, const float* pC, MgLevel F, MgLevel C, const int* skip);
-__global__ void mgProlongD(double* p, const float* pC, MgLevel F, MgLevel C, const int* skip);
-__global__ void mgCoarsestF(float* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
-__global__ void mgCoarsestD(double* p, const float* rhs, MgLevel L, int sweeps, const int* skip);
-__global__ void mgResidualPartialsD(const double* p, const float* rhs, MgLevel L, const SorGate* gate, double* partialSq, float* partialMax);
-__global__ void mgStoreFloat(float* dst, const double* src, int n);
-__global__ void cfgSubtractWide(FaceT* u, FaceT* v, FaceT* w, const double* p, int nx, int ny, int nz, int doWalls);
-__global__ void cfgTopFaces(FaceT* v, const float* p, int nx, int ny, int nz);
-__global__ void mgCycleEnd(SorGate* gate, const double* partialSq, const float* partialMax, int partials, float tolerance, int gated,
-                           int maxCycles, cudaGraphConditionalHandle loop);
+constexpr int kMgMaxLevels = 10;
+constexpr int kMgMaxScenes = 128;     // scenes of one batched solve
+constexpr int kMgTailCells = 6144;    // the tail starts at the first level with at most this many cells
+constexpr size_t kMgTailSmemMax = 160 * 1024;  // larger tails work in global memory
+constexpr int kMgThreads = 1024;      // threads of a CTA of mgSolve (one CTA per SM)
+constexpr int kMgChunkRows = 16;      // level-0 rows per residual chunk
 constexpr int kMgCoarsestSweeps = 32;
 constexpr int kMgHardCycleCap = 1000;  // fireCudaSetPressureMultigrid accepts at most this many cycles
+constexpr unsigned kMgMaxPolls = 1u << 26;
+constexpr unsigned kMgStatusFlag = 0x80000000u;  // host status word: a multigrid barrier wait ran out (low bits: phase)
+// One scene of a solve.  Level l's p and rhs: level 0 is the increment and
+// the divergence array; levels >= 1 are the coarse corrections.
+struct MgScene {
+    MgLevel lv[kMgMaxLevels];
+    float* p[kMgMaxLevels];
+    float* rhs[kMgMaxLevels];
+    float* pressure;   // += the increment at the end of the solve
+    SorGate* gate;     // zeroed before the launch
+    double* chunkSq;   // per residual chunk (kMgChunkRows level-0 rows)
+    float* chunkMax;
+    int levels;        // number of levels
+    int tail;          // first level solved by one CTA (the tail)
+    int tailInGlobal;  // 1: the tail works in the levels' global buffers (too large for shared memory)
+};
+// The work lists of a solve: prefix sums over the scenes of the rows of each
+// grid level (levels l < tail of the scene; 0 rows otherwise), of the coarse
+// rows each restriction writes, of the residual chunks and of all level-0 rows.
+struct MgPlan {
+    int scenes;
+    int gridLevels;  // max over the scenes of tail
+    int maxCycles, pre, post, gated;
+    float tolerance;
+    int rows[kMgMaxLevels][kMgMaxScenes + 1];
+    int coarseRows[kMgMaxLevels][kMgMaxScenes + 1];
+    int chunks[kMgMaxScenes + 1];
+    int allRows[kMgMaxScenes + 1];
+};
+// Grid barrier state of mgSolve (zeroed before each launch).
+struct MgSync {
+    unsigned count, generation, failed, pad;
+};
+__global__ void mgSolve(const MgScene* scenes, const MgPlan* plan, MgSync* sync, unsigned* hostStatus, unsigned long long waitNs);
+__global__ void cfgPrepareIncrement(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, const float* pressure, float* rhs, int nx,
+                                    int ny, int nz);
+__global__ void cfgSubtractIncrement(FaceT* u, FaceT* v, FaceT* w, const float* delta, int nx, int ny, int nz, int doWalls);
+__global__ void cfgTopFaces(FaceT* v, const float* p, int nx, int ny, int nz);
+
+// ---------------------------------------------------------------------------
+// Batched config physics (fire_config.cu, host side fire_batch.cu): one launch
+// per stage over every scene of a batch.  A block belongs to one scene; its
+// threads take consecutive elements of one index space of that scene (x
+// fastest): cells, faces ((nx+1)(ny+1)(nz+1)), half-resolution light cells
+// or pixels.  The per-element work is the single-scene kernels' own body, so
+// a scene gives the same bits alone or in a batch.
+enum BatchSpace { kBatchCells = 0, kBatchFaces = 1, kBatchLight = 2, kBatchPixels = 3, kBatchSpaces = 4 };
+constexpr int kBatchThreads = 128;
+constexpr int kBatchMaxScenes = kMgMaxScenes;
+struct BatchScene {
+    ConfigParams c;        // this step's parameters (c.step: the emitters' jitter counter)
+    Velocity vel;          // faces at the start of the step
+    FaceT* adv[3];         // advected faces
+    const Rec4* aIn;       // record a at the start of the step
+    Rec4* aOut;            // the advanced record a
+    float4* vort;
+    float4* force;
+    const float4* noise;   // curl-noise field (null when its amplitude is 0)
+    FaceT* forced[3];      // faces after the forces
+    FaceT* proj[3];        // faces of the projection (the previous pressure's gradient subtracted)
+    float* pressure;
+    float* divergence;
+    float* delta;          // the multigrid's level-0 increment
+    float* transmittance;
+    float4* hdr;
+    void* slot;            // the scene's HDR output buffer (null: keep the frame in hdr)
+    size_t slotPitch;
+    int slotFormat;        // FireHdrFormat
+    int count[kBatchSpaces];  // elements of each index space
+};
+struct BatchPlan {
+    int scenes;
+    int start[kBatchSpaces][kBatchMaxScenes + 1];  // prefix sums of the blocks of each scene (0 for a scene that does not render)
+};
+__global__ void batchAdvectVelocity(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchAdvectScalars(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchVorticity(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchCellForce(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchApplyForces(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchPrepareIncrement(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchSubtractIncrement(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchTransmittance(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchRaymarch(const BatchScene* scenes, const BatchPlan* plan);
+__global__ void batchPackHdr(const BatchScene* scenes, const BatchPlan* plan);
 
 }  // namespace firesim

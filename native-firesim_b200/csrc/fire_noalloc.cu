@@ -10,6 +10,7 @@
 // caller owns, and keeps the increments in the fixed array below instead.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -26,8 +27,12 @@ static __device__ __align__(256) float4 g_forceScratch[kNoAllocMaxCells];
 // Device address of g_forceScratch per device ordinal.  In host code the
 // symbol is only a host-side stand-in, so the address is resolved with
 // cudaGetSymbolAddress on each device, once, while that device is current.
+// Several host threads may resolve it at once; they store the same value, and
+// the atomics keep that free of data races.  A cudaDeviceReset (or a reset of
+// the primary context) unloads the module, so the cached address is stale
+// after one: a process that resets a device must reload the library.
 constexpr int kMaxDevices = 64;
-float4* g_scratchAddress[kMaxDevices] = {};
+std::atomic<float4*> g_scratchAddress[kMaxDevices] = {};
 
 }  // namespace
 
@@ -56,6 +61,10 @@ extern "C" bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float 
     if (nx < 2 || ny < 2 || nz < 2) {
         return fail("fireCudaForceProjectNoAlloc: grid dimensions must be at least 2.");
     }
+    // The launch grid is (ceil(nx / block), ny, nz): y and z are capped at 65535 blocks.
+    if (ny > 65535 || nz > 65535) {
+        return fail("fireCudaForceProjectNoAlloc: ny and nz must be at most 65535.");
+    }
     const long long cells = static_cast<long long>(nx) * ny * nz;
     if (cells > kNoAllocMaxCells) {
         char buf[200];
@@ -68,17 +77,25 @@ extern "C" bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float 
         (reinterpret_cast<uintptr_t>(recordsC) & 7) != 0) {
         return fail("fireCudaForceProjectNoAlloc: records A/B must be 16-byte aligned and records C 8-byte aligned.");
     }
+    // An error left pending by the caller's own earlier work is not this call's
+    // to clear or to report as its own: refuse to launch and leave it in place.
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        return fail(std::string("fireCudaForceProjectNoAlloc: an earlier CUDA error is pending (") + cudaGetErrorString(e) +
+                    "); nothing was launched.");
+    }
     int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
+    e = cudaGetDevice(&device);
     if (e != cudaSuccess) return fail(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (device < 0 || device >= kMaxDevices) return fail("fireCudaForceProjectNoAlloc: device ordinal out of range.");
-    if (g_scratchAddress[device] == nullptr) {
+    float4* scratch = g_scratchAddress[device].load(std::memory_order_acquire);
+    if (scratch == nullptr) {
         void* addr = nullptr;
         e = cudaGetSymbolAddress(&addr, g_forceScratch);
         if (e != cudaSuccess) return fail(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratchAddress[device] = static_cast<float4*>(addr);
+        scratch = static_cast<float4*>(addr);
+        g_scratchAddress[device].store(scratch, std::memory_order_release);
     }
-    float4* scratch = g_scratchAddress[device];
 
     // The settings clamps of a step; Scene allocates nothing until init().
     firesim::Scene dims;
@@ -99,6 +116,8 @@ extern "C" bool fireCudaForceProjectNoAlloc(const FireSettings* settings, float 
     // No lattice storage here: every curl-noise corner is hashed in place.
     const firesim::HashLattice2 noLattice{};
     firesim::forceContributions<<<grid, bx, 0, s>>>(scratch, in, vel, p, noLattice, noLattice);
+    e = cudaGetLastError();  // nothing was pending on entry, so an error here is this launch's
+    if (e != cudaSuccess) return fail(std::string("force pass launch: ") + cudaGetErrorString(e));
     firesim::forceProjectSetup<<<grid, bx, 0, s>>>(reinterpret_cast<firesim::FaceT*>(uOut), reinterpret_cast<firesim::FaceT*>(vOut),
                                                    reinterpret_cast<firesim::FaceT*>(wOut), divergence, pressure, scratch, vel, p);
     e = cudaGetLastError();

@@ -937,16 +937,7 @@ __global__ void __launch_bounds__(256) packHdr(void* __restrict__ dst, size_t pi
     if (x >= p.frameW || y >= p.frameH) {
         return;
     }
-    const float4 r = __ldg(hdr + y * p.frameW + x);
-    char* row = static_cast<char*>(dst) + static_cast<size_t>(y) * pitchBytes;
-    if (halfFormat) {
-        const __half2 rg = __floats2half2_rn(fmaxf(0.0f, r.x), fmaxf(0.0f, r.y));
-        const __half2 ba = __floats2half2_rn(fmaxf(0.0f, r.z), 1.0f);
-        reinterpret_cast<__half2*>(row)[2 * x] = rg;
-        reinterpret_cast<__half2*>(row)[2 * x + 1] = ba;
-    } else {
-        reinterpret_cast<float4*>(row)[x] = make_float4(r.x, r.y, r.z, 1.0f);
-    }
+    packHdrPixel(dst, pitchBytes, halfFormat, __ldg(hdr + y * p.frameW + x), x, y);
 }
 
 }  // namespace firesim

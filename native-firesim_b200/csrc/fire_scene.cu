@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -44,7 +45,23 @@ bool Scene::check(const char* label, cudaError_t e, std::string& err) {
     return true;
 }
 
+// Host-side fault injection of the scenes' device allocations
+// (fireCudaSetAllocationFault): -1 = off; n >= 0 = n more allocations
+// succeed, then every one fails as cudaMalloc does when memory runs out.
+std::atomic<long long> g_allocationsBeforeFault{-1};
+
+void setAllocationFault(long long succeedBeforeFailing) { g_allocationsBeforeFault.store(succeedBeforeFailing); }
+
 bool Scene::alloc(void** p, size_t bytes, const char* label, std::string& err) {
+    long long left = g_allocationsBeforeFault.load();
+    while (left >= 0) {
+        if (left == 0) {
+            *p = nullptr;
+            err = std::string(label) + ": " + cudaGetErrorString(cudaErrorMemoryAllocation) + " (injected)";
+            return false;
+        }
+        if (g_allocationsBeforeFault.compare_exchange_weak(left, left - 1)) break;
+    }
     if (!check(label, cudaMalloc(p, bytes), err)) {
         *p = nullptr;
         return false;
@@ -60,19 +77,25 @@ void Scene::release() {
     if (stream != nullptr) {
         cudaStreamSynchronize(stream);
     }
+    if (ownStream_ != nullptr && ownStream_ != stream) {
+        cudaStreamSynchronize(ownStream_);
+    }
     if (sorExec_ != nullptr) {
         cudaGraphExecDestroy(sorExec_);
         sorExec_ = nullptr;
     }
-    if (mgExec_ != nullptr) {
-        cudaGraphExecDestroy(mgExec_);
-        mgExec_ = nullptr;
+    mgSolver_.release();
+    mgDeltaValid_ = false;
+    for (float* b : mgP_) {
+        if (b != nullptr) cudaFree(b);
     }
-    if (mgP0_ != nullptr) cudaFree(mgP0_);
-    mgP0_ = nullptr;
-    mgP0Valid_ = false;
-    for (float* b : mgP_) cudaFree(b);
-    for (float* b : mgRhs_) cudaFree(b);
+    for (float* b : mgRhs_) {
+        if (b != nullptr) cudaFree(b);
+    }
+    if (mgChunkSq_ != nullptr) cudaFree(mgChunkSq_);
+    if (mgChunkMax_ != nullptr) cudaFree(mgChunkMax_);
+    mgChunkSq_ = nullptr;
+    mgChunkMax_ = nullptr;
     mgP_.clear();
     mgRhs_.clear();
     mgLevels_.clear();
@@ -108,7 +131,8 @@ void Scene::release() {
         if (e != nullptr) cudaEventDestroy(e);
         e = nullptr;
     }
-    if (stream != nullptr) cudaStreamDestroy(stream);
+    if (ownStream_ != nullptr) cudaStreamDestroy(ownStream_);
+    ownStream_ = nullptr;
     stream = nullptr;
     std::memset(sa_, 0, sizeof(sa_));
     std::memset(sb_, 0, sizeof(sb_));
@@ -151,7 +175,8 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
     lightCells_ = static_cast<size_t>(lnx) * lny * lnz;
     pixels_ = static_cast<size_t>(fw) * fh;
     if (!check("cudaSetDevice", cudaSetDevice(device), err)) return false;
-    if (!check("cudaStreamCreate", cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), err)) return false;
+    if (!check("cudaStreamCreate", cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), err)) return false;
+    stream = ownStream_;
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) {
         ok = alloc(reinterpret_cast<void**>(&sa_[i]), cells_ * sizeof(Rec4), "cudaMalloc scalars a", err) &&
@@ -576,172 +601,217 @@ bool Scene::setPressureMultigrid(int maxCycles, int preSmooth, int postSmooth, s
     return true;
 }
 
-// The multigrid solve (fire_mg.cu), warm-started from the previous solve's
-// level-0 pressure, as one CUDA graph per (cycles, smoothing, tolerance): a
-// memset of the gate, then a conditional WHILE node whose body
-// is one V-cycle, the level-0 residual partials (with a tolerance) and
-// mgCycleEnd, which clears the loop condition when the solve has converged or
-// run maxCycles cycles -- a converged solve launches nothing more.
-bool Scene::runMultigrid(std::string& err) {
+// ---------------------------------------------------------------------------
+// MgSolver: the host side of mgSolve.
+
+MgSolver::~MgSolver() { release(); }
+
+void MgSolver::release() {
+    if (uploaded_ != nullptr) cudaEventSynchronize(uploaded_);
+    if (dScenes_ != nullptr) cudaFree(dScenes_);
+    if (dPlan_ != nullptr) cudaFree(dPlan_);
+    if (dSync_ != nullptr) cudaFree(dSync_);
+    if (hScenes_ != nullptr) cudaFreeHost(hScenes_);
+    if (hPlan_ != nullptr) cudaFreeHost(hPlan_);
+    if (uploaded_ != nullptr) cudaEventDestroy(uploaded_);
+    dScenes_ = nullptr;
+    dPlan_ = nullptr;
+    dSync_ = nullptr;
+    hScenes_ = nullptr;
+    hPlan_ = nullptr;
+    uploaded_ = nullptr;
+    planned_ = false;
+    grid_ = 0;
+    smem_ = 0;
+}
+
+// The work lists and descriptors are built on the host and uploaded on
+// `stream` from pinned staging, so a plan (for example when a serving batch's
+// scenes change) neither allocates nor synchronises after the first one; the
+// next plan waits only for this plan's upload to have run.
+bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycles, int pre, int post, double tolerance,
+                    cudaStream_t stream, std::string& err) {
+    const int n = static_cast<int>(scenes.size());
+    if (n < 1 || n > kMgMaxScenes) {
+        err = "multigrid: a solve takes 1 to " + std::to_string(kMgMaxScenes) + " scenes";
+        return false;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess && dScenes_ == nullptr) {
+        int sms = 0, coop = 0;
+        e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e == cudaSuccess && !coop) {
+            err = "multigrid: the device cannot run the persistent solve (no cooperative launch)";
+            return false;
+        }
+        sms_ = sms;
+        if (e == cudaSuccess) {
+            e = cudaFuncSetAttribute(mgSolve, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMgTailSmemMax));
+        }
+        if (e == cudaSuccess) e = cudaMalloc(&dScenes_, kMgMaxScenes * sizeof(MgScene));
+        if (e == cudaSuccess) e = cudaMalloc(&dPlan_, sizeof(MgPlan));
+        if (e == cudaSuccess) e = cudaMalloc(&dSync_, sizeof(MgSync));
+        if (e == cudaSuccess) e = cudaMemset(dSync_, 0, sizeof(MgSync));
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&hScenes_), kMgMaxScenes * sizeof(MgScene), cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&hPlan_), sizeof(MgPlan), cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&uploaded_, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            err = std::string("multigrid plan: ") + cudaGetErrorString(e);
+            release();
+            return false;
+        }
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(uploaded_);
+    if (e != cudaSuccess) {
+        err = std::string("multigrid plan: ") + cudaGetErrorString(e);
+        return false;
+    }
+    MgPlan& plan = *hPlan_;
+    std::memset(&plan, 0, sizeof(MgPlan));
+    plan.scenes = n;
+    plan.maxCycles = maxCycles;
+    plan.pre = pre;
+    plan.post = post;
+    plan.gated = tolerance > 0.0 ? 1 : 0;
+    plan.tolerance = static_cast<float>(tolerance);
+    size_t smem = 0;
+    for (int s = 0; s < n; ++s) {
+        const MgScene& S = scenes[s];
+        plan.gridLevels = std::max(plan.gridLevels, S.tail);
+        size_t tailFloats = 0;
+        for (int l = S.tail; l < S.levels; ++l) tailFloats += 2 * static_cast<size_t>(S.lv[l].nx) * S.lv[l].ny * S.lv[l].nz;
+        if (!S.tailInGlobal) smem = std::max(smem, tailFloats * sizeof(float));
+    }
+    for (int l = 0; l < kMgMaxLevels; ++l) {
+        for (int s = 0; s < n; ++s) {
+            const MgScene& S = scenes[s];
+            const bool grid = l < S.tail;
+            plan.rows[l][s + 1] = plan.rows[l][s] + (grid ? S.lv[l].ny * S.lv[l].nz : 0);
+            plan.coarseRows[l][s + 1] = plan.coarseRows[l][s] + (grid ? S.lv[l + 1].ny * S.lv[l + 1].nz : 0);
+        }
+    }
+    for (int s = 0; s < n; ++s) {
+        const int rows0 = scenes[s].lv[0].ny * scenes[s].lv[0].nz;
+        plan.chunks[s + 1] = plan.chunks[s] + (rows0 + kMgChunkRows - 1) / kMgChunkRows;
+        plan.allRows[s + 1] = plan.allRows[s] + rows0;
+    }
+    std::memcpy(hScenes_, scenes.data(), n * sizeof(MgScene));
+    int perSm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, mgSolve, kMgThreads, smem);
+    if (e == cudaSuccess && perSm < 1) {
+        err = "multigrid: no CTA of the persistent solve fits an SM";
+        return false;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dScenes_, hScenes_, n * sizeof(MgScene), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dPlan_, hPlan_, sizeof(MgPlan), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(uploaded_, stream);
+    if (e != cudaSuccess) {
+        err = std::string("multigrid plan: ") + cudaGetErrorString(e);
+        return false;
+    }
+    grid_ = perSm * sms_;
+    smem_ = smem;
+    planned_ = true;
+    return true;
+}
+
+bool MgSolver::launch(cudaStream_t stream, unsigned* hostStatus, std::string& err) {
+    if (!planned()) {
+        err = "multigrid: solve launched before it was planned";
+        return false;
+    }
+    cudaError_t e = cudaMemsetAsync(dSync_, 0, sizeof(MgSync), stream);
+    if (e == cudaSuccess) {
+        void* args[] = {&dScenes_, &dPlan_, &dSync_, &hostStatus, &waitNs_};
+        e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(mgSolve), dim3(grid_), dim3(kMgThreads), args, smem_, stream);
+    }
+    if (e != cudaSuccess) {
+        err = std::string("multigrid launch: ") + cudaGetErrorString(e);
+        return false;
+    }
+    return true;
+}
+
+// The levels and buffers of this scene's multigrid (allocated once) and its
+// descriptor: level 0 is the grid with weights (1, 1, 1); each next level
+// halves every axis whose extent is even and at least 4; the shared-memory
+// tail starts at the first level of at most kMgTailCells cells.
+bool Scene::multigridScene(MgScene& out, std::string& err) {
     if (mgLevels_.empty()) {
         auto withWeights = [](MgLevel L) {
             L.diag = 2.0f * (L.wx + L.wy + L.wz);
             L.invDiag = 1.0f / L.diag;
             return L;
         };
-        MgLevel L = withWeights(MgLevel{nx, ny, nz, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0, 0, 0, 1});
+        MgLevel L = withWeights(MgLevel{nx, ny, nz, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0, 0, 0});
         mgLevels_.push_back(L);
-        if (!alloc(reinterpret_cast<void**>(&mgP0_), cells_ * sizeof(double), "cudaMalloc multigrid level-0 pressure", err)) return false;
-        while (mgLevels_.size() < 10) {
+        while (static_cast<int>(mgLevels_.size()) < kMgMaxLevels) {
             const int cx = L.nx % 2 == 0 && L.nx >= 4, cy = L.ny % 2 == 0 && L.ny >= 4, cz = L.nz % 2 == 0 && L.nz >= 4;
             if (!cx && !cy && !cz) break;
             L = withWeights(MgLevel{cx ? L.nx / 2 : L.nx, cy ? L.ny / 2 : L.ny, cz ? L.nz / 2 : L.nz, cx ? L.wx * 0.25f : L.wx,
-                                    cy ? L.wy * 0.25f : L.wy, cz ? L.wz * 0.25f : L.wz, 0.0f, 0.0f, cx, cy, cz, 0});
-            const size_t n = static_cast<size_t>(L.nx) * L.ny * L.nz;
-            float* pl = nullptr;
-            float* rl = nullptr;
-            if (!alloc(reinterpret_cast<void**>(&pl), n * sizeof(float), "cudaMalloc multigrid level", err)) return false;
-            mgP_.push_back(pl);
-            if (!alloc(reinterpret_cast<void**>(&rl), n * sizeof(float), "cudaMalloc multigrid level", err)) return false;
-            mgRhs_.push_back(rl);
-            if (!check("clear multigrid level", cudaMemsetAsync(pl, 0, n * sizeof(float), stream), err) ||
-                !check("clear multigrid level", cudaMemsetAsync(rl, 0, n * sizeof(float), stream), err)) {
-                return false;
-            }
+                                    cy ? L.wy * 0.25f : L.wy, cz ? L.wz * 0.25f : L.wz, 0.0f, 0.0f, cx, cy, cz});
             mgLevels_.push_back(L);
         }
+        mgP_.assign(mgLevels_.size(), nullptr);
+        mgRhs_.assign(mgLevels_.size(), nullptr);
+        for (size_t l = 0; l < mgLevels_.size(); ++l) {
+            const size_t n = static_cast<size_t>(mgLevels_[l].nx) * mgLevels_[l].ny * mgLevels_[l].nz;
+            if (!alloc(reinterpret_cast<void**>(&mgP_[l]), n * sizeof(float), "cudaMalloc multigrid level", err) ||
+                !check("clear multigrid level", cudaMemsetAsync(mgP_[l], 0, n * sizeof(float), stream), err)) {
+                return false;
+            }
+            if (l > 0 && (!alloc(reinterpret_cast<void**>(&mgRhs_[l]), n * sizeof(float), "cudaMalloc multigrid level", err) ||
+                          !check("clear multigrid level", cudaMemsetAsync(mgRhs_[l], 0, n * sizeof(float), stream), err))) {
+                return false;
+            }
+        }
+        const size_t chunks = (static_cast<size_t>(ny) * nz + kMgChunkRows - 1) / kMgChunkRows;
+        if (!alloc(reinterpret_cast<void**>(&mgChunkSq_), chunks * sizeof(double), "cudaMalloc multigrid residual chunks", err) ||
+            !alloc(reinterpret_cast<void**>(&mgChunkMax_), chunks * sizeof(float), "cudaMalloc multigrid residual chunks", err)) {
+            return false;
+        }
     }
-    const bool gated = pressureTolerance_ > 0.0;
-    const double tolKey = gated ? pressureTolerance_ : 0.0;
-    if (mgExec_ == nullptr || mgKeyCycles_ != mgCycles_ || mgKeyPre_ != mgPre_ || mgKeyPost_ != mgPost_ || mgKeyTol_ != tolKey) {
-        if (mgExec_ != nullptr) {
-            cudaGraphExecDestroy(mgExec_);
-            mgExec_ = nullptr;
+    MgScene S{};
+    S.levels = static_cast<int>(mgLevels_.size());
+    S.tail = S.levels - 1;
+    for (int l = 0; l < S.levels; ++l) {
+        S.lv[l] = mgLevels_[l];
+        S.p[l] = mgP_[l];
+        S.rhs[l] = l == 0 ? divergence_ : mgRhs_[l];
+        if (S.tail == S.levels - 1 && static_cast<long long>(mgLevels_[l].nx) * mgLevels_[l].ny * mgLevels_[l].nz <= kMgTailCells) {
+            S.tail = l;
         }
-        const int levels = static_cast<int>(mgLevels_.size());
-        // Level 0's pressure is the double mgP0_; the coarser levels' are float.
-        auto P = [&](int l) { return mgP_[l - 1]; };
-        auto R = [&](int l) { return l == 0 ? divergence_ : mgRhs_[l - 1]; };
-        int count = 0;
-        auto rowBlock = [](int rowThreadCount, int ny) { return dim3(rowThreadCount, std::min(kMgRowBlockThreads / rowThreadCount, ny), 1); };
-        auto smooth = [&](int l, int sweeps) {
-            const MgLevel& L = mgLevels_[l];
-            const int half = (L.nx + 1) / 2;
-            const dim3 bx = rowBlock(rowThreads(half), L.ny);
-            const dim3 g((half + bx.x - 1) / bx.x, (L.ny + bx.y - 1) / bx.y, L.nz);
-            for (int k = 0; k < sweeps; ++k) {
-                for (int colour = 0; colour < 2; ++colour) {
-                    if (l == 0) {
-                        mgSmoothD<<<g, bx, 0, stream>>>(mgP0_, R(0), L, colour, nullptr);
-                    } else {
-                        mgSmoothF<<<g, bx, 0, stream>>>(P(l), R(l), L, colour, nullptr);
-                    }
-                    ++count;
-                }
-            }
-        };
-        cudaGraph_t graph = nullptr;
-        if (!check("multigrid graph create", cudaGraphCreate(&graph, 0), err)) return false;
-        auto failGraph = [&](const char* label, cudaError_t e) {
-            cudaGraphDestroy(graph);
-            return check(label, e, err);
-        };
-        cudaGraphNode_t reset = nullptr;
-        cudaMemsetParams ms{};
-        ms.dst = sorGate_;
-        ms.value = 0;
-        ms.elementSize = 4;
-        ms.width = sizeof(SorGate) / 4;
-        ms.height = 1;
-        cudaError_t e = cudaGraphAddMemsetNode(&reset, graph, nullptr, 0, &ms);
-        if (e != cudaSuccess) return failGraph("multigrid gate reset node", e);
-        cudaGraphConditionalHandle loop{};
-        e = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault);
-        if (e != cudaSuccess) return failGraph("multigrid loop handle", e);
-        cudaGraphNodeParams cp{};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = loop;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t condNode = nullptr;
-        e = cudaGraphAddNode(&condNode, graph, &reset, 1, &cp);
-        if (e != cudaSuccess) return failGraph("multigrid loop node", e);
-        cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
-        e = cudaStreamBeginCaptureToGraph(stream, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return failGraph("multigrid body capture begin", e);
-        for (int l = 0; l + 1 < levels; ++l) {
-            smooth(l, mgPre_);
-            const MgLevel& F = mgLevels_[l];
-            const MgLevel& C = mgLevels_[l + 1];
-            const int bx = rowThreads(C.nx);
-            const dim3 rg((C.nx + bx - 1) / bx, C.ny, C.nz);
-            if (l == 0) {
-                mgRestrictD<<<rg, bx, 0, stream>>>(R(1), P(1), mgP0_, R(0), F, C, nullptr);
-            } else {
-                mgRestrictF<<<rg, bx, 0, stream>>>(R(l + 1), P(l + 1), P(l), R(l), F, C, nullptr);
-            }
-            ++count;
-        }
-        if (levels == 1) {
-            mgCoarsestD<<<1, 256, 0, stream>>>(mgP0_, R(0), mgLevels_[0], kMgCoarsestSweeps, nullptr);
-        } else {
-            mgCoarsestF<<<1, 256, 0, stream>>>(P(levels - 1), R(levels - 1), mgLevels_[levels - 1], kMgCoarsestSweeps, nullptr);
-        }
-        ++count;
-        for (int l = levels - 2; l >= 0; --l) {
-            const MgLevel& F = mgLevels_[l];
-            const MgLevel& C = mgLevels_[l + 1];
-            const dim3 bx = rowBlock(rowThreads(F.nx), F.ny);
-            const dim3 pg((F.nx + bx.x - 1) / bx.x, (F.ny + bx.y - 1) / bx.y, F.nz);
-            if (l == 0) {
-                mgProlongD<<<pg, bx, 0, stream>>>(mgP0_, P(1), F, C, nullptr);
-            } else {
-                mgProlongF<<<pg, bx, 0, stream>>>(P(l), P(l + 1), F, C, nullptr);
-            }
-            ++count;
-            smooth(l, mgPost_);
-        }
-        if (gated) {
-            mgResidualPartialsD<<<kResidualBlocks, kResidualThreads, 0, stream>>>(mgP0_, divergence_, mgLevels_[0], sorGate_,
-                                                                                       residualSq_, residualMax_);
-            ++count;
-        }
-        mgCycleEnd<<<1, 32, 0, stream>>>(sorGate_, residualSq_, residualMax_, kResidualBlocks, static_cast<float>(pressureTolerance_),
-                                         gated ? 1 : 0, mgCycles_, loop);
-        ++count;
-        cudaError_t launchErr = cudaGetLastError();
-        cudaGraph_t captured = nullptr;
-        cudaError_t endErr = cudaStreamEndCapture(stream, &captured);
-        if (launchErr != cudaSuccess) return failGraph("multigrid body launch", launchErr);
-        if (endErr != cudaSuccess) return failGraph("multigrid body capture end", endErr);
-        // After the loop: the float pressure field from the double level-0 pressure.
-        e = cudaStreamBeginCaptureToGraph(stream, graph, &condNode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return failGraph("multigrid store capture begin", e);
-        mgStoreFloat<<<kResidualBlocks, 256, 0, stream>>>(pressure_, mgP0_, static_cast<int>(cells_));
-        launchErr = cudaGetLastError();
-        endErr = cudaStreamEndCapture(stream, &captured);
-        if (launchErr != cudaSuccess) return failGraph("multigrid store launch", launchErr);
-        if (endErr != cudaSuccess) return failGraph("multigrid store capture end", endErr);
-        const cudaError_t instErr = cudaGraphInstantiate(&mgExec_, graph, 0);
-        cudaGraphDestroy(graph);
-        if (!check("multigrid graph instantiate", instErr, err)) return false;
+    }
+    size_t tailBytes = 0;
+    for (int l = S.tail; l < S.levels; ++l) tailBytes += 2 * sizeof(float) * mgLevels_[l].nx * mgLevels_[l].ny * mgLevels_[l].nz;
+    S.tailInGlobal = tailBytes > kMgTailSmemMax ? 1 : 0;
+    S.pressure = pressure_;
+    S.gate = sorGate_;
+    S.chunkSq = mgChunkSq_;
+    S.chunkMax = mgChunkMax_;
+    out = S;
+    return true;
+}
+
+// The multigrid solve of this scene alone: one persistent launch (fire_mg.cu)
+// for the increment, from zero; at its end pressure += increment.
+bool Scene::runMultigrid(std::string& err) {
+    const double tolKey = pressureTolerance_ > 0.0 ? pressureTolerance_ : 0.0;
+    if (!mgSolver_.planned() || mgKeyCycles_ != mgCycles_ || mgKeyPre_ != mgPre_ || mgKeyPost_ != mgPost_ || mgKeyTol_ != tolKey) {
+        MgScene S;
+        if (!multigridScene(S, err)) return false;
+        if (!mgSolver_.plan(device, std::vector<MgScene>{S}, mgCycles_, mgPre_, mgPost_, tolKey, stream, err)) return false;
         mgKeyCycles_ = mgCycles_;
         mgKeyPre_ = mgPre_;
         mgKeyPost_ = mgPost_;
         mgKeyTol_ = tolKey;
-        mgGraphLaunches_ = count;  // per V-cycle
     }
-    // Warm start: the solve starts from the previous solve's double pressure;
-    // after a reset or a write of the pressure field, from zero.
-    if (!mgP0Valid_ && !check("clear multigrid level-0 pressure", cudaMemsetAsync(mgP0_, 0, cells_ * sizeof(double), stream), err)) {
-        return false;
-    }
-    // The launch count cannot know how many cycles will run; it counts one V-cycle's kernels.
-    launches_ += static_cast<unsigned long long>(mgGraphLaunches_) + 1;
+    launches_ += 1;
     lastSolveGated_ = true;
     lastPressurePath_ = 3;
-    mgP0Valid_ = true;
-    return check("multigrid graph launch", cudaGraphLaunch(mgExec_, stream), err);
+    mgDeltaValid_ = true;
+    return mgSolver_.launch(stream, sorHostStatus_, err);
 }
 
 bool Scene::runMetrics(const FrameParams& p, std::string& err) {
@@ -1272,7 +1342,7 @@ bool Scene::getField(int field, void* host, size_t bytes, std::string& err) {
 }
 
 bool Scene::setField(int field, const void* host, size_t bytes, std::string& err) {
-    if (field == FIRE_FIELD_PRESSURE) mgP0Valid_ = false;  // the field, not an older solve, is the pressure now
+    if (field == FIRE_FIELD_PRESSURE) mgDeltaValid_ = false;  // the field, not an older solve, is the pressure now
     FaceT* velNow[3] = {vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_]};
     FieldView v;
     if (field == FIRE_FIELD_CONFIG_TRANSMITTANCE) {
@@ -1353,7 +1423,11 @@ bool Scene::checkSolverStatus(std::string& err) {
     const unsigned st = *reinterpret_cast<volatile unsigned*>(sorHostStatus_);
     if (st == 0) return true;
     *sorHostStatus_ = 0;
-    err = "resident SOR: brick " + std::to_string(st - 1) + " timed out waiting for a neighbour's half sweep";
+    if (st & kMgStatusFlag) {
+        err = "multigrid solve: a grid barrier wait timed out in phase " + std::to_string(st & ~kMgStatusFlag);
+    } else {
+        err = "resident SOR: brick " + std::to_string(st - 1) + " timed out waiting for a neighbour's half sweep";
+    }
     return false;
 }
 
@@ -1574,6 +1648,95 @@ bool Scene::ensureConfigBuffers(std::string& err) {
            check("clear config transmittance", cudaMemsetAsync(cfgLight_, 0, lightCells * sizeof(float), stream), err);
 }
 
+// One step of this scene inside a FireBatch: the frame's bookkeeping (clocks,
+// reset, frame index), the buffers the batched kernels need, and the
+// descriptor of this step's buffers; then the host state advances as the
+// step will leave it (record a and the faces swap once, the jitter counter
+// advances).  Only for the config physics with the incremental multigrid
+// projection; the batch queues the kernels.
+bool Scene::batchStep(BatchScene& d, const FireSettings& s, bool render, std::string& err) {
+    if (!incrementalProjection()) {
+        err = "a batched scene needs the config physics with p = 0 on the top face and the multigrid solve";
+        return false;
+    }
+    if (render && slots_[activeSlot_].ptr == nullptr) {
+        err = "HDR output buffer slot is not registered.";
+        return false;
+    }
+    const float stepDt = std::max(0.001f, std::min(s.dt, 1.0f / 30.0f));
+    renderTime += stepDt;
+    simTime += stepDt;
+    FrameParams p = paramsFrom(s, simTime);
+    if (s.reset != 0) {
+        if (!runStages(kReset, kReset, p, err)) return false;
+        simTime = 0.0f;
+        renderTime = 0.0f;
+        frameIndex = 0;
+    }
+    if (!ensureConfigBuffers(err)) return false;
+    MgScene mg;
+    if (!multigridScene(mg, err)) return false;
+    ConfigParams c = configParams();
+    if (c.noiseAmp != 0.0f) {
+        const float key[3] = {c.noiseAmp, c.invPeriod, static_cast<float>(c.noiseSeed)};
+        if (!cfgNoiseValid_ || std::memcmp(key, cfgNoiseKey_, sizeof(key)) != 0 || cfgNoiseSeed_ != c.noiseSeed) {
+            if (cfgNoise_ == nullptr && !alloc(reinterpret_cast<void**>(&cfgNoise_), cells_ * sizeof(float4), "cudaMalloc config noise field", err)) {
+                return false;
+            }
+            const int bx = rowThreads(nx);
+            cfgNoiseField<<<cellGrid(bx, nx, ny, nz), bx, 0, stream>>>(cfgNoise_, c); ++launches_;
+            if (!check("config noise field launch", cudaGetLastError(), err)) return false;
+            std::memcpy(cfgNoiseKey_, key, sizeof(key));
+            cfgNoiseSeed_ = c.noiseSeed;
+            cfgNoiseValid_ = true;
+        }
+    }
+    BatchScene b{};
+    b.c = c;
+    b.vel = velocity();
+    for (int f = 0; f < 3; ++f) {
+        b.adv[f] = vel_[f][1 - vcur_];     // advection: cur -> other
+        b.forced[f] = vel_[f][vcur_];      // forces: other -> cur
+        b.proj[f] = vel_[f][1 - vcur_];    // prepared faces: cur -> other, then projected in place
+    }
+    b.aIn = sa_[cur_];
+    b.aOut = sa_[1 - cur_];
+    b.vort = cfgVort_;
+    b.force = contrib_;
+    b.noise = c.noiseAmp != 0.0f ? cfgNoise_ : nullptr;
+    b.pressure = pressure_;
+    b.divergence = divergence_;
+    b.delta = mgP_[0];
+    b.transmittance = cfgLight_;
+    b.hdr = hdr_;
+    const HdrSlot& slot = slots_[activeSlot_];
+    b.slot = slot.ptr;
+    b.slotPitch = slot.pitchBytes;
+    b.slotFormat = slot.format;
+    b.count[kBatchCells] = static_cast<int>(cells_);
+    b.count[kBatchFaces] = (nx + 1) * (ny + 1) * (nz + 1);
+    b.count[kBatchLight] = render ? cfgLx_ * cfgLy_ * cfgLz_ : 0;
+    b.count[kBatchPixels] = render ? frameW * frameH : 0;
+    d = b;
+    cur_ = 1 - cur_;
+    vcur_ = 1 - vcur_;
+    ++cfgStep_;
+    mgDeltaValid_ = true;
+    lastSolveGated_ = true;
+    lastPressurePath_ = 3;
+    ++frameIndex;
+    return true;
+}
+
+// Every buffer a batched config-physics step can need (config fields,
+// multigrid levels, the curl-noise field), so that batchStep allocates nothing.
+bool Scene::prepareBatched(std::string& err) {
+    if (!ensureConfigBuffers(err)) return false;
+    MgScene mg;
+    if (!multigridScene(mg, err)) return false;
+    return cfgNoise_ != nullptr || alloc(reinterpret_cast<void**>(&cfgNoise_), cells_ * sizeof(float4), "cudaMalloc config noise field", err);
+}
+
 // The config physics on the frame's stage ids: advect velocity, advect +
 // react + emit, forces (vorticity, cell accelerations, faces with the walls),
 // divergence, SOR, subtract, transmittance, raymarch, camera response,
@@ -1620,16 +1783,26 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                 vcur_ = 1 - vcur_;
                 break;
             case kDivergence:
-                divergenceOf<<<cells, bx, 0, stream>>>(divergence_, pressure_, velocity(), p); ++launches_;
+                if (incrementalProjection()) {
+                    // The previous pressure's gradient first; the solve then finds the increment.
+                    MgScene S;
+                    if (!multigridScene(S, err)) return false;
+                    cfgPrepareIncrement<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(),
+                                                                  pressure_, divergence_, nx, ny, nz); ++launches_;
+                    vcur_ = 1 - vcur_;
+                    mgDeltaValid_ = false;
+                } else {
+                    divergenceOf<<<cells, bx, 0, stream>>>(divergence_, pressure_, velocity(), p); ++launches_;
+                }
                 break;
             case kPressureSor:
                 if (!runSor(p, err)) return false;
                 break;
             case kSubtract:
-                if (physics_.pressureTop == 1 && mgP0Valid_) {
-                    // The Dirichlet top's solve left its pressure in double: subtract from that.
-                    cfgSubtractWide<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], mgP0_, nx, ny, nz,
-                                                            last >= kWallBoundary ? 1 : 0); ++launches_;
+                if (physics_.pressureTop == 1 && mgDeltaValid_) {
+                    // The multigrid solve found the pressure increment: subtract its gradient.
+                    cfgSubtractIncrement<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], mgP_[0], nx, ny, nz,
+                                                                   last >= kWallBoundary ? 1 : 0); ++launches_;
                 } else {
                     subtractWall<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], pressure_, p, 1, last >= kWallBoundary ? 1 : 0); ++launches_;
                     if (physics_.pressureTop == 1) {
@@ -1674,7 +1847,7 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                            cudaMemsetAsync(cfgLight_, 0, static_cast<size_t>(cfgLx_) * cfgLy_ * cfgLz_ * sizeof(float), stream), err);
                 if (!ok) return false;
                 cfgStep_ = 0;
-                mgP0Valid_ = false;
+                mgDeltaValid_ = false;
                 break;
             }
             default:

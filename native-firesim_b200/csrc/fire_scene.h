@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -32,6 +33,42 @@ struct MaterialKey {
     float burnerX0 = 0.0f, burnerZ0 = 0.0f;
     bool operator==(const MaterialKey& o) const;
 };
+
+// The host side of one persistent multigrid solve (mgSolve) over one scene or
+// a batch of scenes: the work lists and scene descriptors in device memory,
+// the launch shape, and the barrier state.  plan() rebuilds them when the
+// scenes or the solver settings change; launch() queues one solve.
+class MgSolver {
+public:
+    MgSolver() = default;
+    ~MgSolver();
+    MgSolver(const MgSolver&) = delete;
+    MgSolver& operator=(const MgSolver&) = delete;
+    bool plan(int device, const std::vector<MgScene>& scenes, int maxCycles, int pre, int post, double tolerance, cudaStream_t stream,
+              std::string& err);
+    bool planned() const { return planned_; }
+    // Queues the barrier reset and the cooperative launch on `stream`; a wait
+    // that runs out writes kMgStatusFlag | phase into *hostStatus (host-mapped).
+    bool launch(cudaStream_t stream, unsigned* hostStatus, std::string& err);
+    void release();
+    int gridBlocks() const { return grid_; }
+
+private:
+    MgScene* dScenes_ = nullptr;  // kMgMaxScenes descriptors
+    MgPlan* dPlan_ = nullptr;
+    MgSync* dSync_ = nullptr;
+    MgScene* hScenes_ = nullptr;  // pinned staging of the uploads
+    MgPlan* hPlan_ = nullptr;
+    cudaEvent_t uploaded_ = nullptr;
+    bool planned_ = false;
+    size_t smem_ = 0;
+    int grid_ = 0, sms_ = 0;
+    unsigned long long waitNs_ = 1000000000ull;
+};
+
+// Host-side fault injection of Scene's device allocations: -1 = off; n >= 0 =
+// n more allocations succeed, then every one fails with cudaErrorMemoryAllocation.
+void setAllocationFault(long long succeedBeforeFailing);
 
 // Defaults of FirePhysicsParams for a grid (fireCudaDefaultPhysicsParams).
 void defaultPhysicsParams(FirePhysicsParams& params, int nx, int ny, int nz);
@@ -193,18 +230,89 @@ private:
     int cfgLx_ = 0, cfgLy_ = 0, cfgLz_ = 0;
     unsigned long long cfgStep_ = 0;
     ConfigParams configParams() const;
-    // Multigrid levels (level 0 is pressure_/divergence_), their buffers and the captured V-cycles.
+    // Multigrid: levels, their buffers (mgP_[0] is the increment, the level-0
+    // rhs is divergence_), the residual chunks, this scene's descriptor and its solver.
     int mgCycles_ = 0, mgPre_ = 2, mgPost_ = 2;
     std::vector<MgLevel> mgLevels_;
-    std::vector<float*> mgP_, mgRhs_;  // levels >= 1
-    double* mgP0_ = nullptr;           // level-0 pressure in double (the float field is written from it)
-    bool mgP0Valid_ = false;           // mgP0_ holds the latest solve's pressure (the next solve starts from it)
-    cudaGraphExec_t mgExec_ = nullptr;
-    int mgKeyCycles_ = -1, mgKeyPre_ = -1, mgKeyPost_ = -1, mgGraphLaunches_ = 0;
+    std::vector<float*> mgP_, mgRhs_;  // mgRhs_[0] is unused (divergence_)
+    double* mgChunkSq_ = nullptr;
+    float* mgChunkMax_ = nullptr;
+    bool mgDeltaValid_ = false;        // mgP_[0] holds the latest solve's increment (the subtraction takes it)
+    MgSolver mgSolver_;
+    int mgKeyCycles_ = -1, mgKeyPre_ = -1, mgKeyPost_ = -1;
     double mgKeyTol_ = -1.0;
     bool runMultigrid(std::string& err);
+
+public:
+    // The multigrid buffers of this scene (allocated on first use) and its
+    // descriptor for a batched solve.
+    bool multigridScene(MgScene& out, std::string& err);
+    // Incremental projection under a Dirichlet top with the multigrid solve.
+    bool incrementalProjection() const { return physics_.mode == 1 && physics_.pressureTop == 1 && mgCycles_ > 0; }
+    int multigridCycles() const { return mgCycles_; }
+    int multigridPre() const { return mgPre_; }
+    int multigridPost() const { return mgPost_; }
+    double pressureTolerance() const { return pressureTolerance_; }
+    unsigned* hostStatus() const { return sorHostStatus_; }
+    // One step inside a FireBatch (see fire_batch.cu): bookkeeping, buffers and
+    // this step's descriptor; the batch queues the kernels on `stream`.
+    bool batchStep(BatchScene& d, const FireSettings& s, bool render, std::string& err);
+    // Allocates every buffer batchStep can need, so that later batched steps allocate nothing.
+    bool prepareBatched(std::string& err);
+    void addLaunches(unsigned long long n) { launches_ += n; }
+    bool hasHdrOutput() const { return slots_[activeSlot_].ptr != nullptr; }
+    // The stream this scene created (`stream` is it, except while a batch holds the scene).
+    cudaStream_t ownStream() const { return ownStream_; }
+
+private:
+    cudaStream_t ownStream_ = nullptr;
     bool ensureConfigBuffers(std::string& err);
     bool runConfigStages(int first, int last, const FrameParams& p, std::string& err);
 };
 
+// Steps a set of config-physics scenes (incremental multigrid projection)
+// together on one stream: per sub-step one upload of their step descriptors,
+// one launch per stage over all of them (fire_config.cu, batch*) and one
+// persistent multigrid launch (fire_mg.cu).  The set may change between
+// sub-steps (setScenes re-plans without allocating or synchronising); the
+// scenes' own work must be on stream() (callers point Scene::stream at it).
+class BatchRunner {
+public:
+    BatchRunner() = default;
+    ~BatchRunner();
+    BatchRunner(const BatchRunner&) = delete;
+    BatchRunner& operator=(const BatchRunner&) = delete;
+    bool init(int device, std::string& err);
+    bool setScenes(const std::vector<Scene*>& scenes, std::string& err);
+    // One sub-step of every scene of the set (settings[i] and render[i] for scene i).
+    bool run(const FireSettings* settings, const int* render, std::string& err);
+    void release();
+    cudaStream_t stream() const { return stream_; }
+    unsigned* hostStatus() const { return hostStatus_; }
+    unsigned long long launches() const { return launches_; }
+    const std::vector<Scene*>& scenes() const { return scenes_; }
+    // After a stream sync: fails once if a multigrid barrier wait ran out since the last check.
+    bool checkStatus(std::string& err);
+
+private:
+    static constexpr int kRing = 2;  // pinned descriptor buffers in flight
+    int device_ = 0;
+    std::vector<Scene*> scenes_;
+    cudaStream_t stream_ = nullptr;
+    MgSolver solver_;
+    BatchScene* dScenes_ = nullptr;   // kBatchMaxScenes
+    BatchPlan* dPlan_ = nullptr;
+    unsigned char* host_[kRing] = {};  // pinned: kBatchMaxScenes descriptors + a plan
+    cudaEvent_t copied_[kRing] = {};
+    int slot_ = 0;
+    unsigned* hostStatus_ = nullptr;  // host-mapped
+    unsigned long long launches_ = 0;
+};
+
 }  // namespace firesim
+
+// The opaque FireScene handle of fire_ext.h: one Scene and its device.
+struct FireScene {
+    std::unique_ptr<firesim::Scene> scene;
+    int device = 0;
+};

@@ -27,11 +27,6 @@ namespace firesim {
 void setLastErrorMessage(const char* msg);
 }  // namespace firesim
 
-struct FireScene {
-    std::unique_ptr<firesim::Scene> scene;
-    int device = 0;
-};
-
 namespace {
 
 bool fail(const std::string& msg) {
@@ -147,6 +142,16 @@ extern "C" bool fireSceneGetStream(FireScene* scene, void** stream) {
     return true;
 }
 
+extern "C" bool fireSceneGetPressureStats(FireScene* scene, int* iterations, float* maxResidual, double* l2Residual) {
+    if (scene == nullptr || iterations == nullptr || maxResidual == nullptr || l2Residual == nullptr) {
+        return fail("fireSceneGetPressureStats: null scene or output pointer.");
+    }
+    if (!useDevice(scene->device)) return false;
+    std::string err;
+    if (!scene->scene->pressureStats(*iterations, *maxResidual, *l2Residual, err)) return fail(err);
+    return true;
+}
+
 extern "C" bool fireSceneGetField(FireScene* scene, int field, void* host, size_t bytes) {
     if (scene == nullptr || host == nullptr) return fail("Scene handle or host pointer was null.");
     if (!useDevice(scene->device)) return false;
@@ -190,6 +195,19 @@ constexpr int kStepsInFlight = 2;
 
 using Shape = std::tuple<int, int, int, int, int>;  // nx, ny, nz, frameW, frameH
 
+namespace {
+
+// A scene of the batched serving loop, created before the run for one shape
+// (with its HDR frame and every buffer a batched step needs).
+struct BatchedSlot {
+    std::unique_ptr<firesim::Scene> scene;
+    void* hdr = nullptr;
+    size_t bytes = 0;
+    bool busy = false;
+};
+
+}  // namespace
+
 struct FireServer {
     int device = 0;
     size_t budget = 0;
@@ -197,6 +215,9 @@ struct FireServer {
     std::vector<FireServeRequest> pending;  // sorted by arrival when the run starts
     std::map<Shape, size_t> bytesByShape;   // measured scene + frame bytes
     std::deque<std::unique_ptr<Active>> pool;  // finished scenes, oldest first
+    // The batched loop: its scenes by shape, and the runner that steps them.
+    std::map<Shape, std::vector<std::unique_ptr<BatchedSlot>>> slots;
+    std::unique_ptr<firesim::BatchRunner> runner;
 };
 
 namespace {
@@ -243,6 +264,13 @@ extern "C" void fireServerDestroy(FireServer* server) {
     if (server == nullptr) return;
     cudaSetDevice(server->device);
     for (auto& a : server->pool) releaseActive(*a);
+    if (server->runner) server->runner->release();
+    for (auto& kv : server->slots) {
+        for (auto& slot : kv.second) {
+            slot->scene->stream = slot->scene->ownStream();
+            if (slot->hdr != nullptr) cudaFree(slot->hdr);
+        }
+    }
     delete server;
 }
 
@@ -260,13 +288,294 @@ extern "C" bool fireServerSubmit(FireServer* server, const FireServeRequest* req
     }
     std::string err;
     if (r.physics.mode != 0 && !firesim::validatePhysicsParams(r.physics, err)) return fail("fireServerSubmit: " + err);
+    if (r.multigridCycles < 0 || r.multigridCycles > 1000 || r.multigridPre < 0 || r.multigridPre > 8 || r.multigridPost < 0 ||
+        r.multigridPost > 8 || !(r.pressureTolerance >= 0.0)) {
+        return fail("fireServerSubmit: invalid multigrid cycles, smoothing sweeps or pressure tolerance.");
+    }
+    if (r.multigridCycles > 0 && (r.physics.mode != 1 || r.physics.pressureTop != 1)) {
+        return fail("fireServerSubmit: multigrid needs the config physics with p = 0 on the top face (pressureTop 1).");
+    }
     server->pending.push_back(r);
     return true;
 }
 
+namespace {
+
+using EventRef = std::shared_ptr<CUevent_st>;
+
+EventRef recordEvent(cudaStream_t stream) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    if (cudaEventRecord(e, stream) != cudaSuccess) {
+        cudaEventDestroy(e);
+        return nullptr;
+    }
+    return EventRef(e, [](cudaEvent_t ev) { cudaEventDestroy(ev); });
+}
+
+bool isBatchable(const FireServeRequest& r) { return r.physics.mode == 1 && r.physics.pressureTop == 1 && r.multigridCycles > 0; }
+
+// The serving loop when every request uses the config physics with the
+// multigrid projection: all admitted scenes advance together, one
+// BatchRunner sub-step (one launch per stage over all of them) per round.
+// Scenes are created before the clock starts, per shape as many as the
+// active-cell limit lets run at once (within the budget), so the loop itself
+// allocates nothing; a request whose shape has no free scene waits.  A
+// round's step latency is the device time between the end of the scene's
+// previous round (its admission, for its first step) and the end of this one.
+bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, double maxSeconds, FireServeReport& rep) {
+    using firesim::BatchRunner;
+    std::string err;
+    if (!server->runner) {
+        server->runner = std::make_unique<BatchRunner>();
+        if (!server->runner->init(server->device, err)) {
+            server->runner.reset();
+            return fail("fireServerRun: " + err);
+        }
+    }
+    BatchRunner& runner = *server->runner;
+    // Scenes per shape before the run.
+    std::map<Shape, int> demand;
+    for (const FireServeRequest& r : waiting) ++demand[shapeOf(r)];
+    size_t inUse = 0;
+    for (auto& kv : server->slots)
+        for (auto& slot : kv.second) inUse += slot->bytes;
+    for (const auto& kv : demand) {
+        const Shape& shape = kv.first;
+        const long long cells = static_cast<long long>(std::get<0>(shape)) * std::get<1>(shape) * std::get<2>(shape);
+        const long long cap = server->maxActiveVoxels > 0 ? std::max(1LL, server->maxActiveVoxels / cells) : kv.second;
+        const int want = static_cast<int>(std::min<long long>({static_cast<long long>(kv.second), cap,
+                                                                 static_cast<long long>(firesim::kBatchMaxScenes)}));
+        auto& have = server->slots[shape];
+        while (static_cast<int>(have.size()) < want) {
+            const auto known = server->bytesByShape.find(shape);
+            if (known != server->bytesByShape.end() && inUse + known->second > server->budget && !have.empty()) break;
+            auto slot = std::make_unique<BatchedSlot>();
+            slot->scene = makeScene(server->device, std::get<3>(shape), std::get<4>(shape), std::get<0>(shape), std::get<1>(shape),
+                                    std::get<2>(shape), err);
+            if (!slot->scene) return fail("fireServerRun: " + err);
+            const size_t frame = static_cast<size_t>(std::get<3>(shape)) * std::get<4>(shape) * sizeof(float) * 4;
+            if (cudaMalloc(&slot->hdr, frame) != cudaSuccess) {
+                cudaGetLastError();
+                return fail("fireServerRun: cudaMalloc of a scene's HDR frame failed.");
+            }
+            // Any request of the shape gives the buffers' sizes; its physics is set again at admission.
+            const FireServeRequest* r0 = nullptr;
+            for (const FireServeRequest& r : waiting) {
+                if (shapeOf(r) == shape) {
+                    r0 = &r;
+                    break;
+                }
+            }
+            firesim::Scene& sc = *slot->scene;
+            if (!sc.setPhysics(r0->physics, err) ||
+                !sc.setPressureMultigrid(r0->multigridCycles, r0->multigridPre > 0 ? r0->multigridPre : 2,
+                                         r0->multigridPost > 0 ? r0->multigridPost : 2, err) ||
+                !sc.setPressureTolerance(r0->pressureTolerance, 1, err) || !sc.prepareBatched(err) ||
+                !sc.registerHdrSlot(0, slot->hdr, static_cast<size_t>(std::get<3>(shape)) * 16, FIRE_HDR_RGBA32F, err) ||
+                !sc.setActiveSlot(0, err) || !sc.synchronize(err)) {
+                cudaFree(slot->hdr);
+                return fail("fireServerRun: " + err);
+            }
+            sc.stream = runner.stream();
+            slot->bytes = sc.deviceBytes() + frame;
+            server->bytesByShape[shape] = slot->bytes;
+            inUse += slot->bytes;
+            have.push_back(std::move(slot));
+            if (inUse > server->budget) break;
+        }
+    }
+    rep.deviceBytesPeak = std::max(rep.deviceBytesPeak, inUse);
+
+    struct Live {
+        FireServeRequest req{};
+        BatchedSlot* slot = nullptr;
+        int queued = 0, done = 0;
+        EventRef last;  // end of its previous round (its admission for the first)
+    };
+    struct Round {
+        EventRef done;
+        std::vector<Live*> members;
+        std::vector<char> rendered;
+    };
+    constexpr int kRoundsInFlight = 2;
+    std::vector<std::unique_ptr<Live>> live;
+    std::deque<Round> rounds;
+    std::vector<firesim::Scene*> members, lastMembers;
+    std::vector<FireSettings> settings;
+    std::vector<int> render;
+    std::vector<double> stepMs, frameMs, queueMs;
+    long long activeVoxels = 0;
+    bool ok = true;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    while (ok && (!waiting.empty() || !live.empty())) {
+        const double t = now();
+        if (t > maxSeconds) break;
+        bool progressed = false;
+        // Admission in arrival order, while the active-cell limit holds and a scene of the shape is free.
+        while (!waiting.empty() && waiting.front().arrivalSeconds <= t && static_cast<int>(live.size()) < firesim::kBatchMaxScenes) {
+            const FireServeRequest& r = waiting.front();
+            const long long voxels = static_cast<long long>(r.nx) * r.ny * r.nz;
+            if (server->maxActiveVoxels > 0 && !live.empty() && activeVoxels + voxels > server->maxActiveVoxels) break;
+            BatchedSlot* slot = nullptr;
+            for (auto& sl : server->slots[shapeOf(r)]) {
+                if (!sl->busy) {
+                    slot = sl.get();
+                    break;
+                }
+            }
+            if (slot == nullptr) break;
+            firesim::Scene& sc = *slot->scene;
+            if (!sc.setPhysics(r.physics, err) ||
+                !sc.setPressureMultigrid(r.multigridCycles, r.multigridPre > 0 ? r.multigridPre : 2, r.multigridPost > 0 ? r.multigridPost : 2,
+                                         err) ||
+                !sc.setPressureTolerance(r.pressureTolerance, 1, err)) {
+                ok = fail("fireServerRun: " + err);
+                break;
+            }
+            auto l = std::make_unique<Live>();
+            l->req = r;
+            l->slot = slot;
+            l->last = recordEvent(runner.stream());
+            if (!l->last) {
+                ok = fail("fireServerRun: cudaEventRecord failed.");
+                break;
+            }
+            slot->busy = true;
+            activeVoxels += voxels;
+            queueMs.push_back((t - r.arrivalSeconds) * 1e3);
+            live.push_back(std::move(l));
+            waiting.pop_front();
+            rep.admittedPeak = std::max(rep.admittedPeak, static_cast<int>(live.size()));
+            progressed = true;
+        }
+        if (!ok) break;
+        // One round over every live scene with steps left to queue.
+        if (static_cast<int>(rounds.size()) < kRoundsInFlight) {
+            members.clear();
+            settings.clear();
+            render.clear();
+            Round round;
+            for (auto& lp : live) {
+                Live& l = *lp;
+                if (l.queued >= l.req.steps) continue;
+                members.push_back(l.slot->scene.get());
+                FireSettings st = l.req.settings;
+                st.reset = l.queued == 0 ? 1 : 0;
+                settings.push_back(st);
+                const bool r = l.req.renderEvery > 0 && (l.queued % l.req.renderEvery) == l.req.renderEvery - 1;
+                render.push_back(r ? 1 : 0);
+                round.members.push_back(&l);
+                round.rendered.push_back(r ? 1 : 0);
+            }
+            if (!members.empty()) {
+                if (members != lastMembers) {
+                    if (!runner.setScenes(members, err)) {
+                        ok = fail("fireServerRun: " + err);
+                        break;
+                    }
+                    lastMembers = members;
+                }
+                if (!runner.run(settings.data(), render.data(), err)) {
+                    ok = fail("fireServerRun: " + err);
+                    break;
+                }
+                round.done = recordEvent(runner.stream());
+                if (!round.done) {
+                    ok = fail("fireServerRun: cudaEventRecord failed.");
+                    break;
+                }
+                for (Live* l : round.members) ++l->queued;
+                rounds.push_back(std::move(round));
+                progressed = true;
+            }
+        }
+        // Completed rounds, in order.
+        while (!rounds.empty() && cudaEventQuery(rounds.front().done.get()) == cudaSuccess) {
+            Round& r = rounds.front();
+            for (size_t i = 0; i < r.members.size(); ++i) {
+                Live& l = *r.members[i];
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, l.last.get(), r.done.get());
+                stepMs.push_back(ms);
+                if (r.rendered[i]) frameMs.push_back(ms);
+                rep.voxelSteps += static_cast<double>(l.req.nx) * l.req.ny * l.req.nz;
+                l.last = r.done;
+                ++l.done;
+            }
+            rounds.pop_front();
+            progressed = true;
+        }
+        // Finished scenes leave; their scene is free for the next request of the shape.
+        for (size_t i = 0; i < live.size();) {
+            Live& l = *live[i];
+            if (l.done < l.req.steps) {
+                ++i;
+                continue;
+            }
+            firesim::Scene& sc = *l.slot->scene;
+            if (l.req.resultHeat && (!sc.synchronize(err) ||
+                                     !sc.getField(FIRE_FIELD_HEAT, l.req.resultHeat,
+                                                  static_cast<size_t>(l.req.nx) * l.req.ny * l.req.nz * sizeof(float), err))) {
+                ok = fail("fireServerRun: " + err);
+                break;
+            }
+            if (l.req.resultHdr &&
+                cudaMemcpy(l.req.resultHdr, l.slot->hdr, frameBytes(l.req), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                ok = fail("fireServerRun: copy of a finished scene's frame failed.");
+                break;
+            }
+            activeVoxels -= static_cast<long long>(l.req.nx) * l.req.ny * l.req.nz;
+            l.slot->busy = false;
+            live.erase(live.begin() + static_cast<long>(i));
+            ++rep.completed;
+            progressed = true;
+        }
+        if (!ok) break;
+        if (!progressed) {
+            if (live.empty() && !waiting.empty()) {
+                const double wait = waiting.front().arrivalSeconds - now();
+                if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.001)));
+            } else {
+                std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
+        }
+    }
+    if (cudaStreamSynchronize(runner.stream()) != cudaSuccess) ok = fail("fireServerRun: the batch stream failed.");
+    if (ok && !runner.checkStatus(err)) ok = fail("fireServerRun: " + err);
+    for (auto& l : live) l->slot->busy = false;
+    rep.seconds = now();
+    rep.stepMsP50 = percentile(stepMs, 0.50);
+    rep.stepMsP95 = percentile(stepMs, 0.95);
+    rep.stepMsP99 = percentile(stepMs, 0.99);
+    rep.stepMsMax = stepMs.empty() ? 0.0 : *std::max_element(stepMs.begin(), stepMs.end());
+    rep.frameMsP50 = percentile(frameMs, 0.50);
+    rep.frameMsP95 = percentile(frameMs, 0.95);
+    rep.frameMsP99 = percentile(frameMs, 0.99);
+    rep.queueMsP50 = percentile(queueMs, 0.50);
+    rep.queueMsP99 = percentile(queueMs, 0.99);
+    return ok;
+}
+
+}  // namespace
+
 extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeReport* report) {
     if (server == nullptr || report == nullptr) return fail("fireServerRun: null server or report.");
     if (!useDevice(server->device)) return false;
+    const bool batched = !server->pending.empty() &&
+                         std::all_of(server->pending.begin(), server->pending.end(), [](const FireServeRequest& r) { return isBatchable(r); });
+    if (batched) {
+        std::stable_sort(server->pending.begin(), server->pending.end(),
+                         [](const FireServeRequest& a, const FireServeRequest& b) { return a.arrivalSeconds < b.arrivalSeconds; });
+        std::deque<FireServeRequest> waiting(server->pending.begin(), server->pending.end());
+        server->pending.clear();
+        FireServeReport rep{};
+        rep.submitted = static_cast<int>(waiting.size());
+        const bool ok = runBatched(server, waiting, maxSeconds, rep);
+        *report = rep;
+        return ok;
+    }
     std::stable_sort(server->pending.begin(), server->pending.end(),
                      [](const FireServeRequest& a, const FireServeRequest& b) { return a.arrivalSeconds < b.arrivalSeconds; });
     std::deque<FireServeRequest> waiting(server->pending.begin(), server->pending.end());
@@ -353,6 +662,13 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
             FirePhysicsParams physics = r.physics;
             if (physics.mode == 0) firesim::defaultPhysicsParams(physics, r.nx, r.ny, r.nz);
             if (!a->scene->setPhysics(physics, err)) {
+                ok = fail(err);
+                break;
+            }
+            // The pressure solver of this request (a pooled scene keeps its previous one otherwise).
+            const int pre = r.multigridPre > 0 ? r.multigridPre : 2, post = r.multigridPost > 0 ? r.multigridPost : 2;
+            if (!a->scene->setPressureMultigrid(r.multigridCycles, pre, post, err) ||
+                !a->scene->setPressureTolerance(r.pressureTolerance, r.multigridCycles > 0 ? 1 : 10, err)) {
                 ok = fail(err);
                 break;
             }

@@ -90,6 +90,7 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireServerSetLimits": (b, [ctypes.c_void_p, ctypes.c_longlong]),
         "fireServerRun": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(abi.FireServeReport)]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
+        "fireCudaSetAllocationFault": (b, [ctypes.c_longlong]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
         "fireCudaSetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -107,6 +108,14 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireSceneSetPhysicsParams": (b, [ctypes.c_void_p, ctypes.POINTER(abi.FirePhysicsParams)]),
         "fireCudaSetPressureMultigrid": (b, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
         "fireSceneSetPressureMultigrid": (b, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "fireSceneGetPressureStats": (b, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+                                          ctypes.POINTER(ctypes.c_double)]),
+        "fireBatchCreate": (ctypes.c_void_p, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+        "fireBatchDestroy": (None, [ctypes.c_void_p]),
+        "fireBatchRun": (b, [ctypes.c_void_p, S, ctypes.POINTER(ctypes.c_int)]),
+        "fireBatchSynchronize": (b, [ctypes.c_void_p]),
+        "fireBatchGetStream": (b, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+        "fireBatchGetLaunchCount": (b, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -346,10 +355,64 @@ class Scene:
 
     def get(self, name: str) -> np.ndarray:
         shape = {"u": (self.nz, self.ny, self.nx + 1), "v": (self.nz, self.ny + 1, self.nx),
-                 "w": (self.nz + 1, self.ny, self.nx)}.get(name, (self.nz, self.ny, self.nx))
+                 "w": (self.nz + 1, self.ny, self.nx), "hdr": (self.frame_h, self.frame_w, 4)}.get(name, (self.nz, self.ny, self.nx))
         out = np.empty(shape, dtype=np.float32)
         self._check(self.lib.fireSceneGetField(self.h, abi.FIELDS[name], out.ctypes.data, out.nbytes), f"get {name}")
         return out
+
+    def pressure_stats(self):
+        """(iterations or multigrid cycles, max |r|, L2 residual) of the latest gated solve."""
+        it, m, l2 = ctypes.c_int(), ctypes.c_float(), ctypes.c_double()
+        self._check(self.lib.fireSceneGetPressureStats(self.h, ctypes.byref(it), ctypes.byref(m), ctypes.byref(l2)),
+                    "fireSceneGetPressureStats")
+        return it.value, m.value, l2.value
+
+
+class Batch:
+    """fireBatch*: scenes of the config physics (p = 0 on the top face, multigrid
+    solve) stepped together, one launch per stage over all of them."""
+
+    def __init__(self, scenes):
+        self.scenes = list(scenes)
+        self.lib = self.scenes[0].lib
+        handles = (ctypes.c_void_p * len(self.scenes))(*[s.h for s in self.scenes])
+        self.h = self.lib.fireBatchCreate(handles, len(self.scenes))
+        if not self.h:
+            raise FireSimError(f"fireBatchCreate: {last_error(self.lib)}")
+
+    def run(self, settings, render=None) -> None:
+        n = len(self.scenes)
+        arr = (abi.FireSettings * n)(*settings)
+        flags = None if render is None else (ctypes.c_int * n)(*[1 if r else 0 for r in render])
+        if not self.lib.fireBatchRun(self.h, arr, flags):
+            raise FireSimError(f"fireBatchRun: {last_error(self.lib)}")
+
+    def synchronize(self) -> None:
+        if not self.lib.fireBatchSynchronize(self.h):
+            raise FireSimError(f"fireBatchSynchronize: {last_error(self.lib)}")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        if not self.lib.fireBatchGetStream(self.h, ctypes.byref(s)):
+            raise FireSimError(f"fireBatchGetStream: {last_error(self.lib)}")
+        return s.value or 0
+
+    def launch_count(self) -> int:
+        c = ctypes.c_ulonglong()
+        if not self.lib.fireBatchGetLaunchCount(self.h, ctypes.byref(c)):
+            raise FireSimError(f"fireBatchGetLaunchCount: {last_error(self.lib)}")
+        return int(c.value)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.fireBatchDestroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 -- interpreter shutdown
+            pass
 
 
 def batch_step(scenes, settings, render=None) -> None:

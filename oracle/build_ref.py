@@ -15,7 +15,8 @@ Everything else -- every kernel, helper and the host sequencing -- is compiled
 as written.  Outputs go only to oracle/_ref/ (git-ignored).  The reference is
 never modified and none of its sources are committed.
 
-Usage: python oracle/build_ref.py [--reference /path/to/native-firesim]
+Usage: python oracle/build_ref.py --reference /path/to/native-firesim
+       (or FIRESIM_REFERENCE=/path/to/native-firesim python oracle/build_ref.py)
 """
 from __future__ import annotations
 
@@ -27,7 +28,11 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_REFERENCE = Path("/root/reference")
+
+def reference_root(explicit: str | None = None) -> Path | None:
+    """The native-firesim checkout: the explicit path, else $FIRESIM_REFERENCE, else None."""
+    value = explicit or os.environ.get("FIRESIM_REFERENCE")
+    return Path(value) if value else None
 
 
 def derive_headless_source(reference: Path) -> str:
@@ -54,7 +59,7 @@ def derive_headless_source(reference: Path) -> str:
     return "\n".join(out)
 
 
-def build(reference: Path = DEFAULT_REFERENCE, verbose: bool = False) -> Path:
+def build(reference: Path, verbose: bool = False) -> Path:
     if not (reference / "src" / "fire_cuda.cu").exists():
         raise FileNotFoundError(f"reference sources not found under {reference}")
     OUT.mkdir(parents=True, exist_ok=True)
@@ -84,9 +89,12 @@ def build(reference: Path = DEFAULT_REFERENCE, verbose: bool = False) -> Path:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=str(DEFAULT_REFERENCE))
+    ap.add_argument("--reference", default=None, help="native-firesim checkout (default: $FIRESIM_REFERENCE)")
     args = ap.parse_args()
-    lib = build(Path(args.reference), verbose=True)
+    root = reference_root(args.reference)
+    if root is None:
+        ap.error("give --reference or set FIRESIM_REFERENCE")
+    lib = build(root, verbose=True)
     print(lib)
     return 0
 

@@ -76,7 +76,7 @@ template <class T>
 struct Scene {
     int nx, ny, nz, lx, ly, lz, W, H;
     std::vector<T> heat, fuel, soot, u, v, w, pressure, divergence, transmittance, hdr;
-    std::vector<double> p64;  // the multigrid's level-0 pressure (Dirichlet top), in double
+    std::vector<T> delta;  // the latest multigrid solve's pressure increment (Dirichlet top)
     std::vector<T> vort;   // 4 per cell
     std::vector<T> force;  // 3 per cell
     FirePhysicsParams phys;
@@ -108,7 +108,7 @@ struct Scene {
         transmittance.assign(size_t(lx) * ly * lz, T(0));
         hdr.assign(size_t(W) * H * 4, T(0));
         vort.assign(n * 4, T(0));
-        p64.clear();
+        delta.clear();
         force.assign(n * 3, T(0));
         step = 0;
     }
@@ -419,7 +419,38 @@ template <class T> void forces(Scene<T>& s, const Derived<T>& d) {
 }
 
 // src/fire_cuda.cu:1185-1199 -- divergence = -(sum of face differences); p = 0.
+// With p = 0 on the top face and the multigrid solve, the projection is
+// incremental: the previous step's pressure gradient is subtracted from the
+// faces first (interior faces, and the top faces with the ghost -p), the
+// divergence of those faces becomes the rhs, and the solve finds only the
+// increment (from zero), so float carries it without the rounding floor of
+// the whole pressure.  The pressure field keeps the previous pressure.
+template <class T> void prepareIncrement(Scene<T>& s) {
+    const T* pr = s.pressure.data();
+    for (int z = 0; z < s.nz; ++z)
+        for (int y = 0; y < s.ny; ++y)
+            for (int x = 0; x < s.nx; ++x) {
+                const T pc = pr[s.sI(x, y, z)];
+                if (x > 0) s.u[size_t(s.uI(x, y, z))] -= pc - pr[s.sI(x - 1, y, z)];
+                if (y > 0) s.v[size_t(s.vI(x, y, z))] -= pc - pr[s.sI(x, y - 1, z)];
+                if (z > 0) s.w[size_t(s.wI(x, y, z))] -= pc - pr[s.sI(x, y, z - 1)];
+                if (y == s.ny - 1) s.v[size_t(s.vI(x, s.ny, z))] -= (T(0) - pc) - pc;
+            }
+    for (int z = 0; z < s.nz; ++z)
+        for (int y = 0; y < s.ny; ++y)
+            for (int x = 0; x < s.nx; ++x) {
+                const T dv = s.u[size_t(s.uI(x + 1, y, z))] - s.u[size_t(s.uI(x, y, z))] + s.v[size_t(s.vI(x, y + 1, z))] -
+                             s.v[size_t(s.vI(x, y, z))] + s.w[size_t(s.wI(x, y, z + 1))] - s.w[size_t(s.wI(x, y, z))];
+                s.divergence[size_t(s.sI(x, y, z))] = -dv;
+            }
+    s.delta.clear();
+}
+
 template <class T> void divergence(Scene<T>& s) {
+    if (s.phys.pressureTop == 1 && s.mgCycles > 0) {
+        prepareIncrement(s);
+        return;
+    }
 #pragma omp parallel for collapse(2) schedule(static)
     for (int z = 0; z < s.nz; ++z) {
         for (int y = 0; y < s.ny; ++y) {
@@ -491,7 +522,6 @@ struct Lvl {
     int nx, ny, nz;
     T wx, wy, wz, diag, invDiag;
     int cx, cy, cz;
-    int wide;  // level 0: smoothing and residuals evaluated in double, p stored in T
     int at(int x, int y, int z) const { return (z * ny + y) * nx + x; }
 };
 
@@ -501,8 +531,7 @@ template <class T> Lvl<T> withWeights(Lvl<T> L) {
     return L;
 }
 
-// The level operations in the level's pressure type P (double on level 0,
-// T on the coarser levels), as the product's fire_mg.cu.
+// The level operations (every level in T), as the product's fire_mg.cu.
 template <class P, class T> P wsum(const std::vector<P>& p, const std::vector<T>& rhs, const Lvl<T>& L, int x, int y, int z, P self) {
     const int i = L.at(x, y, z);
     const P pL = x > 0 ? p[i - 1] : self;
@@ -584,14 +613,14 @@ template <class P, class T> void prolong(std::vector<P>& pf, const std::vector<T
 }
 
 template <class T> void multigrid(Scene<T>& s) {
-    std::vector<Lvl<T>> lv{withWeights(Lvl<T>{s.nx, s.ny, s.nz, T(1), T(1), T(1), T(0), T(0), 0, 0, 0, 1})};
+    std::vector<Lvl<T>> lv{withWeights(Lvl<T>{s.nx, s.ny, s.nz, T(1), T(1), T(1), T(0), T(0), 0, 0, 0})};
     while (lv.size() < 10) {
         const Lvl<T> b = lv.back();
         const int cx = b.nx % 2 == 0 && b.nx >= 4, cy = b.ny % 2 == 0 && b.ny >= 4, cz = b.nz % 2 == 0 && b.nz >= 4;
         if (!cx && !cy && !cz) break;
         lv.push_back(withWeights(Lvl<T>{cx ? b.nx / 2 : b.nx, cy ? b.ny / 2 : b.ny, cz ? b.nz / 2 : b.nz,
                                         cx ? b.wx * T(0.25f) : b.wx, cy ? b.wy * T(0.25f) : b.wy, cz ? b.wz * T(0.25f) : b.wz,
-                                        T(0), T(0), cx, cy, cz, 0}));
+                                        T(0), T(0), cx, cy, cz}));
     }
     const int n = int(lv.size());
     std::vector<std::vector<T>> P(n), R(n);
@@ -599,10 +628,9 @@ template <class T> void multigrid(Scene<T>& s) {
         P[l].assign(size_t(lv[l].nx) * lv[l].ny * lv[l].nz, T(0));
         R[l].assign(P[l].size(), T(0));
     }
-    // Level 0: the pressure in double, warm-started from the previous solve (from zero
-    // after a reset or a write of the pressure field); rhs the divergence array.
-    std::vector<double>& p0 = s.p64;
-    if (p0.size() != size_t(s.cells())) p0.assign(size_t(s.cells()), 0.0);
+    // Level 0: the pressure increment, from zero; rhs the divergence array
+    // (the divergence after the previous pressure's gradient was subtracted).
+    std::vector<T> p0(size_t(s.cells()), T(0));
     const std::vector<T>& r0 = s.divergence;
     s.mgCyclesRun = 0;
     s.mgMaxResidual = -1.0f;
@@ -642,22 +670,24 @@ template <class T> void multigrid(Scene<T>& s) {
             if (s.mgMaxResidual <= s.mgTolerance) break;
         }
     }
-    for (size_t i = 0; i < p0.size(); ++i) s.pressure[i] = T(p0[i]);
+    // The new pressure is the previous one plus the increment; the gradient
+    // subtraction takes the increment.
+    for (size_t i = 0; i < p0.size(); ++i) s.pressure[i] = s.pressure[i] + p0[i];
+    s.delta = std::move(p0);
 }
 
-// The gradient subtraction from the multigrid's double pressure (Dirichlet
-// top): each face difference in double, rounded once to T; top faces with the
-// antisymmetric ghost -p.
-template <class T> void subtractWide(Scene<T>& s) {
-    const std::vector<double>& pr = s.p64;
+// The gradient subtraction of the multigrid's pressure increment (Dirichlet
+// top): interior faces, and the top faces with the antisymmetric ghost -delta.
+template <class T> void subtractIncrement(Scene<T>& s) {
+    const std::vector<T>& pr = s.delta;
     for (int z = 0; z < s.nz; ++z)
         for (int y = 0; y < s.ny; ++y)
             for (int x = 0; x < s.nx; ++x) {
-                const double pc = pr[size_t(s.sI(x, y, z))];
-                if (x > 0) s.u[size_t(s.uI(x, y, z))] -= T(pc - pr[size_t(s.sI(x - 1, y, z))]);
-                if (y > 0) s.v[size_t(s.vI(x, y, z))] -= T(pc - pr[size_t(s.sI(x, y - 1, z))]);
-                if (z > 0) s.w[size_t(s.wI(x, y, z))] -= T(pc - pr[size_t(s.sI(x, y, z - 1))]);
-                if (y == s.ny - 1) s.v[size_t(s.vI(x, s.ny, z))] -= T((0.0 - pc) - pc);
+                const T pc = pr[size_t(s.sI(x, y, z))];
+                if (x > 0) s.u[size_t(s.uI(x, y, z))] -= pc - pr[size_t(s.sI(x - 1, y, z))];
+                if (y > 0) s.v[size_t(s.vI(x, y, z))] -= pc - pr[size_t(s.sI(x, y - 1, z))];
+                if (z > 0) s.w[size_t(s.wI(x, y, z))] -= pc - pr[size_t(s.sI(x, y, z - 1))];
+                if (y == s.ny - 1) s.v[size_t(s.vI(x, s.ny, z))] -= (T(0) - pc) - pc;
             }
 }
 
@@ -794,8 +824,8 @@ template <class T> int runStages(Scene<T>& s, int first, int last) {
                 }
                 break;
             case FIRE_STAGE_SUBTRACT:
-                if (s.phys.pressureTop == 1 && s.p64.size() == size_t(s.cells())) {
-                    subtractWide(s);
+                if (s.phys.pressureTop == 1 && s.delta.size() == size_t(s.cells())) {
+                    subtractIncrement(s);
                 } else {
                     subtract(s);
                     if (s.phys.pressureTop == 1) {
@@ -927,7 +957,7 @@ int cfg_oracle_set_field(void* o, int field, const void* host, long long bytes) 
         } else {
             const float* in = static_cast<const float*>(host);
             for (size_t i = 0; i < f->size(); ++i) (*f)[i] = in[i];
-            if (field == FIRE_FIELD_PRESSURE) s.p64.clear();
+            if (field == FIRE_FIELD_PRESSURE) s.delta.clear();
         }
     });
     return rc;

@@ -2,7 +2,7 @@
 three scenes, about 1 KB each) into tests/golden/scene_contracts/ so the
 contract tests run without the reference checkout.
 
-Usage: python tests/golden/make_scene_contracts.py [reference root]
+Usage: python tests/golden/make_scene_contracts.py <native-firesim checkout>
 """
 from __future__ import annotations
 
@@ -15,7 +15,10 @@ OUT = HERE / "scene_contracts"
 
 
 def main() -> int:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "assets" / "fire-scenes"
+    if len(sys.argv) != 2:
+        print(__doc__.strip().splitlines()[-1], file=sys.stderr)
+        return 2
+    ref = Path(sys.argv[1]) / "assets" / "fire-scenes"
     for asset in ("room", "campfire", "gas-burner-aver1"):
         (OUT / asset).mkdir(parents=True, exist_ok=True)
         for name in ("scene.json", "emitter-mask.json"):

@@ -244,11 +244,12 @@ def test_config_gated_solve_on_both_paths(product, abi):
 def test_multigrid_equals_the_oracle_bitwise(dims, cycles, tol, product, abi, oracle_mod):
     """The multigrid solve (Dirichlet top) from a random right-hand side: the
     same pressure bits and the same number of V-cycles as the oracle, gated
-    and fixed.  The coarsest level is relaxed by one warp (2^3 cells at 32^3
-    and 128^3; 2x3x5 below 64x48x40, semi-coarsened), by one block with its
-    cells fixed per thread (5x9x11 below 20x36x44) or, for the 125x2x99 level
-    below 125x4x99, by one block walking all its cells; 33x17x21 has no
-    coarser level."""
+    and fixed.  The shapes cover the solve's tail (the coarse end of the
+    hierarchy, one CTA): in shared memory from 16^3 down at 128^3 and from
+    8^3 (a one-warp 2^3 coarsest level) at 32^3; semi-coarsened to 2x3x5 at
+    64x48x40; a tail that is level 0 itself (33x17x21 has no coarser level);
+    and, for 125x4x99, whose coarsest level 125x2x99 is too large for shared
+    memory, a tail in global memory."""
     p = abi.default_physics(*dims)
     p.mode, p.pressureTop = 1, 1
     d = (0.3 * np.random.default_rng(4).standard_normal(dims[::-1])).astype(np.float32)

@@ -219,3 +219,53 @@ def test_server_rejects_invalid_physics(pkg, abi):
     with pytest.raises(pkg.firesim.FireSimError, match="sample counts"):
         server.submit(r)
     server.close()
+
+
+def test_batched_server_equals_alone(pkg, abi):
+    """Requests of the config physics with the multigrid projection are served
+    as one batch per round (every admitted scene advanced by one launch per
+    stage); with room for about two scenes by cells, eight requests of three
+    shapes arrive over 40 ms, queue for free scenes and complete, and each
+    served heat field and last frame equal the same scene stepped alone."""
+    import torch
+    server = pkg.Server(budget_bytes=64 << 30)
+    server.set_limits(int(np.prod(SIZES[1]) + np.prod(SIZES[2])))
+    reqs, heats, hdrs = [], [], []
+    for i in range(8):
+        dims = SIZES[i % 3]
+        r = _request(abi, i, dims, steps=5 + i, arrival=0.005 * i, scene=0, render_every=3)
+        r.physics = abi.config_scene(*dims, dims[0] / 2, dims[2] / 2, 3.0 + 0.5 * i, 0.3, -0.2, 200 + i)
+        r.physics.pressureTop = 1
+        r.multigridCycles, r.multigridPre, r.multigridPost, r.pressureTolerance = 20, 2, 2, 1e-5
+        r.settings = abi.FireSettings(width=64, height=48, dt=1.0 / 60.0)
+        heat = np.zeros(dims[::-1], dtype=np.float32)
+        hdr = np.zeros((48, 64, 4), dtype=np.float32)
+        r.resultHeat, r.resultHdr = heat.ctypes.data, hdr.ctypes.data
+        reqs.append(r)
+        heats.append(heat)
+        hdrs.append(hdr)
+        server.submit(r)
+    rep = server.run(60.0)
+    server.close()
+    assert rep["completed"] == 8 and 1 <= rep["admittedPeak"] <= 3
+    assert rep["voxelSteps"] == sum((5 + i) * np.prod(SIZES[i % 3]) for i in range(8))
+    assert 0 < rep["stepMsP50"] <= rep["stepMsP99"] <= rep["stepMsMax"]
+    for i, r in enumerate(reqs):
+        dims = SIZES[i % 3]
+        sc = pkg.Scene(64, 48, *dims)
+        hdr = torch.zeros((48, 64, 4), dtype=torch.float32, device="cuda")
+        sc.set_hdr_buffer(hdr.data_ptr(), 64 * 16, 0)
+        sc.set_physics(r.physics)
+        sc.set_pressure_multigrid(20, 2, 2)
+        sc.set_pressure_tolerance(1e-5, 1)
+        for f in range(r.steps):
+            s = abi.FireSettings.from_buffer_copy(r.settings)
+            s.reset = 1 if f == 0 else 0
+            sc.step(s, render=f % 3 == 2)
+        sc.synchronize()
+        alone_heat = sc.get("heat")
+        alone_hdr = hdr.cpu().numpy()
+        sc.close()
+        np.testing.assert_array_equal(heats[i].view(np.uint32), alone_heat.view(np.uint32), err_msg=f"request {i} heat")
+        np.testing.assert_array_equal(hdrs[i].view(np.uint32), alone_hdr.view(np.uint32), err_msg=f"request {i} hdr")
+        assert heats[i].sum() > 0.0

@@ -22,8 +22,8 @@ import tolerances as T
 pytestmark = pytest.mark.gpu
 
 
-def _no_alloc_fn(pkg):
-    lib = pkg.load_library()
+def _no_alloc_fn(pkg, precision="f32"):
+    lib = pkg.load_library(precision)
     fn = lib.fireCudaForceProjectNoAlloc
     fn.restype = ctypes.c_bool
     fn.argtypes = [ctypes.POINTER(pkg.abi.FireSettings), ctypes.c_float] + [ctypes.c_int] * 3 + [ctypes.c_void_p] * 12
@@ -37,12 +37,18 @@ def _call(fn, pkg, settings, time, dims, inputs, outputs, stream):
     assert ok, pkg.firesim.last_error()
 
 
-def test_no_alloc_force_pass_matches_regular_path(pkg, abi):
+STORAGE = {"f32": "float32", "f16": "float16", "bf16": "bfloat16"}
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16", "bf16"])
+def test_no_alloc_force_pass_matches_regular_path(pkg, abi, precision):
+    """Each library build takes records and faces in its own storage type."""
     import torch
 
-    fn = _no_alloc_fn(pkg)
+    fn = _no_alloc_fn(pkg, precision)
+    storage = getattr(torch, STORAGE[precision])
     dims = (40, 48, 32)
-    sim = pkg.FireSim(64, 40, *dims)
+    sim = pkg.FireSim(64, 40, *dims, precision=precision)
     stream = torch.cuda.current_stream().cuda_stream
     for frame in range(2):
         # Advance the scene so the force pass sees a developed fire.
@@ -52,15 +58,18 @@ def test_no_alloc_force_pass_matches_regular_path(pkg, abi):
         settings = abi.validation_settings(4 * frame + 4, width=64, height=40)
         time = float(np.float32(sim.times()[0]) + np.float32(settings.dt))
         f = {n: sim.get(n) for n in abi.SCALAR_FIELDS + ["u", "v", "w"]}
-        rec_a = torch.tensor(np.stack([f["heat"], f["fuel"], f["oxygen"], f["soot"]], axis=-1), device="cuda")
-        rec_b = torch.tensor(np.stack([f["char"], f["ash"], f["pyrolysis"], f["progress"]], axis=-1), device="cuda")
-        rec_c = torch.tensor(np.stack([f["turbulence_energy"], f["soot_optics"]], axis=-1), device="cuda")
-        faces = [torch.tensor(f[n], device="cuda") for n in ("u", "v", "w")]
+        # The scene's fields come back as float; in the half builds they hold
+        # stored half values, so converting back to the storage type is exact.
+        rec_a = torch.tensor(np.stack([f["heat"], f["fuel"], f["oxygen"], f["soot"]], axis=-1), device="cuda").to(storage)
+        rec_b = torch.tensor(np.stack([f["char"], f["ash"], f["pyrolysis"], f["progress"]], axis=-1), device="cuda").to(storage)
+        rec_c = torch.tensor(np.stack([f["turbulence_energy"], f["soot_optics"]], axis=-1), device="cuda").to(storage)
+        faces = [torch.tensor(f[n], device="cuda").to(storage) for n in ("u", "v", "w")]
         outs = [torch.full_like(t, np.nan) for t in faces]
         div = torch.full(f["heat"].shape, np.nan, device="cuda")
         pres = torch.full(f["heat"].shape, np.nan, device="cuda")
         _call(fn, pkg, settings, time, dims, [rec_a, rec_b, rec_c, *faces], [*outs, div, pres], stream)
         torch.cuda.synchronize()
+        outs = [t.float() for t in outs]
 
         sim.stages("force", "divergence", settings, time)
         expect = {n: sim.get(n) for n in ("u", "v", "w", "divergence", "pressure")}
@@ -80,3 +89,7 @@ def test_no_alloc_rejects_oversized_grid(pkg, abi):
             ctypes.c_void_p(dummy.data_ptr()), ctypes.c_void_p(0))
     assert not ok
     assert "exceeds the 1048576-cell scratch" in pkg.firesim.last_error()
+    ok = fn(ctypes.byref(settings), 0.0, 2, 2, 70000, *[ctypes.c_void_p(dummy.data_ptr())] * 11,
+            ctypes.c_void_p(dummy.data_ptr()), ctypes.c_void_p(0))
+    assert not ok
+    assert "at most 65535" in pkg.firesim.last_error()
