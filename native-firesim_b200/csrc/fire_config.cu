@@ -9,9 +9,11 @@
 // solve and the gradient subtraction are the reference-physics kernels.
 //
 // This file is compiled with -fmad=false: every product and sum rounds as
-// written, so a CPU restatement that evaluates the same expressions in the
-// same order in IEEE float gives the same bits for the whole simulation step
-// (only +, -, *, /, sqrt, floor, min/max and integer hashing occur there).
+// written, and the only fused multiply-adds are the explicit ones of the
+// interpolations (lerp1), so a CPU restatement that evaluates the same
+// expressions in the same order in IEEE float, with std::fma where the
+// kernels fuse, gives the same bits for the whole simulation step (only +, -,
+// *, /, fma, sqrt, floor, min/max and integer hashing occur there).
 // The render uses expf and is compared within a tolerance.
 //
 // Memory: records are read and written through the storage accessors
@@ -27,7 +29,7 @@ __device__ __forceinline__ int faceIndex(int x, int y, int z, int mx, int my) { 
 
 // Clamped trilinear sample of a grid of mx*my*mz values (x fastest) at index-space
 // position q: q clamped to [0, m-1] per axis, i0 = (int)q, i1 = min(i0 + 1, m - 1),
-// t = q - i0; lerp(a, b, t) = a + t * (b - a), along x, then y, then z.
+// t = q - i0; lerp(a, b, t) = fma(t, b - a, a), along x, then y, then z.
 struct Corners {
     int x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
@@ -48,28 +50,36 @@ __device__ __forceinline__ Corners cornersAt(float qx, float qy, float qz, int m
     return c;
 }
 
-__device__ __forceinline__ float lerp1(float a, float b, float t) { return a + t * (b - a); }
+// One fused multiply-add (explicit, as the file is built without contraction).
+__device__ __forceinline__ float lerp1(float a, float b, float t) { return __fmaf_rn(t, b - a, a); }
 
 __device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
     return make_float4(lerp1(a.x, b.x, t), lerp1(a.y, b.y, t), lerp1(a.z, b.z, t), lerp1(a.w, b.w, t));
 }
 
+// The eight corner loads address one base cell plus fixed offsets (0 or 1
+// cell along each axis, 0 where the clamp merges the corners), which saves
+// the index arithmetic of a full (z * my + y) * mx + x per corner.
 template <typename P>
 __device__ __forceinline__ float trilinear1(const P* f, const Corners& c, int mx, int my) {
-    const float a00 = lerp1(ldv(f + faceIndex(c.x0, c.y0, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z0, mx, my)), c.tx);
-    const float a10 = lerp1(ldv(f + faceIndex(c.x0, c.y1, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z0, mx, my)), c.tx);
-    const float a01 = lerp1(ldv(f + faceIndex(c.x0, c.y0, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z1, mx, my)), c.tx);
-    const float a11 = lerp1(ldv(f + faceIndex(c.x0, c.y1, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z1, mx, my)), c.tx);
+    const P* b = f + faceIndex(c.x0, c.y0, c.z0, mx, my);
+    const int dx = c.x1 - c.x0, dy = (c.y1 - c.y0) * mx, dz = (c.z1 - c.z0) * mx * my;
+    const float a00 = lerp1(ldv(b), ldv(b + dx), c.tx);
+    const float a10 = lerp1(ldv(b + dy), ldv(b + dy + dx), c.tx);
+    const float a01 = lerp1(ldv(b + dz), ldv(b + dz + dx), c.tx);
+    const float a11 = lerp1(ldv(b + dz + dy), ldv(b + dz + dy + dx), c.tx);
     const float b0 = lerp1(a00, a10, c.ty);
     const float b1 = lerp1(a01, a11, c.ty);
     return lerp1(b0, b1, c.tz);
 }
 
 __device__ __forceinline__ float4 trilinearRec(const Rec4* f, const Corners& c, int mx, int my) {
-    const float4 a00 = lerp4(ldv(f + faceIndex(c.x0, c.y0, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z0, mx, my)), c.tx);
-    const float4 a10 = lerp4(ldv(f + faceIndex(c.x0, c.y1, c.z0, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z0, mx, my)), c.tx);
-    const float4 a01 = lerp4(ldv(f + faceIndex(c.x0, c.y0, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y0, c.z1, mx, my)), c.tx);
-    const float4 a11 = lerp4(ldv(f + faceIndex(c.x0, c.y1, c.z1, mx, my)), ldv(f + faceIndex(c.x1, c.y1, c.z1, mx, my)), c.tx);
+    const Rec4* b = f + faceIndex(c.x0, c.y0, c.z0, mx, my);
+    const int dx = c.x1 - c.x0, dy = (c.y1 - c.y0) * mx, dz = (c.z1 - c.z0) * mx * my;
+    const float4 a00 = lerp4(ldv(b), ldv(b + dx), c.tx);
+    const float4 a10 = lerp4(ldv(b + dy), ldv(b + dy + dx), c.tx);
+    const float4 a01 = lerp4(ldv(b + dz), ldv(b + dz + dx), c.tx);
+    const float4 a11 = lerp4(ldv(b + dz + dy), ldv(b + dz + dy + dx), c.tx);
     const float4 b0 = lerp4(a00, a10, c.ty);
     const float4 b1 = lerp4(a01, a11, c.ty);
     return lerp4(b0, b1, c.tz);
@@ -90,11 +100,13 @@ __device__ __forceinline__ float3 velocityAtUFace(const Velocity& vel, const Con
     int x0, x1;
     float tx;
     axisOf(static_cast<float>(x) - 0.5f, p.nx, x0, x1, tx);
-    const int yv = y + 1, zw = z + 1;  // v at y and y + 1 (weight 1/2), w at z and z + 1 (weight 1/2)
-    const float v = lerp1(lerp1(faceAt(vel.v, x0, y, z, p.nx, p.ny + 1), faceAt(vel.v, x1, y, z, p.nx, p.ny + 1), tx),
-                          lerp1(faceAt(vel.v, x0, yv, z, p.nx, p.ny + 1), faceAt(vel.v, x1, yv, z, p.nx, p.ny + 1), tx), 0.5f);
-    const float w = lerp1(lerp1(faceAt(vel.w, x0, y, z, p.nx, p.ny), faceAt(vel.w, x1, y, z, p.nx, p.ny), tx),
-                          lerp1(faceAt(vel.w, x0, y, zw, p.nx, p.ny), faceAt(vel.w, x1, y, zw, p.nx, p.ny), tx), 0.5f);
+    // v at y and y + 1 (weight 1/2), w at z and z + 1 (weight 1/2), x0 and x1 along x.
+    const int dx = x1 - x0;
+    const FaceT* vb = vel.v + faceIndex(x0, y, z, p.nx, p.ny + 1);
+    const FaceT* wb = vel.w + faceIndex(x0, y, z, p.nx, p.ny);
+    const int vy = p.nx, wz = p.nx * p.ny;
+    const float v = lerp1(lerp1(ldv(vb), ldv(vb + dx), tx), lerp1(ldv(vb + vy), ldv(vb + vy + dx), tx), 0.5f);
+    const float w = lerp1(lerp1(ldv(wb), ldv(wb + dx), tx), lerp1(ldv(wb + wz), ldv(wb + wz + dx), tx), 0.5f);
     return make_float3(faceAt(vel.u, x, y, z, p.nx + 1, p.ny), v, w);
 }
 
@@ -103,11 +115,11 @@ __device__ __forceinline__ float3 velocityAtVFace(const Velocity& vel, const Con
     int y0, y1;
     float ty;
     axisOf(static_cast<float>(y) - 0.5f, p.ny, y0, y1, ty);
-    const int xu = x + 1, zw = z + 1;
-    const float u = lerp1(lerp1(faceAt(vel.u, x, y0, z, p.nx + 1, p.ny), faceAt(vel.u, xu, y0, z, p.nx + 1, p.ny), 0.5f),
-                          lerp1(faceAt(vel.u, x, y1, z, p.nx + 1, p.ny), faceAt(vel.u, xu, y1, z, p.nx + 1, p.ny), 0.5f), ty);
-    const float w = lerp1(lerp1(faceAt(vel.w, x, y0, z, p.nx, p.ny), faceAt(vel.w, x, y1, z, p.nx, p.ny), ty),
-                          lerp1(faceAt(vel.w, x, y0, zw, p.nx, p.ny), faceAt(vel.w, x, y1, zw, p.nx, p.ny), ty), 0.5f);
+    const FaceT* ub = vel.u + faceIndex(x, y0, z, p.nx + 1, p.ny);
+    const FaceT* wb = vel.w + faceIndex(x, y0, z, p.nx, p.ny);
+    const int du = (y1 - y0) * (p.nx + 1), dw = (y1 - y0) * p.nx, wz = p.nx * p.ny;
+    const float u = lerp1(lerp1(ldv(ub), ldv(ub + 1), 0.5f), lerp1(ldv(ub + du), ldv(ub + du + 1), 0.5f), ty);
+    const float w = lerp1(lerp1(ldv(wb), ldv(wb + dw), ty), lerp1(ldv(wb + wz), ldv(wb + wz + dw), ty), 0.5f);
     return make_float3(u, faceAt(vel.v, x, y, z, p.nx, p.ny + 1), w);
 }
 
@@ -116,19 +128,20 @@ __device__ __forceinline__ float3 velocityAtWFace(const Velocity& vel, const Con
     int z0, z1;
     float tz;
     axisOf(static_cast<float>(z) - 0.5f, p.nz, z0, z1, tz);
-    const int xu = x + 1, yv = y + 1;
-    const float u = lerp1(lerp1(faceAt(vel.u, x, y, z0, p.nx + 1, p.ny), faceAt(vel.u, xu, y, z0, p.nx + 1, p.ny), 0.5f),
-                          lerp1(faceAt(vel.u, x, y, z1, p.nx + 1, p.ny), faceAt(vel.u, xu, y, z1, p.nx + 1, p.ny), 0.5f), tz);
-    const float v = lerp1(lerp1(faceAt(vel.v, x, y, z0, p.nx, p.ny + 1), faceAt(vel.v, x, yv, z0, p.nx, p.ny + 1), 0.5f),
-                          lerp1(faceAt(vel.v, x, y, z1, p.nx, p.ny + 1), faceAt(vel.v, x, yv, z1, p.nx, p.ny + 1), 0.5f), tz);
+    const FaceT* ub = vel.u + faceIndex(x, y, z0, p.nx + 1, p.ny);
+    const FaceT* vb = vel.v + faceIndex(x, y, z0, p.nx, p.ny + 1);
+    const int du = (z1 - z0) * (p.nx + 1) * p.ny, dv = (z1 - z0) * p.nx * (p.ny + 1), vy = p.nx;
+    const float u = lerp1(lerp1(ldv(ub), ldv(ub + 1), 0.5f), lerp1(ldv(ub + du), ldv(ub + du + 1), 0.5f), tz);
+    const float v = lerp1(lerp1(ldv(vb), ldv(vb + vy), 0.5f), lerp1(ldv(vb + dv), ldv(vb + dv + vy), 0.5f), tz);
     return make_float3(u, v, faceAt(vel.w, x, y, z, p.nx, p.ny));
 }
 
 // At the cell centre (x + .5, y + .5, z + .5): the mean of the two faces along each axis.
 __device__ __forceinline__ float3 velocityAtCentre(const Velocity& vel, const ConfigParams& p, int x, int y, int z) {
-    return make_float3(lerp1(faceAt(vel.u, x, y, z, p.nx + 1, p.ny), faceAt(vel.u, x + 1, y, z, p.nx + 1, p.ny), 0.5f),
-                       lerp1(faceAt(vel.v, x, y, z, p.nx, p.ny + 1), faceAt(vel.v, x, y + 1, z, p.nx, p.ny + 1), 0.5f),
-                       lerp1(faceAt(vel.w, x, y, z, p.nx, p.ny), faceAt(vel.w, x, y, z + 1, p.nx, p.ny), 0.5f));
+    const FaceT* ub = vel.u + faceIndex(x, y, z, p.nx + 1, p.ny);
+    const FaceT* vb = vel.v + faceIndex(x, y, z, p.nx, p.ny + 1);
+    const FaceT* wb = vel.w + faceIndex(x, y, z, p.nx, p.ny);
+    return make_float3(lerp1(ldv(ub), ldv(ub + 1), 0.5f), lerp1(ldv(vb), ldv(vb + p.nx), 0.5f), lerp1(ldv(wb), ldv(wb + p.nx * p.ny), 0.5f));
 }
 
 __device__ __forceinline__ float4 recordAt(const Rec4* a, const ConfigParams& p, float x, float y, float z) {

@@ -3,7 +3,7 @@
 // TEST INFRASTRUCTURE, NOT PRODUCT CODE.  A plain restatement of the model of
 // include/fire_ext.h ("Config physics"), written independently of the CUDA
 // kernels.  Every expression is evaluated in the order the model states it
-// (lerp(a, b, t) = a + t * (b - a); trilinear along x, then y, then z; sums
+// (lerp(a, b, t) = fma(t, b - a, a); trilinear along x, then y, then z; sums
 // left to right), so T = float reproduces the product's rounding.  The
 // projection (divergence, red-black SOR, gradient subtraction, wall zeroing)
 // restates the reference's, src/fire_cuda.cu:1185-1245 and :1293-1317,
@@ -187,7 +187,8 @@ template <class T> Axis<T> axis(T q, int m) {
     return a;
 }
 
-template <class T> T lerp(T a, T b, T t) { return a + t * (b - a); }
+// One fused multiply-add, as the kernels' lerp1 (__fmaf_rn).
+template <class T> T lerp(T a, T b, T t) { return std::fma(t, b - a, a); }
 
 // Clamped trilinear sample of grid f (mx * my * mz, x fastest) at index position (qx, qy, qz).
 template <class T> T trilinear(const std::vector<T>& f, int mx, int my, int mz, T qx, T qy, T qz) {
