@@ -214,10 +214,14 @@ struct MgLevel {
 };
 constexpr int kMgMaxLevels = 10;
 constexpr int kMgMaxScenes = 128;     // scenes of one batched solve
-constexpr int kMgTailCells = 6144;    // the tail starts at the first level with at most this many cells
-constexpr size_t kMgTailSmemMax = 160 * 1024;  // larger tails work in global memory
+constexpr int kMgTailCells = 32768;   // the tail starts at the first level with at most this many cells
+constexpr size_t kMgTailSmemMax = 200 * 1024;  // shared memory a tail may use
+// Where a tail keeps its levels: all in shared memory; the tail level's rhs
+// in global memory and the rest in shared memory; all in global memory.
+enum MgTailMode { kMgTailShared = 0, kMgTailRhsGlobal = 1, kMgTailGlobal = 2 };
 constexpr int kMgThreads = 1024;      // threads of a CTA of mgSolve (one CTA per SM)
-constexpr int kMgChunkRows = 16;      // level-0 rows per residual chunk
+constexpr int kMgChunkRows = 4;       // level-0 rows per residual chunk
+constexpr int kMgUnroll = 2;          // 32-cell units a warp of mgSolve has in flight at once
 constexpr int kMgCoarsestSweeps = 32;
 constexpr int kMgHardCycleCap = 1000;  // fireCudaSetPressureMultigrid accepts at most this many cycles
 constexpr unsigned kMgMaxPolls = 1u << 26;
@@ -234,21 +238,29 @@ struct MgScene {
     float* chunkMax;
     int levels;        // number of levels
     int tail;          // first level solved by one CTA (the tail)
-    int tailInGlobal;  // 1: the tail works in the levels' global buffers (too large for shared memory)
+    int tailMode;      // MgTailMode
 };
-// The work lists of a solve: prefix sums over the scenes of the rows of each
-// grid level (levels l < tail of the scene; 0 rows otherwise), of the coarse
-// rows each restriction writes, of the residual chunks and of all level-0 rows.
+// The work lists of a solve, as prefix sums over the scenes (0 for a scene
+// whose tail starts at or above the level).  smoothUnits counts 128-cell
+// chunks of the rows of grid level l (four cells per lane); fineUnits 32-cell
+// chunks of its rows (the prolongation, a cell per lane); coarseUnits 32-cell
+// chunks of the rows of level l + 1 (the restriction).  chunks counts the residual's chunks of kMgChunkRows level-0
+// rows; allRows all level-0 rows.
 struct MgPlan {
     int scenes;
     int gridLevels;  // max over the scenes of tail
     int maxCycles, pre, post, gated;
     float tolerance;
-    int rows[kMgMaxLevels][kMgMaxScenes + 1];
-    int coarseRows[kMgMaxLevels][kMgMaxScenes + 1];
+    int smoothUnits[kMgMaxLevels][kMgMaxScenes + 1];
+    int fineUnits[kMgMaxLevels][kMgMaxScenes + 1];
+    int coarseUnits[kMgMaxLevels][kMgMaxScenes + 1];
     int chunks[kMgMaxScenes + 1];
     int allRows[kMgMaxScenes + 1];
 };
+// Chunks per row of a level: 128-cell chunks (the smoothing's units, four
+// cells per lane) and 32-cell chunks (the prolongation's and restriction's).
+__host__ __device__ inline int mgQuadChunks(int nx) { return (nx + 127) / 128; }
+__host__ __device__ inline int mgRowChunks(int nx) { return (nx + 31) / 32; }
 // Grid barrier state of mgSolve (zeroed before each launch).
 struct MgSync {
     unsigned count, generation, failed, pad;

@@ -132,8 +132,11 @@ __device__ bool gridBarrier(MgSync* sync, unsigned& generation, unsigned long lo
 }
 
 // ---- the tail: levels tail..levels-1 of one scene in one CTA ------------
-// In shared memory (kGlobal false) or, for a tail too large for it, in the
-// levels' own global buffers (kGlobal true, read through L2).
+// The levels' p and rhs live in shared memory, except where the tail's mode
+// puts them in their global buffers (read through L2): kMgTailShared keeps
+// everything in shared memory; kMgTailRhsGlobal keeps the tail level's rhs
+// (read-only within the tail) in global memory; kMgTailGlobal keeps all of it
+// there, for a tail too large for shared memory.
 
 template <bool kGlobal>
 __device__ __forceinline__ float tailLoad(const float* a, int i) {
@@ -144,32 +147,34 @@ __device__ __forceinline__ float tailLoad(const float* a, int i) {
     }
 }
 
-template <bool kGlobal>
-__device__ void tailSmooth(float* p, const float* rhs, const MgLevel& L, int sweeps) {
-    const int cells = L.nx * L.ny * L.nz;
-    auto load = [&](int j) { return tailLoad<kGlobal>(p, j); };
+// `sweeps` red-black sweeps of one tail level.  Each thread walks whole
+// columns (x, y) along z, taking the cells of the colour, so cell
+// coordinates need one division per column.  A level of at most 128 cells is
+// relaxed by the first warp alone, with warp barriers; otherwise by the whole
+// CTA.  The level is passed by value, so its fields stay in registers across
+// the stores to p.
+template <bool PG, bool RG>
+__device__ void tailSmooth(float* p, const float* rhs, const MgLevel L, int sweeps) {
+    const int cols = L.nx * L.ny;
+    const bool warpOnly = cols * L.nz <= 4 * 32;
+    const int stride = warpOnly ? 32 : static_cast<int>(blockDim.x);
+    const bool active = !warpOnly || threadIdx.x < 32;
+    auto load = [&](int j) { return tailLoad<PG>(p, j); };
     for (int s = 0; s < sweeps; ++s) {
         for (int colour = 0; colour < 2; ++colour) {
-            if (cells <= 4 * 32) {
-                // A tiny level: the first warp alone, with warp barriers.
-                if (threadIdx.x < 32) {
-                    for (int i = threadIdx.x; i < cells; i += 32) {
-                        const int x = i % L.nx, y = (i / L.nx) % L.ny, z = i / (L.nx * L.ny);
-                        if (((x + y + z) & 1) == colour) {
-                            p[i] = weightedSum(load, tailLoad<kGlobal>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
-                        }
+            if (active) {
+                for (int col = threadIdx.x; col < cols; col += stride) {
+                    const int y = col / L.nx, x = col - y * L.nx;
+                    for (int z = (colour + x + y) & 1; z < L.nz; z += 2) {
+                        const int i = col + z * cols;
+                        p[i] = weightedSum(load, tailLoad<RG>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
                     }
-                    if constexpr (kGlobal) __threadfence_block();
-                    __syncwarp();
                 }
+            }
+            if constexpr (PG) __threadfence_block();
+            if (warpOnly) {
+                __syncwarp();
             } else {
-                for (int i = threadIdx.x; i < cells; i += blockDim.x) {
-                    const int x = i % L.nx, y = (i / L.nx) % L.ny, z = i / (L.nx * L.ny);
-                    if (((x + y + z) & 1) == colour) {
-                        p[i] = weightedSum(load, tailLoad<kGlobal>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
-                    }
-                }
-                if constexpr (kGlobal) __threadfence_block();
                 __syncthreads();
             }
         }
@@ -221,68 +226,92 @@ __device__ __forceinline__ float prolongAt(LoadC loadC, const MgLevel& F, const 
     return uz * b0 + vz * b1;
 }
 
-// The V-cycle of levels tail..levels-1 of scene S by this CTA.  In shared
-// memory, rhs and p of the tail level come from global memory (p is zero
-// there unless the tail is level 0), everything below lives in shared memory,
-// and the tail level's p goes back to global memory.
-template <bool kGlobal>
+// The V-cycle of levels tail..levels-1 of scene S by this CTA.  The tail
+// level's p comes from global memory (it is zero there unless the tail is
+// level 0) and goes back to it at the end.
+template <int MODE>
 __device__ void tailCycle(const MgScene& S, int pre, int post, float* smem) {
+    constexpr bool PG = MODE == kMgTailGlobal;
     const int t = S.tail;
     float* p[kMgMaxLevels];
     float* r[kMgMaxLevels];
     int off = 0;
     for (int l = t; l < S.levels; ++l) {
         const int n = S.lv[l].nx * S.lv[l].ny * S.lv[l].nz;
-        if constexpr (kGlobal) {
+        if (PG) {
             p[l] = S.p[l];
             r[l] = S.rhs[l];
         } else {
             p[l] = smem + off;
-            r[l] = smem + off + n;
+            off += n;
+            if (MODE == kMgTailRhsGlobal && l == t) {
+                r[l] = S.rhs[l];
+            } else {
+                r[l] = smem + off;
+                off += n;
+            }
         }
-        off += 2 * n;
     }
-    const MgLevel& T0 = S.lv[t];
+    const MgLevel T0 = S.lv[t];
     const int n0 = T0.nx * T0.ny * T0.nz;
-    if constexpr (!kGlobal) {
+    if constexpr (!PG) {
         for (int i = threadIdx.x; i < n0; i += blockDim.x) {
             p[t][i] = __ldcg(S.p[t] + i);
-            r[t][i] = __ldcg(S.rhs[t] + i);
+            if (MODE == kMgTailShared) r[t][i] = __ldcg(S.rhs[t] + i);
         }
     }
     __syncthreads();
     const int last = S.levels - 1;
     for (int l = t; l < last; ++l) {
-        const MgLevel& F = S.lv[l];
-        const MgLevel& C = S.lv[l + 1];
-        tailSmooth<kGlobal>(p[l], r[l], F, pre);
+        const MgLevel F = S.lv[l];
+        const MgLevel C = S.lv[l + 1];
+        const bool rg = PG || (MODE == kMgTailRhsGlobal && l == t);
+        if (rg) {
+            tailSmooth<PG, true>(p[l], r[l], F, pre);
+        } else {
+            tailSmooth<PG, false>(p[l], r[l], F, pre);
+        }
         const float* pf = p[l];
-        auto loadF = [&](int j) { return tailLoad<kGlobal>(pf, j); };
-        const int nc = C.nx * C.ny * C.nz;
-        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
-            const int X = i % C.nx, Y = (i / C.nx) % C.ny, Z = i / (C.nx * C.ny);
-            r[l + 1][i] = restrictAt(loadF, r[l], kGlobal, F, C, X, Y, Z);
-            p[l + 1][i] = 0.0f;
+        auto loadF = [&](int j) { return tailLoad<PG>(pf, j); };
+        const int cols = C.nx * C.ny;
+        for (int col = threadIdx.x; col < cols; col += blockDim.x) {
+            const int Y = col / C.nx, X = col - Y * C.nx;
+            for (int Z = 0; Z < C.nz; ++Z) {
+                const int i = col + Z * cols;
+                r[l + 1][i] = restrictAt(loadF, r[l], rg, F, C, X, Y, Z);
+                p[l + 1][i] = 0.0f;
+            }
         }
-        if constexpr (kGlobal) __threadfence_block();
+        if constexpr (PG) __threadfence_block();
         __syncthreads();
     }
-    tailSmooth<kGlobal>(p[last], r[last], S.lv[last], kMgCoarsestSweeps);
+    if (PG || (MODE == kMgTailRhsGlobal && last == t)) {
+        tailSmooth<PG, true>(p[last], r[last], S.lv[last], kMgCoarsestSweeps);
+    } else {
+        tailSmooth<PG, false>(p[last], r[last], S.lv[last], kMgCoarsestSweeps);
+    }
     for (int l = last - 1; l >= t; --l) {
-        const MgLevel& F = S.lv[l];
-        const MgLevel& C = S.lv[l + 1];
+        const MgLevel F = S.lv[l];
+        const MgLevel C = S.lv[l + 1];
         const float* pc = p[l + 1];
-        auto loadC = [&](int j) { return tailLoad<kGlobal>(pc, j); };
-        const int nf = F.nx * F.ny * F.nz;
-        for (int i = threadIdx.x; i < nf; i += blockDim.x) {
-            const int x = i % F.nx, y = (i / F.nx) % F.ny, z = i / (F.nx * F.ny);
-            p[l][i] = tailLoad<kGlobal>(p[l], i) + prolongAt(loadC, F, C, x, y, z);
+        auto loadC = [&](int j) { return tailLoad<PG>(pc, j); };
+        const int cols = F.nx * F.ny;
+        for (int col = threadIdx.x; col < cols; col += blockDim.x) {
+            const int y = col / F.nx, x = col - y * F.nx;
+            for (int z = 0; z < F.nz; ++z) {
+                const int i = col + z * cols;
+                p[l][i] = tailLoad<PG>(p[l], i) + prolongAt(loadC, F, C, x, y, z);
+            }
         }
-        if constexpr (kGlobal) __threadfence_block();
+        if constexpr (PG) __threadfence_block();
         __syncthreads();
-        tailSmooth<kGlobal>(p[l], r[l], F, post);
+        if (PG || (MODE == kMgTailRhsGlobal && l == t)) {
+            tailSmooth<PG, true>(p[l], r[l], F, post);
+        } else {
+            tailSmooth<PG, false>(p[l], r[l], F, post);
+        }
     }
-    if constexpr (!kGlobal) {
+    if constexpr (!PG) {
         for (int i = threadIdx.x; i < n0; i += blockDim.x) S.p[t][i] = p[t][i];
     }
 }
@@ -307,64 +336,153 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
     const int nwarps = gridDim.x * warpsPerBlock;
     unsigned generation = loadVolatileU(&sync->generation);
     int phase = 0;
-    auto converged = [&](int s) { return loadVolatileI(&scenes[s].gate->converged) != 0; };
+    // The scenes still running, read once after each gate (converged flags
+    // change only in the gate phase).
+    __shared__ unsigned char sRunning[kMgMaxScenes];
+    auto refreshRunning = [&]() {
+        for (int s = threadIdx.x; s < n; s += blockDim.x) sRunning[s] = loadVolatileI(&scenes[s].gate->converged) == 0 ? 1 : 0;
+        __syncthreads();
+    };
+    auto converged = [&](int s) { return sRunning[s] == 0; };
+    // Units are processed kMgUnroll at a time per warp, every load of them
+    // issued before any store, so that their L2 round trips overlap.
+    constexpr int U = kMgUnroll;
 
-    // One colour of red-black Gauss-Seidel on level l of every scene that has it as a grid level.
+    // One colour of red-black Gauss-Seidel on level l of every scene that has
+    // it as a grid level.  A unit is 128 consecutive cells of a row, four per
+    // lane: the lane loads its four cells and the same four of the rows above,
+    // below, behind and in front (one float4 each when the row length is a
+    // multiple of 4, else element by element), the rhs and the two cells
+    // beside them, updates the two of its cells of the colour and stores the
+    // four back (the other two unchanged: no thread writes them in this phase).
     auto smooth = [&](int l, int colour) {
-        const int* off = plan->rows[l];
+        const int* off = plan->smoothUnits[l];
         const int total = __ldg(off + n);
-        for (int item = gwarp; item < total; item += nwarps) {
-            const int s = sceneOf(off, n, item);
+        for (int unit = gwarp; unit < total; unit += nwarps) {
+            const int s = sceneOf(off, n, unit);
             if (converged(s)) continue;
             const MgScene& S = scenes[s];
             const MgLevel L = S.lv[l];
+            const int u = unit - __ldg(off + s);
+            const int cpr = mgQuadChunks(L.nx);
+            const int row = u / cpr, chunk = u - row * cpr;
+            const int y = row % L.ny, z = row / L.ny;
+            const int x0 = chunk * 128 + 4 * lane;
+            if (x0 >= L.nx) continue;
             float* p = S.p[l];
             const float* rhs = S.rhs[l];
-            const int row = item - __ldg(off + s);
-            const int y = row % L.ny, z = row / L.ny;
-            auto load = [&](int j) { return __ldcg(p + j); };
-            for (int x = 2 * lane + ((colour + y + z) & 1); x < L.nx; x += 64) {
-                const int i = mgAt(L, x, y, z);
-                const float rh = l == 0 ? __ldg(rhs + i) : __ldcg(rhs + i);
-                p[i] = weightedSum(load, rh, L, i, x, y, z, __ldcg(p + i)) * L.invDiag;
+            const int i0 = row * L.nx + x0;
+            const int plane = L.nx * L.ny;
+            float c[4], dn[4], up[4], bk[4], fr[4], rh[4];
+            const bool quad = (L.nx & 3) == 0;
+            if (quad) {
+                const float4 v = __ldcg(reinterpret_cast<const float4*>(p + i0));
+                c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+                const float4 vd = y > 0 ? __ldcg(reinterpret_cast<const float4*>(p + i0 - L.nx)) : v;
+                const float4 vu = y < L.ny - 1 ? __ldcg(reinterpret_cast<const float4*>(p + i0 + L.nx))
+                                               : make_float4(0.0f - v.x, 0.0f - v.y, 0.0f - v.z, 0.0f - v.w);
+                const float4 vb = z > 0 ? __ldcg(reinterpret_cast<const float4*>(p + i0 - plane)) : v;
+                const float4 vf = z < L.nz - 1 ? __ldcg(reinterpret_cast<const float4*>(p + i0 + plane)) : v;
+                const float4 vr = l == 0 ? __ldg(reinterpret_cast<const float4*>(rhs + i0)) : __ldcg(reinterpret_cast<const float4*>(rhs + i0));
+                dn[0] = vd.x; dn[1] = vd.y; dn[2] = vd.z; dn[3] = vd.w;
+                up[0] = vu.x; up[1] = vu.y; up[2] = vu.z; up[3] = vu.w;
+                bk[0] = vb.x; bk[1] = vb.y; bk[2] = vb.z; bk[3] = vb.w;
+                fr[0] = vf.x; fr[1] = vf.y; fr[2] = vf.z; fr[3] = vf.w;
+                rh[0] = vr.x; rh[1] = vr.y; rh[2] = vr.z; rh[3] = vr.w;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int i = i0 + e;
+                    if (x0 + e < L.nx) {
+                        c[e] = __ldcg(p + i);
+                        dn[e] = y > 0 ? __ldcg(p + i - L.nx) : c[e];
+                        up[e] = y < L.ny - 1 ? __ldcg(p + i + L.nx) : 0.0f - c[e];
+                        bk[e] = z > 0 ? __ldcg(p + i - plane) : c[e];
+                        fr[e] = z < L.nz - 1 ? __ldcg(p + i + plane) : c[e];
+                        rh[e] = l == 0 ? __ldg(rhs + i) : __ldcg(rhs + i);
+                    } else {
+                        c[e] = dn[e] = up[e] = bk[e] = fr[e] = rh[e] = 0.0f;
+                    }
+                }
+            }
+            const float left = x0 > 0 ? __ldcg(p + i0 - 1) : 0.0f;
+            const float right = x0 + 4 < L.nx ? __ldcg(p + i0 + 4) : 0.0f;
+            const int e0 = (colour + x0 + y + z) & 1;  // the colour's cells are e0 and e0 + 2
+            float o[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int x = x0 + e;
+                o[e] = c[e];
+                if ((e & 1) != e0 || x >= L.nx) continue;
+                const float self = c[e];
+                const float pL = x > 0 ? (e > 0 ? c[e - 1] : left) : self;
+                const float pR = x < L.nx - 1 ? (e < 3 ? c[e + 1] : right) : self;
+                o[e] = (rh[e] + L.wx * (pL + pR) + L.wy * (dn[e] + up[e]) + L.wz * (bk[e] + fr[e])) * L.invDiag;
+            }
+            if (quad) {
+                *reinterpret_cast<float4*>(p + i0) = make_float4(o[0], o[1], o[2], o[3]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if ((e & 1) == e0 && x0 + e < L.nx) p[i0 + e] = o[e];
+                }
             }
         }
     };
     auto restrictTo = [&](int l) {
-        const int* off = plan->coarseRows[l];
+        const int* off = plan->coarseUnits[l];
         const int total = __ldg(off + n);
-        for (int item = gwarp; item < total; item += nwarps) {
-            const int s = sceneOf(off, n, item);
+        for (int unit = gwarp; unit < total; unit += nwarps) {
+            const int s = sceneOf(off, n, unit);
             if (converged(s)) continue;
             const MgScene& S = scenes[s];
             const MgLevel F = S.lv[l], C = S.lv[l + 1];
+            const int u = unit - __ldg(off + s);
+            const int cpr = mgRowChunks(C.nx);
+            const int row = u / cpr, chunk = u - row * cpr;
+            const int Y = row % C.ny, Z = row / C.ny;
+            const int X = chunk * 32 + lane;
+            if (X >= C.nx) continue;
             const float* pf = S.p[l];
             auto loadF = [&](int j) { return __ldcg(pf + j); };
-            const int row = item - __ldg(off + s);
-            const int Y = row % C.ny, Z = row / C.ny;
-            for (int X = lane; X < C.nx; X += 32) {
-                const int c = mgAt(C, X, Y, Z);
-                S.rhs[l + 1][c] = restrictAt(loadF, S.rhs[l], l > 0, F, C, X, Y, Z);
-                S.p[l + 1][c] = 0.0f;
-            }
+            const int c = mgAt(C, X, Y, Z);
+            const float r = restrictAt(loadF, S.rhs[l], l > 0, F, C, X, Y, Z);
+            S.rhs[l + 1][c] = r;
+            S.p[l + 1][c] = 0.0f;
         }
     };
     auto prolongFrom = [&](int l) {
-        const int* off = plan->rows[l];
+        const int* off = plan->fineUnits[l];
         const int total = __ldg(off + n);
-        for (int item = gwarp; item < total; item += nwarps) {
-            const int s = sceneOf(off, n, item);
-            if (converged(s)) continue;
-            const MgScene& S = scenes[s];
-            const MgLevel F = S.lv[l], C = S.lv[l + 1];
-            const float* pc = S.p[l + 1];
-            auto loadC = [&](int j) { return __ldcg(pc + j); };
-            float* pf = S.p[l];
-            const int row = item - __ldg(off + s);
-            const int y = row % F.ny, z = row / F.ny;
-            for (int x = lane; x < F.nx; x += 32) {
+        for (int base = gwarp * U; base < total; base += nwarps * U) {
+            int sc[U], idx[U];
+            float cur[U], add[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int unit = base + k;
+                sc[k] = -1;
+                if (unit >= total) continue;
+                const int s = sceneOf(off, n, unit);
+                if (converged(s)) continue;
+                const MgScene& S = scenes[s];
+                const MgLevel F = S.lv[l], C = S.lv[l + 1];
+                const int u = unit - __ldg(off + s);
+                const int cpr = mgRowChunks(F.nx);
+                const int row = u / cpr, chunk = u - row * cpr;
+                const int y = row % F.ny, z = row / F.ny;
+                const int x = chunk * 32 + lane;
+                if (x >= F.nx) continue;
+                const float* pc = S.p[l + 1];
+                auto loadC = [&](int j) { return __ldcg(pc + j); };
                 const int i = mgAt(F, x, y, z);
-                pf[i] = __ldcg(pf + i) + prolongAt(loadC, F, C, x, y, z);
+                sc[k] = s;
+                idx[k] = i;
+                cur[k] = __ldcg(S.p[l] + i);
+                add[k] = prolongAt(loadC, F, C, x, y, z);
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                if (sc[k] >= 0) scenes[sc[k]].p[l][idx[k]] = cur[k] + add[k];
             }
         }
     };
@@ -383,6 +501,7 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
         }
     }
     if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
+    refreshRunning();
     for (int cycle = 0; cycle < maxCycles; ++cycle) {
         for (int l = 0; l < gridLevels; ++l) {
             for (int k = 0; k < 2 * pre; ++k) {
@@ -394,10 +513,13 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
         }
         for (int s = blockIdx.x; s < n; s += gridDim.x) {
             if (!converged(s)) {
-                if (scenes[s].tailInGlobal) {
-                    tailCycle<true>(scenes[s], pre, post, smem);
+                const int mode = scenes[s].tailMode;
+                if (mode == kMgTailShared) {
+                    tailCycle<kMgTailShared>(scenes[s], pre, post, smem);
+                } else if (mode == kMgTailRhsGlobal) {
+                    tailCycle<kMgTailRhsGlobal>(scenes[s], pre, post, smem);
                 } else {
-                    tailCycle<false>(scenes[s], pre, post, smem);
+                    tailCycle<kMgTailGlobal>(scenes[s], pre, post, smem);
                 }
             }
             __syncthreads();
@@ -424,17 +546,21 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
                 auto load = [&](int j) { return __ldcg(p + j); };
                 const int chunk = item - __ldg(plan->chunks + s);
                 const int rows = L.ny * L.nz;
+                // The chunk's cells in order (rows of x), lane-strided; no
+                // stores in the loop, so the unrolled loads overlap.
+                const int first = chunk * kMgChunkRows;
+                const int count = (min(rows, first + kMgChunkRows) - first) * L.nx;
                 double sq = 0.0;
                 float mx = 0.0f;
-                for (int row = chunk * kMgChunkRows; row < min(rows, (chunk + 1) * kMgChunkRows); ++row) {
+#pragma unroll 4
+                for (int j = lane; j < count; j += 32) {
+                    const int row = first + j / L.nx, x = j - (j / L.nx) * L.nx;
                     const int y = row % L.ny, z = row / L.ny;
-                    for (int x = lane; x < L.nx; x += 32) {
-                        const int i = mgAt(L, x, y, z);
-                        const float self = __ldcg(p + i);
-                        const float r = weightedSum(load, __ldg(S.rhs[0] + i), L, i, x, y, z, self) - L.diag * self;
-                        mx = fmaxf(mx, fabsf(r));
-                        sq += static_cast<double>(r) * static_cast<double>(r);
-                    }
+                    const int i = row * L.nx + x;
+                    const float self = __ldcg(p + i);
+                    const float r = weightedSum(load, __ldg(S.rhs[0] + i), L, i, x, y, z, self) - L.diag * self;
+                    mx = fmaxf(mx, fabsf(r));
+                    sq += static_cast<double>(r) * static_cast<double>(r);
                 }
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {
@@ -478,6 +604,7 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             }
         }
         if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
+        refreshRunning();
         if (threadIdx.x == 0) sActive = 0;
         __syncthreads();
         for (int s = threadIdx.x; s < n; s += blockDim.x) {

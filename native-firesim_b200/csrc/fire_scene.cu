@@ -681,14 +681,24 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
         plan.gridLevels = std::max(plan.gridLevels, S.tail);
         size_t tailFloats = 0;
         for (int l = S.tail; l < S.levels; ++l) tailFloats += 2 * static_cast<size_t>(S.lv[l].nx) * S.lv[l].ny * S.lv[l].nz;
-        if (!S.tailInGlobal) smem = std::max(smem, tailFloats * sizeof(float));
+        if (S.tailMode == kMgTailShared) smem = std::max(smem, tailFloats * sizeof(float));
+        if (S.tailMode == kMgTailRhsGlobal) {
+            smem = std::max(smem, (tailFloats - static_cast<size_t>(S.lv[S.tail].nx) * S.lv[S.tail].ny * S.lv[S.tail].nz) * sizeof(float));
+        }
     }
     for (int l = 0; l < kMgMaxLevels; ++l) {
         for (int s = 0; s < n; ++s) {
             const MgScene& S = scenes[s];
             const bool grid = l < S.tail;
-            plan.rows[l][s + 1] = plan.rows[l][s] + (grid ? S.lv[l].ny * S.lv[l].nz : 0);
-            plan.coarseRows[l][s + 1] = plan.coarseRows[l][s] + (grid ? S.lv[l + 1].ny * S.lv[l + 1].nz : 0);
+            const MgLevel& F = S.lv[l];
+            plan.smoothUnits[l][s + 1] = plan.smoothUnits[l][s] + (grid ? F.ny * F.nz * mgQuadChunks(F.nx) : 0);
+            plan.fineUnits[l][s + 1] = plan.fineUnits[l][s] + (grid ? F.ny * F.nz * mgRowChunks(F.nx) : 0);
+            if (grid) {
+                const MgLevel& C = S.lv[l + 1];
+                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s] + C.ny * C.nz * mgRowChunks(C.nx);
+            } else {
+                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s];
+            }
         }
     }
     for (int s = 0; s < n; ++s) {
@@ -785,7 +795,8 @@ bool Scene::multigridScene(MgScene& out, std::string& err) {
     }
     size_t tailBytes = 0;
     for (int l = S.tail; l < S.levels; ++l) tailBytes += 2 * sizeof(float) * mgLevels_[l].nx * mgLevels_[l].ny * mgLevels_[l].nz;
-    S.tailInGlobal = tailBytes > kMgTailSmemMax ? 1 : 0;
+    const size_t tailRhs = sizeof(float) * mgLevels_[S.tail].nx * mgLevels_[S.tail].ny * mgLevels_[S.tail].nz;
+    S.tailMode = tailBytes <= kMgTailSmemMax ? kMgTailShared : (tailBytes - tailRhs <= kMgTailSmemMax ? kMgTailRhsGlobal : kMgTailGlobal);
     S.pressure = pressure_;
     S.gate = sorGate_;
     S.chunkSq = mgChunkSq_;

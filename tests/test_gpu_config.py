@@ -240,16 +240,18 @@ def test_config_gated_solve_on_both_paths(product, abi):
 
 
 @pytest.mark.parametrize("dims,cycles,tol", [((32, 32, 32), 12, 1e-5), ((64, 48, 40), 12, 1e-5), ((33, 17, 21), 5, 0.0),
-                                             ((128, 128, 128), 10, 1e-5), ((125, 4, 99), 3, 0.0), ((20, 36, 44), 6, 0.0)])
+                                             ((128, 128, 128), 10, 1e-5), ((125, 4, 99), 3, 0.0), ((20, 36, 44), 6, 0.0),
+                                             ((41, 37, 35), 2, 0.0)])
 def test_multigrid_equals_the_oracle_bitwise(dims, cycles, tol, product, abi, oracle_mod):
     """The multigrid solve (Dirichlet top) from a random right-hand side: the
     same pressure bits and the same number of V-cycles as the oracle, gated
     and fixed.  The shapes cover the solve's tail (the coarse end of the
-    hierarchy, one CTA): in shared memory from 16^3 down at 128^3 and from
-    8^3 (a one-warp 2^3 coarsest level) at 32^3; semi-coarsened to 2x3x5 at
-    64x48x40; a tail that is level 0 itself (33x17x21 has no coarser level);
-    and, for 125x4x99, whose coarsest level 125x2x99 is too large for shared
-    memory, a tail in global memory."""
+    hierarchy, one CTA) in its three modes: all in shared memory (from 32^3
+    down at 32^3, with a one-warp 2^3 coarsest level; 64x48x40,
+    semi-coarsened to 2x3x5; 33x17x21, which cannot coarsen, so the tail is
+    level 0; 125x2x99 below 125x4x99); the tail level's rhs in global memory
+    (from 32^3 down at 128^3); and all in global memory (41x37x35, which
+    cannot coarsen and is too large for shared memory)."""
     p = abi.default_physics(*dims)
     p.mode, p.pressureTop = 1, 1
     d = (0.3 * np.random.default_rng(4).standard_normal(dims[::-1])).astype(np.float32)

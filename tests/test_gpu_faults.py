@@ -6,6 +6,8 @@ what it had allocated (src/fire_cuda.cu:2981) and leaves the library usable.
 """
 from __future__ import annotations
 
+import ctypes
+
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -24,7 +26,9 @@ def test_allocation_failure_is_reported_freed_and_recovered(pkg, abi):
         assert not lib.fireCudaInitializeGrid(64, 48, 32, 32, 32)
         msg = pkg.firesim.last_error()
         assert "out of memory (injected)" in msg and ": " in msg, msg
-        assert not lib.fireCudaSynchronize()  # no scene after a failed init
+        dims = (ctypes.c_int * 8)()
+        assert not lib.fireCudaGetGridInfo(dims)  # no scene after a failed init
+        assert "not initialized" in pkg.firesim.last_error()
     assert lib.fireCudaSetAllocationFault(-1)
     torch.cuda.synchronize()
     free_after = torch.cuda.mem_get_info()[0]

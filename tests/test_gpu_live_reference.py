@@ -83,6 +83,52 @@ def test_stages_vs_live_reference(grid, pkg, abi, refmod):
     ref.close()
 
 
+CHECKPOINTS = (6, 25, 50, 100, 200)
+TRAJ_FIELDS = ("heat", "fuel", "oxygen", "soot", "char", "progress", "pressure", "u", "v", "w", "scene_light")
+
+
+def test_trajectory_200_frames_vs_live_reference_128(pkg, abi, refmod):
+    """200 validation frames at 128^3 from a reset: at each checkpoint every
+    field of the product is within max(3 x the reference's own run-to-run
+    spread, 1e-4) relative L2 of the reference's.  The reference's force pass
+    adds with float atomics, so two of its runs drift apart (1e-7 after 6
+    frames, ~1e-2 after 50, O(1) by 150 as the plume turns chaotic); the
+    product, whose force pass is a gather, must drift no faster.  The values
+    are printed (pytest -s)."""
+    fw, fh, n = 256, 192, 128
+
+    def run_ref():
+        ref = refmod.RefFire(abi, fw, fh, n, n, n)
+        snaps = {}
+        for f in range(CHECKPOINTS[-1]):
+            ref.step(_settings(abi, f, fw, fh), mode=2)
+            if f + 1 in CHECKPOINTS:
+                snaps[f + 1] = {name: ref.get(name) for name in TRAJ_FIELDS}
+        ref.close()
+        return snaps
+
+    first, second = run_ref(), run_ref()
+    sim = pkg.FireSim(fw, fh, n, n, n)
+    mine = {}
+    for f in range(CHECKPOINTS[-1]):
+        sim.step(_settings(abi, f, fw, fh))
+        if f + 1 in CHECKPOINTS:
+            mine[f + 1] = {name: sim.get(name) for name in TRAJ_FIELDS}
+    sim.close()
+    worst = 0.0
+    for c in CHECKPOINTS:
+        row = []
+        for name in TRAJ_FIELDS:
+            spread = T.field_stats(first[c][name], second[c][name])["rel_l2"]
+            drift = T.field_stats(mine[c][name], second[c][name])["rel_l2"]
+            bound = max(3.0 * spread, 1e-4)
+            assert drift <= bound, (c, name, drift, spread)
+            worst = max(worst, drift / bound)
+            row.append(f"{name} {drift:.1e}/{spread:.1e}")
+        print(f"frame {c} (product drift / reference spread): " + ", ".join(row))
+    print(f"worst drift / bound: {worst:.2f}")
+
+
 def test_frames_vs_live_reference_128(pkg, abi, refmod):
     fw, fh, n = 256, 192, 128
     ref = refmod.RefFire(abi, fw, fh, n, n, n)
@@ -92,9 +138,11 @@ def test_frames_vs_live_reference_128(pkg, abi, refmod):
         bgra_ref, m_ref = ref.step(s, mode=1)
         bgra, m = sim.step_and_render(s, metrics=True)
         assert list(sim.times()) == pytest.approx(list(ref.times()), abs=0)
+    # Six frames from a reset: within 1e-4 relative L2 on every field (the
+    # reference's own run-to-run spread is ~1e-7 here).
     for name in STATE_FIELDS:
-        tol = T.TRAJECTORY_LIGHT if name == "scene_light" else T.TRAJECTORY
-        T.check_field(f"f5/{name}", sim.get(name), ref.get(name), tol)
+        st = T.field_stats(sim.get(name), ref.get(name))
+        assert st["finite"] and st["rel_l2"] <= 1e-4, (name, st)
     # The reference's render kernel deviates from its own fbm3 (render class
     # SATURATED), so whole frames are compared statistically.
     T.check_field("f5/hdr", sim.get("hdr"), ref.get("hdr"), T.SATURATED)

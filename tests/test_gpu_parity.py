@@ -29,11 +29,13 @@ STAGES = list(STAGE_OUTPUTS)
 # for bit in buildSceneLightKernel, in a standalone probe kernel, and when its
 # octaves are evaluated inline inside renderKernel); the product and the CPU
 # oracle follow the definition.
+# The stages whose arithmetic is all correctly rounded (no sin hash, no atomic
+# order) are the reference's bits; the others keep a statistical class.
 GPU_CLASS = {
-    "advect_velocity": T.GPU_EXACT, "advect_react": T.GPU_NOISE, "force": T.GPU_NOISE,
-    "velocity_boundary": T.GPU_EXACT, "divergence": T.GPU_EXACT, "pressure_sor": T.GPU_EXACT,
-    "subtract": T.GPU_EXACT, "wall_boundary": T.GPU_EXACT, "light_build": T.GPU_NOISE,
-    "light_propagate": T.GPU_EXACT, "render": T.SATURATED, "embers": T.GPU_NOISE, "metrics": T.GPU_EXACT,
+    "advect_velocity": T.BITS, "advect_react": T.GPU_NOISE, "force": T.GPU_NOISE,
+    "velocity_boundary": T.BITS, "divergence": T.BITS, "pressure_sor": T.BITS,
+    "subtract": T.BITS, "wall_boundary": T.BITS, "light_build": T.GPU_NOISE,
+    "light_propagate": T.BITS, "render": T.SATURATED, "embers": T.GPU_NOISE, "metrics": T.GPU_EXACT,
 }
 
 
