@@ -405,6 +405,8 @@ def run_serve(args, pkg, emit: bool = True) -> dict:
     rng = SplitMix64(args.seed)
     server = pkg.Server(budget_bytes=int(args.budget_gb * (1 << 30)), precision=precision)
     server.set_limits(int(args.max_active_mvoxels * 1e6))
+    if args.latency_target_ms > 0:
+        server.set_latency_target(args.latency_target_ms)
     t, n = 0.0, 0
     keep = []
     while True:
@@ -449,7 +451,9 @@ def run_serve(args, pkg, emit: bool = True) -> dict:
                                    + (f"p = 0 on the top face, multigrid until max|r| <= {0.5 * args.div_target:g}; "
                                       if config and args.solver == "mg" else "SOR 40; ")
                                    + "256x256 render (64 samples) every 4 steps; "
-                                   f"HBM budget {args.budget_gb} GB; at most {args.max_active_mvoxels} M active cells; "
+                                   f"HBM budget {args.budget_gb} GB; at most {args.max_active_mvoxels} M active cells"
+                                   + (f", round time target {args.latency_target_ms} ms (batched loop)" if args.latency_target_ms > 0 else "")
+                                   + "; "
                                    f"run bounded at {args.serve_seconds} s",
                        "latency": "device time between a scene's consecutive step completions (events)"}}
     if emit:
@@ -785,6 +789,8 @@ def main() -> int:
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--max-active-mvoxels", type=float, default=24.0,
                     help="serve: admit while the admitted scenes hold at most this many million cells (0 = no limit)")
+    ap.add_argument("--latency-target-ms", type=float, default=6.0,
+                    help="serve (batched loop): admit while the predicted round time stays within this (0 = off)")
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--no-headline", action="store_true",
                     help="single mode: skip the headline block (plain, batched and served at |div u| <= --div-target)")

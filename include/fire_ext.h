@@ -419,6 +419,11 @@ FIRE_API void fireServerDestroy(FireServer* server);
  * so this bounds the round time and with it the step latency.  Requests
  * beyond it wait in arrival order (their wait is queueMs). */
 FIRE_API bool fireServerSetLimits(FireServer* server, long long maxActiveVoxels);
+/* Latency control of the batched loop (see fireServerRun): admit a request
+ * only while the admitted cells times the measured device time per cell of
+ * a round (smoothed over the rounds) stays within roundMs, so a round, and
+ * with it every scene's step, takes about roundMs at most.  0 = off. */
+FIRE_API bool fireServerSetLatencyTarget(FireServer* server, double roundMs);
 
 /* Adds a request; it is admitted no earlier than its arrivalSeconds. */
 FIRE_API bool fireServerSubmit(FireServer* server, const FireServeRequest* request);

@@ -147,24 +147,65 @@ __device__ __forceinline__ float tailLoad(const float* a, int i) {
     }
 }
 
-// `sweeps` red-black sweeps of one tail level.  Each thread walks whole
-// columns (x, y) along z, taking the cells of the colour, so cell
-// coordinates need one division per column.  A level of at most 128 cells is
-// relaxed by the first warp alone, with warp barriers; otherwise by the whole
-// CTA.  The level is passed by value, so its fields stay in registers across
-// the stores to p.
+constexpr int kTailSlots = 4;  // cells per thread of the slot path of tailSmooth
+
+// `sweeps` red-black sweeps of one tail level.  A level of at most 128 cells
+// is relaxed by the first warp alone, with warp barriers; otherwise by the
+// whole CTA.  In shared memory a level of at most kTailSlots cells per
+// thread keeps each thread's cells, their coordinates and their rhs in
+// registers for all the sweeps; a larger one is walked by columns (x, y)
+// along z, one division per column.  The level is passed by value and p and
+// rhs do not alias, so the level's fields and the rhs loads are not reloaded
+// or held back by the stores to p.
 template <bool PG, bool RG>
-__device__ void tailSmooth(float* p, const float* rhs, const MgLevel L, int sweeps) {
+__device__ __noinline__ void tailSmooth(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps) {
     const int cols = L.nx * L.ny;
-    const bool warpOnly = cols * L.nz <= 4 * 32;
+    const int cells = cols * L.nz;
+    const bool warpOnly = cells <= 4 * 32;
     const int stride = warpOnly ? 32 : static_cast<int>(blockDim.x);
     const bool active = !warpOnly || threadIdx.x < 32;
     auto load = [&](int j) { return tailLoad<PG>(p, j); };
+    if (!PG && cells <= kTailSlots * stride) {
+        int packed[kTailSlots];
+        float rh[kTailSlots];
+#pragma unroll
+        for (int k = 0; k < kTailSlots; ++k) {
+            const int i = static_cast<int>(threadIdx.x) + k * stride;
+            packed[k] = -1;
+            rh[k] = 0.0f;
+            if (active && i < cells) {
+                const int x = i % L.nx, y = (i / L.nx) % L.ny, z = i / cols;
+                packed[k] = x | (y << 10) | (z << 20);
+                rh[k] = tailLoad<RG>(rhs, i);
+            }
+        }
+        for (int s = 0; s < sweeps; ++s) {
+            for (int colour = 0; colour < 2; ++colour) {
+#pragma unroll
+                for (int k = 0; k < kTailSlots; ++k) {
+                    const int c = packed[k];
+                    if (c < 0) continue;
+                    const int x = c & 1023, y = (c >> 10) & 1023, z = c >> 20;
+                    if (((x + y + z) & 1) != colour) continue;
+                    const int i = static_cast<int>(threadIdx.x) + k * stride;
+                    p[i] = weightedSum(load, rh[k], L, i, x, y, z, p[i]) * L.invDiag;
+                }
+                if (warpOnly) {
+                    __syncwarp();
+                } else {
+                    __syncthreads();
+                }
+            }
+        }
+        __syncthreads();
+        return;
+    }
     for (int s = 0; s < sweeps; ++s) {
         for (int colour = 0; colour < 2; ++colour) {
             if (active) {
                 for (int col = threadIdx.x; col < cols; col += stride) {
                     const int y = col / L.nx, x = col - y * L.nx;
+#pragma unroll 4
                     for (int z = (colour + x + y) & 1; z < L.nz; z += 2) {
                         const int i = col + z * cols;
                         p[i] = weightedSum(load, tailLoad<RG>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
@@ -230,7 +271,7 @@ __device__ __forceinline__ float prolongAt(LoadC loadC, const MgLevel& F, const 
 // level's p comes from global memory (it is zero there unless the tail is
 // level 0) and goes back to it at the end.
 template <int MODE>
-__device__ void tailCycle(const MgScene& S, int pre, int post, float* smem) {
+__device__ __noinline__ void tailCycle(const MgScene& S, int pre, int post, float* smem) {
     constexpr bool PG = MODE == kMgTailGlobal;
     const int t = S.tail;
     float* p[kMgMaxLevels];

@@ -325,6 +325,55 @@ __device__ __forceinline__ float smoothstepK(float edge0, float edge1, float x) 
     return inverted ? 1.0f - value : value;
 }
 
+// The raymarch's fbm3 (src/fire_cuda.cu:434-443, with valueNoise3 :401-421
+// and hash31 :386-388): three octaves of 3D value noise, written with the
+// reference's plain expressions and compiled as the reference's render
+// compiles them -- one out-of-line function with its value noise and sin
+// hash inlined.  In that form nvcc rounds the sin argument of the eight
+// corner hashes differently from a hash compiled on its own (the form of
+// hash31 in fire_device.cuh, which every other call site matches), and a
+// one-ulp change of that argument scrambles the hash.  Measured on the B200:
+// with this function the raymarch equals the reference's renderKernel bit for
+// bit; with the standalone hash (and with each single rounding form of its
+// argument) it differs in ~13% of pixels.
+namespace {
+
+__device__ __forceinline__ float renderHash31(float3 q) {
+    return fracf(sinf(q.x * 127.1f + q.y * 311.7f + q.z * 74.7f) * 43758.5453123f);
+}
+
+__device__ __forceinline__ float renderValueNoise3(float3 q) {
+    const float3 i = make_float3(floorf(q.x), floorf(q.y), floorf(q.z));
+    const float3 f = make_float3(fracf(q.x), fracf(q.y), fracf(q.z));
+    const float3 u = make_float3(f.x * f.x * (3.0f - 2.0f * f.x), f.y * f.y * (3.0f - 2.0f * f.y), f.z * f.z * (3.0f - 2.0f * f.z));
+    const float c000 = renderHash31(i);
+    const float c100 = renderHash31(make_float3(i.x + 1.0f, i.y, i.z));
+    const float c010 = renderHash31(make_float3(i.x, i.y + 1.0f, i.z));
+    const float c110 = renderHash31(make_float3(i.x + 1.0f, i.y + 1.0f, i.z));
+    const float c001 = renderHash31(make_float3(i.x, i.y, i.z + 1.0f));
+    const float c101 = renderHash31(make_float3(i.x + 1.0f, i.y, i.z + 1.0f));
+    const float c011 = renderHash31(make_float3(i.x, i.y + 1.0f, i.z + 1.0f));
+    const float c111 = renderHash31(make_float3(i.x + 1.0f, i.y + 1.0f, i.z + 1.0f));
+    const float c00 = lerpf(c000, c100, u.x);
+    const float c10 = lerpf(c010, c110, u.x);
+    const float c01 = lerpf(c001, c101, u.x);
+    const float c11 = lerpf(c011, c111, u.x);
+    return lerpf(lerpf(c00, c10, u.y), lerpf(c01, c11, u.y), u.z);
+}
+
+__device__ __noinline__ float renderFbm3(float3 q) {
+    float sum = 0.0f;
+    float amp = 0.5f;
+    for (int octave = 0; octave < 3; ++octave) {
+        sum += amp * renderValueNoise3(q);
+        q = make_float3(q.x * 2.03f + 17.7f, q.y * 2.01f - 9.2f, q.z * 2.07f + 5.1f);
+        amp *= 0.5f;
+    }
+    return saturate(sum * 1.142857f);
+}
+
+}  // namespace
+
 // SC >= 0: the scene id, fixed at compile time (the caller launches this
 // instantiation only for that scene with no debug view); SC < 0: read from p,
 // with the debug views.  Fixing it drops the other scenes' branches and the
@@ -380,8 +429,8 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
                 ++i;
                 continue;
             }
-            const float warpA = fbm3Lattice(fu * 7.0f + p.time * 0.18f, fv * 5.0f - p.time * 0.11f, fw * 9.0f + p.time * 0.07f, lat.warpA) - 0.5f;
-            const float warpB = fbm3Lattice(fw * 8.0f - p.time * 0.14f, fu * 8.0f + p.time * 0.10f, fv * 6.0f - p.time * 0.08f, lat.warpB) - 0.5f;
+            const float warpA = renderFbm3(make_float3(fu * 7.0f + p.time * 0.18f, fv * 5.0f - p.time * 0.11f, fw * 9.0f + p.time * 0.07f)) - 0.5f;
+            const float warpB = renderFbm3(make_float3(fw * 8.0f - p.time * 0.14f, fu * 8.0f + p.time * 0.10f, fv * 6.0f - p.time * 0.08f)) - 0.5f;
             const float warpGain = 0.028f + fv * 0.060f;
             const float wu = saturate(fu + warpA * warpGain);
             const float wv = saturate(fv + (warpA - warpB) * 0.020f);
@@ -411,8 +460,8 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
             const float gradHeatZ = sampleHeat(s, g, wu, wv, ww + cellZ) - sampleHeat(s, g, wu, wv, ww - cellZ);
             const float frontGradient = sqrtf(gradHeatX * gradHeatX + gradHeatY * gradHeatY + gradHeatZ * gradHeatZ) + fabsf(fuel - coarseFuel) * 0.62f;
             const float reactionFront = smoothstepK(0.020f, 0.46f, frontGradient * 1.35f + fuel * oxygen * 0.040f + progress * 0.18f + pyrolysis * 0.080f);
-            const float fineNoise = fbm3Lattice(wu * 42.0f + p.time * 0.72f, wv * 54.0f - p.time * 1.28f, ww * 43.0f + p.time * 0.38f, lat.fine);
-            const float shearNoise = fbm3Lattice(wu * 15.0f - p.time * 0.72f, wv * 13.0f - p.time * 1.08f, ww * 17.0f + p.time * 0.32f, lat.shear);
+            const float fineNoise = renderFbm3(make_float3(wu * 42.0f + p.time * 0.72f, wv * 54.0f - p.time * 1.28f, ww * 43.0f + p.time * 0.38f));
+            const float shearNoise = renderFbm3(make_float3(wu * 15.0f - p.time * 0.72f, wv * 13.0f - p.time * 1.08f, ww * 17.0f + p.time * 0.32f));
             const float plumeNoise = saturate(fineNoise * 0.58f + shearNoise * 0.42f);
             const float holeNoise = saturate((1.0f - fineNoise) * 0.36f + shearNoise * 0.64f);
             const float lesBreakup = saturate(turbulenceEnergy * 0.48f + progress * 0.28f);

@@ -212,6 +212,7 @@ struct FireServer {
     int device = 0;
     size_t budget = 0;
     long long maxActiveVoxels = 0;
+    double latencyTargetMs = 0.0;  // batched loop: admit while the predicted round time stays within it (0 = off)
     std::vector<FireServeRequest> pending;  // sorted by arrival when the run starts
     std::map<Shape, size_t> bytesByShape;   // measured scene + frame bytes
     std::deque<std::unique_ptr<Active>> pool;  // finished scenes, oldest first
@@ -272,6 +273,12 @@ extern "C" void fireServerDestroy(FireServer* server) {
         }
     }
     delete server;
+}
+
+extern "C" bool fireServerSetLatencyTarget(FireServer* server, double roundMs) {
+    if (server == nullptr || !(roundMs >= 0.0)) return fail("fireServerSetLatencyTarget: null server or negative target.");
+    server->latencyTargetMs = roundMs;
+    return true;
 }
 
 extern "C" bool fireServerSetLimits(FireServer* server, long long maxActiveVoxels) {
@@ -394,7 +401,8 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
         EventRef last;  // end of its previous round (its admission for the first)
     };
     struct Round {
-        EventRef done;
+        EventRef start, done;
+        long long voxels = 0;
         std::vector<Live*> members;
         std::vector<char> rendered;
     };
@@ -406,6 +414,7 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
     std::vector<int> render;
     std::vector<double> stepMs, frameMs, queueMs;
     long long activeVoxels = 0;
+    double msPerVoxel = 0.0;  // device time per cell of a round, smoothed over the rounds
     bool ok = true;
     const auto t0 = std::chrono::steady_clock::now();
     auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
@@ -418,6 +427,11 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
             const FireServeRequest& r = waiting.front();
             const long long voxels = static_cast<long long>(r.nx) * r.ny * r.nz;
             if (server->maxActiveVoxels > 0 && !live.empty() && activeVoxels + voxels > server->maxActiveVoxels) break;
+            // Latency target: the rounds' measured device time per cell predicts the round time.
+            if (server->latencyTargetMs > 0.0 && msPerVoxel > 0.0 && !live.empty() &&
+                static_cast<double>(activeVoxels + voxels) * msPerVoxel > server->latencyTargetMs) {
+                break;
+            }
             BatchedSlot* slot = nullptr;
             for (auto& sl : server->slots[shapeOf(r)]) {
                 if (!sl->busy) {
@@ -477,11 +491,13 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
                     }
                     lastMembers = members;
                 }
+                round.start = recordEvent(runner.stream());
                 if (!runner.run(settings.data(), render.data(), err)) {
                     ok = fail("fireServerRun: " + err);
                     break;
                 }
                 round.done = recordEvent(runner.stream());
+                for (Live* l : round.members) round.voxels += static_cast<long long>(l->req.nx) * l->req.ny * l->req.nz;
                 if (!round.done) {
                     ok = fail("fireServerRun: cudaEventRecord failed.");
                     break;
@@ -494,6 +510,11 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
         // Completed rounds, in order.
         while (!rounds.empty() && cudaEventQuery(rounds.front().done.get()) == cudaSuccess) {
             Round& r = rounds.front();
+            float roundMs = 0.0f;
+            if (r.start && cudaEventElapsedTime(&roundMs, r.start.get(), r.done.get()) == cudaSuccess && r.voxels > 0) {
+                const double sample = roundMs / static_cast<double>(r.voxels);
+                msPerVoxel = msPerVoxel > 0.0 ? 0.8 * msPerVoxel + 0.2 * sample : sample;
+            }
             for (size_t i = 0; i < r.members.size(); ++i) {
                 Live& l = *r.members[i];
                 float ms = 0.0f;

@@ -88,6 +88,7 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireServerDestroy": (None, [ctypes.c_void_p]),
         "fireServerSubmit": (b, [ctypes.c_void_p, ctypes.POINTER(abi.FireServeRequest)]),
         "fireServerSetLimits": (b, [ctypes.c_void_p, ctypes.c_longlong]),
+        "fireServerSetLatencyTarget": (b, [ctypes.c_void_p, ctypes.c_double]),
         "fireServerRun": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(abi.FireServeReport)]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaSetAllocationFault": (b, [ctypes.c_longlong]),
@@ -440,6 +441,11 @@ class Server:
         """Admit only while the admitted scenes hold at most this many cells (0 = no limit)."""
         if not self.lib.fireServerSetLimits(self.h, max_active_voxels):
             raise FireSimError(f"fireServerSetLimits: {last_error(self.lib)}")
+
+    def set_latency_target(self, round_ms: float) -> None:
+        """Batched loop: admit while the predicted round time stays within round_ms (0 = off)."""
+        if not self.lib.fireServerSetLatencyTarget(self.h, round_ms):
+            raise FireSimError(f"fireServerSetLatencyTarget: {last_error(self.lib)}")
 
     def submit(self, request) -> None:
         if not self.lib.fireServerSubmit(self.h, ctypes.byref(request)):
