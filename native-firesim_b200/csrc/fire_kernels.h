@@ -214,14 +214,14 @@ struct MgLevel {
 };
 constexpr int kMgMaxLevels = 10;
 constexpr int kMgMaxScenes = 128;     // scenes of one batched solve
-constexpr int kMgTailCells = 32768;   // the tail starts at the first level with at most this many cells
+constexpr int kMgTailCells = 6144;    // the tail starts at the first level with at most this many cells
 constexpr size_t kMgTailSmemMax = 200 * 1024;  // shared memory a tail may use
 // Where a tail keeps its levels: all in shared memory; the tail level's rhs
 // in global memory and the rest in shared memory; all in global memory.
 enum MgTailMode { kMgTailShared = 0, kMgTailRhsGlobal = 1, kMgTailGlobal = 2 };
 constexpr int kMgThreads = 1024;      // threads of a CTA of mgSolve (one CTA per SM)
-constexpr int kMgChunkRows = 4;       // level-0 rows per residual chunk
-constexpr int kMgUnroll = 2;          // 32-cell units a warp of mgSolve has in flight at once
+constexpr int kMgChunkRows = 4;       // level-0 rows per residual chunk (rows whose length is not a multiple of 4)
+constexpr int kMgChunkUnits = 4;      // 128-cell units per residual chunk (rows whose length is a multiple of 4)
 constexpr int kMgCoarsestSweeps = 32;
 constexpr int kMgHardCycleCap = 1000;  // fireCudaSetPressureMultigrid accepts at most this many cycles
 constexpr unsigned kMgMaxPolls = 1u << 26;
@@ -234,18 +234,20 @@ struct MgScene {
     float* rhs[kMgMaxLevels];
     float* pressure;   // += the increment at the end of the solve
     SorGate* gate;     // zeroed before the launch
-    double* chunkSq;   // per residual chunk (kMgChunkRows level-0 rows)
+    double* chunkSq;   // per residual chunk (mgResidualChunks)
     float* chunkMax;
     int levels;        // number of levels
     int tail;          // first level solved by one CTA (the tail)
     int tailMode;      // MgTailMode
 };
 // The work lists of a solve, as prefix sums over the scenes (0 for a scene
-// whose tail starts at or above the level).  smoothUnits counts 128-cell
-// chunks of the rows of grid level l (four cells per lane); fineUnits 32-cell
-// chunks of its rows (the prolongation, a cell per lane); coarseUnits 32-cell
-// chunks of the rows of level l + 1 (the restriction).  chunks counts the residual's chunks of kMgChunkRows level-0
-// rows; allRows all level-0 rows.
+// whose tail starts at or above the level).  smoothUnits and fineUnits count
+// the units of grid level l (the smoothing's and the prolongation's): where
+// the row length is a multiple of 4, 128 consecutive cells in memory, four
+// per lane (mgQuadUnits); otherwise 128-cell (smoothing) or 32-cell
+// (prolongation) chunks of single rows.  coarseUnits counts 32-cell chunks of
+// the rows of level l + 1 (the restriction), chunks the residual's chunks of
+// level 0 (mgResidualChunks), allRows all level-0 rows.
 struct MgPlan {
     int scenes;
     int gridLevels;  // max over the scenes of tail
@@ -261,6 +263,13 @@ struct MgPlan {
 // cells per lane) and 32-cell chunks (the prolongation's and restriction's).
 __host__ __device__ inline int mgQuadChunks(int nx) { return (nx + 127) / 128; }
 __host__ __device__ inline int mgRowChunks(int nx) { return (nx + 31) / 32; }
+// 128-cell units of a level whose row length is a multiple of 4.
+__host__ __device__ inline int mgQuadUnits(int nx, int ny, int nz) { return (nx * ny * nz + 127) / 128; }
+// The level-0 residual's chunks of one scene: kMgChunkUnits quad units, or
+// kMgChunkRows rows where the row length is not a multiple of 4.
+__host__ __device__ inline int mgResidualChunks(int nx, int ny, int nz) {
+    return (nx & 3) == 0 ? (mgQuadUnits(nx, ny, nz) + kMgChunkUnits - 1) / kMgChunkUnits : (ny * nz + kMgChunkRows - 1) / kMgChunkRows;
+}
 // Grid barrier state of mgSolve (zeroed before each launch).
 struct MgSync {
     unsigned count, generation, failed, pad;

@@ -147,76 +147,125 @@ __device__ __forceinline__ float tailLoad(const float* a, int i) {
     }
 }
 
-constexpr int kTailSlots = 4;  // cells per thread of the slot path of tailSmooth
+// A tail level's cells as columns (x, y) along z: with at least as many
+// columns as threads, thread t takes columns t, t + threads, ... whole;
+// otherwise the columns are split along z into `zsplit` groups, thread t
+// taking column t % cols and z group t / cols (every zsplit-th cell of the
+// column, or of its cells of one colour).  Threads past cols * zsplit idle.
+struct TailMap {
+    int col, colStride, zg, zsplit;
+    bool active;
+};
 
-// `sweeps` red-black sweeps of one tail level.  A level of at most 128 cells
-// is relaxed by the first warp alone, with warp barriers; otherwise by the
-// whole CTA.  In shared memory a level of at most kTailSlots cells per
-// thread keeps each thread's cells, their coordinates and their rhs in
-// registers for all the sweeps; a larger one is walked by columns (x, y)
-// along z, one division per column.  The level is passed by value and p and
-// rhs do not alias, so the level's fields and the rhs loads are not reloaded
-// or held back by the stores to p.
-template <bool PG, bool RG>
-__device__ __noinline__ void tailSmooth(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps) {
-    const int cols = L.nx * L.ny;
-    const int cells = cols * L.nz;
-    const bool warpOnly = cells <= 4 * 32;
-    const int stride = warpOnly ? 32 : static_cast<int>(blockDim.x);
-    const bool active = !warpOnly || threadIdx.x < 32;
-    auto load = [&](int j) { return tailLoad<PG>(p, j); };
-    if (!PG && cells <= kTailSlots * stride) {
-        int packed[kTailSlots];
-        float rh[kTailSlots];
-#pragma unroll
-        for (int k = 0; k < kTailSlots; ++k) {
-            const int i = static_cast<int>(threadIdx.x) + k * stride;
-            packed[k] = -1;
-            rh[k] = 0.0f;
-            if (active && i < cells) {
-                const int x = i % L.nx, y = (i / L.nx) % L.ny, z = i / cols;
-                packed[k] = x | (y << 10) | (z << 20);
-                rh[k] = tailLoad<RG>(rhs, i);
-            }
-        }
+__device__ __forceinline__ TailMap tailMap(int cols, int threads) {
+    TailMap m;
+    const int t = static_cast<int>(threadIdx.x);
+    if (cols >= threads) {
+        m.col = t;
+        m.colStride = threads;
+        m.zg = 0;
+        m.zsplit = 1;
+        m.active = t < threads;
+    } else {
+        m.zsplit = threads / cols;
+        m.zg = t / cols;
+        m.col = t - m.zg * cols;
+        m.colStride = cols;
+        m.active = m.zg < m.zsplit;
+    }
+    return m;
+}
+
+// `sweeps` red-black sweeps of a level of at most 32 cells by the first
+// warp, a cell per lane, p in registers: the neighbours' values come by warp
+// shuffles (a Neumann side reads the lane's own value), with the same
+// arithmetic as weightedSum.
+template <bool RG>
+__device__ __forceinline__ void tailSmoothLanes(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps) {
+    if (threadIdx.x < 32) {
+        const int lane = static_cast<int>(threadIdx.x);
+        const int plane = L.nx * L.ny;
+        const bool own = lane < plane * L.nz;
+        const int z = lane / plane, y = (lane - z * plane) / L.nx, x = lane - z * plane - y * L.nx;
+        const int nL = own && x > 0 ? lane - 1 : lane;
+        const int nR = own && x < L.nx - 1 ? lane + 1 : lane;
+        const int nD = own && y > 0 ? lane - L.nx : lane;
+        const int nU = own && y < L.ny - 1 ? lane + L.nx : lane;
+        const int nB = own && z > 0 ? lane - plane : lane;
+        const int nF = own && z < L.nz - 1 ? lane + plane : lane;
+        const bool top = y == L.ny - 1;
+        const int parity = (x + y + z) & 1;
+        const float rh = own ? tailLoad<RG>(rhs, lane) : 0.0f;
+        float v = own ? p[lane] : 0.0f;
         for (int s = 0; s < sweeps; ++s) {
             for (int colour = 0; colour < 2; ++colour) {
-#pragma unroll
-                for (int k = 0; k < kTailSlots; ++k) {
-                    const int c = packed[k];
-                    if (c < 0) continue;
-                    const int x = c & 1023, y = (c >> 10) & 1023, z = c >> 20;
-                    if (((x + y + z) & 1) != colour) continue;
-                    const int i = static_cast<int>(threadIdx.x) + k * stride;
-                    p[i] = weightedSum(load, rh[k], L, i, x, y, z, p[i]) * L.invDiag;
-                }
-                if (warpOnly) {
-                    __syncwarp();
-                } else {
-                    __syncthreads();
-                }
+                const float pL = __shfl_sync(0xffffffffu, v, nL);
+                const float pR = __shfl_sync(0xffffffffu, v, nR);
+                const float pD = __shfl_sync(0xffffffffu, v, nD);
+                const float up = __shfl_sync(0xffffffffu, v, nU);
+                const float pB = __shfl_sync(0xffffffffu, v, nB);
+                const float pF = __shfl_sync(0xffffffffu, v, nF);
+                const float pU = top ? 0.0f - v : up;
+                const float next = combine(rh, pL, pR, pD, pU, pB, pF, L) * L.invDiag;
+                if (own && parity == colour) v = next;
             }
         }
-        __syncthreads();
+        if (own) p[lane] = v;
+    }
+    __syncthreads();
+}
+
+// `sweeps` red-black sweeps of one tail level.  A level of at most 32 cells
+// goes to tailSmoothLanes; one of at most 128 cells is relaxed by the first
+// warp alone, with warp barriers; otherwise by the whole CTA.
+template <bool PG, bool RG>
+__device__ __forceinline__ void tailSmooth(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps) {
+    const int cols = L.nx * L.ny;
+    if (!PG && cols * L.nz <= 32) {
+        tailSmoothLanes<RG>(p, rhs, L, sweeps);
         return;
     }
-    for (int s = 0; s < sweeps; ++s) {
-        for (int colour = 0; colour < 2; ++colour) {
-            if (active) {
-                for (int col = threadIdx.x; col < cols; col += stride) {
-                    const int y = col / L.nx, x = col - y * L.nx;
+    const bool warpOnly = cols * L.nz <= 4 * 32;
+    auto load = [&](int j) { return tailLoad<PG>(p, j); };
+    auto sync = [&]() {
+        if constexpr (PG) __threadfence_block();
+        if (warpOnly) {
+            __syncwarp();
+        } else {
+            __syncthreads();
+        }
+    };
+    if (!warpOnly || threadIdx.x < 32) {
+        const TailMap m = tailMap(cols, warpOnly ? 32 : static_cast<int>(blockDim.x));
+        if (m.colStride >= cols) {
+            // At most one column per thread: its coordinates once.
+            const int y = m.col / L.nx, x = m.col - y * L.nx;
+            const int z0 = 2 * m.zg + ((x + y) & 1), dz = 2 * m.zsplit;
+            for (int s = 0; s < sweeps; ++s) {
+                for (int colour = 0; colour < 2; ++colour) {
+                    if (m.active) {
 #pragma unroll 4
-                    for (int z = (colour + x + y) & 1; z < L.nz; z += 2) {
-                        const int i = col + z * cols;
-                        p[i] = weightedSum(load, tailLoad<RG>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
+                        for (int z = z0 ^ colour; z < L.nz; z += dz) {
+                            const int i = m.col + z * cols;
+                            p[i] = weightedSum(load, tailLoad<RG>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
+                        }
                     }
+                    sync();
                 }
             }
-            if constexpr (PG) __threadfence_block();
-            if (warpOnly) {
-                __syncwarp();
-            } else {
-                __syncthreads();
+        } else {
+            for (int s = 0; s < sweeps; ++s) {
+                for (int colour = 0; colour < 2; ++colour) {
+                    for (int col = m.col; col < cols; col += m.colStride) {
+                        const int y = col / L.nx, x = col - y * L.nx;
+#pragma unroll 4
+                        for (int z = (colour + x + y) & 1; z < L.nz; z += 2) {
+                            const int i = col + z * cols;
+                            p[i] = weightedSum(load, tailLoad<RG>(rhs, i), L, i, x, y, z, load(i)) * L.invDiag;
+                        }
+                    }
+                    sync();
+                }
             }
         }
     }
@@ -229,23 +278,22 @@ template <class Load>
 __device__ __forceinline__ float restrictAt(Load loadP, const float* rhsF, bool rhsViaL2, const MgLevel& F, const MgLevel& C, int X, int Y,
                                            int Z) {
     const int x0 = C.cx ? 2 * X : X, y0 = C.cy ? 2 * Y : Y, z0 = C.cz ? 2 * Z : Z;
-    float az[2] = {0.0f, 0.0f};
-    for (int dz = 0; dz <= C.cz; ++dz) {
-        float ay[2] = {0.0f, 0.0f};
-        for (int dy = 0; dy <= C.cy; ++dy) {
-            float r[2] = {0.0f, 0.0f};
-            for (int dx = 0; dx <= C.cx; ++dx) {
-                const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
-                const int i = mgAt(F, x, y, z);
-                const float self = loadP(i);
-                const float rh = rhsViaL2 ? __ldcg(rhsF + i) : rhsF[i];
-                r[dx] = weightedSum(loadP, rh, F, i, x, y, z, self) - F.diag * self;
-            }
-            ay[dy] = C.cx ? 0.5f * (r[0] + r[1]) : r[0];
-        }
-        az[dz] = C.cy ? 0.5f * (ay[0] + ay[1]) : ay[0];
-    }
-    return C.cz ? 0.5f * (az[0] + az[1]) : az[0];
+    auto residual = [&](int x, int y, int z) {
+        const int i = mgAt(F, x, y, z);
+        const float self = loadP(i);
+        const float rh = rhsViaL2 ? __ldcg(rhsF + i) : rhsF[i];
+        return weightedSum(loadP, rh, F, i, x, y, z, self) - F.diag * self;
+    };
+    auto rowMean = [&](int y, int z) {
+        const float r0 = residual(x0, y, z);
+        return C.cx ? 0.5f * (r0 + residual(x0 + 1, y, z)) : r0;
+    };
+    auto planeMean = [&](int z) {
+        const float a0 = rowMean(y0, z);
+        return C.cy ? 0.5f * (a0 + rowMean(y0 + 1, z)) : a0;
+    };
+    const float b0 = planeMean(z0);
+    return C.cz ? 0.5f * (b0 + planeMean(z0 + 1)) : b0;
 }
 
 // p += the coarse correction interpolated along the halved axes (weights 3/4
@@ -269,92 +317,175 @@ __device__ __forceinline__ float prolongAt(LoadC loadC, const MgLevel& F, const 
 
 // The V-cycle of levels tail..levels-1 of scene S by this CTA.  The tail
 // level's p comes from global memory (it is zero there unless the tail is
-// level 0) and goes back to it at the end.
+// level 0) and goes back to it at the end.  The levels' array addresses are
+// kept in shared memory, so that no per-thread array holds them.
 template <int MODE>
-__device__ __noinline__ void tailCycle(const MgScene& S, int pre, int post, float* smem) {
+__device__ __forceinline__ void tailCycle(const MgScene& S, int pre, int post, float* smem) {
     constexpr bool PG = MODE == kMgTailGlobal;
+    __shared__ float* sP[kMgMaxLevels];
+    __shared__ float* sR[kMgMaxLevels];
     const int t = S.tail;
-    float* p[kMgMaxLevels];
-    float* r[kMgMaxLevels];
-    int off = 0;
-    for (int l = t; l < S.levels; ++l) {
-        const int n = S.lv[l].nx * S.lv[l].ny * S.lv[l].nz;
-        if (PG) {
-            p[l] = S.p[l];
-            r[l] = S.rhs[l];
-        } else {
-            p[l] = smem + off;
-            off += n;
-            if (MODE == kMgTailRhsGlobal && l == t) {
-                r[l] = S.rhs[l];
+    const int last = S.levels - 1;
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int l = t; l <= last; ++l) {
+            const int n = S.lv[l].nx * S.lv[l].ny * S.lv[l].nz;
+            if (PG) {
+                sP[l] = S.p[l];
+                sR[l] = S.rhs[l];
             } else {
-                r[l] = smem + off;
+                sP[l] = smem + off;
                 off += n;
+                if (MODE == kMgTailRhsGlobal && l == t) {
+                    sR[l] = S.rhs[l];
+                } else {
+                    sR[l] = smem + off;
+                    off += n;
+                }
             }
         }
     }
-    const MgLevel T0 = S.lv[t];
-    const int n0 = T0.nx * T0.ny * T0.nz;
-    if constexpr (!PG) {
-        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
-            p[t][i] = __ldcg(S.p[t] + i);
-            if (MODE == kMgTailShared) r[t][i] = __ldcg(S.rhs[t] + i);
-        }
-    }
     __syncthreads();
-    const int last = S.levels - 1;
+    if constexpr (!PG) {
+        const int n0 = S.lv[t].nx * S.lv[t].ny * S.lv[t].nz;
+        float* p0 = sP[t];
+        float* r0 = sR[t];
+        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+            p0[i] = __ldcg(S.p[t] + i);
+            if (MODE == kMgTailShared) r0[i] = __ldcg(S.rhs[t] + i);
+        }
+        __syncthreads();
+    }
+    const int threads = static_cast<int>(blockDim.x);
     for (int l = t; l < last; ++l) {
         const MgLevel F = S.lv[l];
         const MgLevel C = S.lv[l + 1];
         const bool rg = PG || (MODE == kMgTailRhsGlobal && l == t);
+        float* pf = sP[l];
+        const float* rf = sR[l];
         if (rg) {
-            tailSmooth<PG, true>(p[l], r[l], F, pre);
+            tailSmooth<PG, true>(pf, rf, F, pre);
         } else {
-            tailSmooth<PG, false>(p[l], r[l], F, pre);
+            tailSmooth<PG, false>(pf, rf, F, pre);
         }
-        const float* pf = p[l];
         auto loadF = [&](int j) { return tailLoad<PG>(pf, j); };
+        float* pc = sP[l + 1];
+        float* rc = sR[l + 1];
         const int cols = C.nx * C.ny;
-        for (int col = threadIdx.x; col < cols; col += blockDim.x) {
-            const int Y = col / C.nx, X = col - Y * C.nx;
-            for (int Z = 0; Z < C.nz; ++Z) {
-                const int i = col + Z * cols;
-                r[l + 1][i] = restrictAt(loadF, r[l], rg, F, C, X, Y, Z);
-                p[l + 1][i] = 0.0f;
+        const TailMap m = tailMap(cols, threads);
+        if (m.active) {
+            for (int col = m.col; col < cols; col += m.colStride) {
+                const int Y = col / C.nx, X = col - Y * C.nx;
+                for (int Z = m.zg; Z < C.nz; Z += m.zsplit) {
+                    const int i = col + Z * cols;
+                    rc[i] = restrictAt(loadF, rf, rg, F, C, X, Y, Z);
+                    pc[i] = 0.0f;
+                }
             }
         }
         if constexpr (PG) __threadfence_block();
         __syncthreads();
     }
-    if (PG || (MODE == kMgTailRhsGlobal && last == t)) {
-        tailSmooth<PG, true>(p[last], r[last], S.lv[last], kMgCoarsestSweeps);
-    } else {
-        tailSmooth<PG, false>(p[last], r[last], S.lv[last], kMgCoarsestSweeps);
+    {
+        const MgLevel B = S.lv[last];
+        if (PG || (MODE == kMgTailRhsGlobal && last == t)) {
+            tailSmooth<PG, true>(sP[last], sR[last], B, kMgCoarsestSweeps);
+        } else {
+            tailSmooth<PG, false>(sP[last], sR[last], B, kMgCoarsestSweeps);
+        }
     }
     for (int l = last - 1; l >= t; --l) {
         const MgLevel F = S.lv[l];
         const MgLevel C = S.lv[l + 1];
-        const float* pc = p[l + 1];
+        float* pf = sP[l];
+        const float* pc = sP[l + 1];
         auto loadC = [&](int j) { return tailLoad<PG>(pc, j); };
         const int cols = F.nx * F.ny;
-        for (int col = threadIdx.x; col < cols; col += blockDim.x) {
-            const int y = col / F.nx, x = col - y * F.nx;
-            for (int z = 0; z < F.nz; ++z) {
-                const int i = col + z * cols;
-                p[l][i] = tailLoad<PG>(p[l], i) + prolongAt(loadC, F, C, x, y, z);
+        const TailMap m = tailMap(cols, threads);
+        if (m.active) {
+            for (int col = m.col; col < cols; col += m.colStride) {
+                const int y = col / F.nx, x = col - y * F.nx;
+                for (int z = m.zg; z < F.nz; z += m.zsplit) {
+                    const int i = col + z * cols;
+                    pf[i] = tailLoad<PG>(pf, i) + prolongAt(loadC, F, C, x, y, z);
+                }
             }
         }
         if constexpr (PG) __threadfence_block();
         __syncthreads();
         if (PG || (MODE == kMgTailRhsGlobal && l == t)) {
-            tailSmooth<PG, true>(p[l], r[l], F, post);
+            tailSmooth<PG, true>(pf, sR[l], F, post);
         } else {
-            tailSmooth<PG, false>(p[l], r[l], F, post);
+            tailSmooth<PG, false>(pf, sR[l], F, post);
         }
     }
     if constexpr (!PG) {
-        for (int i = threadIdx.x; i < n0; i += blockDim.x) S.p[t][i] = p[t][i];
+        const int n0 = S.lv[t].nx * S.lv[t].ny * S.lv[t].nz;
+        const float* p0 = sP[t];
+        for (int i = threadIdx.x; i < n0; i += blockDim.x) S.p[t][i] = p0[i];
     }
+}
+
+// ---- quads: four consecutive cells of a row, one float4 per lane ----------
+// Used where the row length is a multiple of 4 (rows, and so every quad,
+// start 16-byte aligned).  A lane's edge neighbours (x0 - 1, x0 + 4) come from
+// the lanes beside it by shuffles; lanes 0 and 31 load them.
+
+__device__ __forceinline__ float4 ldcg4(const float* a) { return __ldcg(reinterpret_cast<const float4*>(a)); }
+__device__ __forceinline__ float4 ldg4(const float* a) { return __ldg(reinterpret_cast<const float4*>(a)); }
+__device__ __forceinline__ float at4(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+
+// The operands of a lane's quad: the quad, the quads below, above, behind
+// and in front (the quad itself, or minus it above the top row, where the
+// level has none), the rhs, and the values left and right of the quad.
+struct Quad {
+    float4 c, dn, up, bk, fr, rh;
+    float left, right;
+};
+
+// The cells of a level whose row length is a multiple of 4 are taken in
+// memory order, 128 per warp (a unit), four per lane: the lane's quad starts
+// at flat index i and lies within one row.  quadLoad loads its operands; the
+// values left and right of the quad come from the lanes beside it when they
+// hold the same row (lanes 0 and 31 load them).  Every lane of the warp calls
+// it (the shuffles are warp-wide); a lane past the level's end (live false)
+// gets zeros.
+__device__ __forceinline__ void quadLoad(Quad& q, const float* p, const float* rhs, bool rhsLdg, const MgLevel& L, int i, int x0, int y,
+                                         int z, int lane, bool live) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int plane = L.nx * L.ny;
+    q.c = live ? ldcg4(p + i) : zero;
+    q.dn = live && y > 0 ? ldcg4(p + i - L.nx) : zero;
+    q.up = live && y < L.ny - 1 ? ldcg4(p + i + L.nx) : zero;
+    q.bk = live && z > 0 ? ldcg4(p + i - plane) : zero;
+    q.fr = live && z < L.nz - 1 ? ldcg4(p + i + plane) : zero;
+    q.rh = live ? (rhsLdg ? ldg4(rhs + i) : ldcg4(rhs + i)) : zero;
+    const float eL = lane == 0 && live && x0 > 0 ? __ldcg(p + i - 1) : 0.0f;
+    const float eR = lane == 31 && live && x0 + 4 < L.nx ? __ldcg(p + i + 4) : 0.0f;
+    q.left = __shfl_up_sync(0xffffffffu, q.c.w, 1);
+    q.right = __shfl_down_sync(0xffffffffu, q.c.x, 1);
+    if (lane == 0) q.left = eL;
+    if (lane == 31) q.right = eR;
+}
+
+// weightedSum for cell e of a quad (same boundary rules and order).
+__device__ __forceinline__ float quadSum(const MgLevel& L, const Quad& q, int e, int x, int y, int z) {
+    const float self = at4(q.c, e);
+    const float pL = x > 0 ? (e > 0 ? at4(q.c, e - 1) : q.left) : self;
+    const float pR = x < L.nx - 1 ? (e < 3 ? at4(q.c, e + 1) : q.right) : self;
+    const float pD = y > 0 ? at4(q.dn, e) : self;
+    const float pU = y < L.ny - 1 ? at4(q.up, e) : 0.0f - self;
+    const float pB = z > 0 ? at4(q.bk, e) : self;
+    const float pF = z < L.nz - 1 ? at4(q.fr, e) : self;
+    return combine(at4(q.rh, e), pL, pR, pD, pU, pB, pF, L);
+}
+
+// Coordinates of flat index i of a level.
+__device__ __forceinline__ void flatCoords(const MgLevel& L, int i, int& x, int& y, int& z) {
+    const int row = i / L.nx;
+    x = i - row * L.nx;
+    z = row / L.ny;
+    y = row - z * L.ny;
 }
 
 }  // namespace
@@ -385,17 +516,13 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
         __syncthreads();
     };
     auto converged = [&](int s) { return sRunning[s] == 0; };
-    // Units are processed kMgUnroll at a time per warp, every load of them
-    // issued before any store, so that their L2 round trips overlap.
-    constexpr int U = kMgUnroll;
-
     // One colour of red-black Gauss-Seidel on level l of every scene that has
-    // it as a grid level.  A unit is 128 consecutive cells of a row, four per
-    // lane: the lane loads its four cells and the same four of the rows above,
-    // below, behind and in front (one float4 each when the row length is a
-    // multiple of 4, else element by element), the rhs and the two cells
-    // beside them, updates the two of its cells of the colour and stores the
-    // four back (the other two unchanged: no thread writes them in this phase).
+    // it as a grid level.  Where the row length is a multiple of 4, a unit is
+    // 128 consecutive cells in memory (several short rows, or part of a long
+    // one), four per lane: each lane updates the two of its four cells of the
+    // colour and stores all four (the other two unchanged: no thread writes
+    // them in this phase).  Otherwise a unit is a 128-cell chunk of one row,
+    // taken cell by cell.
     auto smooth = [&](int l, int colour) {
         const int* off = plan->smoothUnits[l];
         const int total = __ldg(off + n);
@@ -405,67 +532,41 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             const MgScene& S = scenes[s];
             const MgLevel L = S.lv[l];
             const int u = unit - __ldg(off + s);
-            const int cpr = mgQuadChunks(L.nx);
-            const int row = u / cpr, chunk = u - row * cpr;
-            const int y = row % L.ny, z = row / L.ny;
-            const int x0 = chunk * 128 + 4 * lane;
-            if (x0 >= L.nx) continue;
             float* p = S.p[l];
             const float* rhs = S.rhs[l];
-            const int i0 = row * L.nx + x0;
-            const int plane = L.nx * L.ny;
-            float c[4], dn[4], up[4], bk[4], fr[4], rh[4];
-            const bool quad = (L.nx & 3) == 0;
-            if (quad) {
-                const float4 v = __ldcg(reinterpret_cast<const float4*>(p + i0));
-                c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
-                const float4 vd = y > 0 ? __ldcg(reinterpret_cast<const float4*>(p + i0 - L.nx)) : v;
-                const float4 vu = y < L.ny - 1 ? __ldcg(reinterpret_cast<const float4*>(p + i0 + L.nx))
-                                               : make_float4(0.0f - v.x, 0.0f - v.y, 0.0f - v.z, 0.0f - v.w);
-                const float4 vb = z > 0 ? __ldcg(reinterpret_cast<const float4*>(p + i0 - plane)) : v;
-                const float4 vf = z < L.nz - 1 ? __ldcg(reinterpret_cast<const float4*>(p + i0 + plane)) : v;
-                const float4 vr = l == 0 ? __ldg(reinterpret_cast<const float4*>(rhs + i0)) : __ldcg(reinterpret_cast<const float4*>(rhs + i0));
-                dn[0] = vd.x; dn[1] = vd.y; dn[2] = vd.z; dn[3] = vd.w;
-                up[0] = vu.x; up[1] = vu.y; up[2] = vu.z; up[3] = vu.w;
-                bk[0] = vb.x; bk[1] = vb.y; bk[2] = vb.z; bk[3] = vb.w;
-                fr[0] = vf.x; fr[1] = vf.y; fr[2] = vf.z; fr[3] = vf.w;
-                rh[0] = vr.x; rh[1] = vr.y; rh[2] = vr.z; rh[3] = vr.w;
-            } else {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int i = i0 + e;
-                    if (x0 + e < L.nx) {
-                        c[e] = __ldcg(p + i);
-                        dn[e] = y > 0 ? __ldcg(p + i - L.nx) : c[e];
-                        up[e] = y < L.ny - 1 ? __ldcg(p + i + L.nx) : 0.0f - c[e];
-                        bk[e] = z > 0 ? __ldcg(p + i - plane) : c[e];
-                        fr[e] = z < L.nz - 1 ? __ldcg(p + i + plane) : c[e];
-                        rh[e] = l == 0 ? __ldg(rhs + i) : __ldcg(rhs + i);
-                    } else {
-                        c[e] = dn[e] = up[e] = bk[e] = fr[e] = rh[e] = 0.0f;
-                    }
+            if ((L.nx & 3) == 0) {
+                const int i = u * 128 + 4 * lane;
+                const bool live = i < L.nx * L.ny * L.nz;
+                int x0, y, z;
+                flatCoords(L, live ? i : 0, x0, y, z);
+                Quad q;
+                quadLoad(q, p, rhs, l == 0, L, i, x0, y, z, lane, live);
+                if (!live) continue;
+                const int e0 = (colour + x0 + y + z) & 1;  // the colour's cells are e0 and e0 + 2
+                const float a = quadSum(L, q, e0, x0 + e0, y, z) * L.invDiag;
+                const float b = quadSum(L, q, e0 + 2, x0 + e0 + 2, y, z) * L.invDiag;
+                float4 o = q.c;
+                if (e0 == 0) {
+                    o.x = a;
+                    o.z = b;
+                } else {
+                    o.y = a;
+                    o.w = b;
                 }
-            }
-            const float left = x0 > 0 ? __ldcg(p + i0 - 1) : 0.0f;
-            const float right = x0 + 4 < L.nx ? __ldcg(p + i0 + 4) : 0.0f;
-            const int e0 = (colour + x0 + y + z) & 1;  // the colour's cells are e0 and e0 + 2
-            float o[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int x = x0 + e;
-                o[e] = c[e];
-                if ((e & 1) != e0 || x >= L.nx) continue;
-                const float self = c[e];
-                const float pL = x > 0 ? (e > 0 ? c[e - 1] : left) : self;
-                const float pR = x < L.nx - 1 ? (e < 3 ? c[e + 1] : right) : self;
-                o[e] = (rh[e] + L.wx * (pL + pR) + L.wy * (dn[e] + up[e]) + L.wz * (bk[e] + fr[e])) * L.invDiag;
-            }
-            if (quad) {
-                *reinterpret_cast<float4*>(p + i0) = make_float4(o[0], o[1], o[2], o[3]);
+                *reinterpret_cast<float4*>(p + i) = o;
             } else {
+                const int cpr = mgQuadChunks(L.nx);
+                const int row = u / cpr, chunk = u - row * cpr;
+                const int y = row % L.ny, z = row / L.ny;
+                const int base = row * L.nx;
+                auto load = [&](int j) { return __ldcg(p + j); };
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    if ((e & 1) == e0 && x0 + e < L.nx) p[i0 + e] = o[e];
+                    const int x = chunk * 128 + 4 * lane + e;
+                    if (x >= L.nx || ((colour + x + y + z) & 1) != 0) continue;
+                    const int i = base + x;
+                    const float rh = l == 0 ? __ldg(rhs + i) : __ldcg(rhs + i);
+                    p[i] = weightedSum(load, rh, L, i, x, y, z, load(i)) * L.invDiag;
                 }
             }
         }
@@ -492,38 +593,86 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             S.p[l + 1][c] = 0.0f;
         }
     };
+    // p += the interpolated coarse correction.  Where the fine row length is
+    // a multiple of 4, units are 128 consecutive fine cells in memory, a quad
+    // per lane: for each of the four coarse rows the quad interpolates from,
+    // the lane loads the coarse values at x0/2 and x0/2 + 1 and takes those
+    // at x0/2 - 1 and x0/2 + 2 from the lanes beside it (clamped at the row's
+    // ends).  Otherwise a unit is a 32-cell chunk of a row, a cell per lane.
     auto prolongFrom = [&](int l) {
         const int* off = plan->fineUnits[l];
         const int total = __ldg(off + n);
-        for (int base = gwarp * U; base < total; base += nwarps * U) {
-            int sc[U], idx[U];
-            float cur[U], add[U];
+        for (int unit = gwarp; unit < total; unit += nwarps) {
+            const int s = sceneOf(off, n, unit);
+            if (converged(s)) continue;
+            const MgScene& S = scenes[s];
+            const MgLevel F = S.lv[l], C = S.lv[l + 1];
+            const int u = unit - __ldg(off + s);
+            float* pf = S.p[l];
+            const float* pc = S.p[l + 1];
+            if ((F.nx & 3) == 0) {
+                const int i = u * 128 + 4 * lane;
+                const bool live = i < F.nx * F.ny * F.nz;
+                int x0, y, z;
+                flatCoords(F, live ? i : 0, x0, y, z);
+                const int Y0 = C.cy ? y >> 1 : y, Z0 = C.cz ? z >> 1 : z;
+                const int Y1 = !C.cy ? Y0 : ((y & 1) ? min(Y0 + 1, C.ny - 1) : max(Y0 - 1, 0));
+                const int Z1 = !C.cz ? Z0 : ((z & 1) ? min(Z0 + 1, C.nz - 1) : max(Z0 - 1, 0));
+                const float4 cur = live ? ldcg4(pf + i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                // v[k][e] = the coarse values at X0 and X1 of fine cell e in
+                // coarse row k: (Y0, Z0), (Y1, Z0), (Y0, Z1), (Y1, Z1).
+                float v[4][4][2];
+                const bool sameRowLeft = lane > 0 && x0 > 0, sameRowRight = lane < 31 && x0 + 4 < F.nx;
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                const int unit = base + k;
-                sc[k] = -1;
-                if (unit >= total) continue;
-                const int s = sceneOf(off, n, unit);
-                if (converged(s)) continue;
-                const MgScene& S = scenes[s];
-                const MgLevel F = S.lv[l], C = S.lv[l + 1];
-                const int u = unit - __ldg(off + s);
+                for (int k = 0; k < 4; ++k) {
+                    const int base = ((k >> 1 ? Z1 : Z0) * C.ny + (k & 1 ? Y1 : Y0)) * C.nx;
+                    if (C.cx) {
+                        const int b = x0 >> 1;  // coarse x of fine x0 and x0 + 1; b + 1 of x0 + 2 and x0 + 3
+                        float2 bc = make_float2(0.0f, 0.0f);
+                        if (live) bc = __ldcg(reinterpret_cast<const float2*>(pc + base + b));
+                        float a = __shfl_up_sync(0xffffffffu, bc.y, 1);    // b - 1
+                        float d = __shfl_down_sync(0xffffffffu, bc.x, 1);  // b + 2
+                        if (!sameRowLeft) a = live && x0 > 0 ? __ldcg(pc + base + b - 1) : bc.x;
+                        if (!sameRowRight) d = live && x0 + 4 < F.nx ? __ldcg(pc + base + b + 2) : bc.y;
+                        v[k][0][0] = bc.x;
+                        v[k][0][1] = a;
+                        v[k][1][0] = bc.x;
+                        v[k][1][1] = bc.y;
+                        v[k][2][0] = bc.y;
+                        v[k][2][1] = bc.x;
+                        v[k][3][0] = bc.y;
+                        v[k][3][1] = d;
+                    } else {
+                        float4 w = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        if (live) w = ldcg4(pc + base + x0);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[k][e][0] = v[k][e][1] = at4(w, e);
+                    }
+                }
+                if (!live) continue;
+                const float ux = C.cx ? 0.75f : 1.0f, vx = C.cx ? 0.25f : 0.0f;
+                const float uy = C.cy ? 0.75f : 1.0f, vy = C.cy ? 0.25f : 0.0f;
+                const float uz = C.cz ? 0.75f : 1.0f, vz = C.cz ? 0.25f : 0.0f;
+                float out[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float a0 = ux * v[0][e][0] + vx * v[0][e][1];
+                    const float a1 = ux * v[1][e][0] + vx * v[1][e][1];
+                    const float a2 = ux * v[2][e][0] + vx * v[2][e][1];
+                    const float a3 = ux * v[3][e][0] + vx * v[3][e][1];
+                    const float b0 = uy * a0 + vy * a1, b1 = uy * a2 + vy * a3;
+                    out[e] = at4(cur, e) + (uz * b0 + vz * b1);
+                }
+                *reinterpret_cast<float4*>(pf + i) = make_float4(out[0], out[1], out[2], out[3]);
+            } else {
                 const int cpr = mgRowChunks(F.nx);
                 const int row = u / cpr, chunk = u - row * cpr;
                 const int y = row % F.ny, z = row / F.ny;
                 const int x = chunk * 32 + lane;
                 if (x >= F.nx) continue;
-                const float* pc = S.p[l + 1];
                 auto loadC = [&](int j) { return __ldcg(pc + j); };
                 const int i = mgAt(F, x, y, z);
-                sc[k] = s;
-                idx[k] = i;
-                cur[k] = __ldcg(S.p[l] + i);
-                add[k] = prolongAt(loadC, F, C, x, y, z);
-            }
-#pragma unroll
-            for (int k = 0; k < U; ++k) {
-                if (sc[k] >= 0) scenes[sc[k]].p[l][idx[k]] = cur[k] + add[k];
+                pf[i] = __ldcg(pf + i) + prolongAt(loadC, F, C, x, y, z);
             }
         }
     };
@@ -575,8 +724,13 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             }
         }
         if (gated) {
-            // Level-0 residual, one warp per chunk of rows (a fixed partition, so
-            // the sums do not depend on the launch shape).
+            // Level-0 residual, one warp per chunk (mgResidualChunk: a fixed
+            // partition of each scene's cells, so the sums do not depend on
+            // the launch shape or the batch).  Where the row length is a
+            // multiple of 4 a chunk is kMgChunkUnits 128-cell units in memory
+            // order, a quad per lane; otherwise kMgChunkRows rows, a cell per
+            // lane.  A lane sums its cells in order, then the warp by a
+            // shuffle tree.
             const int total = __ldg(plan->chunks + n);
             for (int item = gwarp; item < total; item += nwarps) {
                 const int s = sceneOf(plan->chunks, n, item);
@@ -584,24 +738,43 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
                 const MgScene& S = scenes[s];
                 const MgLevel L = S.lv[0];
                 const float* p = S.p[0];
-                auto load = [&](int j) { return __ldcg(p + j); };
+                const float* rhs = S.rhs[0];
                 const int chunk = item - __ldg(plan->chunks + s);
-                const int rows = L.ny * L.nz;
-                // The chunk's cells in order (rows of x), lane-strided; no
-                // stores in the loop, so the unrolled loads overlap.
-                const int first = chunk * kMgChunkRows;
-                const int count = (min(rows, first + kMgChunkRows) - first) * L.nx;
                 double sq = 0.0;
                 float mx = 0.0f;
-#pragma unroll 4
-                for (int j = lane; j < count; j += 32) {
-                    const int row = first + j / L.nx, x = j - (j / L.nx) * L.nx;
-                    const int y = row % L.ny, z = row / L.ny;
-                    const int i = row * L.nx + x;
-                    const float self = __ldcg(p + i);
-                    const float r = weightedSum(load, __ldg(S.rhs[0] + i), L, i, x, y, z, self) - L.diag * self;
+                auto accumulate = [&](float r) {
                     mx = fmaxf(mx, fabsf(r));
                     sq += static_cast<double>(r) * static_cast<double>(r);
+                };
+                if ((L.nx & 3) == 0) {
+                    const int cells = L.nx * L.ny * L.nz;
+#pragma unroll 1
+                    for (int k = 0; k < kMgChunkUnits; ++k) {
+                        const int i = (chunk * kMgChunkUnits + k) * 128 + 4 * lane;
+                        if (i - 4 * lane >= cells) break;
+                        const bool live = i < cells;
+                        int x0, y, z;
+                        flatCoords(L, live ? i : 0, x0, y, z);
+                        Quad q;
+                        quadLoad(q, p, rhs, true, L, i, x0, y, z, lane, live);
+                        if (live) {
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) accumulate(quadSum(L, q, e, x0 + e, y, z) - L.diag * at4(q.c, e));
+                        }
+                    }
+                } else {
+                    auto load = [&](int j) { return __ldcg(p + j); };
+                    const int rows = L.ny * L.nz;
+                    const int first = chunk * kMgChunkRows;
+                    const int count = (min(rows, first + kMgChunkRows) - first) * L.nx;
+#pragma unroll 4
+                    for (int j = lane; j < count; j += 32) {
+                        const int row = first + j / L.nx, x = j - (j / L.nx) * L.nx;
+                        const int y = row % L.ny, z = row / L.ny;
+                        const int i = row * L.nx + x;
+                        const float self = __ldcg(p + i);
+                        accumulate(weightedSum(load, __ldg(rhs + i), L, i, x, y, z, self) - L.diag * self);
+                    }
                 }
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {

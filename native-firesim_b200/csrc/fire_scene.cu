@@ -686,24 +686,9 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
             smem = std::max(smem, (tailFloats - static_cast<size_t>(S.lv[S.tail].nx) * S.lv[S.tail].ny * S.lv[S.tail].nz) * sizeof(float));
         }
     }
-    for (int l = 0; l < kMgMaxLevels; ++l) {
-        for (int s = 0; s < n; ++s) {
-            const MgScene& S = scenes[s];
-            const bool grid = l < S.tail;
-            const MgLevel& F = S.lv[l];
-            plan.smoothUnits[l][s + 1] = plan.smoothUnits[l][s] + (grid ? F.ny * F.nz * mgQuadChunks(F.nx) : 0);
-            plan.fineUnits[l][s + 1] = plan.fineUnits[l][s] + (grid ? F.ny * F.nz * mgRowChunks(F.nx) : 0);
-            if (grid) {
-                const MgLevel& C = S.lv[l + 1];
-                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s] + C.ny * C.nz * mgRowChunks(C.nx);
-            } else {
-                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s];
-            }
-        }
-    }
     for (int s = 0; s < n; ++s) {
         const int rows0 = scenes[s].lv[0].ny * scenes[s].lv[0].nz;
-        plan.chunks[s + 1] = plan.chunks[s] + (rows0 + kMgChunkRows - 1) / kMgChunkRows;
+        plan.chunks[s + 1] = plan.chunks[s] + mgResidualChunks(scenes[s].lv[0].nx, scenes[s].lv[0].ny, scenes[s].lv[0].nz);
         plan.allRows[s + 1] = plan.allRows[s] + rows0;
     }
     std::memcpy(hScenes_, scenes.data(), n * sizeof(MgScene));
@@ -712,6 +697,24 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
     if (e == cudaSuccess && perSm < 1) {
         err = "multigrid: no CTA of the persistent solve fits an SM";
         return false;
+    }
+    for (int l = 0; l < kMgMaxLevels; ++l) {
+        for (int s = 0; s < n; ++s) {
+            const MgScene& S = scenes[s];
+            const bool grid = l < S.tail;
+            const MgLevel& F = S.lv[l];
+            const bool quad = (F.nx & 3) == 0;
+            const int units = quad ? mgQuadUnits(F.nx, F.ny, F.nz) : F.ny * F.nz * mgQuadChunks(F.nx);
+            plan.smoothUnits[l][s + 1] = plan.smoothUnits[l][s] + (grid ? units : 0);
+            const int fine = quad ? mgQuadUnits(F.nx, F.ny, F.nz) : F.ny * F.nz * mgRowChunks(F.nx);
+            plan.fineUnits[l][s + 1] = plan.fineUnits[l][s] + (grid ? fine : 0);
+            if (grid) {
+                const MgLevel& C = S.lv[l + 1];
+                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s] + C.ny * C.nz * mgRowChunks(C.nx);
+            } else {
+                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s];
+            }
+        }
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(dScenes_, hScenes_, n * sizeof(MgScene), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dPlan_, hPlan_, sizeof(MgPlan), cudaMemcpyHostToDevice, stream);
@@ -776,7 +779,7 @@ bool Scene::multigridScene(MgScene& out, std::string& err) {
                 return false;
             }
         }
-        const size_t chunks = (static_cast<size_t>(ny) * nz + kMgChunkRows - 1) / kMgChunkRows;
+        const size_t chunks = static_cast<size_t>(mgResidualChunks(nx, ny, nz));
         if (!alloc(reinterpret_cast<void**>(&mgChunkSq_), chunks * sizeof(double), "cudaMalloc multigrid residual chunks", err) ||
             !alloc(reinterpret_cast<void**>(&mgChunkMax_), chunks * sizeof(float), "cudaMalloc multigrid residual chunks", err)) {
             return false;
