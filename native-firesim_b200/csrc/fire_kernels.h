@@ -235,7 +235,6 @@ struct MgScene {
     float* pressure;   // += the increment at the end of the solve
     SorGate* gate;     // zeroed before the launch
     double* chunkSq;   // per residual chunk (mgResidualChunks)
-    float* chunkMax;
     int levels;        // number of levels
     int tail;          // first level solved by one CTA (the tail)
     int tailMode;      // MgTailMode
@@ -245,9 +244,11 @@ struct MgScene {
 // the units of grid level l (the smoothing's and the prolongation's): where
 // the row length is a multiple of 4, 128 consecutive cells in memory, four
 // per lane (mgQuadUnits); otherwise 128-cell (smoothing) or 32-cell
-// (prolongation) chunks of single rows.  coarseUnits counts 32-cell chunks of
-// the rows of level l + 1 (the restriction), chunks the residual's chunks of
-// level 0 (mgResidualChunks), allRows all level-0 rows.
+// (prolongation) chunks of single rows.  coarseUnits counts the restriction's
+// units of level l + 1: 64 consecutive coarse cells where the fine row length
+// is a multiple of 4, else 32-cell chunks of single rows.  chunks counts the
+// residual's chunks of level 0 (mgResidualChunks), allUnits the units of
+// level 0 as the smoothing takes them (for the first and last phases).
 struct MgPlan {
     int scenes;
     int gridLevels;  // max over the scenes of tail
@@ -257,7 +258,7 @@ struct MgPlan {
     int fineUnits[kMgMaxLevels][kMgMaxScenes + 1];
     int coarseUnits[kMgMaxLevels][kMgMaxScenes + 1];
     int chunks[kMgMaxScenes + 1];
-    int allRows[kMgMaxScenes + 1];
+    int allUnits[kMgMaxScenes + 1];
 };
 // Chunks per row of a level: 128-cell chunks (the smoothing's units, four
 // cells per lane) and 32-cell chunks (the prolongation's and restriction's).
@@ -270,9 +271,13 @@ __host__ __device__ inline int mgQuadUnits(int nx, int ny, int nz) { return (nx 
 __host__ __device__ inline int mgResidualChunks(int nx, int ny, int nz) {
     return (nx & 3) == 0 ? (mgQuadUnits(nx, ny, nz) + kMgChunkUnits - 1) / kMgChunkUnits : (ny * nz + kMgChunkRows - 1) / kMgChunkRows;
 }
-// Grid barrier state of mgSolve (zeroed before each launch).
+// Grid barrier and convergence state of mgSolve (zeroed before each launch):
+// the count of barrier arrivals (barrier k is passed when it reaches
+// k * gridDim.x), a failure flag, and per scene the max |r| of the level-0
+// residual of a cycle (float bits; cycles alternate between the two rows).
 struct MgSync {
-    unsigned count, generation, failed, pad;
+    unsigned count, failed, pad0, pad1;
+    unsigned sceneMax[2][kMgMaxScenes];
 };
 __global__ void mgSolve(const MgScene* scenes, const MgPlan* plan, MgSync* sync, unsigned* hostStatus, unsigned long long waitNs);
 __global__ void cfgPrepareIncrement(FaceT* uOut, FaceT* vOut, FaceT* wOut, Velocity vel, const float* pressure, float* rhs, int nx,

@@ -88,42 +88,44 @@ __device__ __forceinline__ int sceneOf(const int* off, int n, int item) {
     return lo;
 }
 
-// Grid barrier of the persistent solve: the last CTA to arrive resets the
-// count and advances the generation; the others poll the generation.  Every
-// wait gives up after waitNs (or a poll cap), marks the sync failed so the
-// other CTAs stop too, and records the phase in the host-mapped status word.
+// Grid barrier of the persistent solve.  Thread 0 of each CTA adds its
+// arrival to a monotonic count with release semantics (after __syncthreads,
+// so the whole CTA's writes of the phase are published with it) and polls
+// the count with acquire loads until every CTA has arrived at this barrier.
+// Every wait gives up after waitNs (or a poll cap), marks the sync failed so
+// the other CTAs stop too, and records the phase in the host-mapped status
+// word.
+__device__ __forceinline__ unsigned loadAcquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ bool gridBarrier(MgSync* sync, unsigned& generation, unsigned long long waitNs, unsigned* hostStatus, int phase) {
     __syncthreads();
     __shared__ int sFailed;
     if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned target = generation + 1u;
+        const unsigned target = (generation + 1u) * gridDim.x;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&sync->count) : "memory");
         bool failed = false;
-        if (atomicAdd(&sync->count, 1u) == gridDim.x - 1u) {
-            sync->count = 0u;
-            __threadfence();
-            atomicExch(&sync->generation, target);
-        } else {
-            const unsigned long long start = mgTimerNs();
-            for (unsigned n = 0;; ++n) {
-                if (loadVolatileU(&sync->generation) == target) break;
-                if ((n & 7u) == 7u) {
-                    if (loadVolatileU(&sync->failed) != 0u) {
-                        failed = true;
-                        break;
-                    }
-                    if (mgTimerNs() - start > waitNs || n > kMgMaxPolls) {
-                        atomicExch(&sync->failed, 1u);
-                        *reinterpret_cast<volatile unsigned*>(hostStatus) = kMgStatusFlag | static_cast<unsigned>(phase);
-                        __threadfence_system();
-                        failed = true;
-                        break;
-                    }
+        const unsigned long long start = mgTimerNs();
+        for (unsigned n = 0;; ++n) {
+            if (loadAcquire(&sync->count) >= target) break;
+            if ((n & 7u) == 7u) {
+                if (loadVolatileU(&sync->failed) != 0u) {
+                    failed = true;
+                    break;
                 }
-                __nanosleep(32);
+                if (mgTimerNs() - start > waitNs || n > kMgMaxPolls) {
+                    atomicExch(&sync->failed, 1u);
+                    *reinterpret_cast<volatile unsigned*>(hostStatus) = kMgStatusFlag | static_cast<unsigned>(phase);
+                    __threadfence_system();
+                    failed = true;
+                    break;
+                }
             }
+            __nanosleep(20);
         }
-        __threadfence();
         sFailed = (failed || loadVolatileU(&sync->failed) != 0u) ? 1 : 0;
     }
     __syncthreads();
@@ -506,15 +508,20 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
     const int warpsPerBlock = blockDim.x >> 5;
     const int gwarp = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * warpsPerBlock;
-    unsigned generation = loadVolatileU(&sync->generation);
+    unsigned generation = 0;
     int phase = 0;
-    // The scenes still running, read once after each gate (converged flags
-    // change only in the gate phase).
+    // The scenes still running, with the cycles run and the last cycle's max
+    // |r| of each: every CTA keeps the same copy, updated from the per-scene
+    // maxima in sync after each cycle's residual phase (no gate phase).
     __shared__ unsigned char sRunning[kMgMaxScenes];
-    auto refreshRunning = [&]() {
-        for (int s = threadIdx.x; s < n; s += blockDim.x) sRunning[s] = loadVolatileI(&scenes[s].gate->converged) == 0 ? 1 : 0;
-        __syncthreads();
-    };
+    __shared__ int sCycles[kMgMaxScenes];
+    __shared__ float sMax[kMgMaxScenes];
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        sRunning[s] = 1;
+        sCycles[s] = 0;
+        sMax[s] = -1.0f;
+    }
+    __syncthreads();
     auto converged = [&](int s) { return sRunning[s] == 0; };
     // One colour of red-black Gauss-Seidel on level l of every scene that has
     // it as a grid level.  Where the row length is a multiple of 4, a unit is
@@ -571,7 +578,16 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             }
         }
     };
-    auto restrictTo = [&](int l) {
+    // Coarse rhs = the mean residual of the covered fine cells, and coarse p
+    // = 0, or, when `red` (the coarse level is a grid level whose
+    // pre-smoothing starts with the colour-0 half sweep), that half sweep's
+    // result from p = 0: (rhs + 0) / diag on colour-0 cells (every neighbour
+    // sum is +0, so the sweep's arithmetic reduces to this exactly) and 0 on
+    // the others.  Where the fine row length is a multiple of 4, a unit is 64
+    // consecutive coarse cells in memory, two per lane, whose fine quad is
+    // loaded row by row (quadLoad) for each of the fine rows covered;
+    // otherwise a unit is a 32-cell chunk of a coarse row, a cell per lane.
+    auto restrictTo = [&](int l, bool redFirst) {
         const int* off = plan->coarseUnits[l];
         const int total = __ldg(off + n);
         for (int unit = gwarp; unit < total; unit += nwarps) {
@@ -579,18 +595,58 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             if (converged(s)) continue;
             const MgScene& S = scenes[s];
             const MgLevel F = S.lv[l], C = S.lv[l + 1];
+            const bool red = redFirst && l + 1 < S.tail;
             const int u = unit - __ldg(off + s);
-            const int cpr = mgRowChunks(C.nx);
-            const int row = u / cpr, chunk = u - row * cpr;
-            const int Y = row % C.ny, Z = row / C.ny;
-            const int X = chunk * 32 + lane;
-            if (X >= C.nx) continue;
             const float* pf = S.p[l];
-            auto loadF = [&](int j) { return __ldcg(pf + j); };
-            const int c = mgAt(C, X, Y, Z);
-            const float r = restrictAt(loadF, S.rhs[l], l > 0, F, C, X, Y, Z);
-            S.rhs[l + 1][c] = r;
-            S.p[l + 1][c] = 0.0f;
+            const float* rf = S.rhs[l];
+            if ((F.nx & 3) == 0) {
+                const int j = u * 64 + 2 * lane;
+                const bool live = j < C.nx * C.ny * C.nz;
+                int X0, Y, Z;
+                flatCoords(C, live ? j : 0, X0, Y, Z);
+                const int x0 = 2 * X0;
+                float az[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+#pragma unroll
+                for (int dz = 0; dz < 2; ++dz) {
+                    if (dz > C.cz) break;
+                    float ay[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+#pragma unroll
+                    for (int dy = 0; dy < 2; ++dy) {
+                        if (dy > C.cy) break;
+                        const int y = C.cy ? 2 * Y + dy : Y, z = C.cz ? 2 * Z + dz : Z;
+                        const int i = (z * F.ny + y) * F.nx + x0;
+                        Quad q;
+                        quadLoad(q, pf, rf, l == 0, F, i, x0, y, z, lane, live);
+                        float r[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) r[e] = quadSum(F, q, e, x0 + e, y, z) - F.diag * at4(q.c, e);
+                        ay[dy][0] = 0.5f * (r[0] + r[1]);
+                        ay[dy][1] = 0.5f * (r[2] + r[3]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) az[dz][k] = C.cy ? 0.5f * (ay[0][k] + ay[1][k]) : ay[0][k];
+                }
+                if (!live) continue;
+                float rc[2], pc[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    rc[k] = C.cz ? 0.5f * (az[0][k] + az[1][k]) : az[0][k];
+                    pc[k] = red && ((X0 + k + Y + Z) & 1) == 0 ? (rc[k] + 0.0f) * C.invDiag : 0.0f;
+                }
+                *reinterpret_cast<float2*>(S.rhs[l + 1] + j) = make_float2(rc[0], rc[1]);
+                *reinterpret_cast<float2*>(S.p[l + 1] + j) = make_float2(pc[0], pc[1]);
+            } else {
+                const int cpr = mgRowChunks(C.nx);
+                const int row = u / cpr, chunk = u - row * cpr;
+                const int Y = row % C.ny, Z = row / C.ny;
+                const int X = chunk * 32 + lane;
+                if (X >= C.nx) continue;
+                auto loadF = [&](int k) { return __ldcg(pf + k); };
+                const int c = mgAt(C, X, Y, Z);
+                const float r = restrictAt(loadF, rf, l > 0, F, C, X, Y, Z);
+                S.rhs[l + 1][c] = r;
+                S.p[l + 1][c] = red && ((X + Y + Z) & 1) == 0 ? (r + 0.0f) * C.invDiag : 0.0f;
+            }
         }
     };
     // p += the interpolated coarse correction.  Where the fine row length is
@@ -677,28 +733,63 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
         }
     };
 
-    // Every scene starts unconverged with no cycles run, from a zero increment.
-    for (int s = gwarp; s < n; s += nwarps) {
-        if (lane == 0) *scenes[s].gate = SorGate{0, 0, 0.0f, 0, 0.0};
-    }
+    // Every scene starts from a zero increment.  With pre-smoothing, the
+    // first cycle's colour-0 half sweep of level 0 is done here, as in
+    // restrictTo: (rhs + 0) / diag on colour-0 cells, 0 elsewhere (scenes
+    // whose level 0 is in the tail start from 0).  Units as the smoothing's.
+    const bool redFirst = pre > 0;
     {
-        const int total = __ldg(plan->allRows + n);
-        for (int item = gwarp; item < total; item += nwarps) {
-            const int s = sceneOf(plan->allRows, n, item);
+        const int total = __ldg(plan->allUnits + n);
+        for (int unit = gwarp; unit < total; unit += nwarps) {
+            const int s = sceneOf(plan->allUnits, n, unit);
             const MgScene& S = scenes[s];
-            const int base = (item - __ldg(plan->allRows + s)) * S.lv[0].nx;
-            for (int x = lane; x < S.lv[0].nx; x += 32) S.p[0][base + x] = 0.0f;
+            const MgLevel L = S.lv[0];
+            const int u = unit - __ldg(plan->allUnits + s);
+            const bool red = redFirst && S.tail > 0;
+            float* p = S.p[0];
+            const float* rhs = S.rhs[0];
+            if ((L.nx & 3) == 0) {
+                const int i = u * 128 + 4 * lane;
+                if (i >= L.nx * L.ny * L.nz) continue;
+                int x0, y, z;
+                flatCoords(L, i, x0, y, z);
+                float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (red) {
+                    const float4 r = ldg4(rhs + i);
+                    const int e0 = (x0 + y + z) & 1;  // colour-0 cells: e0 and e0 + 2
+                    if (e0 == 0) {
+                        o.x = (r.x + 0.0f) * L.invDiag;
+                        o.z = (r.z + 0.0f) * L.invDiag;
+                    } else {
+                        o.y = (r.y + 0.0f) * L.invDiag;
+                        o.w = (r.w + 0.0f) * L.invDiag;
+                    }
+                }
+                *reinterpret_cast<float4*>(p + i) = o;
+            } else {
+                const int cpr = mgQuadChunks(L.nx);
+                const int row = u / cpr, chunk = u - row * cpr;
+                const int y = row % L.ny, z = row / L.ny;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int x = chunk * 128 + 4 * lane + e;
+                    if (x >= L.nx) continue;
+                    const int i = row * L.nx + x;
+                    p[i] = red && ((x + y + z) & 1) == 0 ? (__ldg(rhs + i) + 0.0f) * L.invDiag : 0.0f;
+                }
+            }
         }
     }
     if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
-    refreshRunning();
     for (int cycle = 0; cycle < maxCycles; ++cycle) {
         for (int l = 0; l < gridLevels; ++l) {
-            for (int k = 0; k < 2 * pre; ++k) {
+            // The colour-0 half sweep of a coarse level, and of level 0 in the
+            // first cycle, was done with the restriction (the initialisation).
+            for (int k = redFirst && (l > 0 || cycle == 0) ? 1 : 0; k < 2 * pre; ++k) {
                 smooth(l, k & 1);
                 if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
             }
-            restrictTo(l);
+            restrictTo(l, redFirst);
             if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
         }
         for (int s = blockIdx.x; s < n; s += gridDim.x) {
@@ -783,42 +874,27 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
                 }
                 if (lane == 0) {
                     S.chunkSq[chunk] = sq;
-                    S.chunkMax[chunk] = mx;
+                    atomicMax(&sync->sceneMax[cycle & 1][s], __float_as_uint(mx));  // mx >= 0: its bits order as the value
                 }
+            }
+            // The other row of per-scene maxima, last read after the previous
+            // cycle's residual (several barriers ago), is cleared for the next.
+            if (blockIdx.x == 0) {
+                for (int s = threadIdx.x; s < n; s += blockDim.x) sync->sceneMax[(cycle + 1) & 1][s] = 0u;
             }
             if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
         }
-        // Gate: one warp per scene that was still running this cycle.
-        for (int s = gwarp; s < n; s += nwarps) {
-            if (converged(s)) continue;
-            const MgScene& S = scenes[s];
+        // Convergence, the same in every CTA: a scene still running has run
+        // this cycle; with a tolerance, it stops once its max |r| is within it.
+        for (int s = threadIdx.x; s < n; s += blockDim.x) {
+            if (!sRunning[s]) continue;
+            sCycles[s] = cycle + 1;
             if (gated) {
-                const int first = __ldg(plan->chunks + s), count = __ldg(plan->chunks + s + 1) - first;
-                double sq = 0.0;
-                float mx = 0.0f;
-                for (int c = lane; c < count; c += 32) {
-                    sq += __ldcg(S.chunkSq + c);
-                    mx = fmaxf(mx, __ldcg(S.chunkMax + c));
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    sq += __shfl_xor_sync(0xffffffffu, sq, o);
-                    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                }
-                if (lane == 0) {
-                    S.gate->maxResidual = mx;
-                    S.gate->l2Residual = sqrt(sq);
-                    S.gate->iterations = cycle + 1;
-                    if (mx <= tolerance) S.gate->converged = 1;
-                }
-            } else if (lane == 0) {
-                S.gate->maxResidual = -1.0f;
-                S.gate->l2Residual = -1.0;
-                S.gate->iterations = cycle + 1;
+                const float m = __uint_as_float(__ldcg(&sync->sceneMax[cycle & 1][s]));
+                sMax[s] = m;
+                if (m <= tolerance) sRunning[s] = 0;
             }
         }
-        if (!gridBarrier(sync, generation, waitNs, hostStatus, ++phase)) return;
-        refreshRunning();
         if (threadIdx.x == 0) sActive = 0;
         __syncthreads();
         for (int s = threadIdx.x; s < n; s += blockDim.x) {
@@ -827,15 +903,59 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
         __syncthreads();
         if (sActive == 0) break;
     }
-    // pressure += delta on every cell of every scene.
-    const int total = __ldg(plan->allRows + n);
-    for (int item = gwarp; item < total; item += nwarps) {
-        const int s = sceneOf(plan->allRows, n, item);
+    // Each scene's gate, by CTA s % gridDim.x: the cycles run, the last
+    // cycle's max |r| and sqrt(sum r^2) of its chunks (summed in a fixed
+    // order: thread t takes chunks t, t + blockDim.x, ..., then shuffle trees
+    // over each warp and over the warps).
+    __shared__ double sSum[kMgThreads / 32];
+    for (int s = blockIdx.x; s < n; s += gridDim.x) {
+        const MgScene& S = scenes[s];
+        double sq = 0.0;
+        if (gated) {
+            const int first = __ldg(plan->chunks + s), count = __ldg(plan->chunks + s + 1) - first;
+            for (int c = threadIdx.x; c < count; c += blockDim.x) sq += __ldcg(S.chunkSq + c);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if (lane == 0) sSum[threadIdx.x >> 5] = sq;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            sq = static_cast<int>(threadIdx.x) < warpsPerBlock ? sSum[threadIdx.x] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+            if (threadIdx.x == 0) {
+                S.gate->iterations = sCycles[s];
+                S.gate->maxResidual = gated ? sMax[s] : -1.0f;
+                S.gate->l2Residual = gated ? sqrt(sq) : -1.0;
+                S.gate->converged = gated && sMax[s] >= 0.0f && sMax[s] <= tolerance ? 1 : 0;
+            }
+        }
+        __syncthreads();
+    }
+    // pressure += delta on every cell of every scene (units as the smoothing's).
+    const int total = __ldg(plan->allUnits + n);
+    for (int unit = gwarp; unit < total; unit += nwarps) {
+        const int s = sceneOf(plan->allUnits, n, unit);
         const MgScene& S = scenes[s];
         const MgLevel L = S.lv[0];
-        const int row = item - __ldg(plan->allRows + s);
-        const int base = row * L.nx;
-        for (int x = lane; x < L.nx; x += 32) S.pressure[base + x] = S.pressure[base + x] + __ldcg(S.p[0] + base + x);
+        const int u = unit - __ldg(plan->allUnits + s);
+        if ((L.nx & 3) == 0) {
+            const int i = u * 128 + 4 * lane;
+            if (i >= L.nx * L.ny * L.nz) continue;
+            const float4 p = *reinterpret_cast<const float4*>(S.pressure + i);
+            const float4 d = ldcg4(S.p[0] + i);
+            *reinterpret_cast<float4*>(S.pressure + i) = make_float4(p.x + d.x, p.y + d.y, p.z + d.z, p.w + d.w);
+        } else {
+            const int cpr = mgQuadChunks(L.nx);
+            const int row = u / cpr, chunk = u - row * cpr;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int x = chunk * 128 + 4 * lane + e;
+                if (x >= L.nx) continue;
+                const int i = row * L.nx + x;
+                S.pressure[i] = S.pressure[i] + __ldcg(S.p[0] + i);
+            }
+        }
     }
 }
 

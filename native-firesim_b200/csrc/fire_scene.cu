@@ -93,9 +93,7 @@ void Scene::release() {
         if (b != nullptr) cudaFree(b);
     }
     if (mgChunkSq_ != nullptr) cudaFree(mgChunkSq_);
-    if (mgChunkMax_ != nullptr) cudaFree(mgChunkMax_);
     mgChunkSq_ = nullptr;
-    mgChunkMax_ = nullptr;
     mgP_.clear();
     mgRhs_.clear();
     mgLevels_.clear();
@@ -689,7 +687,8 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
     for (int s = 0; s < n; ++s) {
         const int rows0 = scenes[s].lv[0].ny * scenes[s].lv[0].nz;
         plan.chunks[s + 1] = plan.chunks[s] + mgResidualChunks(scenes[s].lv[0].nx, scenes[s].lv[0].ny, scenes[s].lv[0].nz);
-        plan.allRows[s + 1] = plan.allRows[s] + rows0;
+        const MgLevel& L0 = scenes[s].lv[0];
+        plan.allUnits[s + 1] = plan.allUnits[s] + ((L0.nx & 3) == 0 ? mgQuadUnits(L0.nx, L0.ny, L0.nz) : rows0 * mgQuadChunks(L0.nx));
     }
     std::memcpy(hScenes_, scenes.data(), n * sizeof(MgScene));
     int perSm = 0;
@@ -710,7 +709,8 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
             plan.fineUnits[l][s + 1] = plan.fineUnits[l][s] + (grid ? fine : 0);
             if (grid) {
                 const MgLevel& C = S.lv[l + 1];
-                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s] + C.ny * C.nz * mgRowChunks(C.nx);
+                const int coarse = quad ? (C.nx * C.ny * C.nz + 63) / 64 : C.ny * C.nz * mgRowChunks(C.nx);
+                plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s] + coarse;
             } else {
                 plan.coarseUnits[l][s + 1] = plan.coarseUnits[l][s];
             }
@@ -780,8 +780,7 @@ bool Scene::multigridScene(MgScene& out, std::string& err) {
             }
         }
         const size_t chunks = static_cast<size_t>(mgResidualChunks(nx, ny, nz));
-        if (!alloc(reinterpret_cast<void**>(&mgChunkSq_), chunks * sizeof(double), "cudaMalloc multigrid residual chunks", err) ||
-            !alloc(reinterpret_cast<void**>(&mgChunkMax_), chunks * sizeof(float), "cudaMalloc multigrid residual chunks", err)) {
+        if (!alloc(reinterpret_cast<void**>(&mgChunkSq_), chunks * sizeof(double), "cudaMalloc multigrid residual chunks", err)) {
             return false;
         }
     }
@@ -803,7 +802,6 @@ bool Scene::multigridScene(MgScene& out, std::string& err) {
     S.pressure = pressure_;
     S.gate = sorGate_;
     S.chunkSq = mgChunkSq_;
-    S.chunkMax = mgChunkMax_;
     out = S;
     return true;
 }

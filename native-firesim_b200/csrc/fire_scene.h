@@ -236,7 +236,6 @@ private:
     std::vector<MgLevel> mgLevels_;
     std::vector<float*> mgP_, mgRhs_;  // mgRhs_[0] is unused (divergence_)
     double* mgChunkSq_ = nullptr;
-    float* mgChunkMax_ = nullptr;
     bool mgDeltaValid_ = false;        // mgP_[0] holds the latest solve's increment (the subtraction takes it)
     MgSolver mgSolver_;
     int mgKeyCycles_ = -1, mgKeyPre_ = -1, mgKeyPost_ = -1;
