@@ -343,68 +343,6 @@ __device__ __forceinline__ float fbmLattice(float px, float py, const HashLattic
     return sum;
 }
 
-// --- hash lattices of 3D fbm3 call sites --------------------------------------
-// The same idea for fbm3 (three octaves of 3D value noise): a HashLattice3
-// holds hash31 at every lattice point one call site can reach in this frame,
-// per octave, and fbm3Lattice(px, py, pz, L) equals fbm3(px, py, pz) exactly.
-constexpr int kFbm3Octaves = 3;
-struct HashLattice3 {
-    const float* values;  // octave o: sx[o] * sy[o] * sz[o] values at offset[o], x fastest
-    int ox[kFbm3Octaves], oy[kFbm3Octaves], oz[kFbm3Octaves];
-    int sx[kFbm3Octaves], sy[kFbm3Octaves], sz[kFbm3Octaves];
-    int offset[kFbm3Octaves];
-};
-
-static __device__ __noinline__ float hash31OutOfLine(float x, float y, float z) { return hash31(x, y, z); }
-
-__device__ __forceinline__ float fbm3Lattice(float px, float py, float pz, const HashLattice3& L) {
-    float sum = 0.0f;
-    float amp = 0.5f;
-#pragma unroll 1
-    for (int i = 0; i < kFbm3Octaves; ++i) {
-        const float ix = floorf(px), iy = floorf(py), iz = floorf(pz);
-        const float ux = smoothWeight(fracf(px)), uy = smoothWeight(fracf(py)), uz = smoothWeight(fracf(pz));
-        const int sx = L.sx[i], sy = L.sy[i];
-        const int tx = static_cast<int>(ix) - L.ox[i];
-        const int ty = static_cast<int>(iy) - L.oy[i];
-        const int tz = static_cast<int>(iz) - L.oz[i];
-        float h000, h100, h010, h110, h001, h101, h011, h111;
-        if (L.values != nullptr && tx >= 0 && tx < sx - 1 && ty >= 0 && ty < sy - 1 && tz >= 0 && tz < L.sz[i] - 1) {
-            const float* q = L.values + L.offset[i] + (tz * sy + ty) * sx + tx;
-            const int plane = sx * sy;
-            h000 = __ldg(q);
-            h100 = __ldg(q + 1);
-            h010 = __ldg(q + sx);
-            h110 = __ldg(q + sx + 1);
-            h001 = __ldg(q + plane);
-            h101 = __ldg(q + plane + 1);
-            h011 = __ldg(q + plane + sx);
-            h111 = __ldg(q + plane + sx + 1);
-        } else {
-            const float jx = ix + 1.0f, jy = iy + 1.0f, jz = iz + 1.0f;
-            h000 = hash31OutOfLine(ix, iy, iz);
-            h100 = hash31OutOfLine(jx, iy, iz);
-            h010 = hash31OutOfLine(ix, jy, iz);
-            h110 = hash31OutOfLine(jx, jy, iz);
-            h001 = hash31OutOfLine(ix, iy, jz);
-            h101 = hash31OutOfLine(jx, iy, jz);
-            h011 = hash31OutOfLine(ix, jy, jz);
-            h111 = hash31OutOfLine(jx, jy, jz);
-        }
-        sum = __fmaf_rn(amp, valueNoise3FromCorners(h000, h100, h010, h110, h001, h101, h011, h111, ux, uy, uz), sum);
-        px = __fmaf_rn(px, 2.03f, 17.7f);
-        py = __fmaf_rn(py, 2.01f, -9.2f);
-        pz = __fmaf_rn(pz, 2.07f, 5.1f);
-        amp *= 0.5f;
-    }
-    return saturate(sum * 1.142857f);
-}
-
-// The four fbm3 fields of the raymarch (src/fire_cuda.cu:2025-2026, :2067-2068).
-struct RenderLattices {
-    HashLattice3 warpA, warpB, fine, shear;
-};
-
 // --- lattice sampling -------------------------------------------------------
 // Trilinear corner set of a sample in normalized coordinates on a lattice whose
 // largest node index per axis is (ex, ey, ez) (src/fire_cuda.cu:489-600):

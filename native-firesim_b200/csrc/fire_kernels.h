@@ -124,16 +124,14 @@ struct RayTiles {
     int tilesX;
     int count;
 };
-__global__ void hashLattice3Build(RenderLattices lat);
-__global__ void raymarch(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p, RayTiles tiles,
-                         RenderLattices lat);
+__global__ void raymarch(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p, RayTiles tiles);
 // The same for one scene id (0, 1, 2) fixed at compile time, without a debug view.
 __global__ void raymarchScene0(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p,
-                               RayTiles tiles, RenderLattices lat);
+                               RayTiles tiles);
 __global__ void raymarchScene1(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p,
-                               RayTiles tiles, RenderLattices lat);
+                               RayTiles tiles);
 __global__ void raymarchScene2(float4* out, ScalarFieldsIn s, Velocity vel, const float4* lightF, const float* shadowF, FrameParams p,
-                               RayTiles tiles, RenderLattices lat);
+                               RayTiles tiles);
 __global__ void emberSetup(EmberSplat* embers, ScalarFieldsIn s, Velocity vel, FrameParams p);
 __global__ void emberGather(float4* hdr, const EmberSplat* embers, FrameParams p);
 __global__ void tonemapOverlay(uint32_t* frame, const float4* hdr, FrameParams p, int doTonemap, int doOverlay);

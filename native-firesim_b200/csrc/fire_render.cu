@@ -380,8 +380,7 @@ __device__ __noinline__ float renderFbm3(float3 q) {
 // debug views' per-sample maxima from the sample loop.
 template <int SC>
 __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int y, const ScalarFieldsIn& s, const Velocity& vel,
-                                           const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
-                                           const RenderLattices& lat) {
+                                           const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p) {
     const Grid g{p.nx, p.ny, p.nz};
     const LightGrid L{p.lnx, p.lny, p.lnz};
     const float2 uv = make_float2((static_cast<float>(x) + 0.5f) / static_cast<float>(p.frameW),
@@ -650,25 +649,6 @@ __device__ __forceinline__ void shadePixel(float4* __restrict__ out, int x, int 
 
 }  // namespace
 
-// hash31 at every entry of the raymarch's four fbm3 lattices of this frame
-// (blockIdx.y selects the lattice); the same function as the in-place hash.
-__global__ void __launch_bounds__(256) hashLattice3Build(RenderLattices lat) {
-    const HashLattice3& L = blockIdx.y == 0 ? lat.warpA : (blockIdx.y == 1 ? lat.warpB : (blockIdx.y == 2 ? lat.fine : lat.shear));
-    float* out = const_cast<float*>(L.values);
-    if (out == nullptr) return;
-    constexpr int last = kFbm3Octaves - 1;
-    const int total = L.offset[last] + L.sx[last] * L.sy[last] * L.sz[last];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        int o = 0;
-        while (o + 1 < kFbm3Octaves && i >= L.offset[o + 1]) ++o;
-        const int local = i - L.offset[o];
-        const int tx = local % L.sx[o];
-        const int ty = (local / L.sx[o]) % L.sy[o];
-        const int tz = local / (L.sx[o] * L.sy[o]);
-        out[i] = hash31(static_cast<float>(L.ox[o] + tx), static_cast<float>(L.oy[o] + ty), static_cast<float>(L.oz[o] + tz));
-    }
-}
-
 // Rays through the flame cost many times more than rays that miss it, so a
 // static grid leaves most SMs idle while the last blocks finish.  Here every
 // warp repeatedly takes the next 8x4-pixel tile from a counter, in an order
@@ -680,7 +660,7 @@ __global__ void __launch_bounds__(256) hashLattice3Build(RenderLattices lat) {
 template <int SC>
 __device__ __forceinline__ void raymarchBody(float4* __restrict__ out, const ScalarFieldsIn& s, const Velocity& vel,
                                              const float4* __restrict__ lightF, const float* __restrict__ shadowF, const FrameParams& p,
-                                             const RayTiles& tiles, const RenderLattices& lat) {
+                                             const RayTiles& tiles) {
     const int lane = threadIdx.x & 31;
     for (;;) {
         int t = 0;
@@ -695,7 +675,7 @@ __device__ __forceinline__ void raymarchBody(float4* __restrict__ out, const Sca
         const int x = (tile % tiles.tilesX) * kRayTileW + (lane % kRayTileW);
         const int y = (tile / tiles.tilesX) * kRayTileH + (lane / kRayTileW);
         if (x < p.frameW && y < p.frameH) {
-            shadePixel<SC>(out, x, y, s, vel, lightF, shadowF, p, lat);
+            shadePixel<SC>(out, x, y, s, vel, lightF, shadowF, p);
         }
     }
 }
@@ -703,24 +683,24 @@ __device__ __forceinline__ void raymarchBody(float4* __restrict__ out, const Sca
 // Any scene and debug mode.
 __global__ void __launch_bounds__(128, 4) raymarch(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                    const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
-                                                   RayTiles tiles, RenderLattices lat) {
-    raymarchBody<-1>(out, s, vel, lightF, shadowF, p, tiles, lat);
+                                                   RayTiles tiles) {
+    raymarchBody<-1>(out, s, vel, lightF, shadowF, p, tiles);
 }
 // Scenes 0, 1, 2 without a debug view (renderDebugMode 0).
 __global__ void __launch_bounds__(128, 4) raymarchScene0(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
-                                                         RayTiles tiles, RenderLattices lat) {
-    raymarchBody<0>(out, s, vel, lightF, shadowF, p, tiles, lat);
+                                                         RayTiles tiles) {
+    raymarchBody<0>(out, s, vel, lightF, shadowF, p, tiles);
 }
 __global__ void __launch_bounds__(128, 4) raymarchScene1(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
-                                                         RayTiles tiles, RenderLattices lat) {
-    raymarchBody<1>(out, s, vel, lightF, shadowF, p, tiles, lat);
+                                                         RayTiles tiles) {
+    raymarchBody<1>(out, s, vel, lightF, shadowF, p, tiles);
 }
 __global__ void __launch_bounds__(128, 4) raymarchScene2(float4* __restrict__ out, ScalarFieldsIn s, Velocity vel,
                                                          const float4* __restrict__ lightF, const float* __restrict__ shadowF, FrameParams p,
-                                                         RayTiles tiles, RenderLattices lat) {
-    raymarchBody<2>(out, s, vel, lightF, shadowF, p, tiles, lat);
+                                                         RayTiles tiles) {
+    raymarchBody<2>(out, s, vel, lightF, shadowF, p, tiles);
 }
 
 // ---------------------------------------------------------------------------

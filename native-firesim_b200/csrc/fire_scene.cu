@@ -101,7 +101,7 @@ void Scene::release() {
     void* bufs[] = {sa_[0], sa_[1], sb_[0], sb_[1], sc_[0], sc_[1], vel_[0][0], vel_[0][1], vel_[1][0], vel_[1][1], vel_[2][0],
                     vel_[2][1], pressure_, divergence_, divergenceAfter_, contrib_, material_, breathing_, light_, lightNext_,
                     shadow_, hdr_, bgra_, embers_, partials_, metricDevice_, sorStatus_, sorExchange_, curlLattice_, sourceLattice_,
-                    rayTileOrder_, rayTileCounter_, renderLattice_, sorGate_, residualSq_, residualMax_, split_, splitDiv_,
+                    rayTileOrder_, rayTileCounter_, sorGate_, residualSq_, residualMax_, split_, splitDiv_,
                     cfgVort_, cfgLight_, cfgNoise_};
     for (void* b : bufs) {
         if (b != nullptr) cudaFree(b);
@@ -112,7 +112,6 @@ void Scene::release() {
     sorExchange_ = nullptr;
     rayTileOrder_ = nullptr;
     rayTileCounter_ = nullptr;
-    renderLattice_ = nullptr;
     sorGate_ = nullptr;
     residualSq_ = nullptr;
     residualMax_ = nullptr;
@@ -253,19 +252,6 @@ bool Scene::init(int dev, int fw, int fh, int x, int y, int z, std::string& err)
         sourceCapacity_ =
             static_cast<size_t>(src.offset[kFbmOctaves - 1] + (src.sx[kFbmOctaves - 1] + 1) * (src.sy[kFbmOctaves - 1] + 1)) + 4096;
         ok = ok && alloc(reinterpret_cast<void**>(&sourceLattice_), sourceCapacity_ * sizeof(float), "cudaMalloc source lattice", err);
-        RenderLattices rl;
-        for (size_t& c : renderCapacity_) c = 1u << 30;
-        renderLattices(p0, rl);
-        const HashLattice3* sites[4] = {&rl.warpA, &rl.warpB, &rl.fine, &rl.shear};
-        size_t total = 0;
-        for (int i = 0; i < 4; ++i) {
-            const HashLattice3& l = *sites[i];
-            constexpr int last = kFbm3Octaves - 1;
-            renderCapacity_[i] = static_cast<size_t>(l.offset[last]) +
-                                 static_cast<size_t>(l.sx[last] + 1) * (l.sy[last] + 1) * (l.sz[last] + 1) + 4096;
-            total += renderCapacity_[i];
-        }
-        ok = ok && alloc(reinterpret_cast<void**>(&renderLattice_), total * sizeof(float), "cudaMalloc render lattices", err);
     }
     for (int i = 0; i < 9 && ok; ++i) {
         ok = check("cudaEventCreate", cudaEventCreate(&events_[i]), err);
@@ -888,66 +874,6 @@ bool Scene::sourceLattice(const FrameParams& p, HashLattice2& l) const {
     return fits;
 }
 
-namespace {
-
-// Lattice of one fbm3 call site whose octave-0 inputs lie in the box
-// lo[0..2] .. hi[0..2]; later octaves map the box through the octave step
-// (x * 2.03 + 17.7, y * 2.01 - 9.2, z * 2.07 + 5.1, src/fire_cuda.cu:434-443),
-// widened by one lattice cell per octave for rounding.
-int planLattice3(double lo[3], double hi[3], HashLattice3& L) {
-    const double scale[3] = {2.03, 2.01, 2.07}, shift[3] = {17.7, -9.2, 5.1};
-    int offset = 0;
-    for (int o = 0; o < kFbm3Octaves; ++o) {
-        int* origin[3] = {L.ox, L.oy, L.oz};
-        int* size[3] = {L.sx, L.sy, L.sz};
-        int count = 1;
-        for (int a = 0; a < 3; ++a) {
-            origin[a][o] = static_cast<int>(std::floor(lo[a])) - 2;
-            size[a][o] = static_cast<int>(std::floor(hi[a])) - origin[a][o] + 4;
-            count *= size[a][o];
-            lo[a] = lo[a] * scale[a] + shift[a] - 1.0;
-            hi[a] = hi[a] * scale[a] + shift[a] + 1.0;
-        }
-        L.offset[o] = offset;
-        offset += count;
-    }
-    return offset;
-}
-
-}  // namespace
-
-// The raymarch's fbm3 fields hash, per sample at (u, v, w) in [0, 1]^3 (the
-// domain-warped coordinates for the last two):
-//   warpA (u * 7 + t * 0.18, v * 5 - t * 0.11, w * 9 + t * 0.07)
-//   warpB (w * 8 - t * 0.14, u * 8 + t * 0.10, v * 6 - t * 0.08)
-//   fine  (u * 42 + t * 0.72, v * 54 - t * 1.28, w * 43 + t * 0.38)
-//   shear (u * 15 - t * 0.72, v * 13 - t * 1.08, w * 17 + t * 0.32)   (src/fire_cuda.cu:2025-2068)
-bool Scene::renderLattices(const FrameParams& p, RenderLattices& lat) const {
-    const double t = p.time;
-    const double ranges[4][3][2] = {
-        {{0.18 * t, 7.0 + 0.18 * t}, {-0.11 * t, 5.0 - 0.11 * t}, {0.07 * t, 9.0 + 0.07 * t}},
-        {{-0.14 * t, 8.0 - 0.14 * t}, {0.10 * t, 8.0 + 0.10 * t}, {-0.08 * t, 6.0 - 0.08 * t}},
-        {{0.72 * t, 42.0 + 0.72 * t}, {-1.28 * t, 54.0 - 1.28 * t}, {0.38 * t, 43.0 + 0.38 * t}},
-        {{-0.72 * t, 15.0 - 0.72 * t}, {-1.08 * t, 13.0 - 1.08 * t}, {0.32 * t, 17.0 + 0.32 * t}},
-    };
-    HashLattice3* sites[4] = {&lat.warpA, &lat.warpB, &lat.fine, &lat.shear};
-    bool fits = latticesEnabled_ && renderLattice_ != nullptr;
-    size_t base = 0;
-    for (int i = 0; i < 4; ++i) {
-        double lo[3], hi[3];
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = ranges[i][a][0] - 1.0;
-            hi[a] = ranges[i][a][1] + 1.0;
-        }
-        const int n = planLattice3(lo, hi, *sites[i]);
-        const bool siteFits = fits && static_cast<size_t>(n) <= renderCapacity_[i];
-        sites[i]->values = siteFits ? renderLattice_ + base : nullptr;
-        fits = fits && siteFits;
-        base += renderCapacity_[i];
-    }
-    return fits;
-}
-
 bool Scene::runStages(int first, int last, const FrameParams& p, std::string& err) {
     if (first < 0 || last > kReset || first > last) {
         err = "stage range out of order";
@@ -1032,16 +958,13 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
             }
             case kRender:
             {
-                RenderLattices lat{};
-                renderLattices(p, lat);
-                hashLattice3Build<<<dim3(512, 4), 256, 0, stream>>>(lat); ++launches_;
                 if (!check("clear ray tile counter", cudaMemsetAsync(rayTileCounter_, 0, sizeof(int), stream), err)) return false;
                 // Scenes 0-2 without a debug view take the instantiation with
                 // the scene id fixed; the generic kernel draws the debug views.
                 const int k = p.renderDebugMode == 0 && p.sceneId >= 0 && p.sceneId <= 2 ? 1 + p.sceneId : 0;
                 const RayTiles tiles{rayTileCounter_, rayTileOrder_, rayTilesX_, rayTileCount_};
                 auto kernel = k == 1 ? raymarchScene0 : (k == 2 ? raymarchScene1 : (k == 3 ? raymarchScene2 : raymarch));
-                kernel<<<rayBlocks_[k], 128, 0, stream>>>(hdr_, scalarsIn(), velocity(), light_, shadow_, p, tiles, lat); ++launches_;
+                kernel<<<rayBlocks_[k], 128, 0, stream>>>(hdr_, scalarsIn(), velocity(), light_, shadow_, p, tiles); ++launches_;
             }
                 s = kEmbers;
                 break;

@@ -191,10 +191,6 @@ private:
     bool sourceLattice(const FrameParams& p, HashLattice2& l) const;
     float* sourceLattice_ = nullptr;
     size_t sourceCapacity_ = 0;
-    // hash31 lattices of the raymarch's four fbm3 fields.
-    bool renderLattices(const FrameParams& p, RenderLattices& lat) const;
-    float* renderLattice_ = nullptr;
-    size_t renderCapacity_[4] = {0, 0, 0, 0};
     // Raymarch work list: tile order (centre first) and the tile counter.
     int* rayTileOrder_ = nullptr;
     int* rayTileCounter_ = nullptr;

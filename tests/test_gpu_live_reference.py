@@ -143,11 +143,12 @@ def test_frames_vs_live_reference_128(pkg, abi, refmod):
     for name in STATE_FIELDS:
         st = T.field_stats(sim.get(name), ref.get(name))
         assert st["finite"] and st["rel_l2"] <= 1e-4, (name, st)
-    # The reference's render kernel deviates from its own fbm3 (render class
-    # SATURATED), so whole frames are compared statistically.
-    T.check_field("f5/hdr", sim.get("hdr"), ref.get("hdr"), T.SATURATED)
+    # The raymarch matches the reference's render kernel to float rounding
+    # (HDR relative L2 ~1e-8 measured); the 8-bit frame may differ by one
+    # step where a value sits on a rounding boundary.
+    T.check_field("f5/hdr", sim.get("hdr"), ref.get("hdr"), T.GPU_EXACT)
     d = np.abs(T.bgra_channels(bgra) - T.bgra_channels(bgra_ref))
-    assert float(d.mean()) <= 1.0 and float(np.mean(np.any(d > 8, axis=-1))) <= 0.05, (float(d.mean()), float(np.mean(np.any(d > 8, axis=-1))))
+    assert float(d.max()) <= 1.0 and float(np.mean(np.any(d > 0, axis=-1))) <= 1e-3, (float(d.max()), float(np.mean(np.any(d > 0, axis=-1))))
     got, want = m.as_dict(), m_ref.as_dict()
     for k in ("frameIndex", "gridX", "gridY", "gridZ", "pressureIterations", "invalidCells"):
         assert got[k] == want[k], k
