@@ -139,7 +139,8 @@ bool BatchRunner::run(const FireSettings* settings, const int* render, std::stri
             return false;
         }
         for (int sp = 0; sp < kBatchSpaces; ++sp) {
-            plan->start[sp][i + 1] = plan->start[sp][i] + (desc[i].count[sp] + kBatchThreads - 1) / kBatchThreads;
+            const int perBlock = kBatchThreads * batchPerThread(sp);
+            plan->start[sp][i + 1] = plan->start[sp][i] + (desc[i].count[sp] + perBlock - 1) / perBlock;
         }
     }
     cudaStream_t s = stream_;

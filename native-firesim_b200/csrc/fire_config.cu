@@ -579,12 +579,48 @@ __device__ __forceinline__ int batchSceneOf(const int* start, int n) {
     return lo;
 }
 
-// This thread's scene and element of index space `space`; false past the end.
-__device__ __forceinline__ bool batchElement(const BatchScene* scenes, const BatchPlan* plan, int space, int& s, int& i) {
+// This thread's batchPerThread(space) elements of index space `space`, in
+// rows of w elements and planes of h rows: body(B, i, x, y, z) for each.  A
+// block takes kBatchThreads * K consecutive elements and thread t the
+// elements t, t + kBatchThreads, ... of them (so that every pass of the
+// block is coalesced); the scene lookup and the division of the first index
+// into coordinates happen once per thread, later coordinates step from it.
+template <int SPACE, class Dims, class Body>
+__device__ __forceinline__ void batchForEach(const BatchScene* scenes, const BatchPlan* plan, Dims dims, Body body) {
+    constexpr int K = batchPerThread(SPACE);
     const int n = plan->scenes;
-    s = batchSceneOf(plan->start[space], n);
-    i = (static_cast<int>(blockIdx.x) - __ldg(plan->start[space] + s)) * kBatchThreads + static_cast<int>(threadIdx.x);
-    return i < scenes[s].count[space];
+    const int s = batchSceneOf(plan->start[SPACE], n);
+    const BatchScene& B = scenes[s];
+    const int count = B.count[SPACE];
+    const int first = (static_cast<int>(blockIdx.x) - __ldg(plan->start[SPACE] + s)) * kBatchThreads * K + static_cast<int>(threadIdx.x);
+    if (first >= count) return;
+    int w, h;
+    dims(B, w, h);
+    const int row = first / w;
+    int x = first - row * w, y = row % h, z = row / h;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int i = first + k * kBatchThreads;
+        if (i >= count) break;
+        body(B, i, x, y, z);
+        x += kBatchThreads;
+        while (x >= w) {
+            x -= w;
+            if (++y == h) {
+                y = 0;
+                ++z;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void cellDims(const BatchScene& B, int& w, int& h) {
+    w = B.c.nx;
+    h = B.c.ny;
+}
+__device__ __forceinline__ void faceDims(const BatchScene& B, int& w, int& h) {
+    w = B.c.nx + 1;
+    h = B.c.ny + 1;
 }
 
 __device__ __forceinline__ Velocity velocityOf(FaceT* const (&f)[3]) { return Velocity{f[0], f[1], f[2]}; }
@@ -592,82 +628,82 @@ __device__ __forceinline__ Velocity velocityOf(FaceT* const (&f)[3]) { return Ve
 }  // namespace
 
 __global__ void __launch_bounds__(kBatchThreads) batchAdvectVelocity(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchFaces, s, i)) return;
-    const BatchScene& B = scenes[s];
-    const int mx = B.c.nx + 1, my = B.c.ny + 1;
-    cfgAdvectVelocityAt(B.adv[0], B.adv[1], B.adv[2], B.vel, B.c, i % mx, (i / mx) % my, i / (mx * my));
+    batchForEach<kBatchFaces>(scenes, plan, faceDims, [](const BatchScene& B, int, int x, int y, int z) {
+        cfgAdvectVelocityAt(B.adv[0], B.adv[1], B.adv[2], B.vel, B.c, x, y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchAdvectScalars(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
-    const BatchScene& B = scenes[s];
-    cfgAdvectScalarsAt(B.aOut, B.aIn, velocityOf(B.adv), B.c, i % B.c.nx, (i / B.c.nx) % B.c.ny, i / (B.c.nx * B.c.ny));
+    batchForEach<kBatchCells>(scenes, plan, cellDims, [](const BatchScene& B, int, int x, int y, int z) {
+        cfgAdvectScalarsAt(B.aOut, B.aIn, velocityOf(B.adv), B.c, x, y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchVorticity(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
-    const BatchScene& B = scenes[s];
-    if (B.c.eps == 0.0f) return;
-    cfgVorticityAt(B.vort, velocityOf(B.adv), B.c, i % B.c.nx, (i / B.c.nx) % B.c.ny, i / (B.c.nx * B.c.ny));
+    batchForEach<kBatchCells>(scenes, plan, cellDims, [](const BatchScene& B, int, int x, int y, int z) {
+        if (B.c.eps == 0.0f) return;
+        cfgVorticityAt(B.vort, velocityOf(B.adv), B.c, x, y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchCellForce(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
-    const BatchScene& B = scenes[s];
-    cfgCellForceAt(B.force, B.vort, B.aOut, B.noise, B.c, i % B.c.nx, (i / B.c.nx) % B.c.ny, i / (B.c.nx * B.c.ny));
+    batchForEach<kBatchCells>(scenes, plan, cellDims, [](const BatchScene& B, int, int x, int y, int z) {
+        cfgCellForceAt(B.force, B.vort, B.aOut, B.noise, B.c, x, y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchApplyForces(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchFaces, s, i)) return;
-    const BatchScene& B = scenes[s];
-    const int mx = B.c.nx + 1, my = B.c.ny + 1;
-    cfgApplyForcesAt(B.forced[0], B.forced[1], B.forced[2], velocityOf(B.adv), B.force, B.c, i % mx, (i / mx) % my, i / (mx * my));
+    batchForEach<kBatchFaces>(scenes, plan, faceDims, [](const BatchScene& B, int, int x, int y, int z) {
+        cfgApplyForcesAt(B.forced[0], B.forced[1], B.forced[2], velocityOf(B.adv), B.force, B.c, x, y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchPrepareIncrement(const BatchScene* __restrict__ scenes,
                                                                       const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
-    const BatchScene& B = scenes[s];
-    const int nx = B.c.nx, ny = B.c.ny, nz = B.c.nz;
-    cfgPrepareIncrementAt(B.proj[0], B.proj[1], B.proj[2], velocityOf(B.forced), B.pressure, B.divergence, nx, ny, nz, i % nx,
-                          (i / nx) % ny, i / (nx * ny));
+    batchForEach<kBatchCells>(scenes, plan, cellDims, [](const BatchScene& B, int, int x, int y, int z) {
+        cfgPrepareIncrementAt(B.proj[0], B.proj[1], B.proj[2], velocityOf(B.forced), B.pressure, B.divergence, B.c.nx, B.c.ny, B.c.nz, x,
+                              y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchSubtractIncrement(const BatchScene* __restrict__ scenes,
                                                                        const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchCells, s, i)) return;
-    const BatchScene& B = scenes[s];
-    const int nx = B.c.nx, ny = B.c.ny, nz = B.c.nz;
-    cfgSubtractIncrementAt(B.proj[0], B.proj[1], B.proj[2], B.delta, nx, ny, nz, 1, i % nx, (i / nx) % ny, i / (nx * ny));
+    batchForEach<kBatchCells>(scenes, plan, cellDims, [](const BatchScene& B, int, int x, int y, int z) {
+        cfgSubtractIncrementAt(B.proj[0], B.proj[1], B.proj[2], B.delta, B.c.nx, B.c.ny, B.c.nz, 1, x, y, z);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchTransmittance(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchLight, s, i)) return;
-    const BatchScene& B = scenes[s];
-    cfgTransmittanceAt(B.transmittance, B.aOut, B.c, i % B.c.lx, (i / B.c.lx) % B.c.ly, i / (B.c.lx * B.c.ly));
+    batchForEach<kBatchLight>(
+        scenes, plan,
+        [](const BatchScene& B, int& w, int& h) {
+            w = B.c.lx;
+            h = B.c.ly;
+        },
+        [](const BatchScene& B, int, int x, int y, int z) { cfgTransmittanceAt(B.transmittance, B.aOut, B.c, x, y, z); });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchRaymarch(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchPixels, s, i)) return;
-    const BatchScene& B = scenes[s];
-    cfgRaymarchAt(B.hdr, B.aOut, B.transmittance, B.c, i % B.c.frameW, i / B.c.frameW);
+    batchForEach<kBatchPixels>(
+        scenes, plan,
+        [](const BatchScene& B, int& w, int& h) {
+            w = B.c.frameW;
+            h = B.c.frameH;
+        },
+        [](const BatchScene& B, int, int x, int y, int) { cfgRaymarchAt(B.hdr, B.aOut, B.transmittance, B.c, x, y); });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batchPackHdr(const BatchScene* __restrict__ scenes, const BatchPlan* __restrict__ plan) {
-    int s, i;
-    if (!batchElement(scenes, plan, kBatchPixels, s, i)) return;
-    const BatchScene& B = scenes[s];
-    if (B.slot == nullptr) return;
-    packHdrPixel(B.slot, B.slotPitch, B.slotFormat, B.hdr[i], i % B.c.frameW, i / B.c.frameW);
+    batchForEach<kBatchPixels>(
+        scenes, plan,
+        [](const BatchScene& B, int& w, int& h) {
+            w = B.c.frameW;
+            h = B.c.frameH;
+        },
+        [](const BatchScene& B, int i, int x, int y, int) {
+            if (B.slot == nullptr) return;
+            packHdrPixel(B.slot, B.slotPitch, B.slotFormat, B.hdr[i], x, y);
+        });
 }
 
 }  // namespace firesim

@@ -292,6 +292,10 @@ __global__ void cfgTopFaces(FaceT* v, const float* p, int nx, int ny, int nz);
 // a scene gives the same bits alone or in a batch.
 enum BatchSpace { kBatchCells = 0, kBatchFaces = 1, kBatchLight = 2, kBatchPixels = 3, kBatchSpaces = 4 };
 constexpr int kBatchThreads = 128;
+// Elements per thread of a batched stage: runs of consecutive cells or faces
+// (one scene lookup and one coordinate division per run); one light column or
+// pixel per thread.
+__host__ __device__ constexpr int batchPerThread(int space) { return space == kBatchCells || space == kBatchFaces ? 4 : 1; }
 constexpr int kBatchMaxScenes = kMgMaxScenes;
 struct BatchScene {
     ConfigParams c;        // this step's parameters (c.step: the emitters' jitter counter)
@@ -316,7 +320,8 @@ struct BatchScene {
 };
 struct BatchPlan {
     int scenes;
-    int start[kBatchSpaces][kBatchMaxScenes + 1];  // prefix sums of the blocks of each scene (0 for a scene that does not render)
+    int start[kBatchSpaces][kBatchMaxScenes + 1];  // prefix sums of the blocks of each scene (0 for a scene that does not render);
+                                                   // a block takes kBatchThreads * batchPerThread(space) elements
 };
 __global__ void batchAdvectVelocity(const BatchScene* scenes, const BatchPlan* plan);
 __global__ void batchAdvectScalars(const BatchScene* scenes, const BatchPlan* plan);
