@@ -414,7 +414,7 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
     std::vector<int> render;
     std::vector<double> stepMs, frameMs, queueMs;
     long long activeVoxels = 0;
-    double msPerVoxel = 0.0;  // device time per cell of a round, smoothed over the rounds
+    double msPerVoxel = 0.0;  // device time per cell of a round: a decaying peak over the rounds
     bool ok = true;
     const auto t0 = std::chrono::steady_clock::now();
     auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
@@ -512,8 +512,11 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
             Round& r = rounds.front();
             float roundMs = 0.0f;
             if (r.start && cudaEventElapsedTime(&roundMs, r.start.get(), r.done.get()) == cudaSuccess && r.voxels > 0) {
+                // A decaying peak of the rounds' time per cell, so that the
+                // admission plans for the dearer rounds (renders, more
+                // multigrid cycles) rather than the mean.
                 const double sample = roundMs / static_cast<double>(r.voxels);
-                msPerVoxel = msPerVoxel > 0.0 ? 0.8 * msPerVoxel + 0.2 * sample : sample;
+                msPerVoxel = std::max(sample, 0.97 * msPerVoxel);
             }
             for (size_t i = 0; i < r.members.size(); ++i) {
                 Live& l = *r.members[i];
