@@ -939,7 +939,8 @@ def main() -> int:
         per_step_ms["render"] = render_in_region_ms / args.render_every
     dominant = max((k for k in per_step_ms if k != "render_end_state"), key=per_step_ms.get)
     peaks, peak_src = measured_peaks()
-    roofline = roofline_block(dominant, st, args, cells, peaks, peak_src, sim.pressure_path_used())
+    roofline = roofline_block(dominant, st, args, cells, peaks, peak_src, sim.pressure_path_used(),
+                              clocks.get("sm_mhz") if isinstance(clocks, dict) else None)
 
     divergence = divergence_after(pkg, lib, sim, workload_settings(abi, frame, args), args.frame, args.frame)
     sim.close()
@@ -978,9 +979,15 @@ def ctypes_sizeof_settings(abi) -> int:
 # (profiles/sor_split_256cubed_halfsweep.md: 4.72 TB/s x 23.42 us).
 NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): 30157312 + 1525760,
                      ("pressure_sor", "split", 256, 60): 110542400}
+# Shared-memory wavefronts of one resident solve (l1tex__data_pipe_lsu_wavefronts_mem_shared.sum
+# from one ncu capture of sorResident<32,16,16>, profiles/sor_resident_128cubed_sor60.md): the
+# resident solve lives in shared memory, so its roofline is the shared-memory pipe, one
+# wavefront per clock per SM.
+NCU_SMEM_WAVEFRONTS = {("pressure_sor", "resident", 128, 60): 50.3e6}
 
 
-def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str, sor_path: int) -> dict:
+def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str, sor_path: int,
+                   sm_mhz: float | None = None) -> dict:
     """achieved = algorithmic bytes of one launch / that launch's device time.
 
     The pressure solve's algorithmic bytes are those of the global-memory
@@ -1003,9 +1010,19 @@ def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_
         bytes_per_launch = 40.0 * cells + 16.0 * args.frame * args.frame
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
-    return {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-            "bytes_per_launch": bytes_per_launch, "launch_ms": per_launch_ms}
+    out = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+           "bytes_per_launch": bytes_per_launch, "launch_ms": per_launch_ms}
+    if dominant == "pressure_sor" and sor_path == 2:
+        wavefronts = NCU_SMEM_WAVEFRONTS.get(("pressure_sor", "resident", args.grid, args.sor_iters))
+        if wavefronts is not None:
+            mhz = sm_mhz if sm_mhz else 1965.0
+            per_clock = wavefronts / (per_launch_ms * 1e-3 * mhz * 1e6 * 148)
+            out["smem"] = {"achieved": per_clock, "peak": 1.0, "unit": "wavefronts/clock/SM", "frac": per_clock,
+                           "wavefronts_per_launch": wavefronts, "sm_mhz": mhz,
+                           "note": "the resident solve's data stay in shared memory (DRAM traffic per launch is the "
+                                   "'traffic' figure); its bound is the shared-memory pipe; wavefronts from one ncu capture"}
+    return out
 
 
 if __name__ == "__main__":

@@ -136,6 +136,20 @@ FIRE_API bool fireCudaSetPressureTolerance(double maxResidual, int checkEvery);
  * for the scene's stream); after a fixed-count solve: the count and -1. */
 FIRE_API bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Residual);
 
+/* Autotuner of the shared-memory-resident SOR's brick shape (no counterpart
+ * in the reference, which has no resident solve).  When both 32x16x16 and
+ * 16x16x16 bricks fit co-resident, the first resident solve of a grid times
+ * one solve with each, from the same pressure (the results are the same
+ * bits), and keeps the faster for that grid and device for the life of the
+ * process; later scenes of the grid reuse the choice.  On by default; off,
+ * the fixed rule picks (32x16x16 when it gives every SM a brick).
+ * Process-wide; needs no scene. */
+FIRE_API bool fireCudaSetAutotune(int enabled);
+/* The autotuner's record for an nx x ny x nz grid on the current device:
+ * *brickX = 32 or 16 (the brick kept) and the measured time of one solve
+ * with each; false when the grid has not been timed. */
+FIRE_API bool fireCudaGetTunedBrick(int nx, int ny, int nz, int* brickX, float* msBrick32, float* msBrick16);
+
 /* Path the latest pressure solve took: 0 = none yet (or no grid),
  * 1 = colour-split SOR, 2 = shared-memory-resident SOR, 3 = multigrid. */
 FIRE_API int fireCudaGetPressurePathUsed(void);

@@ -9,6 +9,6 @@ tests, benchmarks and Python callers; it performs no computation itself.
 from __future__ import annotations
 
 from . import abi  # noqa: F401
-from .firesim import Batch, FireSim, FireSimError, Scene, Server, batch_step, load_library  # noqa: F401
+from .firesim import Batch, FireSim, FireSimError, Scene, Server, batch_step, load_library, set_autotune, tuned_brick  # noqa: F401
 
-__all__ = ["abi", "Batch", "FireSim", "FireSimError", "Scene", "Server", "batch_step", "load_library"]
+__all__ = ["abi", "Batch", "FireSim", "FireSimError", "Scene", "Server", "batch_step", "load_library", "set_autotune", "tuned_brick"]

@@ -256,6 +256,24 @@ bool fireCudaGetPressureStats(int* iterations, float* maxResidual, double* l2Res
 
 int fireCudaGetPressurePathUsed(void) { return g_scene ? g_scene->lastPressurePath() : 0; }
 
+bool fireCudaSetAutotune(int enabled) {
+    firesim::setAutotune(enabled != 0);
+    return true;
+}
+
+bool fireCudaGetTunedBrick(int nx, int ny, int nz, int* brickX, float* msBrick32, float* msBrick16) {
+    if (brickX == nullptr || msBrick32 == nullptr || msBrick16 == nullptr) return fail("fireCudaGetTunedBrick: null output");
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail("fireCudaGetTunedBrick: no CUDA device");
+    }
+    int pick = 0;
+    if (!firesim::tunedBrickRecord(device, nx, ny, nz, pick, *msBrick32, *msBrick16)) return fail("fireCudaGetTunedBrick: grid not timed");
+    *brickX = pick == 0 ? 32 : 16;
+    return true;
+}
+
 bool fireCudaSetResidentSorFault(int silentBrick, long long waitUs) {
     if (!requireScene()) return false;
     std::string err;

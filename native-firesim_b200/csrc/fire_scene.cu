@@ -6,6 +6,9 @@
 #include <cstdio>
 #include <atomic>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace firesim {
@@ -379,6 +382,44 @@ bool Scene::setPressurePath(int path, std::string& err) {
     return true;
 }
 
+namespace {
+
+// Measured brick choices of the resident solve, per device and grid, for the
+// life of the process: index 0 = 32x16x16, 1 = 16x16x16, with both timings.
+struct TunedBrick {
+    int pick;
+    float ms[2];
+};
+std::mutex g_tuneMutex;
+std::map<std::tuple<int, int, int, int>, TunedBrick> g_tuned;
+std::atomic<bool> g_autotune{true};
+
+}  // namespace
+
+bool autotuneEnabled() { return g_autotune.load(); }
+void setAutotune(bool enabled) { g_autotune.store(enabled); }
+
+int tunedBrick(int device, int nx, int ny, int nz) {
+    std::lock_guard<std::mutex> lock(g_tuneMutex);
+    const auto it = g_tuned.find(std::make_tuple(device, nx, ny, nz));
+    return it == g_tuned.end() ? -1 : it->second.pick;
+}
+
+void rememberTunedBrick(int device, int nx, int ny, int nz, int pick, float msLarge, float msSmall) {
+    std::lock_guard<std::mutex> lock(g_tuneMutex);
+    g_tuned[std::make_tuple(device, nx, ny, nz)] = TunedBrick{pick, {msLarge, msSmall}};
+}
+
+bool tunedBrickRecord(int device, int nx, int ny, int nz, int& pick, float& msLarge, float& msSmall) {
+    std::lock_guard<std::mutex> lock(g_tuneMutex);
+    const auto it = g_tuned.find(std::make_tuple(device, nx, ny, nz));
+    if (it == g_tuned.end()) return false;
+    pick = it->second.pick;
+    msLarge = it->second.ms[0];
+    msSmall = it->second.ms[1];
+    return true;
+}
+
 // Brick plan of the shared-memory-resident SOR: 32x16x16 bricks (256 threads,
 // 93 KB of shared memory, two CTAs per SM), or 16^3 bricks (128 threads, 67 KB)
 // when the larger ones do not fit co-resident; one CTA per brick.
@@ -424,7 +465,9 @@ bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
         cand[c].fits = cand[c].bricks <= static_cast<long long>(perSm) * sms;
     }
     // The larger bricks when they give every SM at least one; the smaller ones
-    // when the larger would leave SMs idle (small grids) or do not fit.
+    // when the larger would leave SMs idle (small grids) or do not fit.  When
+    // both fit and the autotuner is on, the first solve times both
+    // (tuneResident), unless this grid was timed before in this process.
     int pick = -1;
     if (cand[0].fits && cand[0].bricks >= sms) {
         pick = 0;
@@ -434,6 +477,20 @@ bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
         pick = 0;
     }
     if (pick < 0) return false;
+    tuneCount_ = 0;
+    if (cand[0].fits && cand[1].fits && autotuneEnabled()) {
+        const int known = tunedBrick(device, nx, ny, nz);
+        if (known >= 0) {
+            pick = known;
+        } else {
+            for (int c = 0; c < 2; ++c) {
+                tuneBricks_[c] = cand[c].r;
+                tuneSmem_[c] = cand[c].smem;
+                tuneThreads_[c] = cand[c].threads;
+            }
+            tuneCount_ = 2;
+        }
+    }
     plan_ = cand[pick].r;
     planSmem_ = cand[pick].smem;
     planThreads_ = cand[pick].threads;
@@ -441,6 +498,73 @@ bool Scene::residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads) {
     r = plan_;
     smemBytes = planSmem_;
     threads = planThreads_;
+    return true;
+}
+
+// Autotuner of the resident solve's brick shape.  Both shapes give the same
+// bits, so the choice is speed only: one ungated solve of the configured
+// iterations with each, from the same pressure (saved in divergenceAfter_, a
+// scratch field until the metrics recompute it, and put back before the real
+// solve), timed with CUDA events on the scene's stream.  The faster is kept
+// for this grid for the life of the process (tunedBrick).  While the stream
+// is being captured into a graph the heuristic's choice stands.
+bool Scene::tuneResident(std::string& err) {
+    const int count = tuneCount_;
+    tuneCount_ = 0;
+    if (sorSilentBrick_ >= 0) return true;  // an injected fault: keep the heuristic's choice
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess || capture != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return true;
+    }
+    const size_t bytes = cells_ * sizeof(float);
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    bool ok = true;
+    for (int i = 0; i < 3 && ok; ++i) ok = check("autotune event", cudaEventCreate(&ev[i]), err);
+    ok = ok && check("autotune save", cudaMemcpyAsync(divergenceAfter_, pressure_, bytes, cudaMemcpyDeviceToDevice, stream), err);
+    Grid g{nx, ny, nz};
+    float omega = pressureOmega;
+    int iterations = pressureIterations;
+    for (int c = 0; c < count && ok; ++c) {
+        ResidentBrick r = tuneBricks_[c];
+        const unsigned bricks = static_cast<unsigned>(r.nbx * r.nby * r.nbz);
+        void* fn = const_cast<void*>(sorResidentKernel(r.bx));
+        ResidentSync sync{sorExchange_, sorStatus_, sorHostStatus_, sorEpoch_, sorSilentBrick_, sorWaitNs_, nullptr};
+        sorEpoch_ += 2u * static_cast<unsigned>(iterations);
+        void* args[] = {&pressure_, &divergence_, &g, &r, &sync, &iterations, &omega};
+        ok = check("autotune restore", cudaMemcpyAsync(pressure_, divergenceAfter_, bytes, cudaMemcpyDeviceToDevice, stream), err) &&
+             check("autotune event", cudaEventRecord(ev[c], stream), err) &&
+             check("autotune launch", cudaLaunchCooperativeKernel(fn, dim3(bricks), dim3(tuneThreads_[c]), args, tuneSmem_[c], stream), err);
+        launches_ += 1;
+    }
+    ok = ok && check("autotune event", cudaEventRecord(ev[2], stream), err) &&
+         check("autotune restore", cudaMemcpyAsync(pressure_, divergenceAfter_, bytes, cudaMemcpyDeviceToDevice, stream), err) &&
+         check("autotune wait", cudaEventSynchronize(ev[2]), err);
+    if (ok) ok = checkSolverStatus(err);
+    float ms[2] = {0.0f, 0.0f};
+    if (ok) {
+        // Each solve is timed from its own start to the next one's start (the
+        // restore copy between them is the same for both).
+        ok = check("autotune time", cudaEventElapsedTime(&ms[0], ev[0], ev[1]), err) &&
+             check("autotune time", cudaEventElapsedTime(&ms[1], ev[1], ev[2]), err);
+    }
+    for (cudaEvent_t e : ev) {
+        if (e != nullptr) cudaEventDestroy(e);
+    }
+    if (!ok) return false;
+    const int best = ms[1] < ms[0] ? 1 : 0;
+    rememberTunedBrick(device, nx, ny, nz, best, ms[0], ms[1]);
+    plan_ = tuneBricks_[best];
+    planSmem_ = tuneSmem_[best];
+    planThreads_ = tuneThreads_[best];
+    return true;
+}
+
+bool Scene::residentBrick(int& bx, int& by, int& bz) const {
+    if (planState_ != 1) return false;
+    bx = plan_.bx;
+    by = plan_.by;
+    bz = plan_.bz;
     return true;
 }
 
@@ -468,6 +592,10 @@ bool Scene::runSor(const FrameParams& p, std::string& err) {
         size_t smem = 0;
         int threads = 0;
         if (residentPlan(r, smem, threads)) {
+            if (tuneCount_ > 1) {
+                if (!tuneResident(err)) return false;
+                residentPlan(r, smem, threads);
+            }
             Grid g{nx, ny, nz};
             float omega = pressureOmega;
             const unsigned bricks = static_cast<unsigned>(r.nbx * r.nby * r.nbz);

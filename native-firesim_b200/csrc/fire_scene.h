@@ -75,6 +75,14 @@ void defaultPhysicsParams(FirePhysicsParams& params, int nx, int ny, int nz);
 // Range and finiteness checks of fireCudaSetPhysicsParams.
 bool validatePhysicsParams(const FirePhysicsParams& params, std::string& err);
 
+// Autotuner of the resident SOR's brick shape (process-wide): on by default;
+// the measured choice per device and grid (-1: not timed yet).
+bool autotuneEnabled();
+void setAutotune(bool enabled);
+int tunedBrick(int device, int nx, int ny, int nz);
+void rememberTunedBrick(int device, int nx, int ny, int nz, int pick, float msLarge, float msSmall);
+bool tunedBrickRecord(int device, int nx, int ny, int nz, int& pick, float& msLarge, float& msSmall);
+
 class Scene {
 public:
     Scene() = default;
@@ -105,6 +113,8 @@ public:
     // 0 = automatic (shared-memory-resident when the grid fits co-resident), 1 = colour-split, 2 = resident only.
     bool setPressurePath(int path, std::string& err);
     int lastPressurePath() const { return lastPressurePath_; }
+    // The brick of the resident solve (after its first solve), or false.
+    bool residentBrick(int& bx, int& by, int& bz) const;
     // Fault injection for the resident SOR's bounded waits: brick `silentBrick`
     // (-1 = none) never announces its half sweeps; each wait gives up after waitUs.
     bool setResidentFault(int silentBrick, long long waitUs, std::string& err);
@@ -175,10 +185,19 @@ private:
     int activeSlot_ = 0;
     cudaEvent_t events_[9] = {};
     bool residentPlan(ResidentBrick& r, size_t& smemBytes, int& threads);
+    // Times one solve with each brick shape that fits (both from the same
+    // pressure, which is put back) and keeps the faster (autotuneResident).
+    bool tuneResident(std::string& err);
     int planState_ = 0;  // 0 not planned, 1 resident plan, 2 no resident plan
     ResidentBrick plan_{};
     size_t planSmem_ = 0;
     int planThreads_ = 0;
+    // Brick shapes that fit co-resident, for the autotuner (tuneCount_ > 1:
+    // not yet timed for this grid).
+    ResidentBrick tuneBricks_[2]{};
+    size_t tuneSmem_[2] = {0, 0};
+    int tuneThreads_[2] = {0, 0};
+    int tuneCount_ = 0;
     int pressurePath_ = 0;
     int lastPressurePath_ = 0;
     cudaGraphExec_t sorExec_ = nullptr;

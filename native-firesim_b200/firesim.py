@@ -71,6 +71,9 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireCudaSetPressurePath": (b, [ctypes.c_int]),
         "fireCudaGetPressurePathUsed": (ctypes.c_int, []),
         "fireCudaSetHashLattices": (b, [ctypes.c_int]),
+        "fireCudaSetAutotune": (b, [ctypes.c_int]),
+        "fireCudaGetTunedBrick": (b, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+                                      ctypes.POINTER(ctypes.c_float)]),
         "fireCudaSetPressureTolerance": (b, [ctypes.c_double, ctypes.c_int]),
         "fireCudaGetPressureStats": (b, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
         "fireCudaApplySceneContract": (b, [ctypes.c_int, ctypes.c_char_p, S]),
@@ -287,6 +290,23 @@ class FireSim:
 
     def set_times(self, sim_time: float, render_time: float, frame_index: int) -> None:
         self._check(self.lib.fireCudaSetTimes(sim_time, render_time, frame_index), "set times")
+
+
+def set_autotune(enabled: bool, precision: str = "f32") -> None:
+    """The resident SOR's brick-shape autotuner on (default) or off, process-wide."""
+    lib = load_library(precision)
+    if not lib.fireCudaSetAutotune(1 if enabled else 0):
+        raise FireSimError(f"fireCudaSetAutotune: {last_error(lib)}")
+
+
+def tuned_brick(nx: int, ny: int, nz: int, precision: str = "f32"):
+    """(brick x, ms per solve with 32x16x16 bricks, with 16x16x16) as the autotuner
+    measured them for this grid on the current device, or None if not timed."""
+    lib = load_library(precision)
+    bx, a, c = ctypes.c_int(), ctypes.c_float(), ctypes.c_float()
+    if not lib.fireCudaGetTunedBrick(nx, ny, nz, ctypes.byref(bx), ctypes.byref(a), ctypes.byref(c)):
+        return None
+    return bx.value, a.value, c.value
 
 
 def apply_scene_contract(scene_id: int, fire_scenes_dir, settings) -> None:
