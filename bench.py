@@ -789,9 +789,9 @@ def main() -> int:
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--max-active-mvoxels", type=float, default=24.0,
                     help="serve: admit while the admitted scenes hold at most this many million cells (0 = no limit)")
-    ap.add_argument("--latency-target-ms", type=float, default=4.5,
+    ap.add_argument("--latency-target-ms", type=float, default=4.0,
                     help="serve (batched loop): admit while the predicted round time (cells x the rounds' decaying peak "
-                         "time per cell) stays within this (0 = off); 4.5 ms keeps p99 step latency under 8 ms on the B200")
+                         "time per cell) stays within this (0 = off); chosen to keep p99 step latency under 8 ms on the B200")
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--no-headline", action="store_true",
                     help="single mode: skip the headline block (plain, batched and served at |div u| <= --div-target)")
@@ -983,7 +983,7 @@ NCU_TRAFFIC_BYTES = {("pressure_sor", "resident", 128, 60): 30157312 + 1525760,
 # from one ncu capture of sorResident<32,16,16>, profiles/sor_resident_128cubed_sor60.md): the
 # resident solve lives in shared memory, so its roofline is the shared-memory pipe, one
 # wavefront per clock per SM.
-NCU_SMEM_WAVEFRONTS = {("pressure_sor", "resident", 128, 60): 50.3e6}
+NCU_SMEM_WAVEFRONTS = {("pressure_sor", "resident", 128, 60): 50293124}
 
 
 def roofline_block(dominant: str, st: dict, args, cells: int, peaks: dict, peak_src: str, sor_path: int,

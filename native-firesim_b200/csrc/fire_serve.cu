@@ -516,7 +516,7 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
                 // admission plans for the dearer rounds (renders, more
                 // multigrid cycles) rather than the mean.
                 const double sample = roundMs / static_cast<double>(r.voxels);
-                msPerVoxel = std::max(sample, 0.97 * msPerVoxel);
+                msPerVoxel = std::max(sample, 0.99 * msPerVoxel);
             }
             for (size_t i = 0; i < r.members.size(); ++i) {
                 Live& l = *r.members[i];
