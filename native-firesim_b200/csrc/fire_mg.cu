@@ -183,7 +183,8 @@ __device__ __forceinline__ TailMap tailMap(int cols, int threads) {
 // shuffles (a Neumann side reads the lane's own value), with the same
 // arithmetic as weightedSum.
 template <bool RG>
-__device__ __forceinline__ void tailSmoothLanes(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps) {
+__device__ __forceinline__ void tailSmoothLanes(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps,
+                                                bool skipFirst) {
     if (threadIdx.x < 32) {
         const int lane = static_cast<int>(threadIdx.x);
         const int plane = L.nx * L.ny;
@@ -200,7 +201,7 @@ __device__ __forceinline__ void tailSmoothLanes(float* __restrict__ p, const flo
         const float rh = own ? tailLoad<RG>(rhs, lane) : 0.0f;
         float v = own ? p[lane] : 0.0f;
         for (int s = 0; s < sweeps; ++s) {
-            for (int colour = 0; colour < 2; ++colour) {
+            for (int colour = skipFirst && s == 0 ? 1 : 0; colour < 2; ++colour) {
                 const float pL = __shfl_sync(0xffffffffu, v, nL);
                 const float pR = __shfl_sync(0xffffffffu, v, nR);
                 const float pD = __shfl_sync(0xffffffffu, v, nD);
@@ -219,12 +220,15 @@ __device__ __forceinline__ void tailSmoothLanes(float* __restrict__ p, const flo
 
 // `sweeps` red-black sweeps of one tail level.  A level of at most 32 cells
 // goes to tailSmoothLanes; one of at most 128 cells is relaxed by the first
-// warp alone, with warp barriers; otherwise by the whole CTA.
+// warp alone, with warp barriers; otherwise by the whole CTA.  skipFirst:
+// the first colour-0 half sweep was already done (from p = 0, by whoever
+// wrote the level's rhs).
 template <bool PG, bool RG>
-__device__ __forceinline__ void tailSmooth(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps) {
+__device__ __forceinline__ void tailSmooth(float* __restrict__ p, const float* __restrict__ rhs, const MgLevel L, int sweeps,
+                                           bool skipFirst) {
     const int cols = L.nx * L.ny;
     if (!PG && cols * L.nz <= 32) {
-        tailSmoothLanes<RG>(p, rhs, L, sweeps);
+        tailSmoothLanes<RG>(p, rhs, L, sweeps, skipFirst);
         return;
     }
     const bool warpOnly = cols * L.nz <= 4 * 32;
@@ -244,7 +248,7 @@ __device__ __forceinline__ void tailSmooth(float* __restrict__ p, const float* _
             const int y = m.col / L.nx, x = m.col - y * L.nx;
             const int z0 = 2 * m.zg + ((x + y) & 1), dz = 2 * m.zsplit;
             for (int s = 0; s < sweeps; ++s) {
-                for (int colour = 0; colour < 2; ++colour) {
+                for (int colour = skipFirst && s == 0 ? 1 : 0; colour < 2; ++colour) {
                     if (m.active) {
 #pragma unroll 4
                         for (int z = z0 ^ colour; z < L.nz; z += dz) {
@@ -257,7 +261,7 @@ __device__ __forceinline__ void tailSmooth(float* __restrict__ p, const float* _
             }
         } else {
             for (int s = 0; s < sweeps; ++s) {
-                for (int colour = 0; colour < 2; ++colour) {
+                for (int colour = skipFirst && s == 0 ? 1 : 0; colour < 2; ++colour) {
                     for (int col = m.col; col < cols; col += m.colStride) {
                         const int y = col / L.nx, x = col - y * L.nx;
 #pragma unroll 4
@@ -348,17 +352,33 @@ __device__ __forceinline__ void tailCycle(const MgScene& S, int pre, int post, f
         }
     }
     __syncthreads();
-    if constexpr (!PG) {
-        const int n0 = S.lv[t].nx * S.lv[t].ny * S.lv[t].nz;
-        float* p0 = sP[t];
-        float* r0 = sR[t];
-        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
-            p0[i] = __ldcg(S.p[t] + i);
-            if (MODE == kMgTailShared) r0[i] = __ldcg(S.rhs[t] + i);
+    const int threads = static_cast<int>(blockDim.x);
+    // A level whose p starts at 0 gets its first colour-0 half sweep where its
+    // rhs is written: (rhs + 0) / diag on colour-0 cells, 0 elsewhere (every
+    // neighbour sum is +0, so this is the half sweep's result to the bit).
+    // That holds for every level below the tail level, and for the tail level
+    // itself unless it is level 0 (whose p carries over between cycles).
+    auto firstRed = [&](int l, int sweeps) { return sweeps > 0 && (l > t || t > 0); };
+    {
+        const MgLevel T = S.lv[t];
+        const bool fuse = firstRed(t, t == last ? kMgCoarsestSweeps : pre);
+        const int cols = T.nx * T.ny;
+        const TailMap m = tailMap(cols, threads);
+        if (m.active && (!PG || fuse)) {
+            for (int col = m.col; col < cols; col += m.colStride) {
+                const int y = col / T.nx, x = col - y * T.nx;
+                for (int z = m.zg; z < T.nz; z += m.zsplit) {
+                    const int i = col + z * cols;
+                    const float r = __ldcg(S.rhs[t] + i);
+                    if (MODE == kMgTailShared) sR[t][i] = r;
+                    const float v = !fuse ? __ldcg(S.p[t] + i) : (((x + y + z) & 1) == 0 ? (r + 0.0f) * T.invDiag : 0.0f);
+                    sP[t][i] = v;
+                }
+            }
         }
+        if constexpr (PG) __threadfence_block();
         __syncthreads();
     }
-    const int threads = static_cast<int>(blockDim.x);
     for (int l = t; l < last; ++l) {
         const MgLevel F = S.lv[l];
         const MgLevel C = S.lv[l + 1];
@@ -366,10 +386,11 @@ __device__ __forceinline__ void tailCycle(const MgScene& S, int pre, int post, f
         float* pf = sP[l];
         const float* rf = sR[l];
         if (rg) {
-            tailSmooth<PG, true>(pf, rf, F, pre);
+            tailSmooth<PG, true>(pf, rf, F, pre, firstRed(l, pre));
         } else {
-            tailSmooth<PG, false>(pf, rf, F, pre);
+            tailSmooth<PG, false>(pf, rf, F, pre, firstRed(l, pre));
         }
+        const bool fuseC = firstRed(l + 1, l + 1 == last ? kMgCoarsestSweeps : pre);
         auto loadF = [&](int j) { return tailLoad<PG>(pf, j); };
         float* pc = sP[l + 1];
         float* rc = sR[l + 1];
@@ -380,8 +401,9 @@ __device__ __forceinline__ void tailCycle(const MgScene& S, int pre, int post, f
                 const int Y = col / C.nx, X = col - Y * C.nx;
                 for (int Z = m.zg; Z < C.nz; Z += m.zsplit) {
                     const int i = col + Z * cols;
-                    rc[i] = restrictAt(loadF, rf, rg, F, C, X, Y, Z);
-                    pc[i] = 0.0f;
+                    const float r = restrictAt(loadF, rf, rg, F, C, X, Y, Z);
+                    rc[i] = r;
+                    pc[i] = fuseC && ((X + Y + Z) & 1) == 0 ? (r + 0.0f) * C.invDiag : 0.0f;
                 }
             }
         }
@@ -390,10 +412,11 @@ __device__ __forceinline__ void tailCycle(const MgScene& S, int pre, int post, f
     }
     {
         const MgLevel B = S.lv[last];
+        const bool skip = firstRed(last, kMgCoarsestSweeps);
         if (PG || (MODE == kMgTailRhsGlobal && last == t)) {
-            tailSmooth<PG, true>(sP[last], sR[last], B, kMgCoarsestSweeps);
+            tailSmooth<PG, true>(sP[last], sR[last], B, kMgCoarsestSweeps, skip);
         } else {
-            tailSmooth<PG, false>(sP[last], sR[last], B, kMgCoarsestSweeps);
+            tailSmooth<PG, false>(sP[last], sR[last], B, kMgCoarsestSweeps, skip);
         }
     }
     for (int l = last - 1; l >= t; --l) {
@@ -416,9 +439,9 @@ __device__ __forceinline__ void tailCycle(const MgScene& S, int pre, int post, f
         if constexpr (PG) __threadfence_block();
         __syncthreads();
         if (PG || (MODE == kMgTailRhsGlobal && l == t)) {
-            tailSmooth<PG, true>(pf, sR[l], F, post);
+            tailSmooth<PG, true>(pf, sR[l], F, post, false);
         } else {
-            tailSmooth<PG, false>(pf, sR[l], F, post);
+            tailSmooth<PG, false>(pf, sR[l], F, post, false);
         }
     }
     if constexpr (!PG) {
