@@ -221,15 +221,21 @@ def test_server_rejects_invalid_physics(pkg, abi):
     server.close()
 
 
-def test_batched_server_equals_alone(pkg, abi):
+@pytest.mark.parametrize("round_ms", [0.0, 0.3])
+def test_batched_server_equals_alone(pkg, abi, round_ms):
     """Requests of the config physics with the multigrid projection are served
     as one batch per round (every admitted scene advanced by one launch per
     stage); with room for about two scenes by cells, eight requests of three
     shapes arrive over 40 ms, queue for free scenes and complete, and each
-    served heat field and last frame equal the same scene stepped alone."""
+    served heat field and last frame equal the same scene stepped alone.
+    With a round-time target (0.3 ms: tighter than most rounds) admission
+    waits for the predicted round time, which changes the mix and not the
+    results."""
     import torch
     server = pkg.Server(budget_bytes=64 << 30)
     server.set_limits(int(np.prod(SIZES[1]) + np.prod(SIZES[2])))
+    if round_ms > 0:
+        server.set_latency_target(round_ms)
     reqs, heats, hdrs = [], [], []
     for i in range(8):
         dims = SIZES[i % 3]
