@@ -719,19 +719,24 @@ bool Scene::setPressureMultigrid(int maxCycles, int preSmooth, int postSmooth, s
 MgSolver::~MgSolver() { release(); }
 
 void MgSolver::release() {
-    if (uploaded_ != nullptr) cudaEventSynchronize(uploaded_);
+    for (cudaEvent_t e : uploadedRing_) {
+        if (e != nullptr) cudaEventSynchronize(e);
+    }
     if (dScenes_ != nullptr) cudaFree(dScenes_);
     if (dPlan_ != nullptr) cudaFree(dPlan_);
     if (dSync_ != nullptr) cudaFree(dSync_);
-    if (hScenes_ != nullptr) cudaFreeHost(hScenes_);
-    if (hPlan_ != nullptr) cudaFreeHost(hPlan_);
-    if (uploaded_ != nullptr) cudaEventDestroy(uploaded_);
+    for (int k = 0; k < kStaging; ++k) {
+        if (hScenesRing_[k] != nullptr) cudaFreeHost(hScenesRing_[k]);
+        if (hPlanRing_[k] != nullptr) cudaFreeHost(hPlanRing_[k]);
+        if (uploadedRing_[k] != nullptr) cudaEventDestroy(uploadedRing_[k]);
+        hScenesRing_[k] = nullptr;
+        hPlanRing_[k] = nullptr;
+        uploadedRing_[k] = nullptr;
+    }
+    slot_ = 0;
     dScenes_ = nullptr;
     dPlan_ = nullptr;
     dSync_ = nullptr;
-    hScenes_ = nullptr;
-    hPlan_ = nullptr;
-    uploaded_ = nullptr;
     planned_ = false;
     grid_ = 0;
     smem_ = 0;
@@ -740,7 +745,8 @@ void MgSolver::release() {
 // The work lists and descriptors are built on the host and uploaded on
 // `stream` from pinned staging, so a plan (for example when a serving batch's
 // scenes change) neither allocates nor synchronises after the first one; the
-// next plan waits only for this plan's upload to have run.
+// staging is a ring, so a plan waits only for the upload made kStaging plans
+// before it (the device copies are stream-ordered after the previous launch).
 bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycles, int pre, int post, double tolerance,
                     cudaStream_t stream, std::string& err) {
     const int n = static_cast<int>(scenes.size());
@@ -765,21 +771,28 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
         if (e == cudaSuccess) e = cudaMalloc(&dPlan_, sizeof(MgPlan));
         if (e == cudaSuccess) e = cudaMalloc(&dSync_, sizeof(MgSync));
         if (e == cudaSuccess) e = cudaMemset(dSync_, 0, sizeof(MgSync));
-        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&hScenes_), kMgMaxScenes * sizeof(MgScene), cudaHostAllocDefault);
-        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&hPlan_), sizeof(MgPlan), cudaHostAllocDefault);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&uploaded_, cudaEventDisableTiming);
+        for (int k = 0; k < kStaging; ++k) {
+            if (e == cudaSuccess) {
+                e = cudaHostAlloc(reinterpret_cast<void**>(&hScenesRing_[k]), kMgMaxScenes * sizeof(MgScene), cudaHostAllocDefault);
+            }
+            if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&hPlanRing_[k]), sizeof(MgPlan), cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&uploadedRing_[k], cudaEventDisableTiming);
+        }
         if (e != cudaSuccess) {
             err = std::string("multigrid plan: ") + cudaGetErrorString(e);
             release();
             return false;
         }
     }
-    if (e == cudaSuccess) e = cudaEventSynchronize(uploaded_);
+    const int k = slot_;
+    if (e == cudaSuccess) e = cudaEventSynchronize(uploadedRing_[k]);
     if (e != cudaSuccess) {
         err = std::string("multigrid plan: ") + cudaGetErrorString(e);
         return false;
     }
-    MgPlan& plan = *hPlan_;
+    MgScene* hScenes = hScenesRing_[k];
+    MgPlan* hPlan = hPlanRing_[k];
+    MgPlan& plan = *hPlan;
     std::memset(&plan, 0, sizeof(MgPlan));
     plan.scenes = n;
     plan.maxCycles = maxCycles;
@@ -804,7 +817,7 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
         const MgLevel& L0 = scenes[s].lv[0];
         plan.allUnits[s + 1] = plan.allUnits[s] + ((L0.nx & 3) == 0 ? mgQuadUnits(L0.nx, L0.ny, L0.nz) : rows0 * mgQuadChunks(L0.nx));
     }
-    std::memcpy(hScenes_, scenes.data(), n * sizeof(MgScene));
+    std::memcpy(hScenes, scenes.data(), n * sizeof(MgScene));
     int perSm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, mgSolve, kMgThreads, smem);
     if (e == cudaSuccess && perSm < 1) {
@@ -830,9 +843,10 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
             }
         }
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dScenes_, hScenes_, n * sizeof(MgScene), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dPlan_, hPlan_, sizeof(MgPlan), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaEventRecord(uploaded_, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dScenes_, hScenes, n * sizeof(MgScene), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dPlan_, hPlan, sizeof(MgPlan), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(uploadedRing_[k], stream);
+    if (e == cudaSuccess) slot_ = (k + 1) % kStaging;
     if (e != cudaSuccess) {
         err = std::string("multigrid plan: ") + cudaGetErrorString(e);
         return false;

@@ -57,9 +57,13 @@ private:
     MgScene* dScenes_ = nullptr;  // kMgMaxScenes descriptors
     MgPlan* dPlan_ = nullptr;
     MgSync* dSync_ = nullptr;
-    MgScene* hScenes_ = nullptr;  // pinned staging of the uploads
-    MgPlan* hPlan_ = nullptr;
-    cudaEvent_t uploaded_ = nullptr;
+    // Pinned staging of the uploads, a ring of kStaging slots: a new plan
+    // waits only for the upload made kStaging plans ago, not the last one.
+    static constexpr int kStaging = 3;
+    MgScene* hScenesRing_[kStaging] = {};
+    MgPlan* hPlanRing_[kStaging] = {};
+    cudaEvent_t uploadedRing_[kStaging] = {};
+    int slot_ = 0;
     bool planned_ = false;
     size_t smem_ = 0;
     int grid_ = 0, sms_ = 0;

@@ -398,7 +398,7 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
         FireServeRequest req{};
         BatchedSlot* slot = nullptr;
         int queued = 0, done = 0;
-        EventRef last;  // end of its previous round (its admission for the first)
+        EventRef last;  // end of its previous round (the start of its first round, for the first)
     };
     struct Round {
         EventRef start, done;
@@ -492,6 +492,12 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
                     lastMembers = members;
                 }
                 round.start = recordEvent(runner.stream());
+                // A scene's first step is timed from the start of its first
+                // round; the wait before it (behind the rounds in flight) is
+                // its queue time, like the wait before admission.
+                for (Live* l : round.members) {
+                    if (l->queued == 0) l->last = round.start;
+                }
                 if (!runner.run(settings.data(), render.data(), err)) {
                     ok = fail("fireServerRun: " + err);
                     break;
