@@ -789,7 +789,7 @@ def main() -> int:
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--max-active-mvoxels", type=float, default=24.0,
                     help="serve: admit while the admitted scenes hold at most this many million cells (0 = no limit)")
-    ap.add_argument("--latency-target-ms", type=float, default=5.0,
+    ap.add_argument("--latency-target-ms", type=float, default=4.0,
                     help="serve (batched loop): admit while the predicted round time (cells x the rounds' decaying peak "
                          "time per cell) stays within this (0 = off); chosen to keep p99 step latency under 8 ms on the B200")
     ap.add_argument("--seed", type=int, default=5)

@@ -208,13 +208,23 @@ __device__ __forceinline__ void cfgAdvectVelocityAt(FaceT* __restrict__ uOut, Fa
     }
 }
 
+// The single-scene face kernels run on the cell grid: the thread of cell
+// (x, y, z) owns its u, v and w faces and, as the last cell of its row,
+// column or plane, the far wall's face beside it (x = nx, y = ny, z = nz).
+// A face grid of nx + 1 columns would leave a nearly empty block per row.
+template <class Face>
+__device__ __forceinline__ void facesOfCell(const ConfigParams& p, int x, int y, int z, Face face) {
+    face(x, y, z);
+    if (x == p.nx - 1) face(p.nx, y, z);
+    if (y == p.ny - 1) face(x, p.ny, z);
+    if (z == p.nz - 1) face(x, y, p.nz);
+}
+
 __global__ void __launch_bounds__(128) cfgAdvectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
                                                          Velocity vel, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
-    if (x > p.nx) return;
-    cfgAdvectVelocityAt(uOut, vOut, wOut, vel, p, x, y, z);
+    if (x >= p.nx) return;
+    facesOfCell(p, x, blockIdx.y, blockIdx.z, [&](int fx, int fy, int fz) { cfgAdvectVelocityAt(uOut, vOut, wOut, vel, p, fx, fy, fz); });
 }
 
 // Backtrace of record a from the cell centre, then burn, decay and emitters.
@@ -380,10 +390,9 @@ __device__ __forceinline__ void cfgApplyForcesAt(FaceT* __restrict__ uOut, FaceT
 __global__ void __launch_bounds__(128) cfgApplyForces(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
                                                       Velocity vel, const float4* __restrict__ force, ConfigParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
-    if (x > p.nx) return;
-    cfgApplyForcesAt(uOut, vOut, wOut, vel, force, p, x, y, z);
+    if (x >= p.nx) return;
+    facesOfCell(p, x, blockIdx.y, blockIdx.z,
+                [&](int fx, int fy, int fz) { cfgApplyForcesAt(uOut, vOut, wOut, vel, force, p, fx, fy, fz); });
 }
 
 // Transmittance toward the point light from the centre of each 2x2x2 block of

@@ -1023,14 +1023,12 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
     }
     if (physics_.mode == 1) return runConfigStages(first, last, p, err);
     const int bx = rowThreads(nx);
-    const int bxFace = rowThreads(nx + 1);
     const dim3 cells = cellGrid(bx, nx, ny, nz);
-    const dim3 faces = cellGrid(bxFace, nx + 1, ny + 1, nz + 1);
     int s = first;
     while (s <= last) {
         switch (s) {
             case kAdvectVelocity:
-                advectVelocity<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), p); ++launches_;
+                advectVelocity<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), p); ++launches_;
                 vcur_ = 1 - vcur_;
                 s = kAdvectReact;
                 break;
@@ -1058,14 +1056,14 @@ bool Scene::runStages(int first, int last, const FrameParams& p, std::string& er
                     vcur_ = 1 - vcur_;
                     s = kPressureSor;
                 } else {
-                    forceApply<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], contrib_, velocity(), p); ++launches_;
+                    forceApply<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], contrib_, velocity(), p); ++launches_;
                     vcur_ = 1 - vcur_;
                     s = kVelocityBoundary;
                 }
                 break;
             }
             case kVelocityBoundary:
-                velocityBoundary<<<faces, bxFace, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], p, 1); ++launches_;
+                velocityBoundary<<<cells, bx, 0, stream>>>(vel_[0][vcur_], vel_[1][vcur_], vel_[2][vcur_], p, 1); ++launches_;
                 s = kDivergence;
                 break;
             case kDivergence:
@@ -1822,14 +1820,12 @@ bool Scene::prepareBatched(std::string& err) {
 bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::string& err) {
     if (!ensureConfigBuffers(err)) return false;
     const int bx = rowThreads(nx);
-    const int bxFace = rowThreads(nx + 1);
     const dim3 cells = cellGrid(bx, nx, ny, nz);
-    const dim3 faces = cellGrid(bxFace, nx + 1, ny + 1, nz + 1);
     for (int s = first; s <= last; ++s) {
         const ConfigParams c = configParams();
         switch (s) {
             case kAdvectVelocity:
-                cfgAdvectVelocity<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), c); ++launches_;
+                cfgAdvectVelocity<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), c); ++launches_;
                 vcur_ = 1 - vcur_;
                 break;
             case kAdvectReact:
@@ -1856,7 +1852,7 @@ bool Scene::runConfigStages(int first, int last, const FrameParams& p, std::stri
                     }
                 }
                 cfgCellForce<<<cells, bx, 0, stream>>>(contrib_, cfgVort_, sa_[cur_], cfgNoise_, c); ++launches_;
-                cfgApplyForces<<<faces, bxFace, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), contrib_, c); ++launches_;
+                cfgApplyForces<<<cells, bx, 0, stream>>>(vel_[0][1 - vcur_], vel_[1][1 - vcur_], vel_[2][1 - vcur_], velocity(), contrib_, c); ++launches_;
                 vcur_ = 1 - vcur_;
                 break;
             case kDivergence:

@@ -88,13 +88,25 @@ __global__ void __launch_bounds__(256) resetCells(ScalarFields out, float* __res
 }
 
 // ---------------------------------------------------------------------------
+// The face kernels run on the cell grid: the thread of cell (x, y, z) takes
+// the u, v and w faces of index (x, y, z) and, as the last cell of its row,
+// column or plane, the far wall's faces of index (nx, y, z), (x, ny, z) and
+// (x, y, nz).  Every face index of the (nx + 1) x (ny + 1) x (nz + 1) space
+// that holds a face is visited once; a face grid of nx + 1 columns would
+// leave a nearly empty block per row.
+template <class Face>
+__device__ __forceinline__ void facesOfCell(const FrameParams& p, int x, int y, int z, Face face) {
+    face(x, y, z);
+    if (x == p.nx - 1) face(p.nx, y, z);
+    if (y == p.ny - 1) face(x, p.ny, z);
+    if (z == p.nz - 1) face(x, y, p.nz);
+}
+
+// ---------------------------------------------------------------------------
 // src/fire_cuda.cu:880-932 -- self-advection of the three face grids.  One
 // thread owns the u, v and w faces that share its (x, y, z) index.
-__global__ void __launch_bounds__(256) advectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
-                                                      Velocity vel, FrameParams p) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
+__device__ __forceinline__ void advectVelocityAt(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                 const Velocity& vel, const FrameParams& p, int x, int y, int z) {
     const Grid g{p.nx, p.ny, p.nz};
     const float back = p.dt;
     if (x <= p.nx && y < p.ny && z < p.nz) {
@@ -133,6 +145,13 @@ __global__ void __launch_bounds__(256) advectVelocity(FaceT* __restrict__ uOut, 
         }
         stv(wOut + wAt(g, x, y, z), r);
     }
+}
+
+__global__ void __launch_bounds__(256) advectVelocity(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
+                                                      Velocity vel, FrameParams p) {
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cx >= p.nx) return;
+    facesOfCell(p, cx, blockIdx.y, blockIdx.z, [&](int x, int y, int z) { advectVelocityAt(uOut, vOut, wOut, vel, p, x, y, z); });
 }
 
 // ---------------------------------------------------------------------------
@@ -480,13 +499,14 @@ __device__ __forceinline__ float forcedW(const FaceT* __restrict__ w, const floa
 // The force gather alone (stage "force"): every face adds its cells' increments.
 __global__ void __launch_bounds__(256) forceApply(FaceT* __restrict__ uOut, FaceT* __restrict__ vOut, FaceT* __restrict__ wOut,
                                                   const float4* __restrict__ contrib, Velocity vel, FrameParams p) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cx >= p.nx) return;
     const Grid g{p.nx, p.ny, p.nz};
-    if (x <= p.nx && y < p.ny && z < p.nz) stv(uOut + uAt(g, x, y, z), forcedU(vel.u, contrib, g, x, y, z, false));
-    if (x < p.nx && y <= p.ny && z < p.nz) stv(vOut + vAt(g, x, y, z), forcedV(vel.v, contrib, g, x, y, z, false));
-    if (x < p.nx && y < p.ny && z <= p.nz) stv(wOut + wAt(g, x, y, z), forcedW(vel.w, contrib, g, x, y, z, false));
+    facesOfCell(p, cx, blockIdx.y, blockIdx.z, [&](int x, int y, int z) {
+        if (x <= p.nx && y < p.ny && z < p.nz) stv(uOut + uAt(g, x, y, z), forcedU(vel.u, contrib, g, x, y, z, false));
+        if (x < p.nx && y <= p.ny && z < p.nz) stv(vOut + vAt(g, x, y, z), forcedV(vel.v, contrib, g, x, y, z, false));
+        if (x < p.nx && y < p.ny && z <= p.nz) stv(wOut + wAt(g, x, y, z), forcedW(vel.w, contrib, g, x, y, z, false));
+    });
 }
 
 // Fused force gather + boundary clamp + divergence (+ pressure reset): one cell
@@ -523,10 +543,10 @@ __global__ void __launch_bounds__(256) forceProjectSetup(FaceT* __restrict__ uOu
 // src/fire_cuda.cu:1261-1317 -- wall zeroing, with (clampValues) or without the value clamps.
 __global__ void __launch_bounds__(256) velocityBoundary(FaceT* __restrict__ u, FaceT* __restrict__ v, FaceT* __restrict__ w,
                                                         FrameParams p, int clampValues) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cx >= p.nx) return;
     const Grid g{p.nx, p.ny, p.nz};
+    facesOfCell(p, cx, blockIdx.y, blockIdx.z, [&](int x, int y, int z) {
     if (x <= p.nx && y < p.ny && z < p.nz) {
         FaceT* f = u + uAt(g, x, y, z);
         if (x == 0 || x == p.nx) stv(f, 0.0f);
@@ -542,6 +562,7 @@ __global__ void __launch_bounds__(256) velocityBoundary(FaceT* __restrict__ u, F
         if (z == 0 || z == p.nz) stv(f, 0.0f);
         else if (clampValues) stv(f, fminf(4.0f, fmaxf(-4.0f, ldv(f))));
     }
+    });
 }
 
 // src/fire_cuda.cu:1185-1199 / :1247-1259.
