@@ -29,8 +29,12 @@
 //
 // One launch (mgSolve) runs every cycle of every scene of the batch.  Its
 // CTAs are all co-resident (cooperative launch); the phases of a cycle are
-// separated by a grid barrier whose waits are bounded in time.  Within a
-// phase, warps take rows of all scenes at that level from one work list.
+// separated by a grid barrier (a monotonic arrival count with release and
+// acquire semantics) whose waits are bounded in time.  Within a phase, warps
+// take the units of all scenes at that level from one work list.  A level's
+// first colour-0 half sweep from p = 0 is written with its rhs (by the
+// restriction, or the first phase for level 0 in the first cycle), as its
+// arithmetic reduces to (rhs + 0) / diag there.
 // The coarse end of each scene's hierarchy (from the first level of at most
 // kMgTailCells cells down) is solved by one CTA in shared memory (in its
 // global buffers if it does not fit, as for a grid that cannot coarsen).  Reads of
@@ -516,9 +520,12 @@ __device__ __forceinline__ void flatCoords(const MgLevel& L, int i, int& x, int&
 }  // namespace
 
 // The persistent batched solve (see the file comment).  Work items of the
-// grid levels are rows of one level of one scene, one warp per row; the
-// tail is one CTA per scene; the residual is one warp per chunk of
-// kMgChunkRows level-0 rows; the gate is one warp per scene.
+// grid levels are units of one level of one scene (128 cells in memory order,
+// a quad per lane, where the row length is a multiple of 4; else chunks of
+// one row), one warp per unit; the tail is one CTA per scene; the residual is
+// one warp per chunk (mgResidualChunks); every CTA decides convergence from
+// the per-scene maxima, and one CTA per scene writes its gate record at the
+// end.
 __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restrict__ scenes, const MgPlan* __restrict__ plan, MgSync* sync,
                                                         unsigned* hostStatus, unsigned long long waitNs) {
     extern __shared__ float smem[];
