@@ -509,6 +509,12 @@ __device__ __forceinline__ float quadSum(const MgLevel& L, const Quad& q, int e,
     return combine(at4(q.rh, e), pL, pR, pD, pU, pB, pF, L);
 }
 
+// Asks L2 to fetch the line holding a (no register or shared memory holds
+// the data; the load that follows finds it there).
+__device__ __forceinline__ void prefetchLineL2(const float* a) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(a)));
+}
+
 // Coordinates of flat index i of a level.
 __device__ __forceinline__ void flatCoords(const MgLevel& L, int i, int& x, int& y, int& z) {
     const int row = i / L.nx;
@@ -574,6 +580,13 @@ __global__ void __launch_bounds__(kMgThreads, 1) mgSolve(const MgScene* __restri
             if ((L.nx & 3) == 0) {
                 const int i = u * 128 + 4 * lane;
                 const bool live = i < L.nx * L.ny * L.nz;
+                // Ask L2 for this lane's cells of the warp's next unit (when it
+                // is in the same scene), so that its loads find them there.
+                const int ahead = i + nwarps * 128;
+                if (ahead < L.nx * L.ny * L.nz) {
+                    prefetchLineL2(rhs + ahead);
+                    prefetchLineL2(p + ahead);
+                }
                 int x0, y, z;
                 flatCoords(L, live ? i : 0, x0, y, z);
                 Quad q;
