@@ -172,6 +172,25 @@ FIRE_API bool fireCudaSetResidentSorFault(int silentBrick, long long waitUs);
  * (src/fire_cuda.cu:2981). */
 FIRE_API bool fireCudaSetAllocationFault(long long succeedBeforeFailing);
 
+/* Bounds checks (no counterpart in the reference, whose kernels index
+ * unchecked, src/fire_cuda.cu:445-487).  The FIRE_BOUNDS_CHECK build of this
+ * library, libfiresim_b200_checked.so, places every device buffer it owns
+ * between two 2 MiB guard zones and fills the whole allocation with 0xFF
+ * bytes (NaN in every float field, -1 in every integer) when it is made.
+ * fireCudaCheckGuards synchronizes the current device and scans the guard
+ * zones of every live buffer on it and of those freed since the last call.
+ * *corrupted = the number of buffers with a changed zone (0: every zone
+ * intact; -1: this library is not the checked build).  Returns false when
+ * a zone changed (fireCudaLastError names the first buffer, the side and
+ * the byte), on a CUDA error, and in the default builds.  Changed zones are
+ * re-armed, so each change is reported once. */
+FIRE_API bool fireCudaCheckGuards(int* corrupted);
+
+/* Checked build only: sets the byte `offset` bytes past the end of the first
+ * live buffer named `bufferLabel` (e.g. "pressure") to 0 with a host-side
+ * cudaMemset inside that buffer's allocation: the checker's own test. */
+FIRE_API bool fireCudaPlantGuardByte(const char* bufferLabel, size_t offset);
+
 /* nx, ny, nz, lightNx, lightNy, lightNz, frameWidth, frameHeight. */
 FIRE_API bool fireCudaGetGridInfo(int* dims8);
 

@@ -9,6 +9,7 @@ tests, benchmarks and Python callers; it performs no computation itself.
 from __future__ import annotations
 
 from . import abi  # noqa: F401
-from .firesim import Batch, FireSim, FireSimError, Scene, Server, batch_step, load_library, set_autotune, tuned_brick  # noqa: F401
+from .firesim import (Batch, FireSim, FireSimError, Scene, Server, batch_step, check_guards, load_library, set_autotune,  # noqa: F401
+                      tuned_brick)
 
-__all__ = ["abi", "Batch", "FireSim", "FireSimError", "Scene", "Server", "batch_step", "load_library", "set_autotune", "tuned_brick"]
+__all__ = ["abi", "Batch", "FireSim", "FireSimError", "Scene", "Server", "batch_step", "check_guards", "load_library", "set_autotune", "tuned_brick"]

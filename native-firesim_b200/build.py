@@ -25,6 +25,8 @@ VARIANTS = {
     "f32": (HERE / "_build", HERE / "libfiresim_b200.so", []),
     "f16": (HERE / "_build_f16", HERE / "libfiresim_b200_f16.so", ["-DFIRE_STORAGE_F16"]),
     "bf16": (HERE / "_build_bf16", HERE / "libfiresim_b200_bf16.so", ["-DFIRE_STORAGE_BF16"]),
+    # FP32 storage with guard zones around every device buffer (csrc/fire_guard.h).
+    "checked": (HERE / "_build_checked", HERE / "libfiresim_b200_checked.so", ["-DFIRE_BOUNDS_CHECK"]),
 }
 INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -85,11 +87,13 @@ def _build_variant(variant: str, force: bool, verbose_ptxas: bool, quiet: bool) 
 
 
 def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True, f16: bool = True) -> Path:
-    """Builds the FP32 library (returned) and, unless f16=False, the FP16- and BF16-storage variants."""
+    """Builds the FP32 library (returned) and, unless f16=False, the FP16- and BF16-storage
+    variants and the bounds-checking FP32 build."""
     lib = _build_variant("f32", force, verbose_ptxas, quiet)
     if f16:
         _build_variant("f16", force, False, quiet)
         _build_variant("bf16", force, False, quiet)
+        _build_variant("checked", force, False, quiet)
     return lib
 
 

@@ -80,6 +80,21 @@ bool fireCudaSetAllocationFault(long long succeedBeforeFailing) {
     return true;
 }
 
+bool fireCudaCheckGuards(int* corrupted) {
+    int count = -1;
+    std::string report;
+    const bool ok = firesim::checkGuards(count, report);
+    if (corrupted != nullptr) *corrupted = count;
+    if (!ok || count != 0) return fail(report);
+    return true;
+}
+
+bool fireCudaPlantGuardByte(const char* bufferLabel, size_t offset) {
+    std::string err;
+    if (!firesim::plantGuardByte(bufferLabel, offset, err)) return fail(err);
+    return true;
+}
+
 bool fireCudaStepAndRender(uint32_t* bgraPixels, const FireSettings& settings) {
     return frame(bgraPixels, &settings, nullptr, false, true, true);
 }

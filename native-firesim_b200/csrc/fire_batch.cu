@@ -36,8 +36,8 @@ BatchRunner::~BatchRunner() { release(); }
 void BatchRunner::release() {
     if (stream_ != nullptr) cudaStreamSynchronize(stream_);
     solver_.release();
-    if (dScenes_ != nullptr) cudaFree(dScenes_);
-    if (dPlan_ != nullptr) cudaFree(dPlan_);
+    deviceFree(dScenes_);
+    deviceFree(dPlan_);
     for (int k = 0; k < kRing; ++k) {
         if (host_[k] != nullptr) cudaFreeHost(host_[k]);
         if (copied_[k] != nullptr) cudaEventDestroy(copied_[k]);
@@ -59,8 +59,8 @@ bool BatchRunner::init(int device, std::string& err) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&hostStatus_), sizeof(unsigned), cudaHostAllocMapped);
-    if (e == cudaSuccess) e = cudaMalloc(&dScenes_, kBatchMaxScenes * sizeof(BatchScene));
-    if (e == cudaSuccess) e = cudaMalloc(&dPlan_, sizeof(BatchPlan));
+    if (e == cudaSuccess) e = deviceAlloc(reinterpret_cast<void**>(&dScenes_), kBatchMaxScenes * sizeof(BatchScene), "batch scene table");
+    if (e == cudaSuccess) e = deviceAlloc(reinterpret_cast<void**>(&dPlan_), sizeof(BatchPlan), "batch plan");
     for (int k = 0; k < kRing && e == cudaSuccess; ++k) {
         e = cudaHostAlloc(reinterpret_cast<void**>(&host_[k]), staging, cudaHostAllocDefault);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&copied_[k], cudaEventDisableTiming);

@@ -65,7 +65,9 @@ bool Scene::alloc(void** p, size_t bytes, const char* label, std::string& err) {
         }
         if (g_allocationsBeforeFault.compare_exchange_weak(left, left - 1)) break;
     }
-    if (!check(label, cudaMalloc(p, bytes), err)) {
+    // The buffer's name for the bounds-checking build's reports: the label without "cudaMalloc ".
+    const char* name = std::strncmp(label, "cudaMalloc ", 11) == 0 ? label + 11 : label;
+    if (!check(label, deviceAlloc(p, bytes, name), err)) {
         *p = nullptr;
         return false;
     }
@@ -90,12 +92,12 @@ void Scene::release() {
     mgSolver_.release();
     mgDeltaValid_ = false;
     for (float* b : mgP_) {
-        if (b != nullptr) cudaFree(b);
+        deviceFree(b);
     }
     for (float* b : mgRhs_) {
-        if (b != nullptr) cudaFree(b);
+        deviceFree(b);
     }
-    if (mgChunkSq_ != nullptr) cudaFree(mgChunkSq_);
+    deviceFree(mgChunkSq_);
     mgChunkSq_ = nullptr;
     mgP_.clear();
     mgRhs_.clear();
@@ -107,7 +109,7 @@ void Scene::release() {
                     rayTileOrder_, rayTileCounter_, sorGate_, residualSq_, residualMax_, split_, splitDiv_,
                     cfgVort_, cfgLight_, cfgNoise_};
     for (void* b : bufs) {
-        if (b != nullptr) cudaFree(b);
+        deviceFree(b);
     }
     if (metricHost_ != nullptr) cudaFreeHost(metricHost_);
     if (sorHostStatus_ != nullptr) cudaFreeHost(sorHostStatus_);
@@ -722,9 +724,9 @@ void MgSolver::release() {
     for (cudaEvent_t e : uploadedRing_) {
         if (e != nullptr) cudaEventSynchronize(e);
     }
-    if (dScenes_ != nullptr) cudaFree(dScenes_);
-    if (dPlan_ != nullptr) cudaFree(dPlan_);
-    if (dSync_ != nullptr) cudaFree(dSync_);
+    deviceFree(dScenes_);
+    deviceFree(dPlan_);
+    deviceFree(dSync_);
     for (int k = 0; k < kStaging; ++k) {
         if (hScenesRing_[k] != nullptr) cudaFreeHost(hScenesRing_[k]);
         if (hPlanRing_[k] != nullptr) cudaFreeHost(hPlanRing_[k]);
@@ -767,9 +769,9 @@ bool MgSolver::plan(int device, const std::vector<MgScene>& scenes, int maxCycle
         if (e == cudaSuccess) {
             e = cudaFuncSetAttribute(mgSolve, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMgTailSmemMax));
         }
-        if (e == cudaSuccess) e = cudaMalloc(&dScenes_, kMgMaxScenes * sizeof(MgScene));
-        if (e == cudaSuccess) e = cudaMalloc(&dPlan_, sizeof(MgPlan));
-        if (e == cudaSuccess) e = cudaMalloc(&dSync_, sizeof(MgSync));
+        if (e == cudaSuccess) e = deviceAlloc(reinterpret_cast<void**>(&dScenes_), kMgMaxScenes * sizeof(MgScene), "multigrid scene table");
+        if (e == cudaSuccess) e = deviceAlloc(reinterpret_cast<void**>(&dPlan_), sizeof(MgPlan), "multigrid plan");
+        if (e == cudaSuccess) e = deviceAlloc(reinterpret_cast<void**>(&dSync_), sizeof(MgSync), "multigrid sync");
         if (e == cudaSuccess) e = cudaMemset(dSync_, 0, sizeof(MgSync));
         for (int k = 0; k < kStaging; ++k) {
             if (e == cudaSuccess) {

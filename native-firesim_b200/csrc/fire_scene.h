@@ -15,6 +15,7 @@
 
 #include "../../include/fire_cuda.h"
 #include "../../include/fire_ext.h"
+#include "fire_guard.h"
 #include "fire_kernels.h"
 
 namespace firesim {

@@ -242,7 +242,7 @@ void releaseActive(Active& a) {
     a.inflight.clear();
     a.spare.clear();
     a.last = nullptr;
-    if (a.hdr) cudaFree(a.hdr);
+    firesim::deviceFree(a.hdr);
     a.hdr = nullptr;
     a.scene.reset();
 }
@@ -269,7 +269,7 @@ extern "C" void fireServerDestroy(FireServer* server) {
     for (auto& kv : server->slots) {
         for (auto& slot : kv.second) {
             slot->scene->stream = slot->scene->ownStream();
-            if (slot->hdr != nullptr) cudaFree(slot->hdr);
+            firesim::deviceFree(slot->hdr);
         }
     }
     delete server;
@@ -362,7 +362,7 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
                                     std::get<2>(shape), err);
             if (!slot->scene) return fail("fireServerRun: " + err);
             const size_t frame = static_cast<size_t>(std::get<3>(shape)) * std::get<4>(shape) * sizeof(float) * 4;
-            if (cudaMalloc(&slot->hdr, frame) != cudaSuccess) {
+            if (firesim::deviceAlloc(&slot->hdr, frame, "served HDR frame") != cudaSuccess) {
                 cudaGetLastError();
                 return fail("fireServerRun: cudaMalloc of a scene's HDR frame failed.");
             }
@@ -381,7 +381,7 @@ bool runBatched(FireServer* server, std::deque<FireServeRequest>& waiting, doubl
                 !sc.setPressureTolerance(r0->pressureTolerance, 1, err) || !sc.prepareBatched(err) ||
                 !sc.registerHdrSlot(0, slot->hdr, static_cast<size_t>(std::get<3>(shape)) * 16, FIRE_HDR_RGBA32F, err) ||
                 !sc.setActiveSlot(0, err) || !sc.synchronize(err)) {
-                cudaFree(slot->hdr);
+                firesim::deviceFree(slot->hdr);
                 return fail("fireServerRun: " + err);
             }
             sc.stream = runner.stream();
@@ -656,7 +656,7 @@ extern "C" bool fireServerRun(FireServer* server, double maxSeconds, FireServeRe
                     ok = fail(err);
                     break;
                 }
-                if (cudaMalloc(&a->hdr, frameBytes(r)) != cudaSuccess) {
+                if (firesim::deviceAlloc(&a->hdr, frameBytes(r), "served HDR frame") != cudaSuccess) {
                     cudaGetLastError();
                     ok = fail("fireServerRun: cudaMalloc of a scene's HDR frame failed.");
                     break;

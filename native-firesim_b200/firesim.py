@@ -22,6 +22,9 @@ LIB_PATH = HERE / "libfiresim_b200.so"
 # The same library built with FP16 / BF16 storage of the transported fields (FP32 arithmetic).
 LIB_PATH_F16 = HERE / "libfiresim_b200_f16.so"
 LIB_PATH_BF16 = HERE / "libfiresim_b200_bf16.so"
+# The FP32 library built with -DFIRE_BOUNDS_CHECK: guard zones around every
+# device buffer, checked by fireCudaCheckGuards (check_guards below).
+LIB_PATH_CHECKED = HERE / "libfiresim_b200_checked.so"
 
 
 class FireSimError(RuntimeError):
@@ -33,12 +36,13 @@ _LIBS: dict = {}
 
 def load_library(precision: str = "f32") -> ctypes.CDLL:
     """Loads the in-tree library (build it with native-firesim_b200/build.py):
-    precision "f32" (the reference's storage), "f16" or "bf16" (half storage)."""
+    precision "f32" (the reference's storage), "f16" or "bf16" (half storage),
+    or "checked" (FP32 storage, the bounds-checking build)."""
     if precision in _LIBS:
         return _LIBS[precision]
-    paths = {"f32": LIB_PATH, "f16": LIB_PATH_F16, "bf16": LIB_PATH_BF16}
+    paths = {"f32": LIB_PATH, "f16": LIB_PATH_F16, "bf16": LIB_PATH_BF16, "checked": LIB_PATH_CHECKED}
     if precision not in paths:
-        raise FireSimError(f"unknown precision {precision!r}: 'f32', 'f16' or 'bf16'")
+        raise FireSimError(f"unknown precision {precision!r}: 'f32', 'f16', 'bf16' or 'checked'")
     path = paths[precision]
     if not path.exists():
         raise FireSimError(f"{path} is missing: run `python native-firesim_b200/build.py` first")
@@ -95,6 +99,8 @@ def load_library(precision: str = "f32") -> ctypes.CDLL:
         "fireServerRun": (b, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(abi.FireServeReport)]),
         "fireCudaSetResidentSorFault": (b, [ctypes.c_int, ctypes.c_longlong]),
         "fireCudaSetAllocationFault": (b, [ctypes.c_longlong]),
+        "fireCudaCheckGuards": (b, [ctypes.POINTER(ctypes.c_int)]),
+        "fireCudaPlantGuardByte": (b, [ctypes.c_char_p, ctypes.c_size_t]),
         "fireCudaGetGridInfo": (b, [ctypes.POINTER(ctypes.c_int)]),
         "fireCudaGetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
         "fireCudaSetField": (b, [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
@@ -297,6 +303,20 @@ def set_autotune(enabled: bool, precision: str = "f32") -> None:
     lib = load_library(precision)
     if not lib.fireCudaSetAutotune(1 if enabled else 0):
         raise FireSimError(f"fireCudaSetAutotune: {last_error(lib)}")
+
+
+def check_guards(precision: str = "checked") -> int:
+    """Scans the guard zones of the bounds-checking build's device buffers
+    (fireCudaCheckGuards): returns 0 when every zone is intact, raises
+    FireSimError naming the first changed buffer otherwise, and returns -1
+    for a library built without the checks."""
+    lib = load_library(precision)
+    n = ctypes.c_int(-1)
+    if lib.fireCudaCheckGuards(ctypes.byref(n)):
+        return 0
+    if n.value < 0:
+        return -1
+    raise FireSimError(lib.fireCudaLastError().decode())
 
 
 def tuned_brick(nx: int, ny: int, nz: int, precision: str = "f32"):

@@ -35,9 +35,9 @@ def test_headers_declare_the_reference_abi():
     assert reference <= names, reference - names
 
 
-@pytest.mark.parametrize("precision", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("precision", ["f32", "f16", "bf16", "checked"])
 def test_library_exports_every_declared_symbol(pkg, precision):
-    """Both builds (FP32 and FP16 storage) export the whole declared ABI."""
+    """Every build (FP32, FP16 and BF16 storage, bounds-checking) exports the whole declared ABI."""
     lib = pkg.load_library(precision)
     for name in sorted(declared_symbols()):
         assert hasattr(lib, name), name
@@ -64,6 +64,19 @@ def test_uninitialised_calls_fail_with_reference_messages(pkg, abi):
     assert not lib.fireCudaRunStages(0, 0, ctypes.byref(s), 0.0)
     assert not lib.fireCudaGetDiagnostics(None)
     assert pkg.firesim.last_error() == "Diagnostics output pointer was null."
+
+
+def test_guard_checks_report_the_default_build(pkg):
+    """Outside the FIRE_BOUNDS_CHECK build the guard entry points say so and
+    make no CUDA call."""
+    lib = pkg.load_library()
+    n = ctypes.c_int(7)
+    assert not lib.fireCudaCheckGuards(ctypes.byref(n))
+    assert n.value == -1
+    assert "FIRE_BOUNDS_CHECK" in pkg.firesim.last_error()
+    assert pkg.check_guards("f32") == -1
+    assert not lib.fireCudaPlantGuardByte(b"pressure", 0)
+    assert "FIRE_BOUNDS_CHECK" in pkg.firesim.last_error()
 
 
 def test_d3d11_entry_points_report_headless(pkg):
