@@ -90,7 +90,9 @@ TRAJ_FIELDS = ("heat", "fuel", "oxygen", "soot", "char", "progress", "pressure",
 def test_trajectory_200_frames_vs_live_reference_128(pkg, abi, refmod):
     """200 validation frames at 128^3 from a reset: at each checkpoint every
     field of the product is within max(3 x the reference's own run-to-run
-    spread, 1e-4) relative L2 of the reference's.  The reference's force pass
+    spread, 1e-4) relative L2 of the reference's, measured over three
+    reference runs (the product's median distance to them against the
+    largest distance between two of them).  The reference's force pass
     adds with float atomics, so two of its runs drift apart (1e-7 after 6
     frames, ~1e-2 after 50, O(1) by 150 as the plume turns chaotic); the
     product, whose force pass is a gather, must drift no faster.  The values
@@ -107,7 +109,7 @@ def test_trajectory_200_frames_vs_live_reference_128(pkg, abi, refmod):
         ref.close()
         return snaps
 
-    first, second = run_ref(), run_ref()
+    refs = [run_ref() for _ in range(3)]
     sim = pkg.FireSim(fw, fh, n, n, n)
     mine = {}
     for f in range(CHECKPOINTS[-1]):
@@ -119,8 +121,11 @@ def test_trajectory_200_frames_vs_live_reference_128(pkg, abi, refmod):
     for c in CHECKPOINTS:
         row = []
         for name in TRAJ_FIELDS:
-            spread = T.field_stats(first[c][name], second[c][name])["rel_l2"]
-            drift = T.field_stats(mine[c][name], second[c][name])["rel_l2"]
+            # The reference's spread: the largest distance between two of its
+            # runs; the product's drift: its median distance to them.  Both are
+            # samples of a chaotic growth, so one pair alone is a noisy yardstick.
+            spread = max(T.field_stats(refs[i][c][name], refs[j][c][name])["rel_l2"] for i, j in ((0, 1), (0, 2), (1, 2)))
+            drift = sorted(T.field_stats(mine[c][name], r[c][name])["rel_l2"] for r in refs)[1]
             bound = max(3.0 * spread, 1e-4)
             assert drift <= bound, (c, name, drift, spread)
             worst = max(worst, drift / bound)
