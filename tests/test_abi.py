@@ -91,7 +91,7 @@ def test_d3d11_entry_points_report_headless(pkg):
 def test_library_has_no_oracle_dependency():
     """The product neither links nor names the oracle."""
     import subprocess
-    for name in ("libfiresim_b200.so", "libfiresim_b200_f16.so", "libfiresim_b200_bf16.so"):
+    for name in ("libfiresim_b200.so", "libfiresim_b200_f16.so", "libfiresim_b200_bf16.so", "libfiresim_b200_checked.so"):
         lib = ROOT / "native-firesim_b200" / name
         needed = subprocess.run(["readelf", "-d", str(lib)], capture_output=True, text=True).stdout
         assert "oracle" not in needed and "fire_ref" not in needed
