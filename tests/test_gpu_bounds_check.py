@@ -204,3 +204,50 @@ def test_batched_server_keeps_guards_and_bits(pkg, abi):
         _bits_equal(f"request {i} heat", runs["checked"][0][i], runs["f32"][0][i])
         _bits_equal(f"request {i} hdr", runs["checked"][1][i], runs["f32"][1][i])
         assert runs["f32"][0][i].sum() > 0.0
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8), (17, 9, 5)])
+def test_tiny_grids_keep_guards_and_follow_the_oracle(pkg, abi, oracle_mod, dims):
+    """Grids smaller than one resident-SOR brick along every axis (every brick
+    partial, light grid at its minimum size): four frames of the reference
+    physics, rendered.  The checked build changes no guard byte; only then
+    does the default build run them, equal to the checked build bit for bit.
+    Against the CPU oracle the fields are compared in the TINY_GRID class:
+    on so few cells the reaction's sin-hash noise, which the oracle cannot
+    round as CUDA's sinf does, moves most burning cells (ash at 8^3: 3e-2
+    relative L2 after four frames, 48 % of cells beyond 1e-5 of the field's
+    scale).  The statistics are printed (pytest -s)."""
+    import tolerances as T
+    from conftest import STATE_FIELDS
+
+    fields = STATE_FIELDS[:10] + ["u", "v", "w"]
+    runs = {}
+    for precision in ("checked", "f32"):
+        sim = pkg.FireSim(48, 32, *dims, precision=precision)
+        frames = []
+        for f in range(4):
+            s = abi.validation_settings(f, scene=0, width=48, height=32)
+            s.reset = 1 if f == 0 else 0
+            frames.append(sim.step_and_render(s)[0])
+        sim.synchronize()
+        runs[precision] = ({n: sim.get(n) for n in fields}, frames)
+        if precision == "checked":
+            assert pkg.check_guards() == 0
+        sim.close()
+        if precision == "checked":
+            assert pkg.check_guards() == 0
+    o = oracle_mod.OracleFire(abi, 48, 32, *dims)
+    for f in range(4):
+        s = abi.validation_settings(f, scene=0, width=48, height=32)
+        s.reset = 1 if f == 0 else 0
+        o.step(s, mode=2)
+    (got, got_frames), (want, want_frames) = runs["checked"], runs["f32"]
+    for n in fields:
+        _bits_equal(f"{dims}/{n}", got[n], want[n])
+    for j, (g, w) in enumerate(zip(got_frames, want_frames)):
+        _bits_equal(f"{dims}/frame{j}", g, w)
+    ref = {n: o.get(n) for n in fields}
+    print(f"{dims} vs oracle (rel L2):", ", ".join(f"{n} {T.field_stats(want[n], ref[n])['rel_l2']:.1e}" for n in fields))
+    for n in fields:
+        T.check_field(f"{dims}/{n} vs oracle", want[n], ref[n], T.TINY_GRID)
+    assert want["heat"].sum() > 0.0
