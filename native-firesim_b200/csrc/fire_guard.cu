@@ -76,9 +76,9 @@ cudaError_t scan(const std::vector<Guarded>& bufs, std::vector<std::string>& bad
     for (size_t i = 0; i < bufs.size() && e == cudaSuccess; ++i) {
         const char* zone[2] = {bufs[i].base, bufs[i].base + kGuardBytes + bufs[i].bytes};
         for (int side = 0; side < 2; ++side) {
-            // The payload's size need not be a multiple of 16: scan the after-zone
-            // from the 16-byte boundary below its end, whose leading bytes then
-            // belong to the payload; those bytes are skipped when reporting.
+            // The payload's size need not be a multiple of 16: the after-zone is
+            // scanned in 16-byte words from the boundary below its start, and the
+            // kernel skips the leading bytes, which belong to the payload.
             const size_t lead = reinterpret_cast<size_t>(zone[side]) & 15;
             const uint4* start = reinterpret_cast<const uint4*>(zone[side] - lead);
             guardScan<<<64, 256>>>(start, kGuardBytes / 16, static_cast<unsigned>(lead), d + 2 * i + side);
